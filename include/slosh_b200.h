@@ -1,0 +1,269 @@
+/*
+ * slosh_b200.h — C ABI of the B200-native slosh MPM substep.
+ *
+ * The library replaces the device side of slosh's `MpmPipeline::launch_step`
+ * (src/pipeline.rs:562-770 in dimforge/slosh): the sparse hashed grid build,
+ * the APIC/MLS P2G scatter, the grid velocity update with collider boundary
+ * conditions, the G2P gather fused with the particle update and constitutive
+ * models, and the rigid-body integration pass.  All entry points are plain C:
+ * pointers, sizes and status codes, no C++ or torch types.
+ *
+ * Conventions
+ *  - Every function returns SLOSH_OK (0) or a negative SLOSH_E_* status.  The
+ *    text of the last error of a context is available from slosh_last_error.
+ *  - A context owns all of its device memory.  A context must not be used
+ *    from two host threads at once (it mirrors `&mut MpmData`).
+ *  - `stream` arguments are `cudaStream_t` values passed as `void*`; NULL
+ *    means the context's own stream.
+ *  - Matrices in the particle records are column-major 3x3 (glam `Mat3`), the
+ *    layout slosh uploads and reads back.  In 2D only the top-left 2x2 block
+ *    (elements 0, 1, 3, 4) is used.
+ */
+#ifndef SLOSH_B200_H
+#define SLOSH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SLOSH_OK 0
+#define SLOSH_E_INVALID (-1)   /* bad argument or record                  */
+#define SLOSH_E_CUDA (-2)      /* a CUDA call failed                      */
+#define SLOSH_E_OVERFLOW (-3)  /* block hash map / block list overflowed  */
+#define SLOSH_E_CAPACITY (-4)  /* particle, body or material capacity     */
+#define SLOSH_E_NOMEM (-5)     /* device allocation failed                */
+#define SLOSH_E_STATE (-6)     /* call out of order (e.g. no particles)   */
+#define SLOSH_E_MATERIAL (-7)  /* too many distinct materials             */
+
+/* ---- particle models: GpuParticleModel discriminants ------------------- */
+/* src/solver/particle_model.rs:89-98; shaders/slosh/models/default.slang:73-80 */
+#define SLOSH_MODEL_ELASTIC_LINEAR 0u      /* fixed-corotated (ElasticCoefficients) */
+#define SLOSH_MODEL_ELASTIC_NEO_HOOKEAN 1u
+#define SLOSH_MODEL_SAND_LINEAR 2u         /* Drucker-Prager + fixed-corotated  */
+#define SLOSH_MODEL_SAND_NEO_HOOKEAN 3u
+/* Extension through slosh's IParticleModel seam (ModelFlags::FLUID,
+ * shaders/slosh/models/interfaces.slang:22-25): weakly compressible Tait
+ * fluid.  data[0] = rest density, data[1] = bulk modulus K, data[2] = gamma.
+ * Kirchhoff stress tau = -J p I with p = (K/gamma) (J^-gamma - 1) and
+ * J = F[0][0] (the FLUID update keeps F = F00 I). */
+#define SLOSH_MODEL_FLUID_TAIT 4u
+
+/* 52-byte model record, byte-compatible with slosh's GpuParticleModel
+ * (src/solver/particle_model.rs:102).  Payload words:
+ *   ELASTIC_*: lambda, mu, cfl_coeff, 9 x 0
+ *   SAND_*:    plastic det, plastic hardening q, log_vol_gain,
+ *              h0, h1, h2, h3, plastic lambda, plastic mu,
+ *              elastic lambda, elastic mu, cfl_coeff
+ *   FLUID_TAIT: rest density, bulk modulus, gamma, 9 x 0 */
+typedef struct slosh_model {
+    uint32_t tag;
+    float data[12];
+} slosh_model;
+
+/* One particle, the flattened form of slosh's `Particle<ParticleModel>`
+ * (src/solver/particle.rs:23-55, :226-233).  192 bytes. */
+typedef struct slosh_particle {
+    float position[3];
+    float velocity[3];
+    float def_grad[9]; /* column-major */
+    float affine[9];   /* column-major APIC affine matrix C */
+    float force_dt[3];
+    float vel_grad_det;
+    float init_volume;
+    float init_radius;
+    float mass;
+    float damping;
+    float phase;
+    uint32_t enabled;
+    uint32_t fixed;
+    slosh_model model;
+} slosh_particle;
+
+/* Collider shape types: shaders/slosh/rbd/shapes/shape.slang:19-25. */
+#define SLOSH_SHAPE_BALL 0u
+#define SLOSH_SHAPE_CUBOID 1u
+
+/* Boundary conditions: src/solver/boundary_condition.rs:14-19. */
+#define SLOSH_BC_STICK 0u
+#define SLOSH_BC_SLIP 1u
+#define SLOSH_BC_SEPARATE 2u
+#define SLOSH_BC_FRICTION_Z_UP 3u
+#define SLOSH_BC_NON_REFLECTING 4u
+#define SLOSH_BC_DISABLED 5u
+
+/* One rigid body with its collider shape and boundary condition: an entry of
+ * slosh's GpuBodySet (src/rbd/dynamics/body.rs:74-90) plus its
+ * GpuBoundaryCondition (src/solver/boundary_condition.rs:8-12).  192 bytes.
+ * Shape layout as shaders/slosh/rbd/shapes/shape.slang:44-62:
+ *   ball:   shape_a = (radius, -, -, type)
+ *   cuboid: shape_a = (hx, hy, hz, type)
+ * where `type` is the shape type stored as uint32 bits.  The pose is a
+ * similarity: rotation (3D unit quaternion i,j,k,w; 2D cos,sin), translation
+ * xyz and uniform scale in translation[3].  Bodies coupled one-way (the
+ * MpmData::new default, src/pipeline.rs:328) carry zero inverse mass. */
+typedef struct slosh_body {
+    float shape_a[4];
+    float shape_b[4];
+    float rotation[4];
+    float translation[4];
+    float linvel[4];
+    float angvel[4];
+    float inv_mass[4];
+    float local_com[4];
+    float inv_inertia[12]; /* world-space, 3 padded columns */
+    uint32_t bc_type;
+    float bc_friction;
+    uint32_t pad[2];
+} slosh_body;
+
+/* Context creation parameters: the arguments of MpmData::new that size the
+ * device state (src/pipeline.rs:311-320). */
+typedef struct slosh_config {
+    uint32_t dim;           /* 2 or 3 */
+    float cell_width;       /* grid spacing h */
+    uint32_t grid_capacity; /* max active blocks; the block hash map holds
+                               2 x next_pow2(grid_capacity) slots */
+    uint32_t max_particles;
+    int32_t device;         /* CUDA device ordinal */
+    uint32_t flags;         /* reserved, 0 */
+} slosh_config;
+
+/* SimulationParams (src/solver/params.rs:13-21). */
+typedef struct slosh_params {
+    float gravity[3];
+    float dt;
+} slosh_params;
+
+typedef struct slosh_ctx slosh_ctx;
+
+/* Creates the device state of one scene.  Replaces MpmData::new and
+ * MpmPipeline::new_with_kernels (src/pipeline.rs:311, :462). */
+int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out);
+
+/* Frees every device buffer of the context. */
+void slosh_ctx_destroy(slosh_ctx *ctx);
+
+/* Sets gravity and dt.  Replaces GpuSimulationParams::new
+ * (src/solver/params.rs:40-49). */
+int slosh_set_params(slosh_ctx *ctx, const slosh_params *params);
+
+/* Uploads `n` particles from HOST memory (pinned memory gives full PCIe
+ * speed) and converts them to the device layout.  Replaces
+ * GpuParticles::from_particles (src/solver/particle.rs:474-500).  Particle
+ * models are deduplicated into a per-context material table on the device. */
+int slosh_upload_particles(slosh_ctx *ctx, const slosh_particle *particles,
+                           uint32_t n, void *stream);
+
+/* Reads the particles back into the record layout above (in upload order).
+ * Replaces the staging readbacks of src_testbed/step.rs:260-334.
+ * `vel_grad_det` is transient inside the fused G2P/update and reads as 0. */
+int slosh_download_particles(slosh_ctx *ctx, slosh_particle *out, uint32_t n,
+                             void *stream);
+
+/* Reads positions back as vec4 (x, y, z, 0), the layout of slosh's position
+ * buffer (src/solver/particle.rs:384-389). */
+int slosh_download_positions(slosh_ctx *ctx, float *out_xyzw, uint32_t n,
+                             void *stream);
+
+/* Sets the rigid bodies and their colliders (<= 16).  Replaces
+ * GpuBodySet::from_rapier + GpuMaterials::new (src/rbd/dynamics/body.rs:183;
+ * src/solver/boundary_condition.rs:76-85). */
+int slosh_set_bodies(slosh_ctx *ctx, const slosh_body *bodies, uint32_t n);
+
+/* Reads the bodies back (poses and velocities after integration). */
+int slosh_get_bodies(slosh_ctx *ctx, slosh_body *out, uint32_t n);
+
+/* Enqueues `n_substeps` substeps on `stream` without any host round trip.
+ * Replaces MpmPipeline::launch_step (src/pipeline.rs:562-770) called
+ * n_substeps times into one encoder.  Asynchronous: errors raised on the
+ * device are reported by slosh_sync. */
+int slosh_step(slosh_ctx *ctx, uint32_t n_substeps, void *stream);
+
+/* Waits for the context's work and returns the device error status
+ * (SLOSH_E_OVERFLOW when the block hash map or block list overflowed). */
+int slosh_sync(slosh_ctx *ctx, void *stream);
+
+/* Number of device kernels one substep launches (for launch accounting). */
+uint32_t slosh_kernels_per_substep(const slosh_ctx *ctx);
+
+/* Runs `n_substeps` substeps with direct launches (not the CUDA graph) and a
+ * pair of CUDA events around every kernel, and writes the summed device time
+ * of each kernel in milliseconds to kernel_ms[0 .. *n_kernels).  Kernel names
+ * come from slosh_kernel_name.  Stands in for slosh's per-pass
+ * GpuTimestamps (src/pipeline.rs:588-757); advances the simulation like
+ * slosh_step and synchronises after every substep. */
+int slosh_profile_substeps(slosh_ctx *ctx, uint32_t n_substeps, void *stream,
+                           float *kernel_ms, uint32_t cap, uint32_t *n_kernels);
+
+/* Name of profiled kernel `index`. */
+int slosh_kernel_name(uint32_t index, char *buf, size_t len);
+
+/* Counters of the last completed substep (synchronises the context). */
+typedef struct slosh_stats {
+    uint32_t n_particles;
+    uint32_t n_blocks;         /* active blocks of the last substep */
+    uint32_t n_primary_blocks; /* blocks holding at least one particle */
+    uint32_t n_materials;      /* distinct particle models */
+    uint32_t n_svd_fp64;       /* SVDs recomputed in FP64 since upload */
+    uint32_t pad[3];
+} slosh_stats;
+
+int slosh_get_stats(slosh_ctx *ctx, slosh_stats *out);
+
+/* Grid-build result of the current positions, computed without advancing
+ * the simulation (bit-exactness checks).  Blocks are in canonical order
+ * (ascending packed key).  Two views are returned:
+ *  - the hot path's own arrays: per block the first primary entry and the
+ *    canonical permutation of primaries, ordered by (slab bucket, id);
+ *  - slosh's complete layout (shaders/slosh/grid/sort.slang:248-357):
+ *    per-block counts of all NB buckets, first_particle over primaries and
+ *    extras, and the sorted ids with extras, each bucket ordered by id.
+ * Any output pointer may be NULL.  Sizes are reported in the struct; arrays
+ * must hold cap_blocks blocks (x NB or x (NASSOC-1) where noted), n
+ * particles and cap_sorted entries. */
+typedef struct slosh_grid_dump {
+    uint32_t n_blocks;       /* out */
+    uint32_t n_sorted;       /* out: entries of the full layout */
+    uint32_t nb_buckets;     /* out: NB (10 in 3D, 18 in 2D) */
+    uint32_t n_neighbors;    /* out: NASSOC - 1 (7 in 3D, 3 in 2D) */
+    uint32_t *keys;          /* [cap_blocks] packed keys, ascending */
+    uint32_t *first_particle;            /* [cap_blocks] full layout */
+    uint32_t *num_particles;             /* [cap_blocks] primaries */
+    uint32_t *num_particles_with_extras; /* [cap_blocks] */
+    uint32_t *bucket_counts; /* [cap_blocks * NB] */
+    uint32_t *sorted_ids;    /* [cap_sorted] full layout */
+    uint32_t *primary_first; /* [cap_blocks] hot path */
+    uint32_t *primary_perm;  /* [n particles] hot path */
+    uint32_t *neighbors;     /* [cap_blocks * (NASSOC-1)] neighbour ranks */
+} slosh_grid_dump;
+
+int slosh_grid_debug(slosh_ctx *ctx, slosh_grid_dump *dump,
+                     uint32_t cap_blocks, uint32_t cap_sorted);
+
+/* Runs one substep's grid build followed by P2G (stage 1) or by P2G and the
+ * grid update (stage 2) without advancing the particles, and copies the
+ * nodes out: 64 nodes per block in canonical block order, 4 floats each
+ * (momentum or velocity, mass).  Node id = block * 64 + local index as in
+ * shaders/slosh/grid/grid.slang:409-417. */
+int slosh_debug_nodes(slosh_ctx *ctx, int stage, float *nodes,
+                      uint32_t cap_blocks, uint32_t *n_blocks);
+
+/* Exclusive prefix sum of `n` u32 values (host arrays) with slosh's
+ * semantics (src/grid/prefix_sum.rs:97-110: the result is as if a 0 had been
+ * prepended; the total is dropped).  Uses the context's scan workspace;
+ * n <= grid_capacity. */
+int slosh_prefix_sum(slosh_ctx *ctx, const uint32_t *in, uint32_t *out,
+                     uint32_t n);
+
+/* Copies the last error message of the context into `buf`. */
+int slosh_last_error(const slosh_ctx *ctx, char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLOSH_B200_H */

@@ -1,0 +1,185 @@
+"""ctypes binding of ``libslosh_b200.so`` and numpy dtypes of its records.
+
+The shared library is built in-tree (``slosh_b200/lib/libslosh_b200.so``) by
+:func:`slosh_b200.build.build_library`.  Loading fails loudly when it is
+missing: there is no CPU fallback for the substep.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libslosh_b200.so")
+
+# Status codes (include/slosh_b200.h).
+SLOSH_OK = 0
+SLOSH_E_INVALID = -1
+SLOSH_E_CUDA = -2
+SLOSH_E_OVERFLOW = -3
+SLOSH_E_CAPACITY = -4
+SLOSH_E_NOMEM = -5
+SLOSH_E_STATE = -6
+SLOSH_E_MATERIAL = -7
+
+STATUS_NAMES = {
+    SLOSH_E_INVALID: "SLOSH_E_INVALID",
+    SLOSH_E_CUDA: "SLOSH_E_CUDA",
+    SLOSH_E_OVERFLOW: "SLOSH_E_OVERFLOW",
+    SLOSH_E_CAPACITY: "SLOSH_E_CAPACITY",
+    SLOSH_E_NOMEM: "SLOSH_E_NOMEM",
+    SLOSH_E_STATE: "SLOSH_E_STATE",
+    SLOSH_E_MATERIAL: "SLOSH_E_MATERIAL",
+}
+
+# Particle model tags (GpuParticleModel discriminants + the Tait fluid).
+MODEL_ELASTIC_LINEAR = 0
+MODEL_ELASTIC_NEO_HOOKEAN = 1
+MODEL_SAND_LINEAR = 2
+MODEL_SAND_NEO_HOOKEAN = 3
+MODEL_FLUID_TAIT = 4
+
+SHAPE_BALL = 0
+SHAPE_CUBOID = 1
+
+BC_STICK = 0
+BC_SLIP = 1
+BC_SEPARATE = 2
+BC_FRICTION_Z_UP = 3
+BC_NON_REFLECTING = 4
+BC_DISABLED = 5
+
+# slosh_particle: 192 bytes.
+PARTICLE_DTYPE = np.dtype(
+    [
+        ("position", "<f4", 3),
+        ("velocity", "<f4", 3),
+        ("def_grad", "<f4", 9),  # column-major
+        ("affine", "<f4", 9),  # column-major
+        ("force_dt", "<f4", 3),
+        ("vel_grad_det", "<f4"),
+        ("init_volume", "<f4"),
+        ("init_radius", "<f4"),
+        ("mass", "<f4"),
+        ("damping", "<f4"),
+        ("phase", "<f4"),
+        ("enabled", "<u4"),
+        ("fixed", "<u4"),
+        ("model_tag", "<u4"),
+        ("model", "<f4", 12),
+    ]
+)
+assert PARTICLE_DTYPE.itemsize == 192
+
+# slosh_body: 192 bytes.
+BODY_DTYPE = np.dtype(
+    [
+        ("shape_a", "<f4", 4),
+        ("shape_b", "<f4", 4),
+        ("rotation", "<f4", 4),
+        ("translation", "<f4", 4),
+        ("linvel", "<f4", 4),
+        ("angvel", "<f4", 4),
+        ("inv_mass", "<f4", 4),
+        ("local_com", "<f4", 4),
+        ("inv_inertia", "<f4", 12),
+        ("bc_type", "<u4"),
+        ("bc_friction", "<f4"),
+        ("pad", "<u4", 2),
+    ]
+)
+assert BODY_DTYPE.itemsize == 192
+
+
+class SloshConfig(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_uint32),
+        ("cell_width", ctypes.c_float),
+        ("grid_capacity", ctypes.c_uint32),
+        ("max_particles", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+    ]
+
+
+class SloshParams(ctypes.Structure):
+    _fields_ = [("gravity", ctypes.c_float * 3), ("dt", ctypes.c_float)]
+
+
+class SloshGridDump(ctypes.Structure):
+    _fields_ = [
+        ("n_blocks", ctypes.c_uint32),
+        ("n_sorted", ctypes.c_uint32),
+        ("nb_buckets", ctypes.c_uint32),
+        ("n_neighbors", ctypes.c_uint32),
+        ("keys", ctypes.c_void_p),
+        ("first_particle", ctypes.c_void_p),
+        ("num_particles", ctypes.c_void_p),
+        ("num_particles_with_extras", ctypes.c_void_p),
+        ("bucket_counts", ctypes.c_void_p),
+        ("sorted_ids", ctypes.c_void_p),
+        ("primary_first", ctypes.c_void_p),
+        ("primary_perm", ctypes.c_void_p),
+        ("neighbors", ctypes.c_void_p),
+    ]
+
+
+# Every symbol include/slosh_b200.h declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+SIGNATURES = {
+    "slosh_ctx_create": (ctypes.c_int, [ctypes.POINTER(SloshConfig), ctypes.POINTER(_P)]),
+    "slosh_ctx_destroy": (None, [_P]),
+    "slosh_set_params": (ctypes.c_int, [_P, ctypes.POINTER(SloshParams)]),
+    "slosh_upload_particles": (ctypes.c_int, [_P, _P, _U32, _P]),
+    "slosh_download_particles": (ctypes.c_int, [_P, _P, _U32, _P]),
+    "slosh_download_positions": (ctypes.c_int, [_P, _P, _U32, _P]),
+    "slosh_set_bodies": (ctypes.c_int, [_P, _P, _U32]),
+    "slosh_get_bodies": (ctypes.c_int, [_P, _P, _U32]),
+    "slosh_step": (ctypes.c_int, [_P, _U32, _P]),
+    "slosh_sync": (ctypes.c_int, [_P, _P]),
+    "slosh_kernels_per_substep": (_U32, [_P]),
+    "slosh_profile_substeps": (ctypes.c_int, [_P, _U32, _P, _P, _U32, ctypes.POINTER(_U32)]),
+    "slosh_kernel_name": (ctypes.c_int, [_U32, ctypes.c_char_p, ctypes.c_size_t]),
+    "slosh_get_stats": (ctypes.c_int, [_P, _P]),
+    "slosh_grid_debug": (ctypes.c_int, [_P, ctypes.POINTER(SloshGridDump), _U32, _U32]),
+    "slosh_debug_nodes": (ctypes.c_int, [_P, ctypes.c_int, _P, _U32, ctypes.POINTER(_U32)]),
+    "slosh_prefix_sum": (ctypes.c_int, [_P, _P, _P, _U32]),
+    "slosh_last_error": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the CUDA library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with slosh_b200.build.build_library() "
+            "(nvcc, sm_100a). The MPM substep has no CPU fallback."
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class SloshError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def ptr(a: np.ndarray | None) -> ctypes.c_void_p | None:
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return ctypes.c_void_p(a.ctypes.data)

@@ -1,0 +1,166 @@
+// Device-side constants and helpers shared by the slosh_b200 kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/slosh_b200.h"
+
+namespace slosh {
+
+constexpr uint32_t NONE = 0xffffffffu;
+constexpr unsigned FULL_MASK = 0xffffffffu;
+constexpr uint32_t MAX_BODIES = 16;       // collide() unrolls 16 shapes (collide.slang:362-363)
+constexpr uint32_t MAX_MATERIALS = 4096;  // distinct particle models per context
+constexpr uint32_t MAT_HASH = 8192;       // material hash slots (power of two)
+constexpr uint32_t HIST_BINS = 65536;     // top-16-bit bins of the packed block key
+
+// Device error bits (accumulated; read by slosh_sync).
+constexpr uint32_t ERR_HASH_OVERFLOW = 1u << 0;    // block hash map full
+constexpr uint32_t ERR_BLOCK_OVERFLOW = 1u << 1;   // more active blocks than capacity
+constexpr uint32_t ERR_MATERIALS = 1u << 2;        // too many distinct materials
+constexpr uint32_t ERR_MATERIAL_HASH = 1u << 3;    // two materials share a 32-bit hash
+constexpr uint32_t ERR_KEY_RANGE = 1u << 4;        // a block coordinate outside the packed-key range
+
+// Sparse grid geometry per dimension (shaders/slosh/grid/grid.slang:224-257).
+template <int D> struct Geo;
+template <> struct Geo<3> {
+    static constexpr int BW = 4;         // cells per block edge
+    static constexpr int NASSOC = 8;     // primary block + 7 (+1) neighbours
+    static constexpr int NPB = 4;        // primary slab buckets (sort.slang:15-21)
+    static constexpr int NEB = 6;        // extra slab buckets
+    static constexpr int NB = 10;
+    static constexpr int MIN_SHIFT = 2;  // stencil spills into the +1 block when a >= 2
+    static constexpr int TW = 6;         // halo tile edge: block + 2
+    static constexpr int TILE = 216;     // TW^3
+    static constexpr int NST = 27;       // stencil size
+};
+template <> struct Geo<2> {
+    static constexpr int BW = 8;
+    static constexpr int NASSOC = 4;
+    static constexpr int NPB = 8;
+    static constexpr int NEB = 10;
+    static constexpr int NB = 18;
+    static constexpr int MIN_SHIFT = 6;
+    static constexpr int TW = 10;
+    static constexpr int TILE = 100;
+    static constexpr int NST = 9;
+};
+
+// Packed block key (grid.slang:77-91): x,z get 11 bits and y 10 bits in 3D,
+// 16 bits per axis in 2D.
+template <int D> __host__ __device__ __forceinline__ uint32_t pack_key(const int *b) {
+    if constexpr (D == 3) {
+        return ((uint32_t)(b[0] + 0x3ff) & 0x7ffu) | (((uint32_t)(b[1] + 0x1ff) & 0x3ffu) << 11) |
+               (((uint32_t)(b[2] + 0x3ff) & 0x7ffu) << 21);
+    } else {
+        return ((uint32_t)(b[0] + 0x7fff) & 0xffffu) | (((uint32_t)(b[1] + 0x7fff) & 0xffffu) << 16);
+    }
+}
+
+template <int D> __host__ __device__ __forceinline__ void unpack_key(uint32_t k, int *b) {
+    if constexpr (D == 3) {
+        b[0] = (int)(k & 0x7ffu) - 0x3ff;
+        b[1] = (int)((k >> 11) & 0x3ffu) - 0x1ff;
+        b[2] = (int)((k >> 21) & 0x7ffu) - 0x3ff;
+    } else {
+        b[0] = (int)(k & 0xffffu) - 0x7fff;
+        b[1] = (int)((k >> 16) & 0xffffu) - 0x7fff;
+    }
+}
+
+// MurmurHash3 mixing step used by slosh's block hash map (grid.slang:93-100).
+__host__ __device__ __forceinline__ uint32_t murmur_mix(uint32_t key) {
+    key *= 0xcc9e2d51u;
+    key = (key << 15) | (key >> 17);
+    key *= 0x1b873593u;
+    return key;
+}
+
+// Offsets of the blocks associated with a block, in slosh's order
+// (grid.slang:362-382): index 0 is the block itself.
+template <int D> __host__ __device__ __forceinline__ void assoc_offset(int s, int *o) {
+    if constexpr (D == 3) {
+        o[0] = (s >> 2) & 1;
+        o[1] = (s >> 1) & 1;
+        o[2] = s & 1;
+    } else {
+        o[0] = (s >> 1) & 1;
+        o[1] = s & 1;
+    }
+}
+
+// Base cell of a position: round(x/h) - 1 with round-half-to-even (WGSL
+// round), its block and its index inside the block
+// (grid.slang:346-354; particle.slang:79-87).
+template <int D> struct CellLoc {
+    int block[D];
+    int local[D];
+};
+
+template <int D> __device__ __forceinline__ CellLoc<D> locate(const float *x, float h) {
+    CellLoc<D> c;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        float assoc = rintf(__fdiv_rn(x[k], h)) - 1.0f;
+        float ab = floorf(assoc * (1.0f / Geo<D>::BW));
+        c.block[k] = (int)ab;
+        c.local[k] = (int)(assoc - ab * (float)Geo<D>::BW);
+    }
+    return c;
+}
+
+// Quadratic B-spline weights of the 3 stencil nodes for fractional offset x
+// in [0.5, 1.5) (kernel.slang:62-68).
+__device__ __forceinline__ void bspline_weights(float x, float *w) {
+    float a = 1.5f - x, b = x - 1.0f, c = x - 0.5f;
+    w[0] = 0.5f * a * a;
+    w[1] = 0.75f - b * b;
+    w[2] = 0.5f * c * c;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Material record: GpuParticleModel without the per-particle plastic state.
+struct Material {
+    uint32_t tag;
+    float p[12];
+};
+
+// Flags word of a particle: material id, enabled, fixed.
+constexpr uint32_t FLAG_MAT_MASK = 0xffffu;
+constexpr uint32_t FLAG_ENABLED = 1u << 16;
+constexpr uint32_t FLAG_FIXED = 1u << 17;
+
+// Collider body on the device (slosh_body in device form).
+struct DevBody {
+    uint32_t shape_type;
+    float sa[4];
+    float rot[4];
+    float tra[3];
+    float scale;
+    float linvel[3];
+    float angvel[3];
+    float inv_mass[3];
+    float local_com[3];
+    uint32_t bc_type;
+    float friction;
+};
+
+// Per-substep device counters.
+struct Counters {
+    uint32_t n_primary;  // primary blocks appended by the touch pass
+    uint32_t n_extra;    // neighbour-only blocks appended by the neighbour pass
+    uint32_t n_blocks;   // active blocks after ranking (min(total, capacity))
+    uint32_t n_sorted;   // debug: sorted entries with extras
+    uint32_t n_svd_fp64; // particles whose SVD fell back to FP64 (cumulative)
+    uint32_t pad[3];
+};
+
+}  // namespace slosh

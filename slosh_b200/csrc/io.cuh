@@ -1,0 +1,323 @@
+// Particle upload/download between slosh's record layout and the device
+// structure of arrays, and the debug kernels that rebuild slosh's complete
+// sorted-particle layout (primaries + extras).
+#pragma once
+
+#include "grid_build.cuh"
+
+namespace slosh {
+
+struct IoBuffers {
+    const slosh_particle *in;  // staging, device
+    slosh_particle *out;       // staging, device
+    uint32_t *mat_hkeys;       // MAT_HASH material-key hashes
+    uint32_t *mat_dense;       // MAT_HASH dense material ids
+    uint32_t *n_mat;           // device counter
+    uint32_t *scene_flags;     // bit0 damping, bit1 force, bit2 sand
+    float *r0;
+    float *phase;
+};
+
+constexpr uint32_t SCENE_DAMPING = 1u, SCENE_FORCE = 2u, SCENE_SAND = 4u;
+
+// Words of the material key: tag + 12 payload words, with the per-particle
+// plastic state (payload words 0..2 of the sand models) zeroed.
+__device__ __forceinline__ void material_key(const slosh_model &m, uint32_t *w) {
+    w[0] = m.tag;
+    const bool sand = m.tag == SLOSH_MODEL_SAND_LINEAR || m.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) w[1 + k] = (sand && k < 3) ? 0u : __float_as_uint(m.data[k]);
+}
+
+__device__ __forceinline__ uint32_t material_hash(const uint32_t *w) {
+    uint32_t h = 0x9747b28cu;
+#pragma unroll
+    for (int k = 0; k < 13; ++k) h = murmur_mix(h ^ w[k]) * 5u + 0xe6546b64u;
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    return h == NONE ? 0x7fffffffu : h;
+}
+
+// Pass 1 of the upload: distinct materials into the material table.
+__global__ void k_mat_insert(DevScene s, IoBuffers io) {
+    const uint32_t lane = lane_id();
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < s.n; base += stride) {
+        const uint32_t i = base + lane;
+        const bool valid = i < s.n;
+        const unsigned mask = __ballot_sync(FULL_MASK, valid);
+        if (!valid) continue;
+        uint32_t w[13];
+        material_key(io.in[i].model, w);
+        const uint32_t hsh = material_hash(w);
+        const unsigned peers = __match_any_sync(mask, hsh);
+        if ((int)lane != __ffs(peers) - 1) continue;
+        uint32_t slot = hsh & (MAT_HASH - 1u);
+        for (uint32_t k = 0; k < MAT_HASH; ++k) {
+            const uint32_t old = atomicCAS(&io.mat_hkeys[slot], NONE, hsh);
+            if (old == NONE) {
+                const uint32_t dense = atomicAdd(io.n_mat, 1u);
+                if (dense < MAX_MATERIALS) {
+                    Material m;
+                    m.tag = w[0];
+                    for (int q = 0; q < 12; ++q) m.p[q] = __uint_as_float(w[1 + q]);
+                    const_cast<Material *>(s.materials)[dense] = m;
+                    io.mat_dense[slot] = dense;
+                } else {
+                    io.mat_dense[slot] = NONE;
+                    atomicOr(s.err, ERR_MATERIALS);
+                }
+                break;
+            }
+            if (old == hsh) break;
+            slot = (slot + 1u) & (MAT_HASH - 1u);
+        }
+    }
+}
+
+// Pass 2 of the upload: record -> structure of arrays.
+template <int D> __global__ void k_ingest(DevScene s, IoBuffers io) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const size_t n = s.n;
+    uint32_t sflags = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+        const slosh_particle &p = io.in[i];
+        uint32_t w[13];
+        material_key(p.model, w);
+        const uint32_t hsh = material_hash(w);
+        uint32_t slot = hsh & (MAT_HASH - 1u), dense = NONE;
+        for (uint32_t k = 0; k < MAT_HASH; ++k) {
+            const uint32_t kk = io.mat_hkeys[slot];
+            if (kk == hsh) {
+                dense = io.mat_dense[slot];
+                break;
+            }
+            if (kk == NONE) break;
+            slot = (slot + 1u) & (MAT_HASH - 1u);
+        }
+        if (dense == NONE || dense >= MAX_MATERIALS) {
+            atomicOr(s.err, ERR_MATERIALS);
+            dense = 0;
+        } else {
+            const Material &m = s.materials[dense];
+            bool same = m.tag == w[0];
+            for (int q = 0; q < 12; ++q) same = same && (__float_as_uint(m.p[q]) == w[1 + q]);
+            if (!same) atomicOr(s.err, ERR_MATERIAL_HASH);
+        }
+        s.pm[i] = make_float4(p.position[0], p.position[1], D == 3 ? p.position[2] : 0.f, p.mass);
+        for (int k = 0; k < D; ++k) {
+            s.vel[k * n + i] = p.velocity[k];
+            s.fdt[k * n + i] = p.force_dt[k];
+            if (p.force_dt[k] != 0.f) sflags |= SCENE_FORCE;
+        }
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                s.F[(r * D + c) * n + i] = p.def_grad[c * 3 + r];
+                s.C[(r * D + c) * n + i] = p.affine[c * 3 + r];
+            }
+        s.V0[i] = p.init_volume;
+        s.damping[i] = p.damping;
+        if (p.damping != 0.f) sflags |= SCENE_DAMPING;
+        io.r0[i] = p.init_radius;
+        io.phase[i] = p.phase;
+        s.flags[i] = (dense & FLAG_MAT_MASK) | (p.enabled ? FLAG_ENABLED : 0u) | (p.fixed ? FLAG_FIXED : 0u);
+        const bool sand = p.model.tag == SLOSH_MODEL_SAND_LINEAR || p.model.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN;
+        for (int k = 0; k < 3; ++k) s.plastic[k * n + i] = sand ? p.model.data[k] : 0.f;
+        if (sand) sflags |= SCENE_SAND;
+    }
+    sflags = __reduce_or_sync(FULL_MASK, sflags);
+    if (lane_id() == 0 && sflags) atomicOr(io.scene_flags, sflags);
+}
+
+// Structure of arrays -> records.
+template <int D> __global__ void k_egest(DevScene s, IoBuffers io) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const size_t n = s.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+        slosh_particle p;
+        const float4 pm = s.pm[i];
+        p.position[0] = pm.x;
+        p.position[1] = pm.y;
+        p.position[2] = D == 3 ? pm.z : 0.f;
+        for (int k = 0; k < 3; ++k) {
+            p.velocity[k] = k < D ? s.vel[k * n + i] : 0.f;
+            p.force_dt[k] = (k < D && s.force_pending) ? s.fdt[k * n + i] : 0.f;
+        }
+        for (int q = 0; q < 9; ++q) {
+            p.def_grad[q] = 0.f;
+            p.affine[q] = 0.f;
+        }
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                p.def_grad[c * 3 + r] = s.F[(r * D + c) * n + i];
+                p.affine[c * 3 + r] = s.C[(r * D + c) * n + i];
+            }
+        if (D == 2) p.def_grad[8] = 0.f;
+        p.vel_grad_det = 0.f;
+        p.init_volume = s.V0[i];
+        p.init_radius = io.r0[i];
+        p.mass = pm.w;
+        p.damping = s.damping[i];
+        p.phase = io.phase[i];
+        const uint32_t fl = s.flags[i];
+        p.enabled = (fl & FLAG_ENABLED) ? 1u : 0u;
+        p.fixed = (fl & FLAG_FIXED) ? 1u : 0u;
+        const Material &m = s.materials[fl & FLAG_MAT_MASK];
+        p.model.tag = m.tag;
+        for (int q = 0; q < 12; ++q) p.model.data[q] = m.p[q];
+        if (m.tag == SLOSH_MODEL_SAND_LINEAR || m.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN)
+            for (int q = 0; q < 3; ++q) p.model.data[q] = s.plastic[q * n + i];
+        io.out[i] = p;
+    }
+}
+
+// Positions as vec4 (x, y, z, 0).
+__global__ void k_positions(DevScene s, float4 *out) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+        const float4 p = s.pm[i];
+        out[i] = make_float4(p.x, p.y, p.z, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Debug: slosh's full layout with extras (update_block_particle_count and
+// finalize_particles_sort, sort.slang:208-246 and 304-357), in canonical
+// order, built from the hot-path block ranks.
+// ---------------------------------------------------------------------------
+struct DebugBuffers {
+    uint32_t *counts;  // nb * NB
+    uint32_t *first;   // nb
+    uint32_t *npe;     // nb
+    uint32_t *np;      // nb
+    uint32_t *cursor;  // nb * NB
+    uint32_t *sorted;  // entries
+    uint32_t *sorted2; // entries (canonicalised)
+    uint32_t *total;   // 1
+    uint32_t cap_entries;
+};
+
+template <int D>
+__device__ __forceinline__ bool particle_rank_local(const DevScene &s, uint32_t i, uint32_t &r0, int *a) {
+    const float4 p = s.pm[i];
+    const float x[3] = {p.x, p.y, p.z};
+    const CellLoc<D> c = locate<D>(x, s.h);
+    const uint32_t slot = hash_find(s.hkeys, s.hcap, pack_key<D>(c.block));
+    if (slot == NONE) return false;
+    r0 = s.hvals[slot];
+    if (r0 == NONE) return false;
+    for (int k = 0; k < D; ++k) a[k] = c.local[k];
+    return true;
+}
+
+template <int D> __device__ __forceinline__ bool spills(const int *a, const int *o) {
+    for (int k = 0; k < D; ++k)
+        if (o[k] == 1 && a[k] < Geo<D>::MIN_SHIFT) return false;
+    return true;
+}
+
+template <int D> __device__ __forceinline__ uint32_t extra_bucket(const int *a, const int *o) {
+    const int local = a[D - 1] - o[D - 1] * Geo<D>::BW;
+    return (uint32_t)(Geo<D>::NPB + (max(local, -2) + 2));
+}
+
+template <int D> __global__ void k_dbg_count(DevScene s, DebugBuffers d) {
+    constexpr int NB = Geo<D>::NB, NN = Geo<D>::NASSOC - 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+        uint32_t r0;
+        int a[D];
+        if (!particle_rank_local<D>(s, i, r0, a)) continue;
+        atomicAdd(&d.counts[r0 * NB + a[D - 1]], 1u);
+        for (int sidx = 1; sidx <= NN; ++sidx) {
+            int o[D];
+            assoc_offset<D>(sidx, o);
+            if (!spills<D>(a, o)) continue;
+            const uint32_t rb = s.bnbh[r0 * NN + sidx - 1];
+            if (rb != NONE) atomicAdd(&d.counts[rb * NB + extra_bucket<D>(a, o)], 1u);
+        }
+    }
+}
+
+template <int D, int NT> __global__ void __launch_bounds__(NT) k_dbg_scan(DevScene s, DebugBuffers d) {
+    constexpr int NB = Geo<D>::NB, NPB = Geo<D>::NPB;
+    __shared__ uint32_t total_sh;
+    const uint32_t nb = s.ctr->n_blocks;
+    const uint32_t per = (nb + NT - 1) / NT;
+    const uint32_t r0 = threadIdx.x * per, r1 = min(r0 + per, nb);
+    uint32_t local = 0;
+    for (uint32_t r = r0; r < r1; ++r)
+        for (int b = 0; b < NB; ++b) local += d.counts[r * NB + b];
+    uint32_t run = block_exclusive_scan<NT>(local, &total_sh);
+    for (uint32_t r = r0; r < r1; ++r) {
+        d.first[r] = run;
+        uint32_t tot = 0;
+        for (int b = 0; b < NB; ++b) {
+            if (b == NPB) d.np[r] = tot;
+            d.cursor[r * NB + b] = run + tot;
+            tot += d.counts[r * NB + b];
+        }
+        d.npe[r] = tot;
+        run += tot;
+    }
+    if (threadIdx.x == 0) *d.total = total_sh;
+}
+
+template <int D> __global__ void k_dbg_scatter(DevScene s, DebugBuffers d) {
+    constexpr int NB = Geo<D>::NB, NN = Geo<D>::NASSOC - 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+        uint32_t r0;
+        int a[D];
+        if (!particle_rank_local<D>(s, i, r0, a)) continue;
+        uint32_t pos = atomicAdd(&d.cursor[r0 * NB + a[D - 1]], 1u);
+        if (pos < d.cap_entries) d.sorted[pos] = i;
+        for (int sidx = 1; sidx <= NN; ++sidx) {
+            int o[D];
+            assoc_offset<D>(sidx, o);
+            if (!spills<D>(a, o)) continue;
+            const uint32_t rb = s.bnbh[r0 * NN + sidx - 1];
+            if (rb == NONE) continue;
+            pos = atomicAdd(&d.cursor[rb * NB + extra_bucket<D>(a, o)], 1u);
+            if (pos < d.cap_entries) d.sorted[pos] = i;
+        }
+    }
+}
+
+// One thread per entry: rank by id inside its (block, bucket) segment.
+template <int D> __global__ void k_dbg_canon(DevScene s, DebugBuffers d) {
+    constexpr int NB = Geo<D>::NB;
+    const uint32_t nb = s.ctr->n_blocks;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * NB; t += stride) {
+        const uint32_t r = t / NB, b = t % NB;
+        uint32_t lo = d.first[r];
+        for (uint32_t q = 0; q < b; ++q) lo += d.counts[r * NB + q];
+        const uint32_t hi = lo + d.counts[r * NB + b];
+        if (hi > d.cap_entries) continue;
+        for (uint32_t e = lo; e < hi; ++e) {
+            const uint32_t id = d.sorted[e];
+            uint32_t rank = 0;
+            for (uint32_t j = lo; j < hi; ++j) rank += (d.sorted[j] < id) ? 1u : 0u;
+            d.sorted2[lo + rank] = id;
+        }
+    }
+}
+
+// Generic exclusive scan of n u32 (one CTA), slosh's prefix-sum semantics.
+template <int NT> __global__ void __launch_bounds__(NT) k_exclusive_scan(const uint32_t *in, uint32_t *out, uint32_t n) {
+    __shared__ uint32_t total_sh;
+    const uint32_t per = (n + NT - 1) / NT;
+    const uint32_t i0 = threadIdx.x * per, i1 = min(i0 + per, n);
+    uint32_t local = 0;
+    for (uint32_t i = i0; i < i1; ++i) local += in[i];
+    uint32_t run = block_exclusive_scan<NT>(local, &total_sh);
+    for (uint32_t i = i0; i < i1; ++i) {
+        const uint32_t v = in[i];
+        out[i] = run;
+        run += v;
+    }
+}
+
+}  // namespace slosh

@@ -1,0 +1,68 @@
+// Device view of one scene: every pointer the substep kernels read or
+// write, passed by value to each kernel.
+#pragma once
+
+#include "common.cuh"
+
+namespace slosh {
+
+struct DevScene {
+    // ---- particles (structure of arrays, math convention) -------------------
+    uint32_t n;            // particle count
+    float h;               // cell width
+    float dt;
+    float gravity[3];
+    float4 *pm;            // (x, y, z, mass); 2D: (x, y, 0, mass)
+    float *vel;            // D planes of n floats
+    float *C;              // D*D planes: APIC affine matrix, row-major math
+    float *F;              // D*D planes: deformation gradient
+    float *V0;             // initial volume
+    uint32_t *flags;       // material id | enabled | fixed
+    float *damping;        // read only when has_damping
+    float *plastic;        // 3 planes (det_p, q, log_vol_gain) for sand models
+    float *fdt;            // D planes of force*dt, read by P2G while force_pending
+    uint32_t has_damping;
+    uint32_t force_pending;
+    const Material *materials;
+
+    // ---- sparse grid --------------------------------------------------------
+    uint32_t cap;          // block capacity (power of two)
+    uint32_t hcap;         // hash slots = 2 * cap
+    uint32_t *hkeys;       // current substep hash map: packed keys
+    uint32_t *hvals;       // current substep hash map: canonical block rank
+    const uint32_t *prev_hkeys;
+    const uint32_t *prev_hvals;
+    uint32_t *slot_counts; // hcap * NPB primary-bucket counts per hash slot
+    uint32_t *blist_key;   // primary blocks in append order [cap]
+    uint32_t *blist_slot;
+    uint32_t *blist2_key;  // neighbour-only blocks in append order [cap]
+    uint32_t *blist2_slot;
+    uint32_t *hist;        // HIST_BINS counts of key >> 16
+    uint32_t *hist_start;
+    uint32_t *hist_fill;
+    uint32_t *tmp_key;     // [2 cap] keys grouped by key >> 16
+    uint32_t *tmp_slot;
+    uint32_t *bkey;        // canonical block order: packed key [cap]
+    uint32_t *bslot;       // hash slot of the block
+    uint32_t *bfirst;      // first primary entry in perm
+    uint32_t *bnp;         // number of primary particles
+    uint32_t *bcur;        // NPB insertion cursors per block
+    uint32_t *bnbh;        // (NASSOC - 1) neighbour ranks per block, NONE if inactive
+    uint32_t *pslot;       // per particle: slot * NPB + bucket
+    uint32_t *perm_tmp;    // scatter output
+    uint32_t *perm;        // canonical primary order
+    float4 *nodes;         // 64 nodes per block: (momentum | velocity, mass)
+    float4 *coll;          // node collision cache of this substep: (normal, d0)
+    uint32_t *coll_id;     // collider id or NONE
+    const float4 *prev_coll;
+    const uint32_t *prev_coll_id;
+
+    // ---- bodies -------------------------------------------------------------
+    DevBody *bodies;
+    uint32_t n_bodies;
+
+    Counters *ctr;
+    uint32_t *err;
+};
+
+}  // namespace slosh

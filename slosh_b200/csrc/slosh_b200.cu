@@ -1,0 +1,745 @@
+// C ABI of the B200-native slosh MPM substep: context lifetime, uploads and
+// downloads, the substep launch sequence (captured once per parity as a CUDA
+// graph) and the debug entry points used by the parity tests.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "grid_build.cuh"
+#include "io.cuh"
+#include "transfer.cuh"
+
+using namespace slosh;
+
+struct slosh_ctx {
+    int dim = 3;
+    float h = 0.f;
+    uint32_t cap = 0, hcap = 0, max_n = 0, n = 0;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    slosh_params params{};
+
+    // particles
+    float4 *pm = nullptr;
+    float *vel = nullptr, *C = nullptr, *F = nullptr, *V0 = nullptr, *damping = nullptr, *plastic = nullptr,
+          *fdt = nullptr, *r0 = nullptr, *phase = nullptr;
+    uint32_t *flags = nullptr;
+    Material *materials = nullptr;
+    uint32_t *mat_hkeys = nullptr, *mat_dense = nullptr;
+    uint32_t has_damping = 0, force_pending = 0, has_sand = 0, n_materials = 0;
+
+    // grid
+    uint32_t *hkeys[2] = {nullptr, nullptr}, *hvals[2] = {nullptr, nullptr};
+    uint32_t *slot_counts = nullptr, *blist_key = nullptr, *blist_slot = nullptr, *blist2_key = nullptr,
+             *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_fill = nullptr, *tmp_key = nullptr,
+             *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
+             *bcur = nullptr, *bnbh = nullptr;
+    uint32_t *pslot = nullptr, *perm_tmp = nullptr, *perm = nullptr;
+    float4 *nodes = nullptr, *coll[2] = {nullptr, nullptr};
+    uint32_t *coll_id[2] = {nullptr, nullptr};
+
+    DevBody *bodies = nullptr;
+    uint32_t n_bodies = 0;
+    Counters *ctr = nullptr;
+    uint32_t *err = nullptr;
+    uint32_t *small = nullptr;  // [0] n_mat, [1] scene flags, [2] debug total
+    uint32_t parity = 0;
+
+    slosh_particle *staging = nullptr;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graphs_valid = false;
+
+    std::string last_error;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+int fail(slosh_ctx *c, int code, const char *fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        c->last_error = buf;
+    }
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(c, SLOSH_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T> int dalloc(slosh_ctx *c, T **p, size_t count) {
+    void *q = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(c, SLOSH_E_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    c->allocs.push_back(q);
+    *p = (T *)q;
+    return SLOSH_OK;
+}
+
+uint32_t next_pow2(uint32_t v) {
+    uint32_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+int npb(int dim) { return dim == 3 ? Geo<3>::NPB : Geo<2>::NPB; }
+int nnb(int dim) { return dim == 3 ? Geo<3>::NASSOC - 1 : Geo<2>::NASSOC - 1; }
+int nbk(int dim) { return dim == 3 ? Geo<3>::NB : Geo<2>::NB; }
+
+DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
+    DevScene s{};
+    s.n = c->n;
+    s.h = c->h;
+    s.dt = c->params.dt;
+    for (int k = 0; k < 3; ++k) s.gravity[k] = c->params.gravity[k];
+    s.pm = c->pm;
+    s.vel = c->vel;
+    s.C = c->C;
+    s.F = c->F;
+    s.V0 = c->V0;
+    s.flags = c->flags;
+    s.damping = c->damping;
+    s.plastic = c->plastic;
+    s.fdt = c->fdt;
+    s.has_damping = c->has_damping;
+    s.force_pending = force ? 1u : 0u;
+    s.materials = c->materials;
+    s.cap = c->cap;
+    s.hcap = c->hcap;
+    const uint32_t cur = parity & 1u, prv = cur ^ 1u;
+    s.hkeys = c->hkeys[cur];
+    s.hvals = c->hvals[cur];
+    s.prev_hkeys = c->hkeys[prv];
+    s.prev_hvals = c->hvals[prv];
+    s.slot_counts = c->slot_counts;
+    s.blist_key = c->blist_key;
+    s.blist_slot = c->blist_slot;
+    s.blist2_key = c->blist2_key;
+    s.blist2_slot = c->blist2_slot;
+    s.hist = c->hist;
+    s.hist_start = c->hist_start;
+    s.hist_fill = c->hist_fill;
+    s.tmp_key = c->tmp_key;
+    s.tmp_slot = c->tmp_slot;
+    s.bkey = c->bkey;
+    s.bslot = c->bslot;
+    s.bfirst = c->bfirst;
+    s.bnp = c->bnp;
+    s.bcur = c->bcur;
+    s.bnbh = c->bnbh;
+    s.pslot = c->pslot;
+    s.perm_tmp = c->perm_tmp;
+    s.perm = c->perm;
+    s.nodes = c->nodes;
+    s.coll = c->coll[cur];
+    s.coll_id = c->coll_id[cur];
+    s.prev_coll = c->coll[prv];
+    s.prev_coll_id = c->coll_id[prv];
+    s.bodies = c->bodies;
+    s.n_bodies = c->n_bodies;
+    s.ctr = c->ctr;
+    s.err = c->err;
+    return s;
+}
+
+uint32_t grid_for(uint64_t work, uint32_t threads, uint32_t max_ctas) {
+    const uint64_t g = (work + threads - 1) / threads;
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(g, max_ctas));
+}
+
+// Kernels of one substep, in launch order (profiling names).
+constexpr int N_KERNELS = 14;
+const char *const KERNEL_NAMES[N_KERNELS] = {
+    "k_clear",       "k_touch",      "k_neighbors", "k_hist_scan", "k_bin_scatter", "k_rank",
+    "k_block_setup", "k_block_scan", "k_scatter",   "k_canon",     "k_p2g",         "k_grid_update",
+    "k_g2p_update",  "k_rigid"};
+
+// Optional per-kernel CUDA-event timing of the substep launches.
+struct Prof {
+    cudaEvent_t ev[N_KERNELS][2];
+    bool used[N_KERNELS];
+    cudaStream_t st;
+    void begin(int k) {
+        used[k] = true;
+        cudaEventRecord(ev[k][0], st);
+    }
+    void end(int k) { cudaEventRecord(ev[k][1], st); }
+};
+
+#define PROF_BEGIN(k) \
+    if (p) p->begin(k)
+#define PROF_END(k) \
+    if (p) p->end(k)
+
+// Grid build of one substep (stages shared by the substep and the debug
+// entry points).
+template <int D> void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
+    const uint32_t sm = (uint32_t)c->sm_count;
+    PROF_BEGIN(0);
+    k_clear<D><<<sm * 4, 256, 0, st>>>(s);
+    PROF_END(0);
+    PROF_BEGIN(1);
+    k_touch<D><<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
+    PROF_END(1);
+    PROF_BEGIN(2);
+    k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
+    PROF_END(2);
+    PROF_BEGIN(3);
+    k_hist_scan<1024><<<1, 1024, 0, st>>>(s);
+    PROF_END(3);
+    PROF_BEGIN(4);
+    k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    PROF_END(4);
+    PROF_BEGIN(5);
+    k_rank<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    PROF_END(5);
+    PROF_BEGIN(6);
+    k_block_setup<D><<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
+    PROF_END(6);
+    PROF_BEGIN(7);
+    k_block_scan<D, 1024><<<1, 1024, 0, st>>>(s);
+    PROF_END(7);
+    PROF_BEGIN(8);
+    k_scatter<D><<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
+    PROF_END(8);
+    PROF_BEGIN(9);
+    k_canon<D, 256><<<std::min<uint32_t>(c->cap, sm * 8), 256, 0, st>>>(s);
+    PROF_END(9);
+}
+
+template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
+    PROF_BEGIN(10);
+    k_p2g<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
+    PROF_END(10);
+}
+
+template <int D> void enqueue_grid_update(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
+    PROF_BEGIN(11);
+    k_grid_update<D><<<grid_for((uint64_t)c->cap * 64, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s);
+    PROF_END(11);
+}
+
+template <int D>
+void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force, Prof *p = nullptr) {
+    const DevScene s = make_scene(c, parity, force);
+    enqueue_grid_build<D>(c, s, st, p);
+    enqueue_p2g<D>(c, s, st, p);
+    enqueue_grid_update<D>(c, s, st, p);
+    PROF_BEGIN(12);
+    k_g2p_update<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), 128, 0, st>>>(s);
+    PROF_END(12);
+    if (c->n_bodies > 0) {
+        PROF_BEGIN(13);
+        k_rigid<D><<<1, 32, 0, st>>>(s);
+        PROF_END(13);
+    }
+}
+
+void enqueue_substep_any(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force, Prof *p = nullptr) {
+    if (c->dim == 3) enqueue_substep<3>(c, st, parity, force, p);
+    else enqueue_substep<2>(c, st, parity, force, p);
+}
+
+void destroy_graphs(slosh_ctx *c) {
+    for (int k = 0; k < 2; ++k)
+        if (c->graph[k]) {
+            cudaGraphExecDestroy(c->graph[k]);
+            c->graph[k] = nullptr;
+        }
+    c->graphs_valid = false;
+}
+
+int build_graphs(slosh_ctx *c) {
+    destroy_graphs(c);
+    for (uint32_t par = 0; par < 2; ++par) {
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_substep_any(c, c->stream, par, false);
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(c->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&c->graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    c->graphs_valid = true;
+    return SLOSH_OK;
+}
+
+int check_device_error(slosh_ctx *c) {
+    uint32_t e = 0;
+    CK(cudaMemcpy(&e, c->err, 4, cudaMemcpyDeviceToHost));
+    if (e == 0) return SLOSH_OK;
+    CK(cudaMemset(c->err, 0, 4));
+    if (e & (ERR_HASH_OVERFLOW | ERR_BLOCK_OVERFLOW))
+        return fail(c, SLOSH_E_OVERFLOW, "active blocks exceed the grid capacity %u (error bits 0x%x)", c->cap, e);
+    if (e & ERR_KEY_RANGE)
+        return fail(c, SLOSH_E_OVERFLOW, "a particle left the packed block-key range (error bits 0x%x)", e);
+    if (e & (ERR_MATERIALS | ERR_MATERIAL_HASH))
+        return fail(c, SLOSH_E_MATERIAL, "material table error (bits 0x%x; max %u materials)", e, MAX_MATERIALS);
+    return fail(c, SLOSH_E_CUDA, "device error bits 0x%x", e);
+}
+
+cudaStream_t pick(slosh_ctx *c, void *stream) { return stream ? (cudaStream_t)stream : c->stream; }
+
+void to_dev_body(const slosh_body &b, DevBody &d) {
+    std::memset(&d, 0, sizeof(d));
+    std::memcpy(&d.shape_type, &b.shape_a[3], 4);
+    for (int k = 0; k < 4; ++k) {
+        d.sa[k] = b.shape_a[k];
+        d.rot[k] = b.rotation[k];
+    }
+    for (int k = 0; k < 3; ++k) {
+        d.tra[k] = b.translation[k];
+        d.linvel[k] = b.linvel[k];
+        d.angvel[k] = b.angvel[k];
+        d.inv_mass[k] = b.inv_mass[k];
+        d.local_com[k] = b.local_com[k];
+    }
+    d.scale = b.translation[3];
+    d.bc_type = b.bc_type;
+    d.friction = b.bc_friction;
+}
+
+}  // namespace
+
+extern "C" {
+
+int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
+    if (!cfg || !out) return SLOSH_E_INVALID;
+    *out = nullptr;
+    if ((cfg->dim != 2 && cfg->dim != 3) || !(cfg->cell_width > 0.f) || cfg->grid_capacity == 0 ||
+        cfg->max_particles == 0 || cfg->grid_capacity > (1u << 24))
+        return SLOSH_E_INVALID;
+    slosh_ctx *c = new slosh_ctx();
+    c->dim = (int)cfg->dim;
+    c->h = cfg->cell_width;
+    c->cap = next_pow2(cfg->grid_capacity);
+    c->hcap = 2 * c->cap;
+    c->max_n = cfg->max_particles;
+    c->device = cfg->device;
+    int st = SLOSH_OK;
+    auto fail_create = [&](int code) {
+        slosh_ctx_destroy(c);
+        return code;
+    };
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
+    const size_t N = c->max_n;
+    const int D = c->dim;
+    const uint32_t cap = c->cap, hcap = c->hcap;
+    if ((st = dalloc(c, &c->pm, N)) || (st = dalloc(c, &c->vel, N * D)) || (st = dalloc(c, &c->C, N * D * D)) ||
+        (st = dalloc(c, &c->F, N * D * D)) || (st = dalloc(c, &c->V0, N)) || (st = dalloc(c, &c->flags, N)) ||
+        (st = dalloc(c, &c->damping, N)) || (st = dalloc(c, &c->plastic, N * 3)) || (st = dalloc(c, &c->fdt, N * D)) ||
+        (st = dalloc(c, &c->r0, N)) || (st = dalloc(c, &c->phase, N)) ||
+        (st = dalloc(c, &c->materials, MAX_MATERIALS)) || (st = dalloc(c, &c->mat_hkeys, MAT_HASH)) ||
+        (st = dalloc(c, &c->mat_dense, MAT_HASH)) || (st = dalloc(c, &c->hkeys[0], hcap)) ||
+        (st = dalloc(c, &c->hkeys[1], hcap)) || (st = dalloc(c, &c->hvals[0], hcap)) ||
+        (st = dalloc(c, &c->hvals[1], hcap)) || (st = dalloc(c, &c->slot_counts, (size_t)hcap * npb(D))) ||
+        (st = dalloc(c, &c->blist_key, cap)) || (st = dalloc(c, &c->blist_slot, cap)) ||
+        (st = dalloc(c, &c->blist2_key, cap)) || (st = dalloc(c, &c->blist2_slot, cap)) ||
+        (st = dalloc(c, &c->hist, HIST_BINS)) || (st = dalloc(c, &c->hist_start, HIST_BINS)) ||
+        (st = dalloc(c, &c->hist_fill, HIST_BINS)) || (st = dalloc(c, &c->tmp_key, 2 * (size_t)cap)) ||
+        (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) || (st = dalloc(c, &c->bkey, cap)) ||
+        (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
+        (st = dalloc(c, &c->bcur, (size_t)cap * npb(D))) || (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) ||
+        (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm_tmp, N)) || (st = dalloc(c, &c->perm, N)) ||
+        (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
+        (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
+        (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, MAX_BODIES)) ||
+        (st = dalloc(c, &c->ctr, 1)) || (st = dalloc(c, &c->err, 1)) || (st = dalloc(c, &c->small, 4)) ||
+        (st = dalloc(c, &c->staging, N)))
+        return fail_create(st);
+    cudaMemset(c->hkeys[0], 0xff, hcap * 4);
+    cudaMemset(c->hkeys[1], 0xff, hcap * 4);
+    cudaMemset(c->hvals[0], 0xff, hcap * 4);
+    cudaMemset(c->hvals[1], 0xff, hcap * 4);
+    cudaMemset(c->ctr, 0, sizeof(Counters));
+    cudaMemset(c->err, 0, 4);
+    cudaMemset(c->damping, 0, N * 4);
+    if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
+    c->params.gravity[1] = -9.81f;
+    c->params.dt = 1.0f / 60.0f;
+    *out = c;
+    return SLOSH_OK;
+}
+
+void slosh_ctx_destroy(slosh_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    destroy_graphs(c);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int slosh_set_params(slosh_ctx *c, const slosh_params *p) {
+    if (!c || !p || !(p->dt > 0.f)) return fail(c, SLOSH_E_INVALID, "dt must be > 0");
+    c->params = *p;
+    destroy_graphs(c);
+    return SLOSH_OK;
+}
+
+int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32_t n, void *stream) {
+    if (!c || (!particles && n)) return SLOSH_E_INVALID;
+    if (n > c->max_n) return fail(c, SLOSH_E_CAPACITY, "%u particles exceed max_particles %u", n, c->max_n);
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    destroy_graphs(c);
+    c->n = n;
+    CK(cudaMemcpyAsync(c->staging, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(c->mat_hkeys, 0xff, MAT_HASH * 4, st));
+    CK(cudaMemsetAsync(c->small, 0, 16, st));
+    CK(cudaMemsetAsync(c->err, 0, 4, st));
+    CK(cudaMemsetAsync(c->ctr, 0, sizeof(Counters), st));
+    for (int k = 0; k < 2; ++k) {
+        CK(cudaMemsetAsync(c->hkeys[k], 0xff, c->hcap * 4, st));
+        CK(cudaMemsetAsync(c->hvals[k], 0xff, c->hcap * 4, st));
+    }
+    c->parity = 0;
+    if (n > 0) {
+        DevScene s = make_scene(c, 0, false);
+        IoBuffers io{};
+        io.in = c->staging;
+        io.mat_hkeys = c->mat_hkeys;
+        io.mat_dense = c->mat_dense;
+        io.n_mat = c->small;
+        io.scene_flags = c->small + 1;
+        io.r0 = c->r0;
+        io.phase = c->phase;
+        const uint32_t g = grid_for(n, 256, (uint32_t)c->sm_count * 16);
+        k_mat_insert<<<g, 256, 0, st>>>(s, io);
+        if (c->dim == 3) k_ingest<3><<<g, 256, 0, st>>>(s, io);
+        else k_ingest<2><<<g, 256, 0, st>>>(s, io);
+        CK(cudaGetLastError());
+    }
+    uint32_t small[2] = {0, 0};
+    CK(cudaMemcpyAsync(small, c->small, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    c->n_materials = small[0];
+    c->has_damping = (small[1] & SCENE_DAMPING) ? 1u : 0u;
+    c->force_pending = (small[1] & SCENE_FORCE) ? 1u : 0u;
+    c->has_sand = (small[1] & SCENE_SAND) ? 1u : 0u;
+    return check_device_error(c);
+}
+
+int slosh_download_particles(slosh_ctx *c, slosh_particle *out, uint32_t n, void *stream) {
+    if (!c || (!out && n)) return SLOSH_E_INVALID;
+    if (n > c->n) return fail(c, SLOSH_E_INVALID, "asked for %u particles, context holds %u", n, c->n);
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    if (n > 0) {
+        DevScene s = make_scene(c, c->parity, c->force_pending != 0);
+        IoBuffers io{};
+        io.out = c->staging;
+        io.r0 = c->r0;
+        io.phase = c->phase;
+        const uint32_t g = grid_for(c->n, 256, (uint32_t)c->sm_count * 16);
+        if (c->dim == 3) k_egest<3><<<g, 256, 0, st>>>(s, io);
+        else k_egest<2><<<g, 256, 0, st>>>(s, io);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, c->staging, (size_t)n * sizeof(slosh_particle), cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return check_device_error(c);
+}
+
+int slosh_download_positions(slosh_ctx *c, float *out, uint32_t n, void *stream) {
+    if (!c || (!out && n)) return SLOSH_E_INVALID;
+    if (n > c->n) return fail(c, SLOSH_E_INVALID, "asked for %u particles, context holds %u", n, c->n);
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    if (n > 0) {
+        DevScene s = make_scene(c, c->parity, false);
+        float4 *tmp = (float4 *)c->staging;  // staging holds >= 12 float4 per particle
+        k_positions<<<grid_for(c->n, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s, tmp);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, tmp, (size_t)n * 16, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return check_device_error(c);
+}
+
+int slosh_set_bodies(slosh_ctx *c, const slosh_body *bodies, uint32_t n) {
+    if (!c || (!bodies && n)) return SLOSH_E_INVALID;
+    if (n > MAX_BODIES) return fail(c, SLOSH_E_CAPACITY, "%u bodies exceed the limit of %u", n, MAX_BODIES);
+    std::vector<DevBody> db(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        to_dev_body(bodies[i], db[i]);
+        if (!(db[i].scale > 0.f)) return fail(c, SLOSH_E_INVALID, "body %u: scale must be > 0", i);
+        if (db[i].shape_type != SLOSH_SHAPE_BALL && db[i].shape_type != SLOSH_SHAPE_CUBOID)
+            return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u", i, db[i].shape_type);
+    }
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (n) CK(cudaMemcpy(c->bodies, db.data(), n * sizeof(DevBody), cudaMemcpyHostToDevice));
+    c->n_bodies = n;
+    destroy_graphs(c);
+    return SLOSH_OK;
+}
+
+int slosh_get_bodies(slosh_ctx *c, slosh_body *out, uint32_t n) {
+    if (!c || (!out && n) || n > c->n_bodies) return SLOSH_E_INVALID;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<DevBody> db(n);
+    if (n) CK(cudaMemcpy(db.data(), c->bodies, n * sizeof(DevBody), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+        slosh_body &b = out[i];
+        const DevBody &d = db[i];
+        for (int k = 0; k < 4; ++k) {
+            b.shape_a[k] = d.sa[k];
+            b.rotation[k] = d.rot[k];
+        }
+        std::memcpy(&b.shape_a[3], &d.shape_type, 4);
+        for (int k = 0; k < 3; ++k) {
+            b.translation[k] = d.tra[k];
+            b.linvel[k] = d.linvel[k];
+            b.angvel[k] = d.angvel[k];
+            b.inv_mass[k] = d.inv_mass[k];
+            b.local_com[k] = d.local_com[k];
+        }
+        b.translation[3] = d.scale;
+        b.bc_type = d.bc_type;
+        b.bc_friction = d.friction;
+    }
+    return SLOSH_OK;
+}
+
+int slosh_step(slosh_ctx *c, uint32_t n_substeps, void *stream) {
+    if (!c) return SLOSH_E_INVALID;
+    if (c->n == 0) return fail(c, SLOSH_E_STATE, "no particles uploaded");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    for (uint32_t k = 0; k < n_substeps; ++k) {
+        if (c->force_pending) {
+            enqueue_substep_any(c, st, c->parity, true);
+            CK(cudaGetLastError());
+            c->force_pending = 0;
+        } else {
+            if (!c->graphs_valid) {
+                if (st != c->stream) CK(cudaStreamSynchronize(st));
+                int r = build_graphs(c);
+                if (r) return r;
+                if (st != c->stream) CK(cudaStreamSynchronize(c->stream));
+            }
+            CK(cudaGraphLaunch(c->graph[c->parity], st));
+        }
+        c->parity ^= 1u;
+    }
+    return SLOSH_OK;
+}
+
+int slosh_sync(slosh_ctx *c, void *stream) {
+    if (!c) return SLOSH_E_INVALID;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(pick(c, stream)));
+    CK(cudaGetLastError());
+    return check_device_error(c);
+}
+
+uint32_t slosh_kernels_per_substep(const slosh_ctx *c) {
+    if (!c) return 0;
+    return 13u + (c->n_bodies > 0 ? 1u : 0u);
+}
+
+int slosh_profile_substeps(slosh_ctx *c, uint32_t n_substeps, void *stream, float *kernel_ms, uint32_t cap,
+                           uint32_t *n_kernels) {
+    if (!c || (!kernel_ms && cap)) return SLOSH_E_INVALID;
+    if (c->n == 0) return fail(c, SLOSH_E_STATE, "no particles uploaded");
+    CK(cudaSetDevice(c->device));
+    Prof pr{};
+    pr.st = pick(c, stream);
+    for (int k = 0; k < N_KERNELS; ++k) {
+        CK(cudaEventCreate(&pr.ev[k][0]));
+        CK(cudaEventCreate(&pr.ev[k][1]));
+    }
+    double acc[N_KERNELS] = {};
+    int rc = SLOSH_OK;
+    for (uint32_t it = 0; it < n_substeps && rc == SLOSH_OK; ++it) {
+        for (int k = 0; k < N_KERNELS; ++k) pr.used[k] = false;
+        enqueue_substep_any(c, pr.st, c->parity, c->force_pending != 0, &pr);
+        c->force_pending = 0;
+        c->parity ^= 1u;
+        cudaError_t e = cudaEventSynchronize(pr.ev[12][1]);
+        if (e == cudaSuccess && c->n_bodies > 0) e = cudaEventSynchronize(pr.ev[13][1]);
+        if (e != cudaSuccess) {
+            rc = fail(c, SLOSH_E_CUDA, "profiling: %s", cudaGetErrorString(e));
+            break;
+        }
+        for (int k = 0; k < N_KERNELS; ++k) {
+            if (!pr.used[k]) continue;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, pr.ev[k][0], pr.ev[k][1]);
+            acc[k] += ms;
+        }
+    }
+    for (int k = 0; k < N_KERNELS; ++k) {
+        cudaEventDestroy(pr.ev[k][0]);
+        cudaEventDestroy(pr.ev[k][1]);
+    }
+    if (rc) return rc;
+    for (uint32_t k = 0; k < cap && k < (uint32_t)N_KERNELS; ++k) kernel_ms[k] = (float)acc[k];
+    if (n_kernels) *n_kernels = N_KERNELS;
+    return check_device_error(c);
+}
+
+int slosh_get_stats(slosh_ctx *c, slosh_stats *out) {
+    if (!c || !out) return SLOSH_E_INVALID;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaDeviceSynchronize());
+    Counters ctr;
+    CK(cudaMemcpy(&ctr, c->ctr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->n_particles = c->n;
+    out->n_blocks = ctr.n_blocks;
+    out->n_primary_blocks = std::min(ctr.n_primary, c->cap);
+    out->n_materials = c->n_materials;
+    out->n_svd_fp64 = ctr.n_svd_fp64;
+    return SLOSH_OK;
+}
+
+int slosh_kernel_name(uint32_t index, char *buf, size_t len) {
+    if (index >= (uint32_t)N_KERNELS || !buf || len == 0) return SLOSH_E_INVALID;
+    std::snprintf(buf, len, "%s", KERNEL_NAMES[index]);
+    return SLOSH_OK;
+}
+
+int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, uint32_t cap_sorted) {
+    if (!c || !dump) return SLOSH_E_INVALID;
+    if (c->n == 0) return fail(c, SLOSH_E_STATE, "no particles uploaded");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const DevScene s = make_scene(c, c->parity, false);
+    if (c->dim == 3) enqueue_grid_build<3>(c, s, st);
+    else enqueue_grid_build<2>(c, s, st);
+    CK(cudaGetLastError());
+    Counters ctr;
+    CK(cudaMemcpyAsync(&ctr, c->ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int e = check_device_error(c);
+    if (e) return e;
+    const uint32_t nb = ctr.n_blocks;
+    const int NB = nbk(c->dim), NN = nnb(c->dim);
+    dump->n_blocks = nb;
+    dump->nb_buckets = (uint32_t)NB;
+    dump->n_neighbors = (uint32_t)NN;
+    // Full layout with extras, on the device.
+    const uint32_t cap_entries = (uint32_t)std::min<uint64_t>((uint64_t)c->n * (c->dim == 3 ? 8 : 4), 0xffffffffull);
+    DebugBuffers d{};
+    void *blob = nullptr;
+    const size_t nbs = std::max<uint32_t>(nb, 1);
+    const size_t words = nbs * NB * 2 + nbs * 3 + (size_t)cap_entries * 2 + 1;
+    CK(cudaMalloc(&blob, words * 4));
+    uint32_t *w = (uint32_t *)blob;
+    d.counts = w;
+    d.cursor = w + nbs * NB;
+    d.first = w + nbs * NB * 2;
+    d.npe = d.first + nbs;
+    d.np = d.npe + nbs;
+    d.sorted = d.np + nbs;
+    d.sorted2 = d.sorted + cap_entries;
+    d.total = d.sorted2 + cap_entries;
+    d.cap_entries = cap_entries;
+    cudaMemsetAsync(d.counts, 0, nbs * NB * 4, st);
+    const uint32_t g = grid_for(c->n, 256, (uint32_t)c->sm_count * 16);
+    if (c->dim == 3) {
+        k_dbg_count<3><<<g, 256, 0, st>>>(s, d);
+        k_dbg_scan<3, 1024><<<1, 1024, 0, st>>>(s, d);
+        k_dbg_scatter<3><<<g, 256, 0, st>>>(s, d);
+        k_dbg_canon<3><<<grid_for(nbs * NB, 128, 4096), 128, 0, st>>>(s, d);
+    } else {
+        k_dbg_count<2><<<g, 256, 0, st>>>(s, d);
+        k_dbg_scan<2, 1024><<<1, 1024, 0, st>>>(s, d);
+        k_dbg_scatter<2><<<g, 256, 0, st>>>(s, d);
+        k_dbg_canon<2><<<grid_for(nbs * NB, 128, 4096), 128, 0, st>>>(s, d);
+    }
+    uint32_t total = 0;
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&total, d.total, 4, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    dump->n_sorted = total;
+    const uint32_t nbc = std::min(nb, cap_blocks);
+    auto copy = [&](uint32_t *dst, const uint32_t *src, size_t count) {
+        if (dst && count && ce == cudaSuccess) ce = cudaMemcpy(dst, src, count * 4, cudaMemcpyDeviceToHost);
+    };
+    copy(dump->keys, c->bkey, nbc);
+    copy(dump->first_particle, d.first, nbc);
+    copy(dump->num_particles, d.np, nbc);
+    copy(dump->num_particles_with_extras, d.npe, nbc);
+    copy(dump->bucket_counts, d.counts, (size_t)nbc * NB);
+    copy(dump->sorted_ids, d.sorted2, std::min(total, cap_sorted));
+    copy(dump->primary_first, c->bfirst, nbc);
+    copy(dump->primary_perm, c->perm, c->n);
+    copy(dump->neighbors, c->bnbh, (size_t)nbc * NN);
+    cudaFree(blob);
+    if (ce != cudaSuccess) return fail(c, SLOSH_E_CUDA, "grid debug: %s", cudaGetErrorString(ce));
+    if (total > cap_entries) return fail(c, SLOSH_E_CAPACITY, "debug layout overflow");
+    return SLOSH_OK;
+}
+
+int slosh_debug_nodes(slosh_ctx *c, int stage, float *nodes, uint32_t cap_blocks, uint32_t *n_blocks) {
+    if (!c || stage < 1 || stage > 2) return SLOSH_E_INVALID;
+    if (c->n == 0) return fail(c, SLOSH_E_STATE, "no particles uploaded");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const DevScene s = make_scene(c, c->parity, c->force_pending != 0);
+    if (c->dim == 3) {
+        enqueue_grid_build<3>(c, s, st);
+        enqueue_p2g<3>(c, s, st);
+        if (stage >= 2) enqueue_grid_update<3>(c, s, st);
+    } else {
+        enqueue_grid_build<2>(c, s, st);
+        enqueue_p2g<2>(c, s, st);
+        if (stage >= 2) enqueue_grid_update<2>(c, s, st);
+    }
+    CK(cudaGetLastError());
+    Counters ctr;
+    CK(cudaMemcpyAsync(&ctr, c->ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (n_blocks) *n_blocks = ctr.n_blocks;
+    const uint32_t nbc = std::min(ctr.n_blocks, cap_blocks);
+    if (nodes && nbc) CK(cudaMemcpy(nodes, c->nodes, (size_t)nbc * 64 * 16, cudaMemcpyDeviceToHost));
+    return check_device_error(c);
+}
+
+int slosh_prefix_sum(slosh_ctx *c, const uint32_t *in, uint32_t *out, uint32_t n) {
+    if (!c || (n && (!in || !out))) return SLOSH_E_INVALID;
+    if (n > 2 * c->cap) return fail(c, SLOSH_E_CAPACITY, "prefix sum of %u values exceeds %u", n, 2 * c->cap);
+    if (n == 0) return SLOSH_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    CK(cudaMemcpyAsync(c->tmp_key, in, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    k_exclusive_scan<1024><<<1, 1024, 0, st>>>(c->tmp_key, c->tmp_slot, n);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, c->tmp_slot, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SLOSH_OK;
+}
+
+int slosh_last_error(const slosh_ctx *c, char *buf, size_t len) {
+    if (!c || !buf || len == 0) return SLOSH_E_INVALID;
+    std::snprintf(buf, len, "%s", c->last_error.c_str());
+    return SLOSH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,430 @@
+"""Host-side mirror of slosh's pipeline API over the C ABI.
+
+Names and argument meaning follow dimforge/slosh:
+
+* ``SimulationParams``            src/solver/params.rs:13-21
+* ``ElasticCoefficients``          src/models/mod.rs:52-59
+* ``DruckerPrager``                src/models/drucker_prager.rs:12-68
+* ``ParticleModel``                src/solver/particle_model.rs:9-80
+* ``Particle`` / ``ParticleDynamics``  src/solver/particle.rs:23-100, 226-233
+* ``GpuBoundaryCondition``         src/solver/boundary_condition.rs:8-65
+* ``MpmData``                      src/pipeline.rs:311-430
+* ``MpmPipeline.launch_step``      src/pipeline.rs:562-770
+
+Rigid bodies are given directly (shape, pose, velocity, mass properties and
+boundary condition) instead of through rapier's body/collider sets; the
+one-way coupling of ``MpmData::new`` (zero mass properties) is the default.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (
+    BODY_DTYPE,
+    PARTICLE_DTYPE,
+    SloshConfig,
+    SloshError,
+    SloshGridDump,
+    SloshParams,
+    ptr,
+)
+
+
+@dataclass
+class SimulationParams:
+    gravity: Sequence[float] = (0.0, -9.81, 0.0)
+    dt: float = 1.0 / 60.0
+
+
+def lame_lambda_mu(young_modulus: float, poisson_ratio: float) -> tuple[float, float]:
+    """src/models/mod.rs:17-27, in float32 like the reference."""
+    e = np.float32(young_modulus)
+    nu = np.float32(poisson_ratio)
+    one = np.float32(1.0)
+    two = np.float32(2.0)
+    lam = e * nu / ((one + nu) * (one - two * nu))
+    mu = e / (two * (one + nu))
+    return float(np.float32(lam)), float(np.float32(mu))
+
+
+@dataclass
+class ElasticCoefficients:
+    lam: float
+    mu: float
+    cfl_coeff: float = 0.5
+
+    @staticmethod
+    def from_young_modulus(young_modulus: float, poisson_ratio: float) -> "ElasticCoefficients":
+        lam, mu = lame_lambda_mu(young_modulus, poisson_ratio)
+        return ElasticCoefficients(lam, mu, 0.5)
+
+
+@dataclass
+class DruckerPrager:
+    h0: float
+    h1: float
+    h2: float
+    h3: float
+    lam: float
+    mu: float
+
+    @staticmethod
+    def new(young_modulus: float, poisson_ratio: float) -> "DruckerPrager":
+        if young_modulus > 0.0:
+            lam, mu = lame_lambda_mu(young_modulus, poisson_ratio)
+        else:
+            lam, mu = -1.0, -1.0
+        return DruckerPrager.from_lame(lam, mu)
+
+    @staticmethod
+    def from_lame(lam: float, mu: float) -> "DruckerPrager":
+        return DruckerPrager(math.radians(35.0), math.radians(9.0), 0.2, math.radians(10.0), lam, mu)
+
+
+@dataclass
+class ParticleModel:
+    """A GpuParticleModel record: tag + 12 payload words."""
+
+    tag: int
+    data: tuple
+
+    @staticmethod
+    def elastic(young_modulus: float, poisson_ratio: float) -> "ParticleModel":
+        c = ElasticCoefficients.from_young_modulus(young_modulus, poisson_ratio)
+        return ParticleModel(_lib.MODEL_ELASTIC_LINEAR, (c.lam, c.mu, c.cfl_coeff) + (0.0,) * 9)
+
+    @staticmethod
+    def elastic_neo_hookean(young_modulus: float, poisson_ratio: float) -> "ParticleModel":
+        c = ElasticCoefficients.from_young_modulus(young_modulus, poisson_ratio)
+        return ParticleModel(_lib.MODEL_ELASTIC_NEO_HOOKEAN, (c.lam, c.mu, c.cfl_coeff) + (0.0,) * 9)
+
+    @staticmethod
+    def _sand(tag: int, young_modulus: float, poisson_ratio: float, friction_angle_deg: float | None):
+        plastic = DruckerPrager.new(young_modulus, poisson_ratio)
+        if friction_angle_deg is not None:
+            plastic.h0 = math.radians(friction_angle_deg)
+        c = ElasticCoefficients.from_young_modulus(young_modulus, poisson_ratio)
+        state = (1.0, 1.0, 0.0)  # DruckerPragerPlasticState::default
+        return ParticleModel(
+            tag,
+            state
+            + (plastic.h0, plastic.h1, plastic.h2, plastic.h3, plastic.lam, plastic.mu)
+            + (c.lam, c.mu, c.cfl_coeff),
+        )
+
+    @staticmethod
+    def sand(young_modulus: float, poisson_ratio: float, friction_angle_deg: float | None = None) -> "ParticleModel":
+        return ParticleModel._sand(_lib.MODEL_SAND_LINEAR, young_modulus, poisson_ratio, friction_angle_deg)
+
+    @staticmethod
+    def sand_neo_hookean(
+        young_modulus: float, poisson_ratio: float, friction_angle_deg: float | None = None
+    ) -> "ParticleModel":
+        return ParticleModel._sand(_lib.MODEL_SAND_NEO_HOOKEAN, young_modulus, poisson_ratio, friction_angle_deg)
+
+    @staticmethod
+    def fluid_tait(rest_density: float, bulk_modulus: float, gamma: float) -> "ParticleModel":
+        return ParticleModel(_lib.MODEL_FLUID_TAIT, (rest_density, bulk_modulus, gamma) + (0.0,) * 9)
+
+
+def make_particles(
+    positions: np.ndarray,
+    radius: float,
+    density: float,
+    model: ParticleModel,
+    dim: int = 3,
+    velocities: np.ndarray | None = None,
+) -> np.ndarray:
+    """Vectorised ``Particle::new(position, radius, density, model)``
+    (src/solver/particle.rs:66-84, 236-246): V0 = (2r)^dim, mass = V0 density,
+    F = I, C = 0, enabled, not fixed."""
+    pos = np.asarray(positions, dtype=np.float32)
+    n = pos.shape[0]
+    rec = np.zeros(n, dtype=PARTICLE_DTYPE)
+    rec["position"][:, : pos.shape[1]] = pos
+    if velocities is not None:
+        v = np.asarray(velocities, dtype=np.float32)
+        rec["velocity"][:, : v.shape[1]] = v
+    ident = np.zeros(9, np.float32)
+    ident[0] = ident[4] = 1.0
+    if dim == 3:
+        ident[8] = 1.0
+    rec["def_grad"][:] = ident
+    d2 = np.float32(np.float32(radius) * np.float32(2.0))
+    vol = d2 * d2 * d2 if dim == 3 else d2 * d2  # f32 powi, repeated products
+    rec["init_volume"] = vol
+    rec["init_radius"] = radius
+    rec["mass"] = np.float32(vol) * np.float32(density)
+    rec["phase"] = 1.0
+    rec["enabled"] = 1
+    rec["model_tag"] = model.tag
+    rec["model"][:] = np.asarray(model.data, dtype=np.float32)
+    return rec
+
+
+class GpuBoundaryCondition:
+    """Boundary condition of a collider (src/solver/boundary_condition.rs)."""
+
+    def __init__(self, ty: int, friction: float = 0.0):
+        self.ty = ty
+        self.friction = friction
+
+    @staticmethod
+    def stick():
+        return GpuBoundaryCondition(_lib.BC_STICK, 0.0)
+
+    @staticmethod
+    def slip():
+        return GpuBoundaryCondition(_lib.BC_SLIP, 0.0)
+
+    @staticmethod
+    def separate(friction: float):
+        return GpuBoundaryCondition(_lib.BC_SEPARATE, friction)
+
+    @staticmethod
+    def friction_z_up(friction: float):
+        return GpuBoundaryCondition(_lib.BC_FRICTION_Z_UP, friction)
+
+    @staticmethod
+    def disabled():
+        return GpuBoundaryCondition(_lib.BC_DISABLED, 0.0)
+
+    @staticmethod
+    def default():
+        return GpuBoundaryCondition.separate(1.0)
+
+
+@dataclass
+class RigidBody:
+    """One body with its collider (a GpuBodySet entry).  ``shape`` is
+    ("cuboid", half_extents) or ("ball", radius).  Rotation is a unit
+    quaternion (i, j, k, w) in 3D or an angle in radians in 2D."""
+
+    shape: tuple
+    translation: Sequence[float] = (0.0, 0.0, 0.0)
+    rotation: Sequence[float] | float = (0.0, 0.0, 0.0, 1.0)
+    linvel: Sequence[float] = (0.0, 0.0, 0.0)
+    angvel: Sequence[float] = (0.0, 0.0, 0.0)
+    inv_mass: Sequence[float] = (0.0, 0.0, 0.0)
+    local_com: Sequence[float] = (0.0, 0.0, 0.0)
+    boundary_condition: GpuBoundaryCondition = field(default_factory=GpuBoundaryCondition.default)
+    scale: float = 1.0
+
+    def record(self, dim: int) -> np.ndarray:
+        r = np.zeros((), dtype=BODY_DTYPE)
+        kind, param = self.shape
+        if kind == "cuboid":
+            he = list(param) + [0.0] * (3 - len(param))
+            r["shape_a"][:3] = he[:3]
+            r["shape_a"].view(np.uint32)[3] = _lib.SHAPE_CUBOID
+        elif kind == "ball":
+            r["shape_a"][0] = float(param)
+            r["shape_a"].view(np.uint32)[3] = _lib.SHAPE_BALL
+        else:
+            raise ValueError(f"unsupported shape {kind!r}")
+        if dim == 3:
+            r["rotation"][:] = np.asarray(self.rotation, np.float32)
+        else:
+            ang = float(self.rotation) if np.isscalar(self.rotation) else 0.0
+            r["rotation"][:2] = (math.cos(ang), math.sin(ang))
+        t = list(self.translation) + [0.0] * (3 - len(self.translation))
+        r["translation"][:3] = t[:3]
+        r["translation"][3] = self.scale
+        for name in ("linvel", "angvel", "inv_mass", "local_com"):
+            v = list(getattr(self, name))
+            v = v + [0.0] * (3 - len(v))
+            r[name][:3] = v[:3]
+        r["bc_type"] = self.boundary_condition.ty
+        r["bc_friction"] = self.boundary_condition.friction
+        return r
+
+
+def quat_from_axis_angle(axis: Sequence[float], angle: float) -> tuple:
+    a = np.asarray(axis, np.float64)
+    a = a / np.linalg.norm(a)
+    s = math.sin(angle / 2.0)
+    return (float(a[0] * s), float(a[1] * s), float(a[2] * s), math.cos(angle / 2.0))
+
+
+def _check(lib, ctx, code: int):
+    if code != 0:
+        buf = ctypes.create_string_buffer(512)
+        if ctx:
+            lib.slosh_last_error(ctx, buf, 512)
+        raise SloshError(code, buf.value.decode(errors="replace"))
+
+
+class MpmData:
+    """GPU-resident state of one scene: particles, sparse grid, bodies.
+
+    Mirrors ``MpmData::new(backend, params, particles, bodies, colliders,
+    materials, cell_width, grid_capacity)`` (src/pipeline.rs:311)."""
+
+    def __init__(
+        self,
+        params: SimulationParams,
+        particles: np.ndarray,
+        bodies: Iterable[RigidBody] = (),
+        cell_width: float = 1.0,
+        grid_capacity: int = 30_000,
+        dim: int = 3,
+        device: int = 0,
+        max_particles: int | None = None,
+    ):
+        self._lib = _lib.load()
+        self.dim = dim
+        self.cell_width = float(cell_width)
+        self.params = params
+        cfg = SloshConfig(dim, float(cell_width), int(grid_capacity), int(max_particles or max(len(particles), 1)), device, 0)
+        ctx = ctypes.c_void_p()
+        code = self._lib.slosh_ctx_create(ctypes.byref(cfg), ctypes.byref(ctx))
+        if code != 0:
+            raise SloshError(code, "slosh_ctx_create failed")
+        self._ctx = ctx
+        self.set_params(params)
+        self.set_bodies(list(bodies))
+        self.upload(particles)
+
+    @staticmethod
+    def new(params, particles, bodies=(), cell_width=1.0, grid_capacity=30_000, dim=3, device=0) -> "MpmData":
+        return MpmData(params, particles, bodies, cell_width, grid_capacity, dim, device)
+
+    # -- state -----------------------------------------------------------------
+    def set_params(self, params: SimulationParams):
+        g = list(params.gravity) + [0.0] * (3 - len(params.gravity))
+        p = SloshParams((ctypes.c_float * 3)(*g[:3]), float(params.dt))
+        _check(self._lib, self._ctx, self._lib.slosh_set_params(self._ctx, ctypes.byref(p)))
+        self.params = params
+
+    def set_bodies(self, bodies: list):
+        self.bodies = bodies
+        recs = np.zeros(len(bodies), dtype=BODY_DTYPE)
+        for i, b in enumerate(bodies):
+            recs[i] = b.record(self.dim)
+        self.n_bodies = len(bodies)
+        _check(self._lib, self._ctx, self._lib.slosh_set_bodies(self._ctx, ptr(recs) if len(bodies) else None, len(bodies)))
+
+    def upload(self, particles: np.ndarray, stream=None):
+        particles = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        self.n = len(particles)
+        _check(
+            self._lib,
+            self._ctx,
+            self._lib.slosh_upload_particles(self._ctx, ptr(particles), self.n, stream),
+        )
+
+    def download_particles(self, out: np.ndarray | None = None, stream=None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.n, dtype=PARTICLE_DTYPE)
+        _check(self._lib, self._ctx, self._lib.slosh_download_particles(self._ctx, ptr(out), self.n, stream))
+        return out
+
+    def positions(self, out: np.ndarray | None = None, stream=None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((self.n, 4), dtype=np.float32)
+        _check(self._lib, self._ctx, self._lib.slosh_download_positions(self._ctx, ptr(out), self.n, stream))
+        return out
+
+    def get_bodies(self) -> np.ndarray:
+        out = np.zeros(self.n_bodies, dtype=BODY_DTYPE)
+        if self.n_bodies:
+            _check(self._lib, self._ctx, self._lib.slosh_get_bodies(self._ctx, ptr(out), self.n_bodies))
+        return out
+
+    def sync(self, stream=None):
+        _check(self._lib, self._ctx, self._lib.slosh_sync(self._ctx, stream))
+
+    @property
+    def kernels_per_substep(self) -> int:
+        return int(self._lib.slosh_kernels_per_substep(self._ctx))
+
+    def stats(self) -> dict:
+        raw = np.zeros(8, np.uint32)
+        _check(self._lib, self._ctx, self._lib.slosh_get_stats(self._ctx, ptr(raw)))
+        keys = ("n_particles", "n_blocks", "n_primary_blocks", "n_materials", "n_svd_fp64")
+        return {k: int(raw[i]) for i, k in enumerate(keys)}
+
+    def profile_substeps(self, n_substeps: int, stream=None) -> dict:
+        """Per-kernel device milliseconds summed over `n_substeps` substeps
+        (CUDA events around every launch; advances the simulation)."""
+        ms = np.zeros(32, np.float32)
+        nk = ctypes.c_uint32(0)
+        _check(
+            self._lib,
+            self._ctx,
+            self._lib.slosh_profile_substeps(self._ctx, int(n_substeps), stream, ptr(ms), 32, ctypes.byref(nk)),
+        )
+        out = {}
+        buf = ctypes.create_string_buffer(64)
+        for k in range(nk.value):
+            self._lib.slosh_kernel_name(k, buf, 64)
+            out[buf.value.decode()] = float(ms[k])
+        return out
+
+    # -- debug views -------------------------------------------------------------
+    def grid_debug(self) -> dict:
+        d = SloshGridDump()
+        _check(self._lib, self._ctx, self._lib.slosh_grid_debug(self._ctx, ctypes.byref(d), 0, 0))
+        nb, ns, NB, NN = d.n_blocks, d.n_sorted, d.nb_buckets, d.n_neighbors
+        out = {
+            "keys": np.zeros(nb, np.uint32),
+            "first_particle": np.zeros(nb, np.uint32),
+            "num_particles": np.zeros(nb, np.uint32),
+            "num_particles_with_extras": np.zeros(nb, np.uint32),
+            "bucket_counts": np.zeros(nb * NB, np.uint32),
+            "sorted_ids": np.zeros(ns, np.uint32),
+            "primary_first": np.zeros(nb, np.uint32),
+            "primary_perm": np.zeros(self.n, np.uint32),
+            "neighbors": np.zeros(nb * NN, np.uint32),
+        }
+        d2 = SloshGridDump()
+        for name, arr in out.items():
+            setattr(d2, name, arr.ctypes.data if arr.size else None)
+        _check(self._lib, self._ctx, self._lib.slosh_grid_debug(self._ctx, ctypes.byref(d2), nb, ns))
+        out["bucket_counts"] = out["bucket_counts"].reshape(nb, NB)
+        out["neighbors"] = out["neighbors"].reshape(nb, NN)
+        return out
+
+    def debug_nodes(self, stage: int) -> np.ndarray:
+        nb = ctypes.c_uint32(0)
+        _check(self._lib, self._ctx, self._lib.slosh_debug_nodes(self._ctx, stage, None, 0, ctypes.byref(nb)))
+        out = np.zeros((nb.value * 64, 4), np.float32)
+        _check(self._lib, self._ctx, self._lib.slosh_debug_nodes(self._ctx, stage, ptr(out), nb.value, ctypes.byref(nb)))
+        return out
+
+    def prefix_sum(self, values: np.ndarray) -> np.ndarray:
+        v = np.ascontiguousarray(values, dtype=np.uint32)
+        out = np.zeros_like(v)
+        _check(self._lib, self._ctx, self._lib.slosh_prefix_sum(self._ctx, ptr(v), ptr(out), len(v)))
+        return out
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.slosh_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MpmPipeline:
+    """``MpmPipeline::launch_step``: enqueues substeps on the GPU.
+
+    The whole substep is one CUDA graph; no host round trip happens inside
+    ``launch_step``.  Device-side errors (block capacity overflow) surface
+    at the next ``MpmData.sync()`` or download."""
+
+    def __init__(self):
+        self._lib = _lib.load()
+
+    def launch_step(self, data: MpmData, n_substeps: int = 1, stream=None):
+        _check(self._lib, data._ctx, self._lib.slosh_step(data._ctx, int(n_substeps), stream))

@@ -1,0 +1,255 @@
+"""GPU parity of the CUDA substep against the oracle, through the C ABI.
+
+Bit-exact: prefix sum, block keys, per-bucket counts, offsets and the sorted
+permutation (slosh's full layout with extras, and the hot path's primary
+permutation).  FP32 tolerance: nodes after P2G and after the grid update, and
+particle state after 1 and 10 substeps.  The tolerances are stated per check
+as max |gpu - oracle| <= atol + rtol * max |oracle| over the compared field;
+the differences come from the summation order of the atomics, FMA
+contraction, the two independent SVD implementations and the factored
+B-spline weights of the particle-centric P2G.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from slosh_b200 import scenes
+from slosh_b200._lib import BODY_DTYPE, SloshError, SLOSH_E_OVERFLOW
+from slosh_b200.pipeline import (
+    GpuBoundaryCondition,
+    MpmData,
+    MpmPipeline,
+    ParticleModel,
+    RigidBody,
+    SimulationParams,
+    make_particles,
+)
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def small_scenes():
+    return {
+        "sand3d": scenes.sand_column_3d(h=1 / 32, substeps=10),
+        "elastic3d": scenes.elastic_drop_3d(h=1 / 32, substeps=10),
+        "fluid2d": scenes.dam_break_2d(h=1 / 64, substeps=10),
+        "sand3d_fine": scenes.sand_column_3d(h=1 / 64, substeps=10),
+    }
+
+
+def pair(scene):
+    data = scenes.build_mpm_data(scene)
+    orc = O.from_scene(scene, threads=8)
+    return data, orc
+
+
+def close(name, got, exp, atol, rtol):
+    got = np.asarray(got, np.float64)
+    exp = np.asarray(exp, np.float64)
+    err = np.abs(got - exp).max() if got.size else 0.0
+    bound = atol + rtol * (np.abs(exp).max() if exp.size else 0.0)
+    print(f"{name}: max err {err:.3e} bound {bound:.3e}")
+    assert err <= bound, f"{name}: max err {err:.3e} > {bound:.3e}"
+
+
+def grid_equal(gpu, orc):
+    for k in ("keys", "first_particle", "num_particles", "num_particles_with_extras", "sorted_ids"):
+        assert np.array_equal(gpu[k], orc[k]), k
+    assert np.array_equal(gpu["bucket_counts"], orc["bucket_counts"])
+    # hot path: primaries in canonical order = the first num_particles entries of each block
+    prim = np.concatenate(
+        [orc["sorted_ids"][f : f + n] for f, n in zip(orc["first_particle"], orc["num_particles"])]
+    )
+    assert np.array_equal(gpu["primary_perm"], prim)
+    pf = np.zeros_like(orc["num_particles"])
+    pf[1:] = np.cumsum(orc["num_particles"])[:-1]
+    assert np.array_equal(gpu["primary_first"], pf)
+
+
+def test_prefix_sum_recipe(cuda_lib):
+    """src/grid/prefix_sum.rs:219-270: len 15071, ones / iota / random % 10000."""
+    sc = scenes.sand_column_3d(h=1 / 16, substeps=1)
+    sc.grid_capacity = 1 << 14
+    data = scenes.build_mpm_data(sc)
+    g = np.load(os.path.join(GOLDEN, "prefix_sum.npz"))
+    n = 15071
+    for v in (np.ones(n, np.uint32), np.arange(n, dtype=np.uint32), g["input"]):
+        assert np.array_equal(data.prefix_sum(v), O.prefix_sum(v))
+    assert np.array_equal(data.prefix_sum(g["input"]), g["expected"])
+    data.close()
+
+
+@pytest.mark.parametrize("case", ["grid3", "grid2"])
+def test_grid_golden(cuda_lib, case):
+    with open(os.path.join(GOLDEN, "grid_small.json")) as f:
+        g = json.load(f)[case]
+    recs = make_particles(np.asarray(g["positions"]), g["h"] / 4, 1000.0, ParticleModel.elastic(1e5, 0.3), dim=g["dim"])
+    data = MpmData(SimulationParams(), recs, [], cell_width=g["h"], grid_capacity=1024, dim=g["dim"])
+    got = data.grid_debug()
+    exp = {k: np.asarray(v, np.uint32) for k, v in g["layout"].items()}
+    grid_equal(got, exp)
+    data.close()
+
+
+@pytest.mark.parametrize("name", ["sand3d", "elastic3d", "fluid2d", "sand3d_fine"])
+def test_grid_build_bitexact(cuda_lib, name):
+    sc = small_scenes()[name]
+    data, orc = pair(sc)
+    grid_equal(data.grid_debug(), orc.grid())
+    # after some substeps, on the GPU's own positions
+    MpmPipeline().launch_step(data, 20)
+    parts = data.download_particles()
+    orc.set_particles(parts)
+    grid_equal(data.grid_debug(), orc.grid())
+    data.close()
+
+
+@pytest.mark.parametrize("name", ["sand3d", "elastic3d", "fluid2d"])
+def test_p2g_and_grid_update_nodes(cuda_lib, name):
+    sc = small_scenes()[name]
+    rng = np.random.default_rng(7)
+    parts = sc.particles.copy()
+    d = sc.dim
+    parts["velocity"][:, :d] = rng.normal(scale=0.5, size=(len(parts), d)).astype(np.float32)
+    aff = np.zeros((len(parts), 9), np.float32)
+    for r in range(d):
+        for c in range(d):
+            aff[:, c * 3 + r] = rng.normal(scale=2.0, size=len(parts))
+    parts["affine"] = aff
+    sc.particles = parts
+    data, orc = pair(sc)
+    for stage in (1, 2):
+        g = data.debug_nodes(stage)
+        o = orc.nodes(stage)
+        assert g.shape == o.shape
+        scale_m = np.abs(o[:, 3]).max()
+        close(f"{name} stage{stage} mass", g[:, 3], o[:, 3], 1e-6 * scale_m, 2e-6)
+        close(f"{name} stage{stage} momentum/velocity", g[:, :d], o[:, :d], 1e-6, 2e-5)
+    data.close()
+
+
+def compare_particles(tag, g, o, dim, loose=1.0):
+    d = dim
+    assert np.array_equal(g["enabled"], o["enabled"]), f"{tag}: enabled flags differ"
+    close(f"{tag} position", g["position"][:, :d], o["position"][:, :d], 2e-6 * loose, 0)
+    close(f"{tag} velocity", g["velocity"][:, :d], o["velocity"][:, :d], 1e-6 * loose, 1e-4 * loose)
+    idx = [c * 3 + r for c in range(d) for r in range(d)]
+    close(f"{tag} def_grad", g["def_grad"][:, idx], o["def_grad"][:, idx], 2e-6 * loose, 2e-6 * loose)
+    close(f"{tag} affine", g["affine"][:, idx], o["affine"][:, idx], 1e-6 * loose, 2e-3 * loose)
+    close(f"{tag} mass", g["mass"], o["mass"], 0, 0)
+
+
+@pytest.mark.parametrize("name", ["sand3d", "elastic3d", "fluid2d"])
+def test_substep_parity(cuda_lib, name):
+    sc = small_scenes()[name]
+    data, orc = pair(sc)
+    pipe = MpmPipeline()
+    pipe.launch_step(data, 1)
+    orc.step(1)
+    compare_particles(f"{name} 1 step", data.download_particles(), orc.get_particles(), sc.dim)
+    pipe.launch_step(data, 9)
+    orc.step(9)
+    compare_particles(f"{name} 10 steps", data.download_particles(), orc.get_particles(), sc.dim, loose=10.0)
+    data.close()
+
+
+def test_conservation_vs_fp64(cuda_lib):
+    """Mass is exact; P2G momentum equals sum(m v + f dt) of the FP64 oracle."""
+    sc = scenes.elastic_drop_3d(h=1 / 32)
+    rng = np.random.default_rng(9)
+    parts = sc.particles.copy()
+    parts["velocity"] = rng.normal(size=(len(parts), 3)).astype(np.float32)
+    parts["force_dt"] = (1e-3 * rng.normal(size=(len(parts), 3))).astype(np.float32)
+    sc.particles = parts
+    data = scenes.build_mpm_data(sc)
+    o64 = O.from_scene(sc, double=True, threads=8)
+    nodes = data.debug_nodes(1).astype(np.float64)
+    ref = o64.nodes(1).astype(np.float64)
+    m = parts["mass"].astype(np.float64)
+    mom = (parts["velocity"].astype(np.float64) * m[:, None] + parts["force_dt"]).sum(0)
+    rel_m = abs(nodes[:, 3].sum() - m.sum()) / m.sum()
+    rel_p = np.abs(nodes[:, :3].sum(0) - mom).max() / np.abs(mom).max()
+    print(f"P2G mass rel err {rel_m:.2e}, momentum rel err {rel_p:.2e}")
+    assert rel_m < 1e-6 and rel_p < 1e-5
+    assert np.abs(ref[:, :3].sum(0) - mom).max() / np.abs(mom).max() < 1e-9
+    # particle mass is carried exactly through substeps
+    MpmPipeline().launch_step(data, 5)
+    after = data.download_particles()
+    assert np.array_equal(after["mass"], parts["mass"])
+    data.close()
+
+
+def test_rigid_bodies_parity(cuda_lib):
+    sc = scenes.sand_column_3d(h=1 / 32, substeps=5)
+    sc.bodies[1].linvel = (0.3, 0.0, -0.2)
+    sc.bodies[1].angvel = (0.0, 1.5, 0.5)
+    data, orc = pair(sc)
+    MpmPipeline().launch_step(data, 5)
+    orc.step(5)
+    gb, ob = data.get_bodies(), orc.get_bodies()
+    close("body translation", gb["translation"], ob["translation"], 1e-6, 0)
+    close("body rotation", gb["rotation"], ob["rotation"], 1e-6, 0)
+    compare_particles("moving collider", data.download_particles(), orc.get_particles(), 3, loose=5.0)
+    data.close()
+
+
+def test_roundtrip_records(cuda_lib):
+    sc = small_scenes()["sand3d"]
+    data = scenes.build_mpm_data(sc)
+    out = data.download_particles()
+    for k in sc.particles.dtype.names:
+        if k == "vel_grad_det":
+            continue
+        assert np.array_equal(out[k], sc.particles[k]), k
+    data.close()
+
+
+def test_force_damping_fixed(cuda_lib):
+    sc = scenes.elastic_drop_3d(h=1 / 32, substeps=3)
+    parts = sc.particles.copy()
+    parts["force_dt"][::3] = (0.0, 1e-3, 2e-3)
+    parts["damping"][::5] = 2.0
+    parts["fixed"][::7] = 1
+    sc.particles = parts
+    data, orc = pair(sc)
+    MpmPipeline().launch_step(data, 3)
+    orc.step(3)
+    g, o = data.download_particles(), orc.get_particles()
+    compare_particles("force/damping/fixed", g, o, 3, loose=3.0)
+    assert np.all(g["force_dt"] == 0)
+    data.close()
+
+
+def test_divergent_particle_disabled(cuda_lib):
+    """A particle whose F is inverted is disabled (particle_update.slang:145-154)."""
+    sc = scenes.elastic_drop_3d(h=1 / 32, substeps=1)
+    parts = sc.particles.copy()
+    parts["def_grad"][5] = np.array([1, 0, 0, 0, 1, 0, 0, 0, -1], np.float32)
+    sc.particles = parts
+    data, orc = pair(sc)
+    MpmPipeline().launch_step(data, 1)
+    orc.step(1)
+    g, o = data.download_particles(), orc.get_particles()
+    assert g["enabled"][5] == 0 and o["enabled"][5] == 0
+    assert g["mass"][5] == 0
+    compare_particles("divergent", g, o, 3)
+    data.close()
+
+
+def test_overflow_reported_not_faulted(cuda_lib):
+    """More active blocks than the grid capacity: the step reports
+    SLOSH_E_OVERFLOW through slosh_sync and the context stays usable."""
+    sc = scenes.sand_column_3d(h=1 / 32, substeps=1)
+    sc.grid_capacity = 16
+    data = scenes.build_mpm_data(sc)
+    MpmPipeline().launch_step(data, 1)
+    with pytest.raises(SloshError) as ei:
+        data.sync()
+    assert ei.value.code == SLOSH_E_OVERFLOW
+    # the context still answers
+    data.positions()
+    data.close()

@@ -1,0 +1,117 @@
+"""CPU checks of the host side: the C ABI library loads and exports every
+declared symbol, record layouts match the C structs, model constructors and
+scene generators follow the reference's definitions."""
+import math
+import os
+import re
+import subprocess
+import textwrap
+
+import numpy as np
+import pytest
+
+from slosh_b200 import _lib, scenes
+from slosh_b200.pipeline import ParticleModel, lame_lambda_mu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "slosh_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|uint32_t)\s+\*?\s*(slosh_\w+)\s*\(", src, re.M)))
+
+
+@pytest.fixture(scope="module")
+def built_lib():
+    from slosh_b200.build import build_library
+
+    return build_library()
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    names = declared_functions()
+    assert len(names) >= 15
+    out = subprocess.run(["nm", "-D", "--defined-only", built_lib], capture_output=True, text=True, check=True).stdout
+    exported = set(line.split()[-1] for line in out.splitlines() if line.strip())
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    # and the ctypes binding covers exactly those symbols
+    assert sorted(_lib.SIGNATURES) == names
+
+
+def test_library_loads_without_gpu(built_lib):
+    lib = _lib.load()
+    for name in declared_functions():
+        assert getattr(lib, name) is not None
+
+
+def test_record_layouts_match_c_structs(tmp_path):
+    prog = textwrap.dedent(
+        """
+        #include <stdio.h>
+        #include <stddef.h>
+        #include "slosh_b200.h"
+        int main(void) {
+          printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(slosh_particle), offsetof(slosh_particle, model),
+                 offsetof(slosh_particle, enabled), sizeof(slosh_body), offsetof(slosh_body, bc_type),
+                 sizeof(slosh_model));
+          printf("%zu %zu\\n", sizeof(slosh_grid_dump), offsetof(slosh_grid_dump, neighbors));
+          return 0;
+        }
+        """
+    )
+    c = tmp_path / "layout.c"
+    c.write_text(prog)
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)], check=True)
+    vals = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()))
+    P, B = _lib.PARTICLE_DTYPE, _lib.BODY_DTYPE
+    assert vals[0] == P.itemsize
+    assert vals[1] == P.fields["model_tag"][1]
+    assert vals[2] == P.fields["enabled"][1]
+    assert vals[3] == B.itemsize
+    assert vals[4] == B.fields["bc_type"][1]
+    assert vals[5] == 52
+    import ctypes
+
+    assert vals[6] == ctypes.sizeof(_lib.SloshGridDump)
+    assert vals[7] == _lib.SloshGridDump.neighbors.offset
+
+
+def test_lame_parameters():
+    """Config values quoted for the configs (src/models/mod.rs:17-27)."""
+    lam, mu = lame_lambda_mu(3.5e5, 0.3)
+    assert round(lam) == 201923 and round(mu) == 134615
+    lam, mu = lame_lambda_mu(1e5, 0.3)
+    assert round(lam) == 57692 and round(mu) == 38462
+
+
+def test_sand_model_record():
+    m = ParticleModel.sand(3.5e5, 0.3, friction_angle_deg=30.0)
+    assert m.tag == _lib.MODEL_SAND_LINEAR and len(m.data) == 12
+    assert m.data[:3] == (1.0, 1.0, 0.0)  # DruckerPragerPlasticState::default
+    assert math.isclose(m.data[3], math.radians(30.0))
+    assert math.isclose(m.data[4], math.radians(9.0)) and m.data[5] == 0.2
+    assert math.isclose(m.data[6], math.radians(10.0))
+
+
+def test_scene_sizes():
+    d = scenes.dam_break_2d()
+    assert d.n == 204 * 307
+    e = scenes.elastic_drop_3d(h=1 / 64)
+    assert e.n == 2 * 32**3
+    # full-size sand column: count lattice points inside the cylinder only
+    h = 1 / 256
+    sp = h / 2
+    n_axis = int(math.floor(0.3 / sp + 1e-9))
+    c = 0.5 - 0.15 + (np.arange(n_axis) + 0.5) * sp
+    inside = ((c[:, None] - 0.5) ** 2 + (c[None, :] - 0.5) ** 2 <= 0.15**2).sum()
+    n_full = int(inside) * int(math.floor(0.5 / sp + 1e-9))
+    assert 4.6e6 < n_full < 4.8e6
+
+
+def test_scene_determinism():
+    a = scenes.sand_column_3d(h=1 / 32).particles
+    b = scenes.sand_column_3d(h=1 / 32).particles
+    assert np.array_equal(a, b)
