@@ -60,6 +60,7 @@ def load() -> ctypes.CDLL:
             "orc_grid_get": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
             "orc_nodes_get": (ctypes.c_int, [_P, _P]),
             "orc_totals": (None, [_P, _P]),
+            "orc_node_totals": (None, [_P, _P]),
             "orc_prefix_sum": (None, [_P, ctypes.c_uint32]),
             "orc_svd": (None, [ctypes.c_uint32, _P, _P, _P, _P]),
             "orc_model_stress": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
@@ -183,6 +184,13 @@ class Oracle:
         nb = self.lib.orc_num_blocks(self.ctx)
         out = np.zeros((nb * 64, 4), np.float32)
         self.lib.orc_nodes_get(self.ctx, _p(out))
+        return out
+
+    def node_totals(self, stage: int) -> np.ndarray:
+        """Sums (momentum xyz, mass) over the nodes after `stage`, in double."""
+        self.stages(stage)
+        out = np.zeros(4)
+        self.lib.orc_node_totals(self.ctx, _p(out))
         return out
 
     def totals(self) -> np.ndarray:

@@ -22,10 +22,12 @@
 //
 // Canonical order.  The reference numbers active blocks with an atomic
 // counter and fills each sort bucket with atomics, so its order is not
-// deterministic.  The oracle fixes it: blocks in ascending packed key, and
-// inside a block the entries ordered by (bucket, particle id), primaries
-// (buckets 0..NPB-1) before extras.  Every per-block quantity of the
-// reference (counts per bucket, first_particle, sorted ids) is then a
+// deterministic.  The oracle fixes it: blocks in ascending packed key;
+// inside a block the primaries (buckets 0..NPB-1) first, ordered by (cell,
+// particle id) with the cell index x + BW y (+ BW^2 z) -- slab-major, so each
+// slab bucket remains one contiguous range as the reference requires -- then
+// the extras ordered by (bucket, particle id).  Every per-block quantity of
+// the reference (counts per bucket, first_particle, sorted ids) is then a
 // deterministic function of the positions.
 //
 // Rounding conventions: `round` is round-half-to-even (WGSL round, the
@@ -730,13 +732,38 @@ template <typename T, int D> struct Ctx {
             g.npe[r] = run - running;
             running = run;
         }
-        // finalize_particles_sort, in particle-id order (canonical).
+        // finalize_particles_sort in canonical order: primaries by (cell, id),
+        // the cell index being x + BW y (+ BW^2 z), i.e. slab-major so that
+        // every primary slab bucket stays one contiguous range; extras by
+        // (bucket, id).
+        constexpr int NCELL = 64;
+        std::vector<uint32_t> cellcnt(nb * NCELL, 0), cellcur(nb * NCELL);
+        auto cell_index = [](const int *a) {
+            int c = 0, mul = 1;
+            for (int k = 0; k < D; ++k) {
+                c += a[k] * mul;
+                mul *= Geo<D>::BW;
+            }
+            return c;
+        };
+        for (size_t i = 0; i < n; ++i) {
+            int a[D];
+            for (int k = 0; k < D; ++k) a[k] = plocal[i * D + k];
+            cellcnt[prank[i] * NCELL + cell_index(a)] += 1;
+        }
+        for (size_t r = 0; r < nb; ++r) {
+            uint32_t run = g.first[r];
+            for (int c = 0; c < NCELL; ++c) {
+                cellcur[r * NCELL + c] = run;
+                run += cellcnt[r * NCELL + c];
+            }
+        }
         g.sorted.assign(running, 0);
         for (size_t i = 0; i < n; ++i) {
             uint32_t r0 = prank[i];
             int a[D];
             for (int k = 0; k < D; ++k) a[k] = plocal[i * D + k];
-            g.sorted[cursor[r0 * NB + primary_bucket(a)]++] = (uint32_t)i;
+            g.sorted[cellcur[r0 * NCELL + cell_index(a)]++] = (uint32_t)i;
             for (int s = 1; s < Geo<D>::NASSOC; ++s) {
                 const int *sh = assoc_shift<D>(s);
                 if (extra_spills(a, sh)) {
@@ -1242,6 +1269,7 @@ struct AnyCtx {
     virtual int grid_get(uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t *) = 0;
     virtual int nodes_get(float *out) = 0;
     virtual void totals(double *out) = 0;
+    virtual void node_totals(double *out) = 0;
 };
 
 template <typename T, int D> struct CtxImpl : AnyCtx {
@@ -1301,9 +1329,23 @@ template <typename T, int D> struct CtxImpl : AnyCtx {
         if (sorted) std::memcpy(sorted, scratch.sorted.data(), scratch.sorted.size() * 4);
         return SLOSH_OK;
     }
+    // Nodes as 4 floats: (momentum or velocity with z = 0 in 2D, mass).
     int nodes_get(float *out) override {
-        for (size_t i = 0; i < scratch.nodes.size(); ++i) out[i] = (float)scratch.nodes[i];
+        const size_t nn = scratch.nodes.size() / 4;
+        for (size_t i = 0; i < nn; ++i) {
+            for (int k = 0; k < 3; ++k) out[i * 4 + k] = (k < D) ? (float)scratch.nodes[i * 4 + k] : 0.f;
+            out[i * 4 + 3] = (float)scratch.nodes[i * 4 + D];
+        }
         return SLOSH_OK;
+    }
+    // Sums of node mass and momentum in double (conservation checks).
+    void node_totals(double *out) override {
+        for (int k = 0; k < 4; ++k) out[k] = 0;
+        const size_t nn = scratch.nodes.size() / 4;
+        for (size_t i = 0; i < nn; ++i) {
+            for (int k = 0; k < D; ++k) out[k] += (double)scratch.nodes[i * 4 + k];
+            out[3] += (double)scratch.nodes[i * 4 + D];
+        }
     }
     // Totals in double: mass, momentum (D), for conservation checks.
     void totals(double *out) override {
@@ -1366,6 +1408,7 @@ int orc_grid_get(void *c, uint32_t *keys, uint32_t *first, uint32_t *np, uint32_
 }
 int orc_nodes_get(void *c, float *out) { return ((orc::AnyCtx *)c)->nodes_get(out); }
 void orc_totals(void *c, double *out) { ((orc::AnyCtx *)c)->totals(out); }
+void orc_node_totals(void *c, double *out) { ((orc::AnyCtx *)c)->node_totals(out); }
 
 // WgPrefixSum::eval_cpu (src/grid/prefix_sum.rs:97-110): inclusive running
 // sum, then shift right by one with a leading 0.

@@ -5,24 +5,28 @@
 // launches (shaders/slosh/grid/grid.slang, shaders/slosh/grid/sort.slang,
 // shaders/slosh/grid/prefix_sum.slang).  Differences in design:
 //  - one pass per particle both activates its primary block and counts it in
-//    its slab bucket, warp-aggregated (__match_any_sync) so that a warp of
-//    particles sharing a block issues one hash insert and one atomic per
-//    (block, bucket) instead of one per particle;
+//    its cell, warp-aggregated (__match_any_sync) so that a warp of particles
+//    sharing a block issues one hash insert and one atomic per (block, cell);
 //  - the hash map stores 4-byte keys and 4-byte values in separate arrays
 //    (slosh stores 48-byte entries) with twice the block capacity in slots;
 //  - blocks are numbered canonically by ascending packed key (slosh numbers
 //    them with an atomic counter), which makes every block index, offset and
 //    the sorted permutation a deterministic function of the positions;
-//  - the particle permutation covers primaries only: P2G scatters from each
-//    particle to its full 27-node stencil, so the "extra" entries slosh keeps
-//    for its node-centric P2G are not needed on the hot path.  The debug
-//    entry point rebuilds slosh's complete layout (primaries + extras) from
-//    the same data for the bit-exactness checks.
+//  - particles are counted per cell of their primary block (64 cells) rather
+//    than per slab: the canonical primary order is (cell, particle id) with
+//    the cell index slab-major (x + BW y + BW^2 z), so slosh's slab buckets
+//    are still contiguous ranges, and P2G/G2P get per-cell particle ranges;
+//  - the permutation covers primaries only: P2G scatters from each particle
+//    to its full stencil, so the "extra" entries slosh keeps for its
+//    node-centric P2G are not needed on the hot path.  The debug entry point
+//    rebuilds slosh's complete layout (primaries + extras) from the same data.
 #pragma once
 
 #include "scene.cuh"
 
 namespace slosh {
+
+constexpr uint32_t CELLS = 64;  // cells (and nodes) per block in 2D and 3D
 
 // Linear-probing insert bounded by the slot count (slosh's insertion_index,
 // grid.slang:118-174, probes the same way).  Sets ERR_HASH_OVERFLOW and
@@ -58,16 +62,25 @@ __device__ __forceinline__ uint32_t hash_find(const uint32_t *keys, uint32_t hca
     return NONE;
 }
 
-// Clears the current hash map, the per-slot counts, the key histogram and
-// the counters.  Replaces reset_hmap (grid.slang:200-218).
-template <int D> __global__ void k_clear(DevScene s) {
+// Cell index of a local cell inside its block: x + BW y (+ BW^2 z).
+template <int D> __device__ __forceinline__ uint32_t cell_index(const int *a) {
+    if constexpr (D == 3) return (uint32_t)(a[0] + 4 * a[1] + 16 * a[2]);
+    else return (uint32_t)(a[0] + 8 * a[1]);
+}
+
+// Clears the current hash map, the key histogram and the counters.  Replaces
+// reset_hmap (grid.slang:200-218).  The per-slot cell counts are cleared by
+// k_block_setup after they are read; after a substep that raised an error
+// (blocks left without a rank keep their counts) they are all cleared here.
+__global__ void k_clear(DevScene s) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = tid; i < s.hcap; i += stride) {
         s.hkeys[i] = NONE;
         s.hvals[i] = NONE;
     }
-    for (uint32_t i = tid; i < s.hcap * Geo<D>::NPB; i += stride) s.slot_counts[i] = 0u;
+    if (*s.err != 0u)
+        for (size_t i = tid; i < (size_t)s.hcap * CELLS; i += stride) s.slot_counts[i] = 0u;
     for (uint32_t i = tid; i < HIST_BINS; i += stride) {
         s.hist[i] = 0u;
         s.hist_fill[i] = 0u;
@@ -79,8 +92,8 @@ template <int D> __global__ void k_clear(DevScene s) {
     }
 }
 
-// Per particle: activate the primary block and count the particle in its slab
-// bucket.  Replaces touch_primary_blocks (sort.slang:50-67) and the primary
+// Per particle: activate the primary block and count the particle in its
+// cell.  Replaces touch_primary_blocks (sort.slang:50-67) and the primary
 // half of update_block_particle_count (sort.slang:208-246).
 template <int D> __global__ void k_touch(DevScene s) {
     const uint32_t lane = lane_id();
@@ -94,7 +107,7 @@ template <int D> __global__ void k_touch(DevScene s) {
         const float x[3] = {p.x, p.y, p.z};
         const CellLoc<D> c = locate<D>(x, s.h);
         const uint32_t key = pack_key<D>(c.block);
-        const uint32_t bucket = (uint32_t)c.local[D - 1];
+        const uint32_t cell = cell_index<D>(c.local);
         const unsigned peers = __match_any_sync(mask, key);
         const int leader = __ffs(peers) - 1;
         uint32_t slot = NONE;
@@ -113,7 +126,7 @@ template <int D> __global__ void k_touch(DevScene s) {
             }
         }
         slot = __shfl_sync(mask, slot, leader);
-        const uint32_t bin = (slot == NONE) ? NONE : slot * Geo<D>::NPB + bucket;
+        const uint32_t bin = (slot == NONE) ? NONE : (slot << 6) | cell;
         const unsigned peers2 = __match_any_sync(mask, bin);
         if (bin != NONE && (int)lane == __ffs(peers2) - 1) atomicAdd(&s.slot_counts[bin], (uint32_t)__popc(peers2));
         s.pslot[i] = bin;
@@ -182,19 +195,40 @@ template <int NT> __device__ __forceinline__ uint32_t block_exclusive_scan(uint3
     return res;
 }
 
+// Exclusive scan of n u32 by one CTA of NT threads: tiles of NT * PER values
+// staged in shared memory with coalesced loads, each thread scanning PER
+// consecutive values; `carry` holds the running total.  Returns the total.
+template <int NT, int PER>
+__device__ __forceinline__ uint32_t cta_exclusive_scan(const uint32_t *in, uint32_t *out, uint32_t n) {
+    __shared__ uint32_t tile[NT * PER];
+    __shared__ uint32_t tot;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < n; base += NT * PER) {
+        for (uint32_t k = threadIdx.x; k < NT * PER; k += NT) tile[k] = (base + k < n) ? in[base + k] : 0u;
+        __syncthreads();
+        uint32_t local = 0;
+        const uint32_t t0 = threadIdx.x * PER;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) local += tile[t0 + k];
+        uint32_t run = carry + block_exclusive_scan<NT>(local, &tot);
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t v = tile[t0 + k];
+            tile[t0 + k] = run;
+            run += v;
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < NT * PER; k += NT)
+            if (base + k < n) out[base + k] = tile[k];
+        carry += tot;
+        __syncthreads();
+    }
+    return carry;
+}
+
 // Exclusive scan of the key histogram (one CTA) and the final block count.
 template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) {
-    __shared__ uint32_t total_sh;
-    constexpr uint32_t PER = HIST_BINS / NT;
-    uint32_t local = 0;
-    const uint32_t b0 = threadIdx.x * PER;
-    for (uint32_t k = 0; k < PER; ++k) local += s.hist[b0 + k];
-    const uint32_t off = block_exclusive_scan<NT>(local, &total_sh);
-    uint32_t run = off;
-    for (uint32_t k = 0; k < PER; ++k) {
-        s.hist_start[b0 + k] = run;
-        run += s.hist[b0 + k];
-    }
+    cta_exclusive_scan<NT, 8>(s.hist, s.hist_start, HIST_BINS);
     if (threadIdx.x == 0) {
         const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
         if (total > s.cap) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
@@ -236,58 +270,57 @@ __global__ void k_rank(DevScene s) {
     }
 }
 
-// Per block: neighbour ranks (update_nbh_block_ids, sort.slang:100-117) and
-// zeroed nodes (reset, grid.slang:455-485).  Four blocks per 256 threads.
+// One warp per block: per-cell counts (cleared in the hash-slot array once
+// read) with their in-block exclusive scan, the block total, the neighbour
+// ranks (update_nbh_block_ids, sort.slang:100-117) and zeroed nodes (reset,
+// grid.slang:455-485).
 template <int D> __global__ void k_block_setup(DevScene s) {
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t nb = s.ctr->n_blocks;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * 64u; t += stride) {
-        const uint32_t r = t >> 6, node = t & 63u;
-        s.nodes[t] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (node < (uint32_t)NN) {
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
+        const uint32_t sl = s.bslot[r];
+        uint32_t *cnt = s.slot_counts + ((size_t)sl << 6);
+        const uint32_t c0 = cnt[2 * lane], c1 = cnt[2 * lane + 1];
+        cnt[2 * lane] = 0u;
+        cnt[2 * lane + 1] = 0u;
+        const uint32_t pair = c0 + c1;
+        uint32_t incl = pair;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
+            if (lane >= (uint32_t)off) incl += y;
+        }
+        const uint32_t ex = incl - pair;
+        s.bcell[(size_t)r * CELLS + 2 * lane] = ex;
+        s.bcell[(size_t)r * CELLS + 2 * lane + 1] = ex + c0;
+        s.bcur[(size_t)r * CELLS + 2 * lane] = ex;
+        s.bcur[(size_t)r * CELLS + 2 * lane + 1] = ex + c0;
+        if (lane == 31) s.bnp[r] = incl;
+        s.nodes[(size_t)r * 64 + 2 * lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s.nodes[(size_t)r * 64 + 2 * lane + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (lane < (uint32_t)NN) {
             int b[D], o[D];
             unpack_key<D>(s.bkey[r], b);
-            assoc_offset<D>((int)node + 1, o);
+            assoc_offset<D>((int)lane + 1, o);
             for (int k = 0; k < D; ++k) b[k] += o[k];
             const uint32_t slot = hash_find(s.hkeys, s.hcap, pack_key<D>(b));
-            s.bnbh[r * NN + node] = (slot == NONE) ? NONE : s.hvals[slot];
+            s.bnbh[r * NN + lane] = (slot == NONE) ? NONE : s.hvals[slot];
         }
     }
 }
 
-// Exclusive scan of per-block primary totals into first_particle and the
-// per-bucket insertion cursors (copy_particles_len_to_scan_value,
-// prefix_sum, copy_scan_values_to_first_particles_and_prepare_for_finalize:
-// sort.slang:248-302, prefix_sum.slang).  One CTA.
-template <int D, int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) {
-    constexpr int NPB = Geo<D>::NPB;
-    __shared__ uint32_t total_sh;
-    const uint32_t nb = s.ctr->n_blocks;
-    const uint32_t per = (nb + NT - 1) / NT;
-    const uint32_t r0 = threadIdx.x * per, r1 = min(r0 + per, nb);
-    uint32_t local = 0;
-    for (uint32_t r = r0; r < r1; ++r) {
-        const uint32_t sl = s.bslot[r];
-        for (int b = 0; b < NPB; ++b) local += s.slot_counts[sl * NPB + b];
-    }
-    uint32_t run = block_exclusive_scan<NT>(local, &total_sh);
-    for (uint32_t r = r0; r < r1; ++r) {
-        const uint32_t sl = s.bslot[r];
-        s.bfirst[r] = run;
-        uint32_t tot = 0;
-        for (int b = 0; b < NPB; ++b) {
-            s.bcur[r * NPB + b] = run + tot;
-            tot += s.slot_counts[sl * NPB + b];
-        }
-        s.bnp[r] = tot;
-        run += tot;
-    }
+// Exclusive scan of the per-block primary totals into first_particle
+// (copy_particles_len_to_scan_value + prefix_sum +
+// copy_scan_values_to_first_particles, sort.slang:248-302).  One CTA.
+template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) {
+    cta_exclusive_scan<NT, 8>(s.bnp, s.bfirst, s.ctr->n_blocks);
 }
 
-// Per particle: claim its slot in the block's bucket (finalize_particles_sort,
-// sort.slang:304-357, primaries only), warp-aggregated.
-template <int D> __global__ void k_scatter(DevScene s) {
+// Per particle: claim its slot in the block's cell range (the primary part
+// of finalize_particles_sort, sort.slang:304-357), warp-aggregated.
+__global__ void k_scatter(DevScene s) {
     const uint32_t lane = lane_id();
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < s.n; base += stride) {
@@ -300,50 +333,48 @@ template <int D> __global__ void k_scatter(DevScene s) {
         const int leader = __ffs(peers) - 1;
         uint32_t pos = NONE;
         if ((int)lane == leader && bin != NONE) {
-            const uint32_t r = s.hvals[bin / Geo<D>::NPB];
-            if (r != NONE) pos = atomicAdd(&s.bcur[r * Geo<D>::NPB + bin % Geo<D>::NPB], (uint32_t)__popc(peers));
+            const uint32_t r = s.hvals[bin >> 6];
+            if (r != NONE)
+                pos = s.bfirst[r] + atomicAdd(&s.bcur[(size_t)r * CELLS + (bin & 63u)], (uint32_t)__popc(peers));
         }
         pos = __shfl_sync(mask, pos, leader);
         if (pos != NONE) s.perm_tmp[pos + __popc(peers & lanemask_lt())] = i;
     }
 }
 
-// Orders each (block, bucket) range of the permutation by particle id: the
-// canonical order.  Each element's position is its rank among the ids of its
-// bucket (ids are unique).  Ranges up to CANON_SMEM ids are staged in shared
-// memory; larger ones are ranked from global memory.
+// Orders each (block, cell) range of the permutation by particle id: the
+// canonical order.  The scatter already groups a block's particles by cell;
+// each element's final place is its rank among the ids of its cell (a few
+// particles per cell), found from shared memory.
 constexpr uint32_t CANON_SMEM = 4096;
-template <int D, int NT> __global__ void __launch_bounds__(NT) k_canon(DevScene s) {
-    constexpr int NPB = Geo<D>::NPB;
+template <int NT> __global__ void __launch_bounds__(NT) k_canon(DevScene s) {
     __shared__ uint32_t ids[CANON_SMEM];
-    __shared__ uint32_t bstart[NPB + 1];
+    __shared__ uint32_t cstart[CELLS + 1];
     const uint32_t nb = s.ctr->n_blocks;
     for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
-        if (threadIdx.x == 0) {
-            const uint32_t sl = s.bslot[r];
-            uint32_t run = 0;
-            for (int b = 0; b < NPB; ++b) {
-                bstart[b] = run;
-                run += s.slot_counts[sl * NPB + b];
-            }
-            bstart[NPB] = run;
-        }
+        for (uint32_t c = threadIdx.x; c < CELLS; c += NT) cstart[c] = s.bcell[(size_t)r * CELLS + c];
+        if (threadIdx.x == 0) cstart[CELLS] = np;
         const bool in_smem = np <= CANON_SMEM;
         if (in_smem)
             for (uint32_t e = threadIdx.x; e < np; e += NT) ids[e] = s.perm_tmp[first + e];
         __syncthreads();
         const uint32_t *src = in_smem ? ids : s.perm_tmp + first;
         for (uint32_t e = threadIdx.x; e < np; e += NT) {
-            int b = 0;
-            while (b + 1 < NPB && e >= bstart[b + 1]) ++b;
-            const uint32_t lo = bstart[b], hi = bstart[b + 1];
+            // cell of entry e: last c with cstart[c] <= e (binary search)
+            uint32_t lo = 0, hi = CELLS;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (cstart[mid] <= e) lo = mid;
+                else hi = mid;
+            }
+            const uint32_t b0 = cstart[lo], b1 = cstart[lo + 1];
             const uint32_t id = src[e];
             uint32_t rank = 0;
-            for (uint32_t j = lo; j < hi; ++j) rank += (src[j] < id) ? 1u : 0u;
-            s.perm[first + lo + rank] = id;
+            for (uint32_t j = b0; j < b1; ++j) rank += (src[j] < id) ? 1u : 0u;
+            s.perm[first + b0 + rank] = id;
         }
         __syncthreads();
     }

@@ -285,7 +285,19 @@ template <int D> __global__ void k_dbg_scatter(DevScene s, DebugBuffers d) {
     }
 }
 
-// One thread per entry: rank by id inside its (block, bucket) segment.
+// Canonical order of one entry of bucket b: primaries by (cell, id), extras
+// by id.
+template <int D>
+__device__ __forceinline__ uint64_t dbg_order_key(const DevScene &s, uint32_t id, uint32_t b) {
+    if (b >= (uint32_t)Geo<D>::NPB) return id;
+    const float4 p = s.pm[id];
+    const float x[3] = {p.x, p.y, p.z};
+    const CellLoc<D> c = locate<D>(x, s.h);
+    return ((uint64_t)cell_index<D>(c.local) << 32) | id;
+}
+
+// One thread per (block, bucket) segment: rank each entry by its canonical
+// order key inside the segment.
 template <int D> __global__ void k_dbg_canon(DevScene s, DebugBuffers d) {
     constexpr int NB = Geo<D>::NB;
     const uint32_t nb = s.ctr->n_blocks;
@@ -298,8 +310,9 @@ template <int D> __global__ void k_dbg_canon(DevScene s, DebugBuffers d) {
         if (hi > d.cap_entries) continue;
         for (uint32_t e = lo; e < hi; ++e) {
             const uint32_t id = d.sorted[e];
+            const uint64_t key = dbg_order_key<D>(s, id, b);
             uint32_t rank = 0;
-            for (uint32_t j = lo; j < hi; ++j) rank += (d.sorted[j] < id) ? 1u : 0u;
+            for (uint32_t j = lo; j < hi; ++j) rank += (dbg_order_key<D>(s, d.sorted[j], b) < key) ? 1u : 0u;
             d.sorted2[lo + rank] = id;
         }
     }

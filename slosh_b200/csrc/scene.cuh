@@ -32,7 +32,7 @@ struct DevScene {
     uint32_t *hvals;       // current substep hash map: canonical block rank
     const uint32_t *prev_hkeys;
     const uint32_t *prev_hvals;
-    uint32_t *slot_counts; // hcap * NPB primary-bucket counts per hash slot
+    uint32_t *slot_counts; // hcap * 64 per-cell particle counts per hash slot
     uint32_t *blist_key;   // primary blocks in append order [cap]
     uint32_t *blist_slot;
     uint32_t *blist2_key;  // neighbour-only blocks in append order [cap]
@@ -46,9 +46,10 @@ struct DevScene {
     uint32_t *bslot;       // hash slot of the block
     uint32_t *bfirst;      // first primary entry in perm
     uint32_t *bnp;         // number of primary particles
-    uint32_t *bcur;        // NPB insertion cursors per block
+    uint32_t *bcell;       // 64 per block: first entry of each cell, relative to bfirst
+    uint32_t *bcur;        // 64 per block: insertion cursors, relative to bfirst
     uint32_t *bnbh;        // (NASSOC - 1) neighbour ranks per block, NONE if inactive
-    uint32_t *pslot;       // per particle: slot * NPB + bucket
+    uint32_t *pslot;       // per particle: (hash slot << 6) | cell
     uint32_t *perm_tmp;    // scatter output
     uint32_t *perm;        // canonical primary order
     float4 *nodes;         // 64 nodes per block: (momentum | velocity, mass)

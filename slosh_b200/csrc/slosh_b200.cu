@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -40,7 +41,8 @@ struct slosh_ctx {
     uint32_t *slot_counts = nullptr, *blist_key = nullptr, *blist_slot = nullptr, *blist2_key = nullptr,
              *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_fill = nullptr, *tmp_key = nullptr,
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
-             *bcur = nullptr, *bnbh = nullptr;
+             *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr;
+    bool p2g_atomic = false;  // SLOSH_P2G=atomic selects the shared-atomic P2G variant
     uint32_t *pslot = nullptr, *perm_tmp = nullptr, *perm = nullptr;
     float4 *nodes = nullptr, *coll[2] = {nullptr, nullptr};
     uint32_t *coll_id[2] = {nullptr, nullptr};
@@ -100,7 +102,6 @@ uint32_t next_pow2(uint32_t v) {
     return p;
 }
 
-int npb(int dim) { return dim == 3 ? Geo<3>::NPB : Geo<2>::NPB; }
 int nnb(int dim) { return dim == 3 ? Geo<3>::NASSOC - 1 : Geo<2>::NASSOC - 1; }
 int nbk(int dim) { return dim == 3 ? Geo<3>::NB : Geo<2>::NB; }
 
@@ -143,6 +144,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.bslot = c->bslot;
     s.bfirst = c->bfirst;
     s.bnp = c->bnp;
+    s.bcell = c->bcell;
     s.bcur = c->bcur;
     s.bnbh = c->bnbh;
     s.pslot = c->pslot;
@@ -194,7 +196,7 @@ struct Prof {
 template <int D> void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
     const uint32_t sm = (uint32_t)c->sm_count;
     PROF_BEGIN(0);
-    k_clear<D><<<sm * 4, 256, 0, st>>>(s);
+    k_clear<<<sm * 4, 256, 0, st>>>(s);
     PROF_END(0);
     PROF_BEGIN(1);
     k_touch<D><<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
@@ -212,22 +214,25 @@ template <int D> void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaSt
     k_rank<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(5);
     PROF_BEGIN(6);
-    k_block_setup<D><<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
+    k_block_setup<D><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(6);
     PROF_BEGIN(7);
-    k_block_scan<D, 1024><<<1, 1024, 0, st>>>(s);
+    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     PROF_END(7);
     PROF_BEGIN(8);
-    k_scatter<D><<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
+    k_scatter<<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(8);
     PROF_BEGIN(9);
-    k_canon<D, 256><<<std::min<uint32_t>(c->cap, sm * 8), 256, 0, st>>>(s);
+    k_canon<128><<<std::min<uint32_t>(c->cap, sm * 8), 128, 0, st>>>(s);
     PROF_END(9);
 }
 
 template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
     PROF_BEGIN(10);
-    k_p2g<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
+    if (c->p2g_atomic)
+        k_p2g_atomic<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
+    else
+        k_p2g<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), 128, 0, st>>>(s);
     PROF_END(10);
 }
 
@@ -352,14 +357,15 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->materials, MAX_MATERIALS)) || (st = dalloc(c, &c->mat_hkeys, MAT_HASH)) ||
         (st = dalloc(c, &c->mat_dense, MAT_HASH)) || (st = dalloc(c, &c->hkeys[0], hcap)) ||
         (st = dalloc(c, &c->hkeys[1], hcap)) || (st = dalloc(c, &c->hvals[0], hcap)) ||
-        (st = dalloc(c, &c->hvals[1], hcap)) || (st = dalloc(c, &c->slot_counts, (size_t)hcap * npb(D))) ||
+        (st = dalloc(c, &c->hvals[1], hcap)) || (st = dalloc(c, &c->slot_counts, (size_t)hcap * CELLS)) ||
         (st = dalloc(c, &c->blist_key, cap)) || (st = dalloc(c, &c->blist_slot, cap)) ||
         (st = dalloc(c, &c->blist2_key, cap)) || (st = dalloc(c, &c->blist2_slot, cap)) ||
         (st = dalloc(c, &c->hist, HIST_BINS)) || (st = dalloc(c, &c->hist_start, HIST_BINS)) ||
         (st = dalloc(c, &c->hist_fill, HIST_BINS)) || (st = dalloc(c, &c->tmp_key, 2 * (size_t)cap)) ||
         (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) || (st = dalloc(c, &c->bkey, cap)) ||
         (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
-        (st = dalloc(c, &c->bcur, (size_t)cap * npb(D))) || (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) ||
+        (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
+        (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm_tmp, N)) || (st = dalloc(c, &c->perm, N)) ||
         (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
@@ -374,6 +380,9 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     cudaMemset(c->ctr, 0, sizeof(Counters));
     cudaMemset(c->err, 0, 4);
     cudaMemset(c->damping, 0, N * 4);
+    cudaMemset(c->slot_counts, 0, (size_t)hcap * CELLS * 4);
+    const char *variant = std::getenv("SLOSH_P2G");
+    c->p2g_atomic = variant && std::strcmp(variant, "atomic") == 0;
     if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     c->params.gravity[1] = -9.81f;
     c->params.dt = 1.0f / 60.0f;
@@ -414,6 +423,7 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
         CK(cudaMemsetAsync(c->hkeys[k], 0xff, c->hcap * 4, st));
         CK(cudaMemsetAsync(c->hvals[k], 0xff, c->hcap * 4, st));
     }
+    CK(cudaMemsetAsync(c->slot_counts, 0, (size_t)c->hcap * CELLS * 4, st));
     c->parity = 0;
     if (n > 0) {
         DevScene s = make_scene(c, 0, false);

@@ -38,14 +38,12 @@ __device__ __forceinline__ bool tile_node_owner(const DevScene &s, uint32_t r, i
     return rank != NONE;
 }
 
-// Particle-to-grid.  One CTA per active block with primaries; each thread
-// scatters whole particles into a shared (block + 2)^D tile of node
-// momentum/mass (shared-memory atomics), then the tile is added to the global
-// nodes of the block and its +1 neighbours with 16-byte vector atomics.
-// Node momentum/mass match slosh's p2g_scatter_style
-// (shaders/slosh/solver/p2g_scatter_style.slang:84-154):
-//   acc_i = sum_p w_ip [ C_p (x_i - x_p) + m_p v_p + f_p dt ,  m_p ].
-template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g(DevScene s) {
+// Particle-to-grid, shared-memory-atomic variant (kept for comparison).  One
+// CTA per active block with primaries; each thread scatters whole particles
+// into a shared (block + 2)^D tile of node momentum/mass with shared-memory
+// float atomics, then the tile is added to the global nodes of the block and
+// its +1 neighbours with 16-byte vector atomics.
+template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g_atomic(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float tile[4][TILE];
     const uint32_t nb = s.ctr->n_blocks;
@@ -144,6 +142,215 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g(DevScene s)
             uint32_t rank, local;
             if (!tile_node_owner<D>(s, r, t, rank, local)) continue;
             atomicAdd(&s.nodes[(size_t)rank * 64u + local], val);
+        }
+        __syncthreads();
+    }
+}
+
+// Particle-to-grid without atomics inside the block.
+//
+// Node momentum/mass match slosh's p2g_scatter_style
+// (shaders/slosh/solver/p2g_scatter_style.slang:84-154):
+//   acc_i = sum_p w_ip [ C_p (x_i - x_p) + m_p v_p + f_p dt ,  m_p ],
+// with w_ip the product of the quadratic B-spline weights per axis.
+//
+// One CTA per active block with primaries.  The block's particles arrive in
+// canonical (cell, id) order, so every cell is a contiguous range:
+//  1. stage: each thread loads a particle, computes its three weights per
+//     axis, its momentum at the base node (q + C d0) and h C, and stores
+//     them in shared memory (six float4 per particle in 3D);
+//  2. accumulate: a warp takes a cell; its lanes are the stencil offsets s
+//     (27 in 3D; in 2D 9 offsets x 3 particles at a time) and read each
+//     particle of the cell by broadcast, accumulating w_s (mom_s, m) in
+//     registers; the sums land in a shared (cell, offset) array with plain
+//     stores (one owner per entry);
+//  3. reduce: each tile node sums its (cell, offset) entries in a fixed
+//     order, and the (block + 2)^D tile is added to the global nodes of the
+//     block and its +1 neighbours with 16-byte vector atomics.
+template <int D> struct P2GLayout;
+template <> struct P2GLayout<3> {
+    // stencil offsets, particles per step, float4 per staged particle, chunk
+    static constexpr int NOFF = 27, PP = 1, F4 = 6, CH = 128;
+};
+template <> struct P2GLayout<2> {
+    static constexpr int NOFF = 9, PP = 3, F4 = 4, CH = 256;
+};
+
+template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g(DevScene s) {
+    constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
+    constexpr int NOFF = P2GLayout<D>::NOFF, PP = P2GLayout<D>::PP, F4 = P2GLayout<D>::F4;
+    constexpr int CH = P2GLayout<D>::CH;  // particles staged per chunk
+    constexpr int NW = NT / 32;
+    __shared__ float4 pd[CH * F4];
+    __shared__ float4 stage[64 * NOFF];
+    __shared__ uint32_t cstart[65];
+    const uint32_t nb = s.ctr->n_blocks;
+    const float h = s.h, inv_h = 1.0f / s.h;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    // lane -> (stencil offset, particle slot)
+    const int soff = (int)(lane % NOFF), pslot = (int)(lane / NOFF);
+    const bool active = lane < (uint32_t)(NOFF * PP);
+    const float fsx = (float)(soff % 3), fsy = (float)((soff / 3) % 3), fsz = (float)(soff / 9);
+    const int isx = soff % 3, isy = (soff / 3) % 3, isz = soff / 9;
+    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
+        const uint32_t np = s.bnp[r];
+        if (np == 0) continue;
+        const uint32_t first = s.bfirst[r];
+        if (first + np > s.n) {  // only after an earlier overflow left stale counts
+            if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+            continue;
+        }
+        int bv[D];
+        unpack_key<D>(s.bkey[r], bv);
+        for (int c = threadIdx.x; c < 64; c += NT) cstart[c] = s.bcell[(size_t)r * CELLS + c];
+        if (threadIdx.x == 0) cstart[64] = np;
+        for (int t = threadIdx.x; t < 64 * NOFF; t += NT) stage[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        for (uint32_t base = 0; base < np; base += CH) {
+            const uint32_t cnt = min((uint32_t)CH, np - base);
+            // ---- 1. stage ----
+            for (uint32_t e = threadIdx.x; e < cnt; e += NT) {
+                const uint32_t i = s.perm[first + base + e];
+                const float4 p = s.pm[i];
+                const float x[3] = {p.x, p.y, p.z};
+                float m = p.w;
+                float d0[D], w[D][3];
+                bool in_block = true;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    const float assoc = rintf(__fdiv_rn(x[k], h)) - 1.0f;
+                    const int a = (int)assoc - bv[k] * BW;
+                    in_block = in_block && a >= 0 && a < BW;
+                    d0[k] = assoc * h - x[k];
+                    bspline_weights(-d0[k] * inv_h, w[k]);
+                }
+                float q[D], Cm[D][D];
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    q[j] = s.vel[j * s.n + i] * m;
+                    if (s.force_pending) q[j] += s.fdt[j * s.n + i];
+#pragma unroll
+                    for (int k = 0; k < D; ++k) Cm[j][k] = s.C[(j * D + k) * s.n + i];
+                }
+                if (!in_block) {  // packed-key aliasing far outside the key range: contributes nothing
+                    atomicOr(s.err, ERR_KEY_RANGE);
+                    m = 0.f;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) w[k][0] = w[k][1] = w[k][2] = 0.f;
+                }
+                float bm[D];
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    float acc = q[j];
+#pragma unroll
+                    for (int k = 0; k < D; ++k) acc += Cm[j][k] * d0[k];
+                    bm[j] = acc;
+                }
+                float4 *o = &pd[e * F4];
+                if constexpr (D == 3) {
+                    o[0] = make_float4(w[0][0], w[0][1], w[0][2], m);
+                    o[1] = make_float4(w[1][0], w[1][1], w[1][2], bm[0]);
+                    o[2] = make_float4(w[2][0], w[2][1], w[2][2], bm[1]);
+                    o[3] = make_float4(h * Cm[0][0], h * Cm[1][0], h * Cm[2][0], bm[2]);
+                    o[4] = make_float4(h * Cm[0][1], h * Cm[1][1], h * Cm[2][1], 0.f);
+                    o[5] = make_float4(h * Cm[0][2], h * Cm[1][2], h * Cm[2][2], 0.f);
+                } else {
+                    o[0] = make_float4(w[0][0], w[0][1], w[0][2], m);
+                    o[1] = make_float4(w[1][0], w[1][1], w[1][2], 0.f);
+                    o[2] = make_float4(bm[0], bm[1], h * Cm[0][0], h * Cm[1][0]);
+                    o[3] = make_float4(h * Cm[0][1], h * Cm[1][1], 0.f, 0.f);
+                }
+            }
+            __syncthreads();
+            // ---- 2. accumulate per (cell, offset) ----
+            for (int c = warp; c < 64; c += NW) {
+                const uint32_t lo = max(cstart[c], base), hi = min(cstart[c + 1], base + cnt);
+                if (lo >= hi) continue;
+                float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (uint32_t j0 = lo; j0 < hi; j0 += PP) {
+                    const uint32_t j = j0 + (uint32_t)pslot;
+                    if (active && j < hi) {
+                        const float4 *pp = &pd[(j - base) * F4];
+                        const float4 q0 = pp[0], q1 = pp[1];
+                        const float wx = isx == 0 ? q0.x : (isx == 1 ? q0.y : q0.z);
+                        const float wy = isy == 0 ? q1.x : (isy == 1 ? q1.y : q1.z);
+                        if constexpr (D == 3) {
+                            const float4 q2 = pp[2], q3 = pp[3], q4 = pp[4], q5 = pp[5];
+                            const float wz = isz == 0 ? q2.x : (isz == 1 ? q2.y : q2.z);
+                            const float wt = wx * wy * wz;
+                            const float mx = q1.w + fsx * q3.x + fsy * q4.x + fsz * q5.x;
+                            const float my = q2.w + fsx * q3.y + fsy * q4.y + fsz * q5.y;
+                            const float mz = q3.w + fsx * q3.z + fsy * q4.z + fsz * q5.z;
+                            acc.x += wt * mx;
+                            acc.y += wt * my;
+                            acc.z += wt * mz;
+                            acc.w += wt * q0.w;
+                        } else {
+                            const float4 q2 = pp[2], q3 = pp[3];
+                            const float wt = wx * wy;
+                            const float mx = q2.x + fsx * q2.z + fsy * q3.x;
+                            const float my = q2.y + fsx * q2.w + fsy * q3.y;
+                            acc.x += wt * mx;
+                            acc.y += wt * my;
+                            acc.w += wt * q0.w;
+                        }
+                    }
+                }
+                if constexpr (PP > 1) {
+                    // fold the particle slots onto slot 0 (lanes s, s + NOFF, s + 2 NOFF)
+#pragma unroll
+                    for (int k = 1; k < PP; ++k) {
+                        const float ax = __shfl_down_sync(FULL_MASK, acc.x, k * NOFF);
+                        const float ay = __shfl_down_sync(FULL_MASK, acc.y, k * NOFF);
+                        const float aw = __shfl_down_sync(FULL_MASK, acc.w, k * NOFF);
+                        if (pslot == 0) {
+                            acc.x += ax;
+                            acc.y += ay;
+                            acc.w += aw;
+                        }
+                    }
+                }
+                if (active && pslot == 0) {
+                    float4 &st = stage[c * NOFF + soff];
+                    st.x += acc.x;
+                    st.y += acc.y;
+                    st.z += acc.z;
+                    st.w += acc.w;
+                }
+            }
+            __syncthreads();
+        }
+        // ---- 3. reduce per tile node, then add to the global nodes ----
+        for (int t = threadIdx.x; t < TILE; t += NT) {
+            int nc[D];
+            nc[0] = t % TW;
+            if constexpr (D == 3) {
+                nc[1] = (t / TW) % TW;
+                nc[2] = t / (TW * TW);
+            } else {
+                nc[1] = t / TW;
+            }
+            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int so = 0; so < NOFF; ++so) {
+                const int sx = so % 3, sy = (so / 3) % 3, sz = so / 9;
+                const int cx = nc[0] - sx, cy = nc[1] - sy;
+                int cz = 0;
+                if constexpr (D == 3) cz = nc[2] - sz;
+                bool ok = cx >= 0 && cx < BW && cy >= 0 && cy < BW;
+                if constexpr (D == 3) ok = ok && cz >= 0 && cz < BW;
+                if (!ok) continue;
+                const int cell = (D == 3) ? cx + 4 * cy + 16 * cz : cx + 8 * cy;
+                const float4 v = stage[cell * NOFF + so];
+                sum.x += v.x;
+                sum.y += v.y;
+                sum.z += v.z;
+                sum.w += v.w;
+            }
+            if (sum.x == 0.f && sum.y == 0.f && sum.z == 0.f && sum.w == 0.f) continue;
+            uint32_t rank, local;
+            if (!tile_node_owner<D>(s, r, t, rank, local)) continue;
+            atomicAdd(&s.nodes[(size_t)rank * 64u + local], sum);
         }
         __syncthreads();
     }

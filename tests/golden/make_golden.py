@@ -69,7 +69,9 @@ def layout(positions, h, dim):
     buckets = [[[] for _ in range(nb_buckets)] for _ in keys]
     for i, (blk, loc) in enumerate(info):
         r0 = rank[pack_key(blk, dim)]
-        buckets[r0][loc[dim - 1]].append(i)
+        # primaries are ordered by (cell, id); cell = x + BW y (+ BW^2 z)
+        cell = sum(loc[k] * bw**k for k in range(dim))
+        buckets[r0][loc[dim - 1]].append((cell, i))
         for o in assoc_offsets(dim)[1:]:
             if all(loc[k] >= min_shift for k in range(dim) if o[k] == 1):
                 nbk = [blk[k] + o[k] for k in range(dim)]
@@ -85,7 +87,10 @@ def layout(positions, h, dim):
         np_.append(sum(c[:npb]))
         npe.append(sum(c))
         for b in range(nb_buckets):
-            sorted_ids.extend(sorted(buckets[r][b]))
+            if b < npb:
+                sorted_ids.extend(i for _, i in sorted(buckets[r][b]))
+            else:
+                sorted_ids.extend(sorted(buckets[r][b]))
         run += sum(c)
     return {
         "keys": keys,

@@ -168,14 +168,16 @@ def test_conservation_vs_fp64(cuda_lib):
     data = scenes.build_mpm_data(sc)
     o64 = O.from_scene(sc, double=True, threads=8)
     nodes = data.debug_nodes(1).astype(np.float64)
-    ref = o64.nodes(1).astype(np.float64)
+    ref = o64.node_totals(1)
     m = parts["mass"].astype(np.float64)
     mom = (parts["velocity"].astype(np.float64) * m[:, None] + parts["force_dt"]).sum(0)
     rel_m = abs(nodes[:, 3].sum() - m.sum()) / m.sum()
     rel_p = np.abs(nodes[:, :3].sum(0) - mom).max() / np.abs(mom).max()
-    print(f"P2G mass rel err {rel_m:.2e}, momentum rel err {rel_p:.2e}")
+    print(f"P2G FP32 vs FP64 sums: mass rel err {rel_m:.2e}, momentum rel err {rel_p:.2e}")
     assert rel_m < 1e-6 and rel_p < 1e-5
-    assert np.abs(ref[:, :3].sum(0) - mom).max() / np.abs(mom).max() < 1e-9
+    # the FP64 oracle itself conserves to round-off
+    assert abs(ref[3] - m.sum()) / m.sum() < 1e-12
+    assert np.abs(ref[:3] - mom).max() / np.abs(mom).max() < 1e-12
     # particle mass is carried exactly through substeps
     MpmPipeline().launch_step(data, 5)
     after = data.download_particles()

@@ -62,10 +62,19 @@ def test_grid_layout_invariants(oracle_lib):
     # every particle is a primary exactly once
     prim = np.concatenate([g["sorted_ids"][f : f + n] for f, n in zip(g["first_particle"], g["num_particles"])])
     assert np.array_equal(np.sort(prim), np.arange(sc.n))
-    # each bucket holds ascending ids
+    # primaries are ordered by (cell, id), extras by (bucket, id)
+    h = np.float32(sc.cell_width)
+    pos = sc.particles["position"]
+    assoc = np.rint(pos / h).astype(np.float32) - 1.0
+    local = (assoc - np.floor(assoc / 4) * 4).astype(np.int64)
+    cell = local[:, 0] + 4 * local[:, 1] + 16 * local[:, 2]
     for r in range(len(keys)):
         s = g["first_particle"][r]
-        for c in g["bucket_counts"][r]:
+        prim = g["sorted_ids"][s : s + g["num_particles"][r]].astype(np.int64)
+        order = cell[prim] * (1 << 32) + prim
+        assert np.all(np.diff(order) > 0)
+        s += g["num_particles"][r]
+        for c in g["bucket_counts"][r][4:]:
             seg = g["sorted_ids"][s : s + c]
             assert np.all(np.diff(seg.astype(np.int64)) > 0)
             s += c
