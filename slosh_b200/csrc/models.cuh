@@ -133,9 +133,12 @@ __device__ __forceinline__ void drucker_prager(float *st, const float *p, SvdD<D
     const float s_angle = sinf(angle);
     const float alpha = sqrtf(2.0f / 3.0f) * (2.0f * s_angle) / (3.0f - s_angle);
     const float d = (float)D;
-    float strain[D], tr = 0.f;
+    float strain[D], ls[D], tr = 0.f;
 #pragma unroll
-    for (int i = 0; i < D; ++i) strain[i] = logf(sv.s[i]) + st[2] / d;
+    for (int i = 0; i < D; ++i) {
+        ls[i] = logf(sv.s[i]);
+        strain[i] = ls[i] + st[2] / d;
+    }
 #pragma unroll
     for (int i = 0; i < D; ++i) tr += strain[i];
     float dev[D];
@@ -145,13 +148,18 @@ __device__ __forceinline__ void drucker_prager(float *st, const float *p, SvdD<D
         dev[i] = strain[i] - tr / d;
         dev_zero = dev_zero && (dev[i] == 0.f);
     }
-    float ns[D], dq;
+    // ln of the projected singular values: log(new_det) = sum(hh) and
+    // log(prev_det) = sum(ls), so no further log is needed.
+    float ns[D], hh[D], dq;
     if (tr > 0.f || dev_zero) {
         float n2 = 0.f;
 #pragma unroll
         for (int i = 0; i < D; ++i) n2 += strain[i] * strain[i];
 #pragma unroll
-        for (int i = 0; i < D; ++i) ns[i] = 1.f;
+        for (int i = 0; i < D; ++i) {
+            ns[i] = 1.f;
+            hh[i] = 0.f;
+        }
         dq = sqrtf(n2);
     } else {
         float n2 = 0.f;
@@ -160,17 +168,24 @@ __device__ __forceinline__ void drucker_prager(float *st, const float *p, SvdD<D
         const float devn = sqrtf(n2);
         const float gamma = devn + (d * lambda + 2.0f * mu) / (2.0f * mu) * tr * alpha;
         if (gamma <= 0.f) return;
+        const float g = gamma / devn;
 #pragma unroll
-        for (int i = 0; i < D; ++i) ns[i] = expf(strain[i] - dev[i] * (gamma / devn));
+        for (int i = 0; i < D; ++i) {
+            hh[i] = strain[i] - dev[i] * g;
+            ns[i] = expf(hh[i]);
+        }
         dq = gamma;
     }
     float prev_det = sv.s[0] * sv.s[1], new_det = ns[0] * ns[1];
+    float lprev = ls[0] + ls[1], lnew = hh[0] + hh[1];
     if constexpr (D == 3) {
         prev_det = prev_det * sv.s[2];
         new_det = new_det * ns[2];
+        lprev += ls[2];
+        lnew += hh[2];
     }
     st[0] = st[0] * prev_det / new_det;
-    st[2] = st[2] + logf(prev_det) - logf(new_det);
+    st[2] = st[2] + lprev - lnew;
     st[1] = q + dq;
 #pragma unroll
     for (int i = 0; i < D; ++i) sv.s[i] = ns[i];

@@ -232,7 +232,7 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
     if (c->p2g_atomic)
         k_p2g_atomic<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
     else
-        k_p2g<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), 128, 0, st>>>(s);
+        k_p2g<D><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), P2G_THREADS, 0, st>>>(s);
     PROF_END(10);
 }
 

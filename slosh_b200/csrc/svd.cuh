@@ -25,18 +25,26 @@
 
 namespace slosh {
 
+// Per-precision helpers.  The Jacobi angle only steers convergence: any t
+// yields an exactly orthogonal rotation (c = 1/sqrt(1+t^2), s = t c), so the
+// FP32 path takes approximate reciprocals there.  EPS is the relative
+// off-diagonal size at which a sweep stops (near the rounding floor of A).
 template <typename T> struct SvdT;
 template <> struct SvdT<float> {
     static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
     static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
     static constexpr int SWEEPS = 5;
     static constexpr float TINY = 1e-30f;
+    static constexpr float EPS = 1e-7f;
 };
 template <> struct SvdT<double> {
     static __device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
     static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
     static constexpr int SWEEPS = 8;
     static constexpr double TINY = 1e-300;
+    static constexpr double EPS = 1e-16;
 };
 
 template <typename T> struct Svd3 {
@@ -53,8 +61,11 @@ __device__ __forceinline__ void jacobi_rotate(T (&a)[3][3], T (&V)[3][3]) {
     constexpr int r = 3 - p - q;
     const T apq = a[p][q];
     if (!(fabs(apq) > SvdT<T>::TINY)) return;
-    const T theta = (a[q][q] - a[p][p]) / (T(2) * apq);
-    const T t = copysign(T(1), theta) / (fabs(theta) + SvdT<T>::sqrt_(theta * theta + T(1)));
+    const T theta = (a[q][q] - a[p][p]) * SvdT<T>::rcp_(T(2) * apq);
+    // |theta| + sqrt(theta^2 + 1) without overflow for huge theta
+    const T at = fabs(theta);
+    const T den = at > T(1e15) ? T(2) * at : at + SvdT<T>::sqrt_(theta * theta + T(1));
+    const T t = copysign(SvdT<T>::rcp_(den), theta);
     const T c = SvdT<T>::rsqrt_(t * t + T(1));
     const T s = t * c;
     a[p][p] = a[p][p] - t * apq;
@@ -117,7 +128,7 @@ template <typename T> __device__ void svd3_impl(const T (&F)[3][3], Svd3<T> &out
         jacobi_rotate<T, 1, 2>(a, V);
         const T off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
         const T dia = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
-        if (!(off > dia * T(1e-18))) break;
+        if (!(off > dia * SvdT<T>::EPS)) break;
     }
     T l0 = a[0][0], l1 = a[1][1], l2 = a[2][2];
     if (l0 < l1) swap_cols<T>(V, l0, l1, 0, 1);

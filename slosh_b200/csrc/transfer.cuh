@@ -154,44 +154,45 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g_atomic(DevS
 //   acc_i = sum_p w_ip [ C_p (x_i - x_p) + m_p v_p + f_p dt ,  m_p ],
 // with w_ip the product of the quadratic B-spline weights per axis.
 //
-// One CTA per active block with primaries.  The block's particles arrive in
-// canonical (cell, id) order, so every cell is a contiguous range:
+// One CTA of 192 threads per active block with primaries.  The block's
+// particles arrive in canonical (cell, id) order, so every cell is a
+// contiguous range:
 //  1. stage: each thread loads a particle, computes its three weights per
 //     axis, its momentum at the base node (q + C d0) and h C, and stores
 //     them in shared memory (six float4 per particle in 3D);
-//  2. accumulate: a warp takes a cell; its lanes are the stencil offsets s
-//     (27 in 3D; in 2D 9 offsets x 3 particles at a time) and read each
-//     particle of the cell by broadcast, accumulating w_s (mom_s, m) in
-//     registers; the sums land in a shared (cell, offset) array with plain
-//     stores (one owner per entry);
+//  2. accumulate: thread (cell c, slab) owns the particles of cell c and the
+//     stencil offsets of one slab (sz in 3D, sy in 2D): 9 nodes in 3D, 3 in
+//     2D, accumulated in registers across the cell's particles and chunks,
+//     sharing the weight and momentum sub-expressions between the offsets;
+//     the sums land in a shared (cell, offset) array with plain stores (one
+//     owner per entry);
 //  3. reduce: each tile node sums its (cell, offset) entries in a fixed
 //     order, and the (block + 2)^D tile is added to the global nodes of the
 //     block and its +1 neighbours with 16-byte vector atomics.
 template <int D> struct P2GLayout;
 template <> struct P2GLayout<3> {
-    // stencil offsets, particles per step, float4 per staged particle, chunk
-    static constexpr int NOFF = 27, PP = 1, F4 = 6, CH = 128;
+    // stencil offsets, float4 per staged particle, chunk
+    static constexpr int NOFF = 27, F4 = 6, CH = 128;
 };
 template <> struct P2GLayout<2> {
-    static constexpr int NOFF = 9, PP = 3, F4 = 4, CH = 256;
+    static constexpr int NOFF = 9, F4 = 4, CH = 256;
 };
 
-template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g(DevScene s) {
+constexpr int P2G_THREADS = 192;  // 64 cells x 3 slabs
+
+template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s) {
+    constexpr int NT = P2G_THREADS;
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
-    constexpr int NOFF = P2GLayout<D>::NOFF, PP = P2GLayout<D>::PP, F4 = P2GLayout<D>::F4;
+    constexpr int NOFF = P2GLayout<D>::NOFF, F4 = P2GLayout<D>::F4;
     constexpr int CH = P2GLayout<D>::CH;  // particles staged per chunk
-    constexpr int NW = NT / 32;
     __shared__ float4 pd[CH * F4];
     __shared__ float4 stage[64 * NOFF];
     __shared__ uint32_t cstart[65];
     const uint32_t nb = s.ctr->n_blocks;
     const float h = s.h, inv_h = 1.0f / s.h;
-    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    // lane -> (stencil offset, particle slot)
-    const int soff = (int)(lane % NOFF), pslot = (int)(lane / NOFF);
-    const bool active = lane < (uint32_t)(NOFF * PP);
-    const float fsx = (float)(soff % 3), fsy = (float)((soff / 3) % 3), fsz = (float)(soff / 9);
-    const int isx = soff % 3, isy = (soff / 3) % 3, isz = soff / 9;
+    // thread -> (cell, slab offset along the slowest axis)
+    const int mycell = (int)(threadIdx.x & 63u), myslab = (int)(threadIdx.x >> 6);
+    const float fsl = (float)myslab;
     for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
@@ -204,8 +205,12 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g(DevScene s)
         unpack_key<D>(s.bkey[r], bv);
         for (int c = threadIdx.x; c < 64; c += NT) cstart[c] = s.bcell[(size_t)r * CELLS + c];
         if (threadIdx.x == 0) cstart[64] = np;
-        for (int t = threadIdx.x; t < 64 * NOFF; t += NT) stage[t] = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
+        const uint32_t clo = cstart[mycell], chi = cstart[mycell + 1];
+        constexpr int NACC = NOFF / 3;  // offsets owned by one thread
+        float4 acc[NACC];
+#pragma unroll
+        for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         for (uint32_t base = 0; base < np; base += CH) {
             const uint32_t cnt = min((uint32_t)CH, np - base);
             // ---- 1. stage ----
@@ -262,64 +267,53 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g(DevScene s)
                 }
             }
             __syncthreads();
-            // ---- 2. accumulate per (cell, offset) ----
-            for (int c = warp; c < 64; c += NW) {
-                const uint32_t lo = max(cstart[c], base), hi = min(cstart[c + 1], base + cnt);
-                if (lo >= hi) continue;
-                float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-                for (uint32_t j0 = lo; j0 < hi; j0 += PP) {
-                    const uint32_t j = j0 + (uint32_t)pslot;
-                    if (active && j < hi) {
-                        const float4 *pp = &pd[(j - base) * F4];
-                        const float4 q0 = pp[0], q1 = pp[1];
-                        const float wx = isx == 0 ? q0.x : (isx == 1 ? q0.y : q0.z);
-                        const float wy = isy == 0 ? q1.x : (isy == 1 ? q1.y : q1.z);
-                        if constexpr (D == 3) {
-                            const float4 q2 = pp[2], q3 = pp[3], q4 = pp[4], q5 = pp[5];
-                            const float wz = isz == 0 ? q2.x : (isz == 1 ? q2.y : q2.z);
-                            const float wt = wx * wy * wz;
-                            const float mx = q1.w + fsx * q3.x + fsy * q4.x + fsz * q5.x;
-                            const float my = q2.w + fsx * q3.y + fsy * q4.y + fsz * q5.y;
-                            const float mz = q3.w + fsx * q3.z + fsy * q4.z + fsz * q5.z;
-                            acc.x += wt * mx;
-                            acc.y += wt * my;
-                            acc.z += wt * mz;
-                            acc.w += wt * q0.w;
-                        } else {
-                            const float4 q2 = pp[2], q3 = pp[3];
-                            const float wt = wx * wy;
-                            const float mx = q2.x + fsx * q2.z + fsy * q3.x;
-                            const float my = q2.y + fsx * q2.w + fsy * q3.y;
-                            acc.x += wt * mx;
-                            acc.y += wt * my;
-                            acc.w += wt * q0.w;
-                        }
-                    }
-                }
-                if constexpr (PP > 1) {
-                    // fold the particle slots onto slot 0 (lanes s, s + NOFF, s + 2 NOFF)
+            // ---- 2. accumulate: this thread's cell, its slab of offsets ----
+            const uint32_t lo = max(clo, base), hi = min(chi, base + cnt);
+            for (uint32_t j = lo; j < hi; ++j) {
+                const float4 *pp = &pd[(j - base) * F4];
+                const float4 q0 = pp[0], q1 = pp[1];
+                if constexpr (D == 3) {
+                    const float4 q2 = pp[2], q3 = pp[3], q4 = pp[4], q5 = pp[5];
+                    const float wz = myslab == 0 ? q2.x : (myslab == 1 ? q2.y : q2.z);
+                    const float mz0 = q1.w + fsl * q5.x, mz1 = q2.w + fsl * q5.y, mz2 = q3.w + fsl * q5.z;
+                    const float wy[3] = {q1.x, q1.y, q1.z};
+                    const float wx[3] = {q0.x, q0.y, q0.z};
 #pragma unroll
-                    for (int k = 1; k < PP; ++k) {
-                        const float ax = __shfl_down_sync(FULL_MASK, acc.x, k * NOFF);
-                        const float ay = __shfl_down_sync(FULL_MASK, acc.y, k * NOFF);
-                        const float aw = __shfl_down_sync(FULL_MASK, acc.w, k * NOFF);
-                        if (pslot == 0) {
-                            acc.x += ax;
-                            acc.y += ay;
-                            acc.w += aw;
+                    for (int sy = 0; sy < 3; ++sy) {
+                        const float wyz = wy[sy] * wz;
+                        const float my0 = mz0 + (float)sy * q4.x, my1 = mz1 + (float)sy * q4.y,
+                                    my2 = mz2 + (float)sy * q4.z;
+#pragma unroll
+                        for (int sx = 0; sx < 3; ++sx) {
+                            const float wt = wx[sx] * wyz;
+                            float4 &a = acc[sx + 3 * sy];
+                            a.x += wt * (my0 + (float)sx * q3.x);
+                            a.y += wt * (my1 + (float)sx * q3.y);
+                            a.z += wt * (my2 + (float)sx * q3.z);
+                            a.w += wt * q0.w;
                         }
                     }
-                }
-                if (active && pslot == 0) {
-                    float4 &st = stage[c * NOFF + soff];
-                    st.x += acc.x;
-                    st.y += acc.y;
-                    st.z += acc.z;
-                    st.w += acc.w;
+                } else {
+                    const float4 q2 = pp[2], q3 = pp[3];
+                    const float wy = myslab == 0 ? q1.x : (myslab == 1 ? q1.y : q1.z);
+                    const float my0 = q2.x + fsl * q3.x, my1 = q2.y + fsl * q3.y;
+                    const float wx[3] = {q0.x, q0.y, q0.z};
+#pragma unroll
+                    for (int sx = 0; sx < 3; ++sx) {
+                        const float wt = wx[sx] * wy;
+                        float4 &a = acc[sx];
+                        a.x += wt * (my0 + (float)sx * q2.z);
+                        a.y += wt * (my1 + (float)sx * q2.w);
+                        a.w += wt * q0.w;
+                    }
                 }
             }
             __syncthreads();
         }
+        // offsets of this thread: sx + 3 sy + 9 slab (3D), sx + 3 slab (2D)
+#pragma unroll
+        for (int k = 0; k < NACC; ++k) stage[mycell * NOFF + NACC * myslab + k] = acc[k];
+        __syncthreads();
         // ---- 3. reduce per tile node, then add to the global nodes ----
         for (int t = threadIdx.x; t < TILE; t += NT) {
             int nc[D];
@@ -643,49 +637,71 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_g2p_update(DevS
 #pragma unroll
                     for (int k = 0; k < D; ++k) a[k] = 0, w[k][0] = w[k][1] = w[k][2] = 0.f;
                 }
+                // Separable gather.  With w_s = wx[sx] wy[sy] wz[sz] and
+                // dpt_s = d0 + s h, the sums of g2p.slang:196-244 are
+                //   v = M0,  grad v[c][r] = inv_d (d0_r M0_c + h M_r,c),
+                //   vel_grad_det = trace(grad v),
+                // with M0 = sum_s w_s v_s and M_r = sum_s w_s s_r v_s,
+                // accumulated axis by axis.
+                float M0[D], Mr[D][D];
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    M0[c] = 0.f;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) Mr[k][c] = 0.f;
+                }
+                const float wx0 = w[0][0], wx1 = w[0][1], wx2 = w[0][2], wx2b = 2.f * w[0][2];
                 if constexpr (D == 3) {
 #pragma unroll
-                    for (int sz = 0; sz < 3; ++sz)
+                    for (int sz = 0; sz < 3; ++sz) {
+                        float S0[3] = {0.f, 0.f, 0.f}, Sx[3] = {0.f, 0.f, 0.f}, Sy[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                        for (int sy = 0; sy < 3; ++sy)
+                        for (int sy = 0; sy < 3; ++sy) {
+                            const int idx = a[0] + TW * ((a[1] + sy) + TW * (a[2] + sz));
+                            const float wy = w[1][sy], wys = (float)sy * w[1][sy];
 #pragma unroll
-                            for (int sx = 0; sx < 3; ++sx) {
-                                const int idx = (a[0] + sx) + TW * ((a[1] + sy) + TW * (a[2] + sz));
-                                const float wt = w[0][sx] * w[1][sy] * w[2][sz];
-                                const float nvx = tv[0][idx], nvy = tv[1][idx], nvz = tv[2][idx];
-                                const float dp[3] = {d0[0] + (float)sx * h, d0[1] + (float)sy * h,
-                                                     d0[2] + (float)sz * h};
-                                vel[0] += nvx * wt;
-                                vel[1] += nvy * wt;
-                                vel[2] += nvz * wt;
-                                const float wi = wt * inv_d;
-                                const float nvv[3] = {nvx, nvy, nvz};
-#pragma unroll
-                                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                                    for (int rr = 0; rr < 3; ++rr) grad[c][rr] += wi * (nvv[c] * dp[rr]);
-                                div += wi * (nvx * dp[0] + nvy * dp[1] + nvz * dp[2]);
+                            for (int c = 0; c < 3; ++c) {
+                                const float v0 = tv[c][idx], v1 = tv[c][idx + 1], v2 = tv[c][idx + 2];
+                                const float R0 = wx0 * v0 + wx1 * v1 + wx2 * v2;
+                                const float Rx = wx1 * v1 + wx2b * v2;
+                                S0[c] += wy * R0;
+                                Sx[c] += wy * Rx;
+                                Sy[c] += wys * R0;
                             }
+                        }
+                        const float wz = w[2][sz], wzs = (float)sz * w[2][sz];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            M0[c] += wz * S0[c];
+                            Mr[0][c] += wz * Sx[c];
+                            Mr[1][c] += wz * Sy[c];
+                            Mr[2][c] += wzs * S0[c];
+                        }
+                    }
                 } else {
 #pragma unroll
-                    for (int sy = 0; sy < 3; ++sy)
+                    for (int sy = 0; sy < 3; ++sy) {
+                        const int idx = a[0] + TW * (a[1] + sy);
+                        const float wy = w[1][sy], wys = (float)sy * w[1][sy];
 #pragma unroll
-                        for (int sx = 0; sx < 3; ++sx) {
-                            const int idx = (a[0] + sx) + TW * (a[1] + sy);
-                            const float wt = w[0][sx] * w[1][sy];
-                            const float nvx = tv[0][idx], nvy = tv[1][idx];
-                            const float dp[2] = {d0[0] + (float)sx * h, d0[1] + (float)sy * h};
-                            vel[0] += nvx * wt;
-                            vel[1] += nvy * wt;
-                            const float wi = wt * inv_d;
-                            const float nvv[2] = {nvx, nvy};
-#pragma unroll
-                            for (int c = 0; c < 2; ++c)
-#pragma unroll
-                                for (int rr = 0; rr < 2; ++rr) grad[c][rr] += wi * (nvv[c] * dp[rr]);
-                            div += wi * (nvx * dp[0] + nvy * dp[1]);
+                        for (int c = 0; c < 2; ++c) {
+                            const float v0 = tv[c][idx], v1 = tv[c][idx + 1], v2 = tv[c][idx + 2];
+                            const float R0 = wx0 * v0 + wx1 * v1 + wx2 * v2;
+                            const float Rx = wx1 * v1 + wx2b * v2;
+                            M0[c] += wy * R0;
+                            Mr[0][c] += wy * Rx;
+                            Mr[1][c] += wys * R0;
                         }
+                    }
                 }
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    vel[c] = M0[c];
+#pragma unroll
+                    for (int rr = 0; rr < D; ++rr) grad[c][rr] = inv_d * (d0[rr] * M0[c] + h * Mr[rr][c]);
+                }
+                div = grad[0][0] + grad[1][1];
+                if constexpr (D == 3) div += grad[2][2];
             }
             // ---- particle update ----
             const Material &mat = s.materials[fl & FLAG_MAT_MASK];
