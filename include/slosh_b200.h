@@ -259,6 +259,26 @@ int slosh_debug_nodes(slosh_ctx *ctx, int stage, float *nodes,
 int slosh_prefix_sum(slosh_ctx *ctx, const uint32_t *in, uint32_t *out,
                      uint32_t n);
 
+/* Allocation-free variant of slosh_prefix_sum for callers that cannot
+ * allocate device memory where they need the scan (hosts that own every
+ * allocation up front, real-time loops, code inside another framework's
+ * memory pool).  This entry point has no counterpart in the reference.
+ *  - d_in, d_out: DEVICE arrays of n u32 on the current device, not aliased;
+ *    same result as slosh_prefix_sum (exclusive scan, total dropped).
+ *  - n <= 67,108,864 (16384 tiles of 4096); larger n returns
+ *    SLOSH_E_CAPACITY without launching anything.
+ *  - Scratch: a 64 KiB file-scope __device__ array that every GPU loading
+ *    the library holds until exit.  It allocates nothing: no cudaMalloc,
+ *    cudaFree or allocating library call.  The first call on a device looks
+ *    up the array's device address (cudaGetSymbolAddress) with that device
+ *    current; make that first call before any stream capture.
+ *  - Every call shares the scratch array: calls that overlap on the GPU
+ *    (other streams, other host threads) race and must be serialised by the
+ *    caller.  Nothing in the scratch needs to start at zero.
+ *  - Asynchronous on `stream` (a cudaStream_t, NULL = legacy default). */
+int slosh_prefix_sum_noalloc(const uint32_t *d_in, uint32_t *d_out, uint32_t n,
+                             void *stream);
+
 /* Copies the last error message of the context into `buf`. */
 int slosh_last_error(const slosh_ctx *ctx, char *buf, size_t len);
 

@@ -147,6 +147,7 @@ SIGNATURES = {
     "slosh_grid_debug": (ctypes.c_int, [_P, ctypes.POINTER(SloshGridDump), _U32, _U32]),
     "slosh_debug_nodes": (ctypes.c_int, [_P, ctypes.c_int, _P, _U32, ctypes.POINTER(_U32)]),
     "slosh_prefix_sum": (ctypes.c_int, [_P, _P, _P, _U32]),
+    "slosh_prefix_sum_noalloc": (ctypes.c_int, [_P, _P, _U32, _P]),
     "slosh_last_error": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t]),
 }
 

@@ -52,7 +52,14 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *NVCC_FLAGS, os.path.join(SRC, "slosh_b200.cu"), "-o", tmp]
+    cmd = [
+        _nvcc(),
+        *NVCC_FLAGS,
+        os.path.join(SRC, "slosh_b200.cu"),
+        os.path.join(SRC, "noalloc_scan.cu"),
+        "-o",
+        tmp,
+    ]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
