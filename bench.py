@@ -48,7 +48,25 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument(
+        "--ncu-case",
+        action="store_true",
+        help="profiling case for ncu: build the scene at --h, run --steps substeps, print stats, exit",
+    )
     return ap.parse_args()
+
+
+def main_ncu_case(args):
+    from slosh_b200 import scenes
+    from slosh_b200.pipeline import MpmPipeline
+
+    sc = bench_scene(args.h)
+    data = scenes.build_mpm_data(sc)
+    MpmPipeline().launch_step(data, args.steps)
+    data.sync()
+    print(json.dumps({"ncu_case": sc.name, "h": sc.cell_width, "particles": sc.n, **data.stats()}))
+    data.close()
+    return 0
 
 
 def dist_env():
@@ -398,6 +416,8 @@ def main_ours(args):
 
 def main():
     args = parse()
+    if args.ncu_case:
+        return main_ncu_case(args)
     if args.impl == "reference":
         return main_reference(args)
     return main_ours(args)

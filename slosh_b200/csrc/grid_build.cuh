@@ -342,26 +342,35 @@ __global__ void k_scatter(DevScene s) {
     }
 }
 
-// Orders each (block, cell) range of the permutation by particle id: the
-// canonical order.  The scatter already groups a block's particles by cell;
-// each element's final place is its rank among the ids of its cell (a few
-// particles per cell), found from shared memory.
+// Orders each (block, cell) range of the permutation by original particle
+// id: the canonical order.  The scatter already groups a block's particles
+// by cell; each element's final place is its rank among the original ids of
+// its cell (a few particles per cell), found from shared memory.  perm holds
+// storage indices; the order key is oid[storage index].
 constexpr uint32_t CANON_SMEM = 4096;
 template <int NT> __global__ void __launch_bounds__(NT) k_canon(DevScene s) {
     __shared__ uint32_t ids[CANON_SMEM];
+    __shared__ uint32_t keys[CANON_SMEM];
     __shared__ uint32_t cstart[CELLS + 1];
     const uint32_t nb = s.ctr->n_blocks;
     for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
+        if (first + np > s.n) {  // only after an earlier overflow left stale counts
+            if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+            continue;
+        }
         for (uint32_t c = threadIdx.x; c < CELLS; c += NT) cstart[c] = s.bcell[(size_t)r * CELLS + c];
         if (threadIdx.x == 0) cstart[CELLS] = np;
         const bool in_smem = np <= CANON_SMEM;
         if (in_smem)
-            for (uint32_t e = threadIdx.x; e < np; e += NT) ids[e] = s.perm_tmp[first + e];
+            for (uint32_t e = threadIdx.x; e < np; e += NT) {
+                const uint32_t j = s.perm_tmp[first + e];
+                ids[e] = j;
+                keys[e] = s.oid[j];
+            }
         __syncthreads();
-        const uint32_t *src = in_smem ? ids : s.perm_tmp + first;
         for (uint32_t e = threadIdx.x; e < np; e += NT) {
             // cell of entry e: last c with cstart[c] <= e (binary search)
             uint32_t lo = 0, hi = CELLS;
@@ -371,9 +380,16 @@ template <int NT> __global__ void __launch_bounds__(NT) k_canon(DevScene s) {
                 else hi = mid;
             }
             const uint32_t b0 = cstart[lo], b1 = cstart[lo + 1];
-            const uint32_t id = src[e];
-            uint32_t rank = 0;
-            for (uint32_t j = b0; j < b1; ++j) rank += (src[j] < id) ? 1u : 0u;
+            uint32_t rank = 0, id;
+            if (in_smem) {
+                id = ids[e];
+                const uint32_t key = keys[e];
+                for (uint32_t j = b0; j < b1; ++j) rank += (keys[j] < key) ? 1u : 0u;
+            } else {
+                id = s.perm_tmp[first + e];
+                const uint32_t key = s.oid[id];
+                for (uint32_t j = b0; j < b1; ++j) rank += (s.oid[s.perm_tmp[first + j]] < key) ? 1u : 0u;
+            }
             s.perm[first + b0 + rank] = id;
         }
         __syncthreads();

@@ -118,6 +118,7 @@ template <int D> __global__ void k_ingest(DevScene s, IoBuffers io) {
             }
         s.V0[i] = p.init_volume;
         s.damping[i] = p.damping;
+        s.oid[i] = i;
         if (p.damping != 0.f) sflags |= SCENE_DAMPING;
         io.r0[i] = p.init_radius;
         io.phase[i] = p.phase;
@@ -130,11 +131,13 @@ template <int D> __global__ void k_ingest(DevScene s, IoBuffers io) {
     if (lane_id() == 0 && sflags) atomicOr(io.scene_flags, sflags);
 }
 
-// Structure of arrays -> records.
+// Structure of arrays -> records, back in upload order (stored particle i is
+// record oid[i]).
 template <int D> __global__ void k_egest(DevScene s, IoBuffers io) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const size_t n = s.n;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+        const uint32_t orig = s.oid[i];
         slosh_particle p;
         const float4 pm = s.pm[i];
         p.position[0] = pm.x;
@@ -156,10 +159,10 @@ template <int D> __global__ void k_egest(DevScene s, IoBuffers io) {
         if (D == 2) p.def_grad[8] = 0.f;
         p.vel_grad_det = 0.f;
         p.init_volume = s.V0[i];
-        p.init_radius = io.r0[i];
+        p.init_radius = io.r0[orig];
         p.mass = pm.w;
-        p.damping = s.damping[i];
-        p.phase = io.phase[i];
+        p.damping = s.has_damping ? s.damping[i] : 0.f;
+        p.phase = io.phase[orig];
         const uint32_t fl = s.flags[i];
         p.enabled = (fl & FLAG_ENABLED) ? 1u : 0u;
         p.fixed = (fl & FLAG_FIXED) ? 1u : 0u;
@@ -168,17 +171,23 @@ template <int D> __global__ void k_egest(DevScene s, IoBuffers io) {
         for (int q = 0; q < 12; ++q) p.model.data[q] = m.p[q];
         if (m.tag == SLOSH_MODEL_SAND_LINEAR || m.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN)
             for (int q = 0; q < 3; ++q) p.model.data[q] = s.plastic[q * n + i];
-        io.out[i] = p;
+        io.out[orig] = p;
     }
 }
 
-// Positions as vec4 (x, y, z, 0).
+// Positions as vec4 (x, y, z, 0) in upload order.
 __global__ void k_positions(DevScene s, float4 *out) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
         const float4 p = s.pm[i];
-        out[i] = make_float4(p.x, p.y, p.z, 0.f);
+        out[s.oid[i]] = make_float4(p.x, p.y, p.z, 0.f);
     }
+}
+
+// Debug: the hot path's primary permutation in original ids.
+__global__ void k_perm_to_oid(DevScene s, uint32_t *out) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < s.n; e += stride) out[e] = s.oid[s.perm[e]];
 }
 
 // ---------------------------------------------------------------------------
@@ -285,19 +294,19 @@ template <int D> __global__ void k_dbg_scatter(DevScene s, DebugBuffers d) {
     }
 }
 
-// Canonical order of one entry of bucket b: primaries by (cell, id), extras
-// by id.
+// Canonical order of stored particle j in bucket b: primaries by (cell,
+// original id), extras by original id.
 template <int D>
-__device__ __forceinline__ uint64_t dbg_order_key(const DevScene &s, uint32_t id, uint32_t b) {
-    if (b >= (uint32_t)Geo<D>::NPB) return id;
-    const float4 p = s.pm[id];
+__device__ __forceinline__ uint64_t dbg_order_key(const DevScene &s, uint32_t j, uint32_t b) {
+    if (b >= (uint32_t)Geo<D>::NPB) return s.oid[j];
+    const float4 p = s.pm[j];
     const float x[3] = {p.x, p.y, p.z};
     const CellLoc<D> c = locate<D>(x, s.h);
-    return ((uint64_t)cell_index<D>(c.local) << 32) | id;
+    return ((uint64_t)cell_index<D>(c.local) << 32) | s.oid[j];
 }
 
 // One thread per (block, bucket) segment: rank each entry by its canonical
-// order key inside the segment.
+// order key inside the segment; the output holds original ids.
 template <int D> __global__ void k_dbg_canon(DevScene s, DebugBuffers d) {
     constexpr int NB = Geo<D>::NB;
     const uint32_t nb = s.ctr->n_blocks;
@@ -313,7 +322,7 @@ template <int D> __global__ void k_dbg_canon(DevScene s, DebugBuffers d) {
             const uint64_t key = dbg_order_key<D>(s, id, b);
             uint32_t rank = 0;
             for (uint32_t j = lo; j < hi; ++j) rank += (dbg_order_key<D>(s, d.sorted[j], b) < key) ? 1u : 0u;
-            d.sorted2[lo + rank] = id;
+            d.sorted2[lo + rank] = s.oid[id];
         }
     }
 }

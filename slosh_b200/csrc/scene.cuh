@@ -8,6 +8,9 @@ namespace slosh {
 
 struct DevScene {
     // ---- particles (structure of arrays, math convention) -------------------
+    // Storage is double-buffered: the substep reads the arrays below (in the
+    // canonical order of the previous substep) and the fused G2P/update
+    // writes the `out_*` arrays in this substep's canonical order.
     uint32_t n;            // particle count
     float h;               // cell width
     float dt;
@@ -20,8 +23,13 @@ struct DevScene {
     uint32_t *flags;       // material id | enabled | fixed
     float *damping;        // read only when has_damping
     float *plastic;        // 3 planes (det_p, q, log_vol_gain) for sand models
-    float *fdt;            // D planes of force*dt, read by P2G while force_pending
+    uint32_t *oid;         // original (upload) index of each stored particle
+    float4 *out_pm;
+    float *out_vel, *out_C, *out_F, *out_V0, *out_damping, *out_plastic;
+    uint32_t *out_flags, *out_oid;
+    float *fdt;            // D planes of force*dt in upload order, read by P2G while force_pending
     uint32_t has_damping;
+    uint32_t has_sand;
     uint32_t force_pending;
     const Material *materials;
 

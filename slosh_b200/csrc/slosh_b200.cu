@@ -27,11 +27,14 @@ struct slosh_ctx {
     cudaStream_t stream = nullptr;
     slosh_params params{};
 
-    // particles
-    float4 *pm = nullptr;
-    float *vel = nullptr, *C = nullptr, *F = nullptr, *V0 = nullptr, *damping = nullptr, *plastic = nullptr,
-          *fdt = nullptr, *r0 = nullptr, *phase = nullptr;
-    uint32_t *flags = nullptr;
+    // particles: double-buffered storage in canonical order (buffer `parity`
+    // holds the state the next substep reads) + upload-order side arrays
+    struct Storage {
+        float4 *pm = nullptr;
+        float *vel = nullptr, *C = nullptr, *F = nullptr, *V0 = nullptr, *damping = nullptr, *plastic = nullptr;
+        uint32_t *flags = nullptr, *oid = nullptr;
+    } pb[2];
+    float *fdt = nullptr, *r0 = nullptr, *phase = nullptr;
     Material *materials = nullptr;
     uint32_t *mat_hkeys = nullptr, *mat_dense = nullptr;
     uint32_t has_damping = 0, force_pending = 0, has_sand = 0, n_materials = 0;
@@ -111,16 +114,28 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.h = c->h;
     s.dt = c->params.dt;
     for (int k = 0; k < 3; ++k) s.gravity[k] = c->params.gravity[k];
-    s.pm = c->pm;
-    s.vel = c->vel;
-    s.C = c->C;
-    s.F = c->F;
-    s.V0 = c->V0;
-    s.flags = c->flags;
-    s.damping = c->damping;
-    s.plastic = c->plastic;
+    const slosh_ctx::Storage &A = c->pb[parity & 1u], &B = c->pb[(parity & 1u) ^ 1u];
+    s.pm = A.pm;
+    s.vel = A.vel;
+    s.C = A.C;
+    s.F = A.F;
+    s.V0 = A.V0;
+    s.flags = A.flags;
+    s.damping = A.damping;
+    s.plastic = A.plastic;
+    s.oid = A.oid;
+    s.out_pm = B.pm;
+    s.out_vel = B.vel;
+    s.out_C = B.C;
+    s.out_F = B.F;
+    s.out_V0 = B.V0;
+    s.out_flags = B.flags;
+    s.out_damping = B.damping;
+    s.out_plastic = B.plastic;
+    s.out_oid = B.oid;
     s.fdt = c->fdt;
     s.has_damping = c->has_damping;
+    s.has_sand = c->has_sand;
     s.force_pending = force ? 1u : 0u;
     s.materials = c->materials;
     s.cap = c->cap;
@@ -350,10 +365,14 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     const size_t N = c->max_n;
     const int D = c->dim;
     const uint32_t cap = c->cap, hcap = c->hcap;
-    if ((st = dalloc(c, &c->pm, N)) || (st = dalloc(c, &c->vel, N * D)) || (st = dalloc(c, &c->C, N * D * D)) ||
-        (st = dalloc(c, &c->F, N * D * D)) || (st = dalloc(c, &c->V0, N)) || (st = dalloc(c, &c->flags, N)) ||
-        (st = dalloc(c, &c->damping, N)) || (st = dalloc(c, &c->plastic, N * 3)) || (st = dalloc(c, &c->fdt, N * D)) ||
-        (st = dalloc(c, &c->r0, N)) || (st = dalloc(c, &c->phase, N)) ||
+    for (int b = 0; b < 2; ++b) {
+        slosh_ctx::Storage &S = c->pb[b];
+        if ((st = dalloc(c, &S.pm, N)) || (st = dalloc(c, &S.vel, N * D)) || (st = dalloc(c, &S.C, N * D * D)) ||
+            (st = dalloc(c, &S.F, N * D * D)) || (st = dalloc(c, &S.V0, N)) || (st = dalloc(c, &S.flags, N)) ||
+            (st = dalloc(c, &S.damping, N)) || (st = dalloc(c, &S.plastic, N * 3)) || (st = dalloc(c, &S.oid, N)))
+            return fail_create(st);
+    }
+    if ((st = dalloc(c, &c->fdt, N * D)) || (st = dalloc(c, &c->r0, N)) || (st = dalloc(c, &c->phase, N)) ||
         (st = dalloc(c, &c->materials, MAX_MATERIALS)) || (st = dalloc(c, &c->mat_hkeys, MAT_HASH)) ||
         (st = dalloc(c, &c->mat_dense, MAT_HASH)) || (st = dalloc(c, &c->hkeys[0], hcap)) ||
         (st = dalloc(c, &c->hkeys[1], hcap)) || (st = dalloc(c, &c->hvals[0], hcap)) ||
@@ -379,7 +398,8 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     cudaMemset(c->hvals[1], 0xff, hcap * 4);
     cudaMemset(c->ctr, 0, sizeof(Counters));
     cudaMemset(c->err, 0, 4);
-    cudaMemset(c->damping, 0, N * 4);
+    cudaMemset(c->pb[0].damping, 0, N * 4);
+    cudaMemset(c->pb[1].damping, 0, N * 4);
     cudaMemset(c->slot_counts, 0, (size_t)hcap * CELLS * 4);
     const char *variant = std::getenv("SLOSH_P2G");
     c->p2g_atomic = variant && std::strcmp(variant, "atomic") == 0;
@@ -658,7 +678,7 @@ int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, u
     DebugBuffers d{};
     void *blob = nullptr;
     const size_t nbs = std::max<uint32_t>(nb, 1);
-    const size_t words = nbs * NB * 2 + nbs * 3 + (size_t)cap_entries * 2 + 1;
+    const size_t words = nbs * NB * 2 + nbs * 3 + (size_t)cap_entries * 2 + 1 + c->n;
     CK(cudaMalloc(&blob, words * 4));
     uint32_t *w = (uint32_t *)blob;
     d.counts = w;
@@ -670,7 +690,9 @@ int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, u
     d.sorted2 = d.sorted + cap_entries;
     d.total = d.sorted2 + cap_entries;
     d.cap_entries = cap_entries;
+    uint32_t *perm_oid = d.total + 1;
     cudaMemsetAsync(d.counts, 0, nbs * NB * 4, st);
+    k_perm_to_oid<<<grid_for(c->n, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s, perm_oid);
     const uint32_t g = grid_for(c->n, 256, (uint32_t)c->sm_count * 16);
     if (c->dim == 3) {
         k_dbg_count<3><<<g, 256, 0, st>>>(s, d);
@@ -699,7 +721,7 @@ int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, u
     copy(dump->bucket_counts, d.counts, (size_t)nbc * NB);
     copy(dump->sorted_ids, d.sorted2, std::min(total, cap_sorted));
     copy(dump->primary_first, c->bfirst, nbc);
-    copy(dump->primary_perm, c->perm, c->n);
+    copy(dump->primary_perm, perm_oid, c->n);
     copy(dump->neighbors, c->bnbh, (size_t)nbc * NN);
     cudaFree(blob);
     if (ce != cudaSuccess) return fail(c, SLOSH_E_CUDA, "grid debug: %s", cudaGetErrorString(ce));

@@ -765,46 +765,53 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_g2p_update(DevS
                 for (int k = 0; k < 3; ++k) st[k] = s.plastic[k * n + i];
             float tau[D][D];
             model_update<D>(mat, F, st, tau, &s.ctr->n_svd_fp64);
-            const float coef = s.V0[i] * inv_d * dt;
+            const float v0 = s.V0[i];
+            const float coef = v0 * inv_d * dt;
             bool finite = true;
 #pragma unroll
             for (int k = 0; k < D; ++k) finite = finite && (nx[k] == nx[k]);
+            // The particle is stored at its canonical position o in the
+            // output buffers (contiguous, coalesced writes).
+            const size_t o = (size_t)first + e;
             if (finite && det<D>(F) > 0.f) {
                 float4 np4 = p;
                 np4.x = nx[0];
                 np4.y = nx[1];
                 if constexpr (D == 3) np4.z = nx[2];
-                s.pm[i] = np4;
+                s.out_pm[o] = np4;
 #pragma unroll
                 for (int rr = 0; rr < D; ++rr)
 #pragma unroll
-                    for (int c = 0; c < D; ++c) s.C[(rr * D + c) * n + i] = grad[rr][c] * m - tau[rr][c] * coef;
+                    for (int c = 0; c < D; ++c) s.out_C[(rr * D + c) * n + o] = grad[rr][c] * m - tau[rr][c] * coef;
 #pragma unroll
-                for (int k = 0; k < D; ++k) s.vel[k * n + i] = vel[k];
+                for (int k = 0; k < D; ++k) s.out_vel[k * n + o] = vel[k];
             } else {
                 fl &= ~FLAG_ENABLED;
-                s.flags[i] = fl;
                 m = 0.f;
                 float4 np4 = p;
                 np4.w = 0.f;
-                s.pm[i] = np4;
+                s.out_pm[o] = np4;
 #pragma unroll
                 for (int rr = 0; rr < D; ++rr)
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
                         F[rr][c] = (rr == c) ? 1.f : 0.f;
-                        s.C[(rr * D + c) * n + i] = 0.f;
+                        s.out_C[(rr * D + c) * n + o] = 0.f;
                     }
 #pragma unroll
-                for (int k = 0; k < D; ++k) s.vel[k * n + i] = 0.f;
+                for (int k = 0; k < D; ++k) s.out_vel[k * n + o] = 0.f;
             }
 #pragma unroll
             for (int rr = 0; rr < D; ++rr)
 #pragma unroll
-                for (int c = 0; c < D; ++c) s.F[(rr * D + c) * n + i] = F[rr][c];
-            if (sand)
+                for (int c = 0; c < D; ++c) s.out_F[(rr * D + c) * n + o] = F[rr][c];
+            if (s.has_sand)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) s.plastic[k * n + i] = st[k];
+                for (int k = 0; k < 3; ++k) s.out_plastic[k * n + o] = st[k];
+            if (s.has_damping) s.out_damping[o] = s.damping[i];
+            s.out_flags[o] = fl;
+            s.out_V0[o] = v0;
+            s.out_oid[o] = s.oid[i];
         }
         __syncthreads();
     }
