@@ -45,7 +45,10 @@ struct slosh_ctx {
              *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_fill = nullptr, *tmp_key = nullptr,
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
              *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr;
-    bool p2g_atomic = false;  // SLOSH_P2G=atomic selects the shared-atomic P2G variant
+    // P2G variant for A/B measurements (environment SLOSH_P2G at creation):
+    // 0 direct cell-owner (default), 1 "atomic" per-particle shared atomics,
+    // 2 "staged" shared-memory staging with a fixed-order reduction.
+    int p2g_variant = 0;
     uint32_t *pslot = nullptr, *perm_tmp = nullptr, *perm = nullptr;
     float4 *nodes = nullptr, *coll[2] = {nullptr, nullptr};
     uint32_t *coll_id[2] = {nullptr, nullptr};
@@ -244,10 +247,13 @@ template <int D> void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaSt
 
 template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
     PROF_BEGIN(10);
-    if (c->p2g_atomic)
+    const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
+    if (c->p2g_variant == 1)
         k_p2g_atomic<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
+    else if (c->p2g_variant == 2)
+        k_p2g_staged<D><<<g, P2G_THREADS, 0, st>>>(s);
     else
-        k_p2g<D><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), P2G_THREADS, 0, st>>>(s);
+        k_p2g<D><<<g, P2G_THREADS, 0, st>>>(s);
     PROF_END(10);
 }
 
@@ -401,8 +407,10 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     cudaMemset(c->pb[0].damping, 0, N * 4);
     cudaMemset(c->pb[1].damping, 0, N * 4);
     cudaMemset(c->slot_counts, 0, (size_t)hcap * CELLS * 4);
-    const char *variant = std::getenv("SLOSH_P2G");
-    c->p2g_atomic = variant && std::strcmp(variant, "atomic") == 0;
+    if (const char *variant = std::getenv("SLOSH_P2G")) {
+        if (std::strcmp(variant, "atomic") == 0) c->p2g_variant = 1;
+        else if (std::strcmp(variant, "staged") == 0) c->p2g_variant = 2;
+    }
     if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     c->params.gravity[1] = -9.81f;
     c->params.dt = 1.0f / 60.0f;

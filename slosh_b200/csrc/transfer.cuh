@@ -180,7 +180,7 @@ template <> struct P2GLayout<2> {
 
 constexpr int P2G_THREADS = 192;  // 64 cells x 3 slabs
 
-template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s) {
+template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g_staged(DevScene s) {
     constexpr int NT = P2G_THREADS;
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NOFF = P2GLayout<D>::NOFF, F4 = P2GLayout<D>::F4;
@@ -345,6 +345,144 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s
             uint32_t rank, local;
             if (!tile_node_owner<D>(s, r, t, rank, local)) continue;
             atomicAdd(&s.nodes[(size_t)rank * 64u + local], sum);
+        }
+        __syncthreads();
+    }
+}
+
+// Particle-to-grid, direct cell-owner variant (default).
+//
+// One CTA of 192 threads per active block with primaries; thread (cell c,
+// slab) owns cell c and the 9 (3D) or 3 (2D) stencil offsets of one slab.
+// It reads the particles of its cell straight from global memory -- they
+// are contiguous in the canonical storage order -- and accumulates its nodes
+// in registers.  The cell comes from the sort, so the base node position is
+// exact and no division is needed: d0 = (block origin + cell) h - x, and the
+// weights use -d0 / h = -d0 * (1/h) like slosh's p2g (dpt * inv_cell_width).
+// The per-thread sums are added to a shared (block + 2)^D tile with
+// shared-memory atomics (the lanes of a warp own distinct cells, so one
+// instruction never hits the same node twice), and the tile is added to the
+// global nodes of the block and its +1 neighbours with 16-byte atomics.  Two
+// barriers per block; no staging.
+template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s) {
+    constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
+    constexpr int NACC = (D == 3) ? 9 : 3;
+    __shared__ float tile[4][TILE];
+    const uint32_t nb = s.ctr->n_blocks;
+    const float h = s.h, inv_h = 1.0f / s.h;
+    const size_t n = s.n;
+    const int mycell = (int)(threadIdx.x & 63u), myslab = (int)(threadIdx.x >> 6);
+    int ca[D];
+    if constexpr (D == 3) {
+        ca[0] = mycell & 3;
+        ca[1] = (mycell >> 2) & 3;
+        ca[2] = mycell >> 4;
+    } else {
+        ca[0] = mycell & 7;
+        ca[1] = mycell >> 3;
+    }
+    const float fsl = (float)myslab;
+    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
+        const uint32_t np = s.bnp[r];
+        if (np == 0) continue;
+        const uint32_t first = s.bfirst[r];
+        if (first + np > s.n) {  // only after an earlier overflow left stale counts
+            if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+            continue;
+        }
+        for (int t = threadIdx.x; t < 4 * TILE; t += P2G_THREADS) (&tile[0][0])[t] = 0.f;
+        int bv[D];
+        unpack_key<D>(s.bkey[r], bv);
+        const uint32_t lo = s.bcell[(size_t)r * CELLS + mycell];
+        const uint32_t hi = (mycell < 63) ? s.bcell[(size_t)r * CELLS + mycell + 1] : np;
+        float assoc[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) assoc[k] = (float)(bv[k] * BW + ca[k]);
+        float4 acc[NACC];
+#pragma unroll
+        for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        for (uint32_t j = lo; j < hi; ++j) {
+            const uint32_t i = s.perm[first + j];
+            const float4 p = s.pm[i];
+            const float x[3] = {p.x, p.y, p.z};
+            const float m = p.w;
+            float d0[D], w[D][3];
+            bool in_cell = true;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                d0[k] = assoc[k] * h - x[k];
+                const float f = -d0[k] * inv_h;
+                in_cell = in_cell && f >= 0.49f && f <= 1.51f;
+                bspline_weights(f, w[k]);
+            }
+            if (!in_cell) {  // packed-key aliasing far outside the key range
+                atomicOr(s.err, ERR_KEY_RANGE);
+                continue;
+            }
+            float bm[D], hc[D][D];
+#pragma unroll
+            for (int jj = 0; jj < D; ++jj) {
+                float q = s.vel[jj * n + i] * m;
+                if (s.force_pending) q += s.fdt[jj * n + i];
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    const float c = s.C[(jj * D + k) * n + i];
+                    q += c * d0[k];
+                    hc[k][jj] = h * c;
+                }
+                bm[jj] = q;
+            }
+            if constexpr (D == 3) {
+                const float wz = myslab == 0 ? w[2][0] : (myslab == 1 ? w[2][1] : w[2][2]);
+                const float mz0 = bm[0] + fsl * hc[2][0], mz1 = bm[1] + fsl * hc[2][1], mz2 = bm[2] + fsl * hc[2][2];
+#pragma unroll
+                for (int sy = 0; sy < 3; ++sy) {
+                    const float wyz = w[1][sy] * wz;
+                    const float my0 = mz0 + (float)sy * hc[1][0], my1 = mz1 + (float)sy * hc[1][1],
+                                my2 = mz2 + (float)sy * hc[1][2];
+#pragma unroll
+                    for (int sx = 0; sx < 3; ++sx) {
+                        const float wt = w[0][sx] * wyz;
+                        float4 &a = acc[sx + 3 * sy];
+                        a.x += wt * (my0 + (float)sx * hc[0][0]);
+                        a.y += wt * (my1 + (float)sx * hc[0][1]);
+                        a.z += wt * (my2 + (float)sx * hc[0][2]);
+                        a.w += wt * m;
+                    }
+                }
+            } else {
+                const float wy = myslab == 0 ? w[1][0] : (myslab == 1 ? w[1][1] : w[1][2]);
+                const float my0 = bm[0] + fsl * hc[1][0], my1 = bm[1] + fsl * hc[1][1];
+#pragma unroll
+                for (int sx = 0; sx < 3; ++sx) {
+                    const float wt = w[0][sx] * wy;
+                    float4 &a = acc[sx];
+                    a.x += wt * (my0 + (float)sx * hc[0][0]);
+                    a.y += wt * (my1 + (float)sx * hc[0][1]);
+                    a.w += wt * m;
+                }
+            }
+        }
+        if (hi > lo) {
+#pragma unroll
+            for (int k = 0; k < NACC; ++k) {
+                const int sx = k % 3, sy = (D == 3) ? k / 3 : myslab, sz = (D == 3) ? myslab : 0;
+                int idx = (ca[0] + sx) + TW * (ca[1] + sy);
+                if constexpr (D == 3) idx += TW * TW * (ca[2] + sz);
+                atomicAdd(&tile[0][idx], acc[k].x);
+                atomicAdd(&tile[1][idx], acc[k].y);
+                if constexpr (D == 3) atomicAdd(&tile[2][idx], acc[k].z);
+                atomicAdd(&tile[3][idx], acc[k].w);
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < TILE; t += P2G_THREADS) {
+            const float4 val = make_float4(tile[0][t], tile[1][t], tile[2][t], tile[3][t]);
+            if (val.x == 0.f && val.y == 0.f && val.z == 0.f && val.w == 0.f) continue;
+            uint32_t rank, local;
+            if (!tile_node_owner<D>(s, r, t, rank, local)) continue;
+            atomicAdd(&s.nodes[(size_t)rank * 64u + local], val);
         }
         __syncthreads();
     }
@@ -583,7 +721,7 @@ template <int D> __global__ void k_grid_update(DevScene s) {
 // particles (g2p.slang:150-265) and applies the particle update of
 // particle_update.slang:48-159 with the constitutive model, writing the new
 // position, velocity, APIC matrix C and F.
-template <int D, int NT> __global__ void __launch_bounds__(NT) k_g2p_update(DevScene s) {
+template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float tv[D][TILE];
     const uint32_t nb = s.ctr->n_blocks;
