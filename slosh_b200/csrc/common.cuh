@@ -121,6 +121,19 @@ __device__ __forceinline__ void bspline_weights(float x, float *w) {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// Asynchronous global -> shared copies (cp.async), used to stage the next
+// particle's inputs while the current one is computed.
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -155,12 +168,14 @@ struct DevBody {
 
 // Per-substep device counters.
 struct Counters {
-    uint32_t n_primary;  // primary blocks appended by the touch pass
-    uint32_t n_extra;    // neighbour-only blocks appended by the neighbour pass
-    uint32_t n_blocks;   // active blocks after ranking (min(total, capacity))
-    uint32_t n_sorted;   // debug: sorted entries with extras
-    uint32_t n_svd_fp64; // particles whose SVD fell back to FP64 (cumulative)
-    uint32_t pad[3];
+    uint32_t n_primary;      // primary blocks appended by the touch pass
+    uint32_t n_extra;        // neighbour-only blocks appended by the neighbour pass
+    uint32_t n_blocks;       // active blocks after ranking (min(total, capacity))
+    uint32_t n_sorted;       // debug: sorted entries with extras
+    uint32_t n_svd_fp64;     // particles whose SVD fell back to FP64 (cumulative)
+    uint32_t last_n_blocks;  // n_blocks of the last completed substep
+    uint32_t last_n_primary; // n_primary of the last completed substep
+    uint32_t pad;
 };
 
 }  // namespace slosh

@@ -226,9 +226,56 @@ __device__ __forceinline__ uint32_t cta_exclusive_scan(const uint32_t *in, uint3
     return carry;
 }
 
+// Exclusive scan of n u32 by one CTA, each thread owning 16 consecutive
+// values read and written as four 16-byte vectors (in and out must be
+// 16-byte aligned).  Returns the total.
+template <int NT> __device__ __forceinline__ uint32_t cta_scan_vec16(const uint32_t *in, uint32_t *out, uint32_t n) {
+    constexpr uint32_t V = 16, TILE = NT * V;
+    __shared__ uint32_t tot;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < n; base += TILE) {
+        const uint32_t b = base + threadIdx.x * V;
+        uint32_t v[V];
+        if (b + V <= n) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint4 u = reinterpret_cast<const uint4 *>(in + b)[q];
+                v[4 * q] = u.x;
+                v[4 * q + 1] = u.y;
+                v[4 * q + 2] = u.z;
+                v[4 * q + 3] = u.w;
+            }
+        } else {
+#pragma unroll
+            for (uint32_t k = 0; k < V; ++k) v[k] = (b + k < n) ? in[b + k] : 0u;
+        }
+        uint32_t local = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) local += v[k];
+        uint32_t run = carry + block_exclusive_scan<NT>(local, &tot);
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) {
+            const uint32_t x = v[k];
+            v[k] = run;
+            run += x;
+        }
+        if (b + V <= n) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                reinterpret_cast<uint4 *>(out + b)[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (uint32_t k = 0; k < V; ++k)
+                if (b + k < n) out[b + k] = v[k];
+        }
+        carry += tot;
+    }
+    return carry;
+}
+
 // Exclusive scan of the key histogram (one CTA) and the final block count.
 template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) {
-    cta_exclusive_scan<NT, 8>(s.hist, s.hist_start, HIST_BINS);
+    cta_scan_vec16<NT>(s.hist, s.hist_start, HIST_BINS);
     if (threadIdx.x == 0) {
         const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
         if (total > s.cap) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
@@ -315,7 +362,7 @@ template <int D> __global__ void k_block_setup(DevScene s) {
 // (copy_particles_len_to_scan_value + prefix_sum +
 // copy_scan_values_to_first_particles, sort.slang:248-302).  One CTA.
 template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) {
-    cta_exclusive_scan<NT, 8>(s.bnp, s.bfirst, s.ctr->n_blocks);
+    cta_scan_vec16<NT>(s.bnp, s.bfirst, s.ctr->n_blocks);
 }
 
 // Per particle: claim its slot in the block's cell range (the primary part
@@ -338,61 +385,74 @@ __global__ void k_scatter(DevScene s) {
                 pos = s.bfirst[r] + atomicAdd(&s.bcur[(size_t)r * CELLS + (bin & 63u)], (uint32_t)__popc(peers));
         }
         pos = __shfl_sync(mask, pos, leader);
-        if (pos != NONE) s.perm_tmp[pos + __popc(peers & lanemask_lt())] = i;
+        if (pos != NONE) {
+            const uint32_t at = pos + __popc(peers & lanemask_lt());
+            if (at < s.n) s.perm[at] = i;
+            else atomicOr(s.err, ERR_BLOCK_OVERFLOW);  // stale counts after an earlier overflow
+        }
     }
 }
 
 // Orders each (block, cell) range of the permutation by original particle
-// id: the canonical order.  The scatter already groups a block's particles
-// by cell; each element's final place is its rank among the original ids of
-// its cell (a few particles per cell), found from shared memory.  perm holds
-// storage indices; the order key is oid[storage index].
-constexpr uint32_t CANON_SMEM = 4096;
-template <int NT> __global__ void __launch_bounds__(NT) k_canon(DevScene s) {
-    __shared__ uint32_t ids[CANON_SMEM];
-    __shared__ uint32_t keys[CANON_SMEM];
-    __shared__ uint32_t cstart[CELLS + 1];
+// id, in place: the canonical order.  One thread per (block, cell).  perm
+// holds storage indices and the order key is oid[storage index].  Storage is
+// already in the previous substep's canonical order, so the warp-aggregated
+// scatter usually leaves a cell sorted; unsorted cells get an insertion sort
+// (in registers up to 16 particles, in global memory beyond).
+constexpr int CANON_REG = 16;
+__global__ void k_canon_cells(DevScene s) {
     const uint32_t nb = s.ctr->n_blocks;
-    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * CELLS; t += stride) {
+        const uint32_t r = t >> 6, c = t & 63u;
         const uint32_t np = s.bnp[r];
-        if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
-        if (first + np > s.n) {  // only after an earlier overflow left stale counts
-            if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+        const uint32_t b0 = s.bcell[(size_t)r * CELLS + c];
+        const uint32_t b1 = (c < CELLS - 1) ? s.bcell[(size_t)r * CELLS + c + 1] : np;
+        if (b1 <= b0 + 1) continue;
+        if ((size_t)first + b1 > s.n) {  // only after an earlier overflow left stale counts
+            atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
         }
-        for (uint32_t c = threadIdx.x; c < CELLS; c += NT) cstart[c] = s.bcell[(size_t)r * CELLS + c];
-        if (threadIdx.x == 0) cstart[CELLS] = np;
-        const bool in_smem = np <= CANON_SMEM;
-        if (in_smem)
-            for (uint32_t e = threadIdx.x; e < np; e += NT) {
-                const uint32_t j = s.perm_tmp[first + e];
-                ids[e] = j;
-                keys[e] = s.oid[j];
-            }
-        __syncthreads();
-        for (uint32_t e = threadIdx.x; e < np; e += NT) {
-            // cell of entry e: last c with cstart[c] <= e (binary search)
-            uint32_t lo = 0, hi = CELLS;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (cstart[mid] <= e) lo = mid;
-                else hi = mid;
-            }
-            const uint32_t b0 = cstart[lo], b1 = cstart[lo + 1];
-            uint32_t rank = 0, id;
-            if (in_smem) {
-                id = ids[e];
-                const uint32_t key = keys[e];
-                for (uint32_t j = b0; j < b1; ++j) rank += (keys[j] < key) ? 1u : 0u;
-            } else {
-                id = s.perm_tmp[first + e];
-                const uint32_t key = s.oid[id];
-                for (uint32_t j = b0; j < b1; ++j) rank += (s.oid[s.perm_tmp[first + j]] < key) ? 1u : 0u;
-            }
-            s.perm[first + b0 + rank] = id;
+        uint32_t *seg = s.perm + first + b0;
+        const uint32_t m = b1 - b0;
+        bool sorted = true;
+        uint32_t prev = s.oid[seg[0]];
+        for (uint32_t j = 1; j < m; ++j) {
+            const uint32_t k = s.oid[seg[j]];
+            sorted = sorted && (prev < k);
+            prev = k;
         }
-        __syncthreads();
+        if (sorted) continue;
+        if (m <= (uint32_t)CANON_REG) {
+            uint32_t ids[CANON_REG], keys[CANON_REG];
+            for (uint32_t j = 0; j < m; ++j) {
+                ids[j] = seg[j];
+                keys[j] = s.oid[ids[j]];
+            }
+            for (uint32_t j = 1; j < m; ++j) {
+                const uint32_t ki = keys[j], ii = ids[j];
+                int q = (int)j - 1;
+                while (q >= 0 && keys[q] > ki) {
+                    keys[q + 1] = keys[q];
+                    ids[q + 1] = ids[q];
+                    --q;
+                }
+                keys[q + 1] = ki;
+                ids[q + 1] = ii;
+            }
+            for (uint32_t j = 0; j < m; ++j) seg[j] = ids[j];
+        } else {
+            for (uint32_t j = 1; j < m; ++j) {
+                const uint32_t ii = seg[j], ki = s.oid[ii];
+                int q = (int)j - 1;
+                while (q >= 0 && s.oid[seg[q]] > ki) {
+                    seg[q + 1] = seg[q];
+                    --q;
+                }
+                seg[q + 1] = ii;
+            }
+        }
     }
 }
 

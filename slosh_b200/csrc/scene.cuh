@@ -40,6 +40,12 @@ struct DevScene {
     uint32_t *hvals;       // current substep hash map: canonical block rank
     const uint32_t *prev_hkeys;
     const uint32_t *prev_hvals;
+    // The previous substep's map is the next substep's current map: the
+    // fused G2P/update clears it (and the key histogram) once k_grid_update,
+    // its last reader, has run.
+    uint32_t *clr_hkeys;
+    uint32_t *clr_hvals;
+    uint32_t clear_tail;
     uint32_t *slot_counts; // hcap * 64 per-cell particle counts per hash slot
     uint32_t *blist_key;   // primary blocks in append order [cap]
     uint32_t *blist_slot;
@@ -58,8 +64,7 @@ struct DevScene {
     uint32_t *bcur;        // 64 per block: insertion cursors, relative to bfirst
     uint32_t *bnbh;        // (NASSOC - 1) neighbour ranks per block, NONE if inactive
     uint32_t *pslot;       // per particle: (hash slot << 6) | cell
-    uint32_t *perm_tmp;    // scatter output
-    uint32_t *perm;        // canonical primary order
+    uint32_t *perm;        // primary order: scatter output, canonicalised in place
     float4 *nodes;         // 64 nodes per block: (momentum | velocity, mass)
     float4 *coll;          // node collision cache of this substep: (normal, d0)
     uint32_t *coll_id;     // collider id or NONE

@@ -49,7 +49,7 @@ struct slosh_ctx {
     // 0 direct cell-owner (default), 1 "atomic" per-particle shared atomics,
     // 2 "staged" shared-memory staging with a fixed-order reduction.
     int p2g_variant = 0;
-    uint32_t *pslot = nullptr, *perm_tmp = nullptr, *perm = nullptr;
+    uint32_t *pslot = nullptr, *perm = nullptr;
     float4 *nodes = nullptr, *coll[2] = {nullptr, nullptr};
     uint32_t *coll_id[2] = {nullptr, nullptr};
 
@@ -166,7 +166,6 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.bcur = c->bcur;
     s.bnbh = c->bnbh;
     s.pslot = c->pslot;
-    s.perm_tmp = c->perm_tmp;
     s.perm = c->perm;
     s.nodes = c->nodes;
     s.coll = c->coll[cur];
@@ -177,6 +176,9 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.n_bodies = c->n_bodies;
     s.ctr = c->ctr;
     s.err = c->err;
+    s.clr_hkeys = c->hkeys[prv];
+    s.clr_hvals = c->hvals[prv];
+    s.clear_tail = 1u;
     return s;
 }
 
@@ -186,11 +188,10 @@ uint32_t grid_for(uint64_t work, uint32_t threads, uint32_t max_ctas) {
 }
 
 // Kernels of one substep, in launch order (profiling names).
-constexpr int N_KERNELS = 14;
+constexpr int N_KERNELS = 13;
 const char *const KERNEL_NAMES[N_KERNELS] = {
-    "k_clear",       "k_touch",      "k_neighbors", "k_hist_scan", "k_bin_scatter", "k_rank",
-    "k_block_setup", "k_block_scan", "k_scatter",   "k_canon",     "k_p2g",         "k_grid_update",
-    "k_g2p_update",  "k_rigid"};
+    "k_touch",      "k_neighbors", "k_hist_scan", "k_bin_scatter", "k_rank",        "k_block_setup", "k_block_scan",
+    "k_scatter",    "k_canon",     "k_p2g",       "k_grid_update", "k_g2p_update",  "k_rigid"};
 
 // Optional per-kernel CUDA-event timing of the substep launches.
 struct Prof {
@@ -210,43 +211,44 @@ struct Prof {
     if (p) p->end(k)
 
 // Grid build of one substep (stages shared by the substep and the debug
-// entry points).
-template <int D> void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
+// entry points).  Within a substep sequence the hash map, key histogram and
+// counters were cleared by the previous substep's last kernels (or by the
+// upload); a standalone build (debug entry points) clears them first.
+template <int D>
+void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr, bool standalone = false) {
     const uint32_t sm = (uint32_t)c->sm_count;
+    if (standalone) k_clear<<<sm * 4, 256, 0, st>>>(s);
     PROF_BEGIN(0);
-    k_clear<<<sm * 4, 256, 0, st>>>(s);
+    k_touch<D><<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(0);
     PROF_BEGIN(1);
-    k_touch<D><<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
+    k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(1);
     PROF_BEGIN(2);
-    k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
+    k_hist_scan<1024><<<1, 1024, 0, st>>>(s);
     PROF_END(2);
     PROF_BEGIN(3);
-    k_hist_scan<1024><<<1, 1024, 0, st>>>(s);
+    k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(3);
     PROF_BEGIN(4);
-    k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    k_rank<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(4);
     PROF_BEGIN(5);
-    k_rank<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    k_block_setup<D><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(5);
     PROF_BEGIN(6);
-    k_block_setup<D><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     PROF_END(6);
     PROF_BEGIN(7);
-    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
+    k_scatter<<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(7);
     PROF_BEGIN(8);
-    k_scatter<<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
+    k_canon_cells<<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(8);
-    PROF_BEGIN(9);
-    k_canon<128><<<std::min<uint32_t>(c->cap, sm * 8), 128, 0, st>>>(s);
-    PROF_END(9);
 }
 
 template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
-    PROF_BEGIN(10);
+    PROF_BEGIN(9);
     const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
     if (c->p2g_variant == 1)
         k_p2g_atomic<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
@@ -254,13 +256,19 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
         k_p2g_staged<D><<<g, P2G_THREADS, 0, st>>>(s);
     else
         k_p2g<D><<<g, P2G_THREADS, 0, st>>>(s);
-    PROF_END(10);
+    PROF_END(9);
 }
 
 template <int D> void enqueue_grid_update(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
-    PROF_BEGIN(11);
+    PROF_BEGIN(10);
     k_grid_update<D><<<grid_for((uint64_t)c->cap * 64, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s);
-    PROF_END(11);
+    PROF_END(10);
+}
+
+// Restores the cleared state a debug build consumed, so that the next real
+// substep starts from a cleared hash map and counters.
+void enqueue_clear(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
+    k_clear<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
 }
 
 template <int D>
@@ -269,14 +277,12 @@ void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force,
     enqueue_grid_build<D>(c, s, st, p);
     enqueue_p2g<D>(c, s, st, p);
     enqueue_grid_update<D>(c, s, st, p);
-    PROF_BEGIN(12);
+    PROF_BEGIN(11);
     k_g2p_update<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), 128, 0, st>>>(s);
+    PROF_END(11);
+    PROF_BEGIN(12);
+    k_rigid<D><<<1, 32, 0, st>>>(s);
     PROF_END(12);
-    if (c->n_bodies > 0) {
-        PROF_BEGIN(13);
-        k_rigid<D><<<1, 32, 0, st>>>(s);
-        PROF_END(13);
-    }
 }
 
 void enqueue_substep_any(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force, Prof *p = nullptr) {
@@ -391,7 +397,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) ||
-        (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm_tmp, N)) || (st = dalloc(c, &c->perm, N)) ||
+        (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||
         (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, MAX_BODIES)) ||
@@ -452,6 +458,8 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
         CK(cudaMemsetAsync(c->hvals[k], 0xff, c->hcap * 4, st));
     }
     CK(cudaMemsetAsync(c->slot_counts, 0, (size_t)c->hcap * CELLS * 4, st));
+    CK(cudaMemsetAsync(c->hist, 0, HIST_BINS * 4, st));
+    CK(cudaMemsetAsync(c->hist_fill, 0, HIST_BINS * 4, st));
     c->parity = 0;
     if (n > 0) {
         DevScene s = make_scene(c, 0, false);
@@ -596,7 +604,7 @@ int slosh_sync(slosh_ctx *c, void *stream) {
 
 uint32_t slosh_kernels_per_substep(const slosh_ctx *c) {
     if (!c) return 0;
-    return 13u + (c->n_bodies > 0 ? 1u : 0u);
+    return (uint32_t)N_KERNELS;
 }
 
 int slosh_profile_substeps(slosh_ctx *c, uint32_t n_substeps, void *stream, float *kernel_ms, uint32_t cap,
@@ -617,8 +625,7 @@ int slosh_profile_substeps(slosh_ctx *c, uint32_t n_substeps, void *stream, floa
         enqueue_substep_any(c, pr.st, c->parity, c->force_pending != 0, &pr);
         c->force_pending = 0;
         c->parity ^= 1u;
-        cudaError_t e = cudaEventSynchronize(pr.ev[12][1]);
-        if (e == cudaSuccess && c->n_bodies > 0) e = cudaEventSynchronize(pr.ev[13][1]);
+        cudaError_t e = cudaEventSynchronize(pr.ev[N_KERNELS - 1][1]);
         if (e != cudaSuccess) {
             rc = fail(c, SLOSH_E_CUDA, "profiling: %s", cudaGetErrorString(e));
             break;
@@ -649,8 +656,8 @@ int slosh_get_stats(slosh_ctx *c, slosh_stats *out) {
     CK(cudaMemcpy(&ctr, c->ctr, sizeof(ctr), cudaMemcpyDeviceToHost));
     std::memset(out, 0, sizeof(*out));
     out->n_particles = c->n;
-    out->n_blocks = ctr.n_blocks;
-    out->n_primary_blocks = std::min(ctr.n_primary, c->cap);
+    out->n_blocks = ctr.last_n_blocks;
+    out->n_primary_blocks = ctr.last_n_primary;
     out->n_materials = c->n_materials;
     out->n_svd_fp64 = ctr.n_svd_fp64;
     return SLOSH_OK;
@@ -668,14 +675,19 @@ int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, u
     CK(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     const DevScene s = make_scene(c, c->parity, false);
-    if (c->dim == 3) enqueue_grid_build<3>(c, s, st);
-    else enqueue_grid_build<2>(c, s, st);
+    if (c->dim == 3) enqueue_grid_build<3>(c, s, st, nullptr, true);
+    else enqueue_grid_build<2>(c, s, st, nullptr, true);
     CK(cudaGetLastError());
     Counters ctr;
     CK(cudaMemcpyAsync(&ctr, c->ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    int e = check_device_error(c);
-    if (e) return e;
+    uint32_t err_bits = 0;
+    CK(cudaMemcpy(&err_bits, c->err, 4, cudaMemcpyDeviceToHost));
+    if (err_bits) {
+        enqueue_clear(c, s, st);
+        CK(cudaStreamSynchronize(st));
+        return check_device_error(c);
+    }
     const uint32_t nb = ctr.n_blocks;
     const int NB = nbk(c->dim), NN = nnb(c->dim);
     dump->n_blocks = nb;
@@ -732,6 +744,8 @@ int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, u
     copy(dump->primary_perm, perm_oid, c->n);
     copy(dump->neighbors, c->bnbh, (size_t)nbc * NN);
     cudaFree(blob);
+    enqueue_clear(c, s, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) return fail(c, SLOSH_E_CUDA, "grid debug: %s", cudaGetErrorString(ce));
     if (total > cap_entries) return fail(c, SLOSH_E_CAPACITY, "debug layout overflow");
     return SLOSH_OK;
@@ -744,11 +758,11 @@ int slosh_debug_nodes(slosh_ctx *c, int stage, float *nodes, uint32_t cap_blocks
     cudaStream_t st = c->stream;
     const DevScene s = make_scene(c, c->parity, c->force_pending != 0);
     if (c->dim == 3) {
-        enqueue_grid_build<3>(c, s, st);
+        enqueue_grid_build<3>(c, s, st, nullptr, true);
         enqueue_p2g<3>(c, s, st);
         if (stage >= 2) enqueue_grid_update<3>(c, s, st);
     } else {
-        enqueue_grid_build<2>(c, s, st);
+        enqueue_grid_build<2>(c, s, st, nullptr, true);
         enqueue_p2g<2>(c, s, st);
         if (stage >= 2) enqueue_grid_update<2>(c, s, st);
     }
@@ -759,6 +773,8 @@ int slosh_debug_nodes(slosh_ctx *c, int stage, float *nodes, uint32_t cap_blocks
     if (n_blocks) *n_blocks = ctr.n_blocks;
     const uint32_t nbc = std::min(ctr.n_blocks, cap_blocks);
     if (nodes && nbc) CK(cudaMemcpy(nodes, c->nodes, (size_t)nbc * 64 * 16, cudaMemcpyDeviceToHost));
+    enqueue_clear(c, s, st);
+    CK(cudaStreamSynchronize(st));
     return check_device_error(c);
 }
 

@@ -364,13 +364,20 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g_staged(Dev
 // instruction never hits the same node twice), and the tile is added to the
 // global nodes of the block and its +1 neighbours with 16-byte atomics.  Two
 // barriers per block; no staging.
-template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s) {
+template <int D> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
+    constexpr int NT = P2G_THREADS;
     __shared__ float tile[4][TILE];
+    // per-thread double buffer: the next particle of the cell is copied in
+    // (cp.async) while the current one is accumulated
+    __shared__ float4 sp_pm[2][NT];
+    __shared__ float sp_v[2][D][NT];
+    __shared__ float sp_c[2][D * D][NT];
     const uint32_t nb = s.ctr->n_blocks;
     const float h = s.h, inv_h = 1.0f / s.h;
     const size_t n = s.n;
+    const uint32_t tid = threadIdx.x;
     const int mycell = (int)(threadIdx.x & 63u), myslab = (int)(threadIdx.x >> 6);
     int ca[D];
     if constexpr (D == 3) {
@@ -401,10 +408,25 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s
         float4 acc[NACC];
 #pragma unroll
         for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        auto stage = [&](int b, uint32_t j) {
+            if (j < hi) {
+                const uint32_t i = s.perm[first + j];
+                cp_async16(&sp_pm[b][tid], &s.pm[i]);
+#pragma unroll
+                for (int k = 0; k < D; ++k) cp_async4(&sp_v[b][k][tid], &s.vel[k * n + i]);
+#pragma unroll
+                for (int q = 0; q < D * D; ++q) cp_async4(&sp_c[b][q][tid], &s.C[q * n + i]);
+            }
+            cp_async_commit();
+        };
+        stage(0, lo);
         __syncthreads();
-        for (uint32_t j = lo; j < hi; ++j) {
-            const uint32_t i = s.perm[first + j];
-            const float4 p = s.pm[i];
+        int buf = 0;
+        for (uint32_t j = lo; j < hi; ++j, buf ^= 1) {
+            stage(buf ^ 1, j + 1);
+            cp_async_wait<1>();
+            const uint32_t i = s.force_pending ? s.perm[first + j] : 0u;
+            const float4 p = sp_pm[buf][tid];
             const float x[3] = {p.x, p.y, p.z};
             const float m = p.w;
             float d0[D], w[D][3];
@@ -423,11 +445,11 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s
             float bm[D], hc[D][D];
 #pragma unroll
             for (int jj = 0; jj < D; ++jj) {
-                float q = s.vel[jj * n + i] * m;
+                float q = sp_v[buf][jj][tid] * m;
                 if (s.force_pending) q += s.fdt[jj * n + i];
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
-                    const float c = s.C[(jj * D + k) * n + i];
+                    const float c = sp_c[buf][jj * D + k][tid];
                     q += c * d0[k];
                     hc[k][jj] = h * c;
                 }
@@ -464,6 +486,7 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g(DevScene s
                 }
             }
         }
+        cp_async_wait<0>();
         if (hi > lo) {
 #pragma unroll
             for (int k = 0; k < NACC; ++k) {
@@ -720,18 +743,65 @@ template <int D> __global__ void k_grid_update(DevScene s) {
 // shared memory, then each thread gathers v, grad v and div v for its
 // particles (g2p.slang:150-265) and applies the particle update of
 // particle_update.slang:48-159 with the constitutive model, writing the new
-// position, velocity, APIC matrix C and F.
+// position, velocity, APIC matrix C and F.  The inputs of a thread's next
+// particle (x, m, F, V0, flags, original id, plastic state, damping) are
+// staged into shared memory with cp.async while the current particle is
+// computed; each thread consumes only its own staged slot, so the particle
+// loop has no barrier.
 template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float tv[D][TILE];
+    __shared__ float4 st_pm[2][NT];
+    __shared__ float st_F[2][D * D][NT];
+    __shared__ float st_pl[2][3][NT];
+    __shared__ float st_v0[2][NT];
+    __shared__ float st_dmp[2][NT];
+    __shared__ uint32_t st_fl[2][NT];
+    __shared__ uint32_t st_oid[2][NT];
     const uint32_t nb = s.ctr->n_blocks;
     const float h = s.h, dt = s.dt;
     const float inv_d = 4.0f / (h * h);
     const float vmax = h / dt;
     const size_t n = s.n;
+    const uint32_t tid = threadIdx.x;
+    if (s.clear_tail) {
+        // Clear the next substep's hash map and the key histogram (their
+        // readers in this substep have all run).
+        const uint32_t g0 = blockIdx.x * NT + tid, gs = gridDim.x * NT;
+        for (uint32_t q = g0; q < s.hcap; q += gs) {
+            s.clr_hkeys[q] = NONE;
+            s.clr_hvals[q] = NONE;
+        }
+        for (uint32_t q = g0; q < HIST_BINS; q += gs) {
+            s.hist[q] = 0u;
+            s.hist_fill[q] = 0u;
+        }
+        if (*s.err != 0u)
+            for (size_t q = g0; q < (size_t)s.hcap * CELLS; q += gs) s.slot_counts[q] = 0u;
+    }
+    // Issues the copies of sorted entry e of the block into buffer b (an
+    // empty group when e is past the block's particles).
+    auto stage = [&](int b, uint32_t first, uint32_t e, uint32_t np) {
+        if (e < np) {
+            const uint32_t i = s.perm[first + e];
+            cp_async16(&st_pm[b][tid], &s.pm[i]);
+#pragma unroll
+            for (int q = 0; q < D * D; ++q) cp_async4(&st_F[b][q][tid], &s.F[q * n + i]);
+            cp_async4(&st_v0[b][tid], &s.V0[i]);
+            cp_async4(&st_fl[b][tid], &s.flags[i]);
+            cp_async4(&st_oid[b][tid], &s.oid[i]);
+            if (s.has_sand)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) cp_async4(&st_pl[b][q][tid], &s.plastic[q * n + i]);
+            if (s.has_damping) cp_async4(&st_dmp[b][tid], &s.damping[i]);
+        }
+        cp_async_commit();
+    };
     for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
+        const uint32_t first = s.bfirst[r];
+        stage(0, first, tid, np);
         for (int t = threadIdx.x; t < TILE; t += NT) {
             uint32_t rank, local;
             float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -743,13 +813,14 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(D
         __syncthreads();
         int bv[D];
         unpack_key<D>(s.bkey[r], bv);
-        const uint32_t first = s.bfirst[r];
-        for (uint32_t e = threadIdx.x; e < np; e += NT) {
-            const uint32_t i = s.perm[first + e];
-            const float4 p = s.pm[i];
+        int buf = 0;
+        for (uint32_t e = tid; e < np; e += NT, buf ^= 1) {
+            stage(buf ^ 1, first, e + NT, np);
+            cp_async_wait<1>();
+            const float4 p = st_pm[buf][tid];
             const float x[3] = {p.x, p.y, p.z};
             float m = p.w;
-            uint32_t fl = s.flags[i];
+            uint32_t fl = st_fl[buf][tid];
             // ---- G2P ----
             float vel[D], grad[D][D], div = 0.f;
 #pragma unroll
@@ -853,7 +924,7 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(D
 #pragma unroll
                 for (int k = 0; k < D; ++k) vel[k] = vel[k] / len * h / dt;
             if (s.has_damping) {
-                const float dmp = 1.0f + s.damping[i] * dt;
+                const float dmp = 1.0f + st_dmp[buf][tid] * dt;
 #pragma unroll
                 for (int k = 0; k < D; ++k) vel[k] = vel[k] / dmp;
             }
@@ -868,7 +939,7 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(D
 #pragma unroll
             for (int rr = 0; rr < D; ++rr)
 #pragma unroll
-                for (int c = 0; c < D; ++c) F[rr][c] = s.F[(rr * D + c) * n + i];
+                for (int c = 0; c < D; ++c) F[rr][c] = st_F[buf][rr * D + c][tid];
             if (!fluid) {
                 float Fn[D][D];
 #pragma unroll
@@ -900,10 +971,10 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(D
             float st[3] = {0.f, 0.f, 0.f};
             if (sand)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) st[k] = s.plastic[k * n + i];
+                for (int k = 0; k < 3; ++k) st[k] = st_pl[buf][k][tid];
             float tau[D][D];
             model_update<D>(mat, F, st, tau, &s.ctr->n_svd_fp64);
-            const float v0 = s.V0[i];
+            const float v0 = st_v0[buf][tid];
             const float coef = v0 * inv_d * dt;
             bool finite = true;
 #pragma unroll
@@ -946,11 +1017,12 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(D
             if (s.has_sand)
 #pragma unroll
                 for (int k = 0; k < 3; ++k) s.out_plastic[k * n + o] = st[k];
-            if (s.has_damping) s.out_damping[o] = s.damping[i];
+            if (s.has_damping) s.out_damping[o] = st_dmp[buf][tid];
             s.out_flags[o] = fl;
             s.out_V0[o] = v0;
-            s.out_oid[o] = s.oid[i];
+            s.out_oid[o] = st_oid[buf][tid];
         }
+        cp_async_wait<0>();
         __syncthreads();
     }
 }
@@ -959,8 +1031,17 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(D
 // integrate_velocity (shaders/slosh/rbd/dynamics/body.slang:117-130).  The
 // incremental impulse slosh applies here is never written by any of its
 // kernels, so velocity capping (guarded by a non-zero impulse) never runs.
+// The last kernel of the substep: it also resets the grid-build counters for
+// the next substep.
 template <int D> __global__ void k_rigid(DevScene s) {
     const uint32_t id = threadIdx.x;
+    if (id == 0 && s.clear_tail) {
+        s.ctr->last_n_blocks = s.ctr->n_blocks;
+        s.ctr->last_n_primary = min(s.ctr->n_primary, s.cap);
+        s.ctr->n_primary = 0u;
+        s.ctr->n_extra = 0u;
+        s.ctr->n_blocks = 0u;
+    }
     if (id >= s.n_bodies) return;
     DevBody b = s.bodies[id];
     const float dt = s.dt;
