@@ -98,11 +98,19 @@ template <int D> struct CellLoc {
     int local[D];
 };
 
-template <int D> __device__ __forceinline__ CellLoc<D> locate(const float *x, float h) {
+// x / h, correctly rounded.  When h is a power of two its reciprocal is
+// exact and x * (1/h) is the same correctly rounded quotient, so the IEEE
+// division is replaced by a multiplication without changing any bit.
+__device__ __forceinline__ float div_h(float x, float h, float inv_h, uint32_t h_pow2) {
+    return h_pow2 ? x * inv_h : __fdiv_rn(x, h);
+}
+
+template <int D>
+__device__ __forceinline__ CellLoc<D> locate(const float *x, float h, float inv_h, uint32_t h_pow2) {
     CellLoc<D> c;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        float assoc = rintf(__fdiv_rn(x[k], h)) - 1.0f;
+        float assoc = rintf(div_h(x[k], h, inv_h, h_pow2)) - 1.0f;
         float ab = floorf(assoc * (1.0f / Geo<D>::BW));
         c.block[k] = (int)ab;
         c.local[k] = (int)(assoc - ab * (float)Geo<D>::BW);

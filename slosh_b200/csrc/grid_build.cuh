@@ -105,7 +105,7 @@ template <int D> __global__ void k_touch(DevScene s) {
         if (!valid) continue;
         const float4 p = s.pm[i];
         const float x[3] = {p.x, p.y, p.z};
-        const CellLoc<D> c = locate<D>(x, s.h);
+        const CellLoc<D> c = locate<D>(x, s.h, s.inv_h, s.h_pow2);
         const uint32_t key = pack_key<D>(c.block);
         const uint32_t cell = cell_index<D>(c.local);
         const unsigned peers = __match_any_sync(mask, key);
@@ -318,9 +318,9 @@ __global__ void k_rank(DevScene s) {
 }
 
 // One warp per block: per-cell counts (cleared in the hash-slot array once
-// read) with their in-block exclusive scan, the block total, the neighbour
-// ranks (update_nbh_block_ids, sort.slang:100-117) and zeroed nodes (reset,
-// grid.slang:455-485).
+// read) with their in-block exclusive scan, the block total, the +1 and -1
+// neighbour ranks (update_nbh_block_ids, sort.slang:100-117) and, for the
+// atomic P2G variants, zeroed nodes (reset, grid.slang:455-485).
 template <int D> __global__ void k_block_setup(DevScene s) {
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t nb = s.ctr->n_blocks;
@@ -345,15 +345,23 @@ template <int D> __global__ void k_block_setup(DevScene s) {
         s.bcur[(size_t)r * CELLS + 2 * lane] = ex;
         s.bcur[(size_t)r * CELLS + 2 * lane + 1] = ex + c0;
         if (lane == 31) s.bnp[r] = incl;
-        s.nodes[(size_t)r * 64 + 2 * lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-        s.nodes[(size_t)r * 64 + 2 * lane + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (lane < (uint32_t)NN) {
+        if (!s.use_partial) {  // the atomic P2G variants accumulate into the nodes
+            s.nodes[(size_t)r * 64 + 2 * lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s.nodes[(size_t)r * 64 + 2 * lane + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        // lanes [0, NN): the +1 neighbours b + o; lanes [NN, 2 NN): the -1
+        // neighbours b - o, whose P2G tiles overlap this block.
+        if (lane < (uint32_t)(2 * NN)) {
+            const bool fwd = lane < (uint32_t)NN;
+            const int q = fwd ? (int)lane : (int)lane - NN;
             int b[D], o[D];
             unpack_key<D>(s.bkey[r], b);
-            assoc_offset<D>((int)lane + 1, o);
-            for (int k = 0; k < D; ++k) b[k] += o[k];
+            assoc_offset<D>(q + 1, o);
+            for (int k = 0; k < D; ++k) b[k] += fwd ? o[k] : -o[k];
             const uint32_t slot = hash_find(s.hkeys, s.hcap, pack_key<D>(b));
-            s.bnbh[r * NN + lane] = (slot == NONE) ? NONE : s.hvals[slot];
+            const uint32_t rank = (slot == NONE) ? NONE : s.hvals[slot];
+            if (fwd) s.bnbh[r * NN + q] = rank;
+            else s.bnbh_rev[r * NN + q] = rank;
         }
     }
 }

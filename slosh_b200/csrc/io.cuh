@@ -211,7 +211,7 @@ template <int D>
 __device__ __forceinline__ bool particle_rank_local(const DevScene &s, uint32_t i, uint32_t &r0, int *a) {
     const float4 p = s.pm[i];
     const float x[3] = {p.x, p.y, p.z};
-    const CellLoc<D> c = locate<D>(x, s.h);
+    const CellLoc<D> c = locate<D>(x, s.h, s.inv_h, s.h_pow2);
     const uint32_t slot = hash_find(s.hkeys, s.hcap, pack_key<D>(c.block));
     if (slot == NONE) return false;
     r0 = s.hvals[slot];
@@ -301,7 +301,7 @@ __device__ __forceinline__ uint64_t dbg_order_key(const DevScene &s, uint32_t j,
     if (b >= (uint32_t)Geo<D>::NPB) return s.oid[j];
     const float4 p = s.pm[j];
     const float x[3] = {p.x, p.y, p.z};
-    const CellLoc<D> c = locate<D>(x, s.h);
+    const CellLoc<D> c = locate<D>(x, s.h, s.inv_h, s.h_pow2);
     return ((uint64_t)cell_index<D>(c.local) << 32) | s.oid[j];
 }
 

@@ -13,6 +13,8 @@ struct DevScene {
     // writes the `out_*` arrays in this substep's canonical order.
     uint32_t n;            // particle count
     float h;               // cell width
+    float inv_h;           // 1 / h (exact when h_pow2)
+    uint32_t h_pow2;       // h is a power of two
     float dt;
     float gravity[3];
     float4 *pm;            // (x, y, z, mass); 2D: (x, y, 0, mass)
@@ -65,7 +67,11 @@ struct DevScene {
     uint32_t *bnbh;        // (NASSOC - 1) neighbour ranks per block, NONE if inactive
     uint32_t *pslot;       // per particle: (hash slot << 6) | cell
     uint32_t *perm;        // primary order: scatter output, canonicalised in place
+    uint32_t *bnbh_rev;    // (NASSOC - 1) ranks of the blocks b - o (the -1 neighbours), NONE if inactive
     float4 *nodes;         // 64 nodes per block: (momentum | velocity, mass)
+    float4 *partial;       // TILE nodes per block: the block's own P2G sums over its (block + 2)^D tile
+    uint32_t use_partial;  // P2G wrote `partial` (deterministic path); grid update gathers it
+    uint32_t gather_only;  // grid update stops after the gather (P2G node sums, debug)
     float4 *coll;          // node collision cache of this substep: (normal, d0)
     uint32_t *coll_id;     // collider id or NONE
     const float4 *prev_coll;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -44,13 +45,14 @@ struct slosh_ctx {
     uint32_t *slot_counts = nullptr, *blist_key = nullptr, *blist_slot = nullptr, *blist2_key = nullptr,
              *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_fill = nullptr, *tmp_key = nullptr,
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
-             *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr;
+             *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr, *bnbh_rev = nullptr;
     // P2G variant for A/B measurements (environment SLOSH_P2G at creation):
-    // 0 direct cell-owner (default), 1 "atomic" per-particle shared atomics,
-    // 2 "staged" shared-memory staging with a fixed-order reduction.
+    // 0 cell-owner with the fixed-order (bit-reproducible) reduction
+    // (default), 1 "atomic" per-particle shared atomics, 2 "staged"
+    // shared-memory staging, 3 "direct" cell-owner with float atomics.
     int p2g_variant = 0;
     uint32_t *pslot = nullptr, *perm = nullptr;
-    float4 *nodes = nullptr, *coll[2] = {nullptr, nullptr};
+    float4 *nodes = nullptr, *partial = nullptr, *coll[2] = {nullptr, nullptr};
     uint32_t *coll_id[2] = {nullptr, nullptr};
 
     DevBody *bodies = nullptr;
@@ -115,6 +117,11 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     DevScene s{};
     s.n = c->n;
     s.h = c->h;
+    s.inv_h = 1.0f / c->h;
+    {
+        int ex = 0;
+        s.h_pow2 = (std::frexp(c->h, &ex) == 0.5f) ? 1u : 0u;
+    }
     s.dt = c->params.dt;
     for (int k = 0; k < 3; ++k) s.gravity[k] = c->params.gravity[k];
     const slosh_ctx::Storage &A = c->pb[parity & 1u], &B = c->pb[(parity & 1u) ^ 1u];
@@ -165,9 +172,13 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.bcell = c->bcell;
     s.bcur = c->bcur;
     s.bnbh = c->bnbh;
+    s.bnbh_rev = c->bnbh_rev;
     s.pslot = c->pslot;
     s.perm = c->perm;
     s.nodes = c->nodes;
+    s.partial = c->partial;
+    s.use_partial = (c->p2g_variant == 0) ? 1u : 0u;
+    s.gather_only = 0u;
     s.coll = c->coll[cur];
     s.coll_id = c->coll_id[cur];
     s.prev_coll = c->coll[prv];
@@ -254,8 +265,10 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
         k_p2g_atomic<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
     else if (c->p2g_variant == 2)
         k_p2g_staged<D><<<g, P2G_THREADS, 0, st>>>(s);
+    else if (c->p2g_variant == 3)
+        k_p2g<D, false><<<g, P2G_THREADS, 0, st>>>(s);
     else
-        k_p2g<D><<<g, P2G_THREADS, 0, st>>>(s);
+        k_p2g<D, true><<<g, P2G_THREADS, 0, st>>>(s);
     PROF_END(9);
 }
 
@@ -396,7 +409,8 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) || (st = dalloc(c, &c->bkey, cap)) ||
         (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
-        (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) ||
+        (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
+        (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||
         (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
@@ -416,6 +430,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     if (const char *variant = std::getenv("SLOSH_P2G")) {
         if (std::strcmp(variant, "atomic") == 0) c->p2g_variant = 1;
         else if (std::strcmp(variant, "staged") == 0) c->p2g_variant = 2;
+        else if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;
     }
     if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     c->params.gravity[1] = -9.81f;
@@ -757,14 +772,18 @@ int slosh_debug_nodes(slosh_ctx *c, int stage, float *nodes, uint32_t cap_blocks
     CK(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     const DevScene s = make_scene(c, c->parity, c->force_pending != 0);
+    DevScene gather = s;  // stage 1 of the deterministic P2G: node sums only
+    gather.gather_only = 1u;
     if (c->dim == 3) {
         enqueue_grid_build<3>(c, s, st, nullptr, true);
         enqueue_p2g<3>(c, s, st);
         if (stage >= 2) enqueue_grid_update<3>(c, s, st);
+        else if (s.use_partial) enqueue_grid_update<3>(c, gather, st);
     } else {
         enqueue_grid_build<2>(c, s, st, nullptr, true);
         enqueue_p2g<2>(c, s, st);
         if (stage >= 2) enqueue_grid_update<2>(c, s, st);
+        else if (s.use_partial) enqueue_grid_update<2>(c, gather, st);
     }
     CK(cudaGetLastError());
     Counters ctr;

@@ -26,13 +26,14 @@
 namespace slosh {
 
 // Per-precision helpers.  The Jacobi angle only steers convergence: any t
-// yields an exactly orthogonal rotation (c = 1/sqrt(1+t^2), s = t c), so the
-// FP32 path takes approximate reciprocals there.  EPS is the relative
+// yields an orthogonal rotation (c = 1/sqrt(1+t^2), s = t c), so the FP32
+// path takes approximate reciprocals and square roots there.  EPS is the relative
 // off-diagonal size at which a sweep stops (near the rounding floor of A).
 template <typename T> struct SvdT;
 template <> struct SvdT<float> {
     static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
-    static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+    // only used on theta^2 + 1 >= 1, where x rsqrt(x) is finite
+    static __device__ __forceinline__ float sqrt_(float x) { return x * rsqrtf(x); }
     static __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
     static constexpr int SWEEPS = 5;
     static constexpr float TINY = 1e-30f;

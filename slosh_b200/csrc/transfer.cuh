@@ -66,11 +66,11 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g_atomic(DevS
             bool in_block = true;
 #pragma unroll
             for (int k = 0; k < D; ++k) {
-                const float assoc = rintf(__fdiv_rn(x[k], h)) - 1.0f;
+                const float assoc = rintf(div_h(x[k], h, s.inv_h, s.h_pow2)) - 1.0f;
                 a[k] = (int)assoc - bv[k] * BW;
                 in_block = in_block && a[k] >= 0 && a[k] < BW;
                 d0[k] = assoc * h - x[k];
-                bspline_weights(__fdiv_rn(-d0[k], h), w[k]);
+                bspline_weights(div_h(-d0[k], h, s.inv_h, s.h_pow2), w[k]);
             }
             if (!in_block) {  // packed-key aliasing far outside the key range
                 atomicOr(s.err, ERR_KEY_RANGE);
@@ -223,7 +223,7 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g_staged(Dev
                 bool in_block = true;
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
-                    const float assoc = rintf(__fdiv_rn(x[k], h)) - 1.0f;
+                    const float assoc = rintf(div_h(x[k], h, s.inv_h, s.h_pow2)) - 1.0f;
                     const int a = (int)assoc - bv[k] * BW;
                     in_block = in_block && a >= 0 && a < BW;
                     d0[k] = assoc * h - x[k];
@@ -350,7 +350,7 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g_staged(Dev
     }
 }
 
-// Particle-to-grid, direct cell-owner variant (default).
+// Particle-to-grid, direct cell-owner kernel.
 //
 // One CTA of 192 threads per active block with primaries; thread (cell c,
 // slab) owns cell c and the 9 (3D) or 3 (2D) stencil offsets of one slab.
@@ -359,16 +359,35 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g_staged(Dev
 // in registers.  The cell comes from the sort, so the base node position is
 // exact and no division is needed: d0 = (block origin + cell) h - x, and the
 // weights use -d0 / h = -d0 * (1/h) like slosh's p2g (dpt * inv_cell_width).
-// The per-thread sums are added to a shared (block + 2)^D tile with
-// shared-memory atomics (the lanes of a warp own distinct cells, so one
-// instruction never hits the same node twice), and the tile is added to the
-// global nodes of the block and its +1 neighbours with 16-byte atomics.  Two
-// barriers per block; no staging.
-template <int D> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScene s) {
+//
+// DET (default): the per-thread sums are reduced in a fixed order, so the
+// whole substep is bit-reproducible.  Each slab has its own (block + 2)^D
+// tile in shared memory; the 9 (3) offsets of a slab are added in 9 (3)
+// phases, one offset per phase, and since all contributors of a slab-tile
+// node lie in one warp (same cell z in 3D, same cell row group in 2D) the
+// phases only need __syncwarp.  The three slab tiles are then summed in slab
+// order and the block's tile is stored to its own `partial` slot with plain
+// stores; k_grid_update adds the (up to 2^D) tiles overlapping each node in
+// a fixed order.  Without DET the sums go through shared-memory atomics and
+// 16-byte global atomics into the nodes (kept for comparison).
+// Slab-tile layout of the deterministic reduction: pitches chosen so that a
+// quarter-warp's 16-byte accesses hit distinct bank groups (3D: x 1, y 12,
+// z 72; 2D: x 1, y 10).
+template <int D> struct SlabTile;
+template <> struct SlabTile<3> {
+    static constexpr int PY = 12, PZ = 72, SIZE = 432;
+};
+template <> struct SlabTile<2> {
+    static constexpr int PY = 10, PZ = 0, SIZE = 100;
+};
+
+template <int D, bool DET> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
     constexpr int NT = P2G_THREADS;
-    __shared__ float tile[4][TILE];
+    constexpr int PY = SlabTile<D>::PY, PZ = SlabTile<D>::PZ;
+    __shared__ float tile[4][DET ? 1 : TILE];
+    __shared__ float4 stile[DET ? 3 : 1][DET ? SlabTile<D>::SIZE : 1];
     // per-thread double buffer: the next particle of the cell is copied in
     // (cp.async) while the current one is accumulated
     __shared__ float4 sp_pm[2][NT];
@@ -397,7 +416,8 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScen
             if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
         }
-        for (int t = threadIdx.x; t < 4 * TILE; t += P2G_THREADS) (&tile[0][0])[t] = 0.f;
+        if constexpr (!DET)
+            for (int t = threadIdx.x; t < 4 * TILE; t += P2G_THREADS) (&tile[0][0])[t] = 0.f;
         int bv[D];
         unpack_key<D>(s.bkey[r], bv);
         const uint32_t lo = s.bcell[(size_t)r * CELLS + mycell];
@@ -487,6 +507,61 @@ template <int D> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScen
             }
         }
         cp_async_wait<0>();
+        if constexpr (DET) {
+            float4 *pt = stile[myslab];
+            const uint32_t lane = tid & 31u, w = (tid & 63u) >> 5;
+            // zero the slab-tile planes this warp writes: 3D z planes
+            // 2w + slab .. +1 (6 x 6 nodes each), 2D rows 4w + slab .. +3
+            if constexpr (D == 3) {
+                for (uint32_t q = lane; q < 72u; q += 32u) {
+                    const uint32_t pl = 2u * w + (uint32_t)myslab + q / 36u, rem = q % 36u;
+                    pt[(rem % 6u) + PY * (rem / 6u) + PZ * pl] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            } else {
+                for (uint32_t q = lane; q < 40u; q += 32u)
+                    pt[(q % 10u) + PY * (4u * w + (uint32_t)myslab + q / 10u)] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < NACC; ++k) {
+                const int sx = k % 3, sy = (D == 3) ? k / 3 : myslab, sz = (D == 3) ? myslab : 0;
+                int idx = (ca[0] + sx) + PY * (ca[1] + sy);
+                if constexpr (D == 3) idx += PZ * (ca[2] + sz);
+                float4 v = pt[idx];
+                v.x += acc[k].x;
+                v.y += acc[k].y;
+                v.z += acc[k].z;
+                v.w += acc[k].w;
+                pt[idx] = v;
+                __syncwarp();
+            }
+            __syncthreads();
+            for (int t = threadIdx.x; t < TILE; t += P2G_THREADS) {
+                int tc[D];
+                tc[0] = t % TW;
+                if constexpr (D == 3) {
+                    tc[1] = (t / TW) % TW;
+                    tc[2] = t / (TW * TW);
+                } else {
+                    tc[1] = t / TW;
+                }
+                const int lay = (D == 3) ? tc[0] + PY * tc[1] + PZ * tc[2] : tc[0] + PY * tc[1];
+                const int along = tc[D - 1];  // slab axis: z in 3D, y in 2D
+                float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int sl = 0; sl < 3; ++sl) {
+                    if (along - sl < 0 || along - sl >= BW) continue;
+                    const float4 v = stile[sl][lay];
+                    sum.x += v.x;
+                    sum.y += v.y;
+                    sum.z += v.z;
+                    sum.w += v.w;
+                }
+                s.partial[(size_t)r * TILE + t] = sum;
+            }
+            __syncthreads();
+            continue;
+        }
         if (hi > lo) {
 #pragma unroll
             for (int k = 0; k < NACC; ++k) {
@@ -708,7 +783,43 @@ template <int D> __global__ void k_grid_update(DevScene s) {
         float cell_pos[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) cell_pos[k] = (float)(bv[k] * BW + lc[k]) * h;
-        const float4 nv = s.nodes[t];
+        float4 nv;
+        if (s.use_partial) {
+            // Node sums of the deterministic P2G: the tiles of this block and
+            // of its -1 neighbours b - o that cover the node (local
+            // coordinate + BW o inside the tile), added in the fixed order
+            // of o.
+            constexpr int TW = Geo<D>::TW, NN = Geo<D>::NASSOC - 1;
+            nv = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < Geo<D>::NASSOC; ++q) {
+                int o[D];
+                assoc_offset<D>(q, o);
+                bool inside = true;
+                int tix = 0, mul = 1;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    const int tc = lc[k] + BW * o[k];
+                    inside = inside && tc < TW;
+                    tix += tc * mul;
+                    mul *= TW;
+                }
+                if (!inside) continue;
+                const uint32_t ra = (q == 0) ? r : s.bnbh_rev[r * NN + q - 1];
+                if (ra == NONE || ra >= nb || s.bnp[ra] == 0u) continue;
+                const float4 v = s.partial[(size_t)ra * Geo<D>::TILE + tix];
+                nv.x += v.x;
+                nv.y += v.y;
+                nv.z += v.z;
+                nv.w += v.w;
+            }
+            if (s.gather_only) {
+                s.nodes[t] = nv;
+                continue;
+            }
+        } else {
+            nv = s.nodes[t];
+        }
         const float pm[3] = {nv.x, nv.y, nv.z};
         const float mass = nv.w;
         const float inv_mass = mass > 0.f ? 1.0f / mass : 0.f;
@@ -748,7 +859,7 @@ template <int D> __global__ void k_grid_update(DevScene s) {
 // staged into shared memory with cp.async while the current particle is
 // computed; each thread consumes only its own staged slot, so the particle
 // loop has no barrier.
-template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(DevScene s) {
+template <int D, int NT> __global__ void __launch_bounds__(NT, 4) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float tv[D][TILE];
     __shared__ float4 st_pm[2][NT];
@@ -835,11 +946,11 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 5) k_g2p_update(D
                 bool in_block = true;
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
-                    const float assoc = rintf(__fdiv_rn(x[k], h)) - 1.0f;
+                    const float assoc = rintf(div_h(x[k], h, s.inv_h, s.h_pow2)) - 1.0f;
                     a[k] = (int)assoc - bv[k] * BW;
                     in_block = in_block && a[k] >= 0 && a[k] < BW;
                     d0[k] = assoc * h - x[k];
-                    bspline_weights(__fdiv_rn(-d0[k], h), w[k]);
+                    bspline_weights(div_h(-d0[k], h, s.inv_h, s.h_pow2), w[k]);
                 }
                 if (!in_block) {  // packed-key aliasing: gather nothing
                     atomicOr(s.err, ERR_KEY_RANGE);

@@ -5,7 +5,7 @@ permutation (slosh's full layout with extras, and the hot path's primary
 permutation).  FP32 tolerance: nodes after P2G and after the grid update, and
 particle state after 1 and 10 substeps.  The tolerances are stated per check
 as max |gpu - oracle| <= atol + rtol * max |oracle| over the compared field;
-the differences come from the summation order of the atomics, FMA
+the differences come from the summation order, FMA
 contraction, the two independent SVD implementations and the factored
 B-spline weights of the particle-centric P2G.
 """
@@ -155,6 +155,28 @@ def test_substep_parity(cuda_lib, name):
     orc.step(9)
     compare_particles(f"{name} 10 steps", data.download_particles(), orc.get_particles(), sc.dim, loose=10.0)
     data.close()
+
+
+@pytest.mark.parametrize("name", ["sand3d_fine", "fluid2d"])
+def test_bit_reproducible(cuda_lib, name, monkeypatch):
+    """The default P2G reduces in a fixed order (no float atomics), so two
+    runs of the same upload give identical bits; the float-atomic variant
+    agrees within the FP32 tolerance."""
+    sc = small_scenes()[name]
+    runs = []
+    for _ in range(2):
+        data = scenes.build_mpm_data(sc)
+        MpmPipeline().launch_step(data, 20)
+        runs.append(data.download_particles())
+        data.close()
+    assert runs[0].tobytes() == runs[1].tobytes()
+    monkeypatch.setenv("SLOSH_P2G", "direct")
+    data = scenes.build_mpm_data(sc)
+    MpmPipeline().launch_step(data, 20)
+    atomic = data.download_particles()
+    data.close()
+    close(f"{name} atomic vs fixed-order position", atomic["position"], runs[0]["position"], 2e-6, 0)
+    close(f"{name} atomic vs fixed-order velocity", atomic["velocity"], runs[0]["velocity"], 1e-5, 1e-4)
 
 
 def test_conservation_vs_fp64(cuda_lib):
