@@ -282,6 +282,91 @@ int slosh_prefix_sum_noalloc(const uint32_t *d_in, uint32_t *d_out, uint32_t n,
 /* Copies the last error message of the context into `buf`. */
 int slosh_last_error(const slosh_ctx *ctx, char *buf, size_t len);
 
+/* ---- Multi-scene batches -------------------------------------------------
+ * Many independent scenes, each with its own particles, cell width, dt,
+ * gravity and colliders, advance together: a substep launches every kernel
+ * once over the blocks and particles of all live scenes, as one CUDA graph.
+ * Stepping a batch by k substeps is equivalent to calling
+ * MpmPipeline::launch_step (src/pipeline.rs:562-770) k times on each
+ * scene's own MpmData (src/pipeline.rs:311); the reference has no batched
+ * step.  Each scene is sorted and reduced exactly as it would be alone (its
+ * blocks are ranked scene-major, ascending key within the scene, and P2G
+ * reduces in a fixed order), so a scene's results do not depend on the other
+ * scenes in the batch, bit for bit.  External forces (force_dt) are not
+ * supported in batches.  Scenes may be added and removed between steps
+ * (continuous batching); a removed scene's particles leave storage at the
+ * next substep and its slot is reusable after that substep. */
+typedef struct slosh_batch slosh_batch;
+
+typedef struct slosh_batch_config {
+    int32_t dim;             /* 2 or 3, for every scene                     */
+    uint32_t max_particles;  /* particle pool over all scenes              */
+    uint32_t grid_capacity;  /* active blocks over all scenes (pow2 above) */
+    uint32_t max_scenes;     /* scene slots, <= 16384                      */
+    uint32_t max_bodies;     /* collider table over all scenes             */
+    int32_t device;
+    uint32_t flags;          /* reserved, 0                                */
+} slosh_batch_config;
+
+typedef struct slosh_scene_desc {
+    float cell_width;        /* MpmData::new's cell_width                  */
+    slosh_params params;     /* gravity, dt (SimulationParams)             */
+} slosh_scene_desc;
+
+/* Launch shape of the batched substep (no effect on results). */
+typedef struct slosh_tuning {
+    uint32_t p2g_ctas_per_sm;  /* P2G grid = SMs x this (4, 8, 16)          */
+    uint32_t g2p_threads;      /* G2P CTA size: 64, 128 or 256              */
+    uint32_t g2p_ctas_per_sm;  /* G2P grid = SMs x this                     */
+    uint32_t pad;
+} slosh_tuning;
+
+typedef struct slosh_batch_stats {
+    uint32_t live_scenes;
+    uint32_t n_particles;      /* in storage                                */
+    uint32_t n_blocks;         /* active blocks of the last substep         */
+    uint32_t n_materials;
+    uint32_t n_svd_fp64;
+    uint32_t n_bodies;         /* collider table entries in use             */
+    uint32_t pad[2];
+    slosh_tuning tuning;
+} slosh_batch_stats;
+
+int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out);
+void slosh_batch_destroy(slosh_batch *b);
+
+/* Adds a scene of n particles (records as for slosh_upload_particles) and
+ * its colliders (as for slosh_set_bodies; <= 16).  Returns its slot.
+ * SLOSH_E_CAPACITY when the pool, the slots or the body table are full. */
+int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles,
+                          uint32_t n, const slosh_body *bodies, uint32_t n_bodies, uint32_t *slot,
+                          void *stream);
+
+/* Drops a scene (its results should have been downloaded). */
+int slosh_batch_remove_scene(slosh_batch *b, uint32_t slot);
+
+/* Advances every live scene by n_substeps (graph launches on `stream`). */
+int slosh_batch_step(slosh_batch *b, uint32_t n_substeps, void *stream);
+
+/* Particles / positions (x, y, z, 0) of one scene, in its upload order. */
+int slosh_batch_download_particles(slosh_batch *b, uint32_t slot, slosh_particle *out, uint32_t n,
+                                   void *stream);
+int slosh_batch_download_positions(slosh_batch *b, uint32_t slot, float *out_xyzw, uint32_t n, void *stream);
+int slosh_batch_get_bodies(slosh_batch *b, uint32_t slot, slosh_body *out, uint32_t n);
+
+/* Waits for the batch's work; reports device-side errors. */
+int slosh_batch_sync(slosh_batch *b, void *stream);
+int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out);
+
+/* Launch-shape autotuner: times each candidate shape on `substeps` real
+ * substeps of the current scenes (the simulation advances; every shape
+ * gives identical results), keeps the fastest, and caches it per
+ * (dim, material mix, particle-count bucket) for later batches in the
+ * process.  A cached entry is reused without timing. */
+int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream);
+int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t);
+int slosh_batch_last_error(const slosh_batch *b, char *buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -126,6 +126,44 @@ class SloshGridDump(ctypes.Structure):
     ]
 
 
+class SloshBatchConfig(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int32),
+        ("max_particles", ctypes.c_uint32),
+        ("grid_capacity", ctypes.c_uint32),
+        ("max_scenes", ctypes.c_uint32),
+        ("max_bodies", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+    ]
+
+
+class SloshSceneDesc(ctypes.Structure):
+    _fields_ = [("cell_width", ctypes.c_float), ("params", SloshParams)]
+
+
+class SloshTuning(ctypes.Structure):
+    _fields_ = [
+        ("p2g_ctas_per_sm", ctypes.c_uint32),
+        ("g2p_threads", ctypes.c_uint32),
+        ("g2p_ctas_per_sm", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+    ]
+
+
+class SloshBatchStats(ctypes.Structure):
+    _fields_ = [
+        ("live_scenes", ctypes.c_uint32),
+        ("n_particles", ctypes.c_uint32),
+        ("n_blocks", ctypes.c_uint32),
+        ("n_materials", ctypes.c_uint32),
+        ("n_svd_fp64", ctypes.c_uint32),
+        ("n_bodies", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32 * 2),
+        ("tuning", SloshTuning),
+    ]
+
+
 # Every symbol include/slosh_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
@@ -149,6 +187,22 @@ SIGNATURES = {
     "slosh_prefix_sum": (ctypes.c_int, [_P, _P, _P, _U32]),
     "slosh_prefix_sum_noalloc": (ctypes.c_int, [_P, _P, _U32, _P]),
     "slosh_last_error": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "slosh_batch_create": (ctypes.c_int, [ctypes.POINTER(SloshBatchConfig), ctypes.POINTER(_P)]),
+    "slosh_batch_destroy": (None, [_P]),
+    "slosh_batch_add_scene": (
+        ctypes.c_int,
+        [_P, ctypes.POINTER(SloshSceneDesc), _P, _U32, _P, _U32, ctypes.POINTER(_U32), _P],
+    ),
+    "slosh_batch_remove_scene": (ctypes.c_int, [_P, _U32]),
+    "slosh_batch_step": (ctypes.c_int, [_P, _U32, _P]),
+    "slosh_batch_download_particles": (ctypes.c_int, [_P, _U32, _P, _U32, _P]),
+    "slosh_batch_download_positions": (ctypes.c_int, [_P, _U32, _P, _U32, _P]),
+    "slosh_batch_get_bodies": (ctypes.c_int, [_P, _U32, _P, _U32]),
+    "slosh_batch_sync": (ctypes.c_int, [_P, _P]),
+    "slosh_batch_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(SloshBatchStats)]),
+    "slosh_batch_autotune": (ctypes.c_int, [_P, _U32, _P]),
+    "slosh_batch_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(SloshTuning)]),
+    "slosh_batch_last_error": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t]),
 }
 
 _lib = None

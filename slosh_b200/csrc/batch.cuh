@@ -1,0 +1,587 @@
+// Multi-scene batches: many independent scenes advanced by one set of
+// kernel launches per substep (one CUDA graph), and the launch-shape
+// autotuner.  Included at the end of slosh_b200.cu (one translation unit);
+// reuses the single-scene context for buffers, stream and error reporting.
+//
+// Layout.  The particles of all scenes share one pool of structure-of-arrays
+// planes (stride = pool capacity), double-buffered like the single-scene
+// context; each particle's flags word carries its scene slot.  Blocks are
+// hashed by (scene << 32 | packed key) in 64-bit maps and ranked scene-major
+// with ascending key inside a scene, so storage is scene-major after every
+// substep and each scene's blocks, particle order and P2G reduction order are
+// those it would have alone.  Per-scene cell width, dt, gravity and collider
+// range live in a device scene table that every kernel reads through the
+// block's (or particle's, or body's) scene.  All counts the kernels need are
+// read on the device, so the captured graphs stay valid when scenes come and
+// go; only the scene table, the body table and the particle pool change.
+#pragma once
+
+#include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+struct slosh_batch {
+    slosh_ctx c;  // buffers, stream, materials, counters, error string
+    uint32_t max_scenes = 0, max_bodies = 0;
+    unsigned long long *hkeys64[2] = {nullptr, nullptr};
+    uint32_t *bscene = nullptr, *scene_nblk = nullptr, *scene_bbase = nullptr, *scene_fill = nullptr;
+    uint32_t *n_dev = nullptr;
+    SceneRec *scenes_dev = nullptr;
+    std::vector<SceneRec> scenes;  // host mirror of the scene table
+    struct Slot {
+        bool used = false;  // holds particles in storage (live, or dropped before the next substep)
+        bool live = false;
+        uint32_t n = 0, body_first = 0, n_bodies = 0, tags = 0;
+        std::vector<float> r0, phase;  // never change on the device
+    };
+    std::vector<Slot> slots;
+    std::vector<uint32_t> dropped;  // removed since the last substep
+    uint32_t n_storage = 0;         // particles in storage (mirror of *n_dev)
+    uint32_t body_top = 0;          // body table entries in use
+    uint32_t staging_cap = 0;       // records in c.staging
+    slosh_tuning tune{8, 128, 8, 0};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graphs_valid = false;
+    uint32_t graph_flags = 0;       // has_damping | has_sand << 1 the graphs were captured with
+};
+
+namespace {
+
+DevScene make_batch_scene(slosh_batch *b, uint32_t parity) {
+    slosh_ctx *c = &b->c;
+    DevScene s = make_scene(c, parity, false);
+    s.n = c->max_n;  // plane stride; the count is *n_dev
+    s.force_pending = 0u;
+    s.scenes = b->scenes_dev;
+    s.n_scenes = b->max_scenes;
+    s.n_dev = b->n_dev;
+    const uint32_t cur = parity & 1u, prv = cur ^ 1u;
+    s.hkeys64 = b->hkeys64[cur];
+    s.prev_hkeys64 = b->hkeys64[prv];
+    s.clr_hkeys64 = b->hkeys64[prv];
+    s.bscene = b->bscene;
+    s.scene_nblk = b->scene_nblk;
+    s.scene_bbase = b->scene_bbase;
+    s.scene_fill = b->scene_fill;
+    s.n_bodies = b->body_top;
+    s.use_partial = 1u;
+    return s;
+}
+
+template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s, cudaStream_t st) {
+    const uint32_t g = std::min<uint32_t>(b->c.cap, (uint32_t)b->c.sm_count * b->tune.g2p_ctas_per_sm);
+    k_g2p_update<D, NT, true><<<g, NT, 0, st>>>(s);
+}
+
+// One batched substep: 14 kernels over all scenes.
+template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uint32_t parity) {
+    slosh_ctx *c = &b->c;
+    const DevScene s = make_batch_scene(b, parity);
+    const uint32_t sm = (uint32_t)c->sm_count;
+    k_touch<D, true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
+    k_neighbors<D, true><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
+    k_scene_scan<1024><<<1, 1024, 0, st>>>(s);
+    k_scene_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    const uint32_t ns = b->max_scenes;
+    k_scene_sort<256, 0, SCENE_SORT_SMALL>
+        <<<std::min<uint32_t>(ns, sm * 8), 256, SCENE_SORT_SMALL * sizeof(unsigned long long), st>>>(s);
+    k_scene_sort<1024, SCENE_SORT_SMALL, SCENE_SORT_MAX>
+        <<<std::min<uint32_t>(ns, sm), 1024, SCENE_SORT_MAX * sizeof(unsigned long long), st>>>(s);
+    k_block_setup<D, true><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
+    k_scatter<true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
+    k_canon_cells<<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
+    k_p2g<D, true, true><<<std::min<uint32_t>(c->cap, sm * b->tune.p2g_ctas_per_sm), P2G_THREADS, 0, st>>>(s);
+    k_grid_update<D, true><<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
+    if (b->tune.g2p_threads == 64) launch_batch_g2p<D, 64>(b, s, st);
+    else if (b->tune.g2p_threads == 256) launch_batch_g2p<D, 256>(b, s, st);
+    else launch_batch_g2p<D, 128>(b, s, st);
+    k_rigid<D, true><<<std::max<uint32_t>(1, (b->max_bodies + 127) / 128), 128, 0, st>>>(s);
+}
+
+void enqueue_batch_substep_any(slosh_batch *b, cudaStream_t st, uint32_t parity) {
+    if (b->c.dim == 3) enqueue_batch_substep<3>(b, st, parity);
+    else enqueue_batch_substep<2>(b, st, parity);
+}
+
+void destroy_batch_graphs(slosh_batch *b) {
+    for (int k = 0; k < 2; ++k)
+        if (b->graph[k]) {
+            cudaGraphExecDestroy(b->graph[k]);
+            b->graph[k] = nullptr;
+        }
+    b->graphs_valid = false;
+}
+
+int build_batch_graphs(slosh_batch *b) {
+    slosh_ctx *c = &b->c;
+    destroy_batch_graphs(b);
+    for (uint32_t par = 0; par < 2; ++par) {
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_batch_substep_any(b, c->stream, par);
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(c->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&b->graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    b->graphs_valid = true;
+    b->graph_flags = c->has_damping | (c->has_sand << 1);
+    return SLOSH_OK;
+}
+
+int batch_check_error(slosh_batch *b) {
+    slosh_ctx *c = &b->c;
+    uint32_t e = 0;
+    CK(cudaMemcpy(&e, c->err, 4, cudaMemcpyDeviceToHost));
+    if (e & ERR_SCENE_BLOCKS) {
+        CK(cudaMemset(c->err, 0, 4));
+        return fail(c, SLOSH_E_CAPACITY, "a scene exceeds %u active blocks (error bits 0x%x)", SCENE_SORT_MAX, e);
+    }
+    return check_device_error(c);
+}
+
+int upload_scene_rec(slosh_batch *b, uint32_t slot, cudaStream_t st) {
+    slosh_ctx *c = &b->c;
+    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpy(b->scenes_dev + slot, &b->scenes[slot], sizeof(SceneRec), cudaMemcpyHostToDevice));
+    return SLOSH_OK;
+}
+
+// Moves the bodies of live scenes to the front of the body table.
+int compact_bodies(slosh_batch *b) {
+    slosh_ctx *c = &b->c;
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<DevBody> all(b->body_top);
+    if (b->body_top) CK(cudaMemcpy(all.data(), c->bodies, b->body_top * sizeof(DevBody), cudaMemcpyDeviceToHost));
+    std::vector<DevBody> kept;
+    for (uint32_t s = 0; s < b->max_scenes; ++s) {
+        slosh_batch::Slot &sl = b->slots[s];
+        if (!sl.used) continue;
+        const uint32_t first = (uint32_t)kept.size();
+        for (uint32_t k = 0; k < sl.n_bodies; ++k) kept.push_back(all[sl.body_first + k]);
+        sl.body_first = first;
+        b->scenes[s].body_first = first;
+    }
+    b->body_top = (uint32_t)kept.size();
+    if (!kept.empty()) CK(cudaMemcpy(c->bodies, kept.data(), kept.size() * sizeof(DevBody), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->scenes_dev, b->scenes.data(), b->max_scenes * sizeof(SceneRec), cudaMemcpyHostToDevice));
+    destroy_batch_graphs(b);  // the graphs captured the body count
+    return SLOSH_OK;
+}
+
+// Process-wide autotuner cache: (dim, material tags, log2 particle count).
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, uint32_t, int>, slosh_tuning> g_tune_cache;
+
+std::tuple<int, uint32_t, int> tune_key(const slosh_batch *b) {
+    uint32_t tags = 0;
+    for (const auto &sl : b->slots)
+        if (sl.live) tags |= sl.tags;
+    int lg = 0;
+    while ((1u << (lg + 1)) <= std::max<uint32_t>(b->n_storage, 1u)) ++lg;
+    return {b->c.dim, tags, lg};
+}
+
+}  // namespace
+
+extern "C" {
+
+int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
+    if (!cfg || !out) return SLOSH_E_INVALID;
+    *out = nullptr;
+    if ((cfg->dim != 2 && cfg->dim != 3) || cfg->grid_capacity == 0 || cfg->max_particles == 0 ||
+        cfg->grid_capacity > (1u << 24) || cfg->max_scenes == 0 || cfg->max_scenes > MAX_SCENES)
+        return SLOSH_E_INVALID;
+    slosh_batch *b = new slosh_batch();
+    slosh_ctx *c = &b->c;
+    c->dim = (int)cfg->dim;
+    c->h = 1.0f;  // per scene
+    c->cap = next_pow2(cfg->grid_capacity);
+    c->hcap = 2 * c->cap;
+    c->max_n = cfg->max_particles;
+    c->device = cfg->device;
+    b->max_scenes = cfg->max_scenes;
+    b->max_bodies = std::max<uint32_t>(cfg->max_bodies, 1u);
+    auto fail_create = [&](int code) {
+        slosh_batch_destroy(b);
+        return code;
+    };
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
+    const size_t N = c->max_n;
+    const int D = c->dim;
+    const uint32_t cap = c->cap, hcap = c->hcap;
+    int st = SLOSH_OK;
+    for (int k = 0; k < 2; ++k) {
+        slosh_ctx::Storage &S = c->pb[k];
+        if ((st = dalloc(c, &S.pm, N)) || (st = dalloc(c, &S.vel, N * D)) || (st = dalloc(c, &S.C, N * D * D)) ||
+            (st = dalloc(c, &S.F, N * D * D)) || (st = dalloc(c, &S.V0, N)) || (st = dalloc(c, &S.flags, N)) ||
+            (st = dalloc(c, &S.damping, N)) || (st = dalloc(c, &S.plastic, N * 3)) || (st = dalloc(c, &S.oid, N)))
+            return fail_create(st);
+    }
+    if ((st = dalloc(c, &c->materials, MAX_MATERIALS)) || (st = dalloc(c, &c->mat_hkeys, MAT_HASH)) ||
+        (st = dalloc(c, &c->mat_dense, MAT_HASH)) || (st = dalloc(c, &b->hkeys64[0], hcap)) ||
+        (st = dalloc(c, &b->hkeys64[1], hcap)) || (st = dalloc(c, &c->hvals[0], hcap)) ||
+        (st = dalloc(c, &c->hvals[1], hcap)) || (st = dalloc(c, &c->slot_counts, (size_t)hcap * CELLS)) ||
+        (st = dalloc(c, &c->blist_key, cap)) || (st = dalloc(c, &c->blist_slot, cap)) ||
+        (st = dalloc(c, &c->blist2_key, cap)) || (st = dalloc(c, &c->blist2_slot, cap)) ||
+        (st = dalloc(c, &c->hist, HIST_BINS)) || (st = dalloc(c, &c->hist_fill, HIST_BINS)) ||
+        (st = dalloc(c, &c->tmp_key, 2 * (size_t)cap)) || (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) ||
+        (st = dalloc(c, &c->bkey, cap)) || (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &b->bscene, cap)) ||
+        (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
+        (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
+        (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
+        (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
+        (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||
+        (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
+        (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
+        (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, b->max_bodies)) ||
+        (st = dalloc(c, &c->ctr, 1)) || (st = dalloc(c, &c->err, 1)) || (st = dalloc(c, &c->small, 4)) ||
+        (st = dalloc(c, &b->scene_nblk, b->max_scenes)) || (st = dalloc(c, &b->scene_bbase, b->max_scenes)) ||
+        (st = dalloc(c, &b->scene_fill, b->max_scenes)) || (st = dalloc(c, &b->scenes_dev, b->max_scenes)) ||
+        (st = dalloc(c, &b->n_dev, 1)))
+        return fail_create(st);
+    cudaMemset(b->hkeys64[0], 0xff, (size_t)hcap * 8);
+    cudaMemset(b->hkeys64[1], 0xff, (size_t)hcap * 8);
+    cudaMemset(c->hvals[0], 0xff, (size_t)hcap * 4);
+    cudaMemset(c->hvals[1], 0xff, (size_t)hcap * 4);
+    cudaMemset(c->slot_counts, 0, (size_t)hcap * CELLS * 4);
+    cudaMemset(c->ctr, 0, sizeof(Counters));
+    cudaMemset(c->err, 0, 4);
+    cudaMemset(c->small, 0, 16);
+    cudaMemset(c->mat_hkeys, 0xff, MAT_HASH * 4);
+    cudaMemset(c->pb[0].damping, 0, N * 4);
+    cudaMemset(c->pb[1].damping, 0, N * 4);
+    cudaMemset(b->scene_nblk, 0, b->max_scenes * 4);
+    cudaMemset(b->scenes_dev, 0, b->max_scenes * sizeof(SceneRec));
+    cudaMemset(b->n_dev, 0, 4);
+    cudaFuncSetAttribute(k_scene_sort<1024, SCENE_SORT_SMALL, SCENE_SORT_MAX>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, SCENE_SORT_MAX * sizeof(unsigned long long));
+    if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
+    b->scenes.assign(b->max_scenes, SceneRec{});
+    b->slots.assign(b->max_scenes, slosh_batch::Slot{});
+    *out = b;
+    return SLOSH_OK;
+}
+
+void slosh_batch_destroy(slosh_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->c.device);
+    destroy_batch_graphs(b);
+    release_ctx(&b->c);
+    delete b;
+}
+
+int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles, uint32_t n,
+                          const slosh_body *bodies, uint32_t n_bodies, uint32_t *slot_out, void *stream) {
+    if (!b || !desc || (!particles && n) || (!bodies && n_bodies) || !slot_out) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    if (n == 0) return fail(c, SLOSH_E_INVALID, "a scene needs particles");
+    if (!(desc->cell_width > 0.f) || !(desc->params.dt > 0.f))
+        return fail(c, SLOSH_E_INVALID, "cell width and dt must be > 0");
+    if (n_bodies > MAX_BODIES) return fail(c, SLOSH_E_CAPACITY, "%u bodies exceed %u per scene", n_bodies, MAX_BODIES);
+    if ((uint64_t)b->n_storage + n > c->max_n)
+        return fail(c, SLOSH_E_CAPACITY, "%u + %u particles exceed the pool of %u", b->n_storage, n, c->max_n);
+    uint32_t tags = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const slosh_particle &p = particles[i];
+        if (p.force_dt[0] != 0.f || p.force_dt[1] != 0.f || p.force_dt[2] != 0.f)
+            return fail(c, SLOSH_E_INVALID, "external forces (force_dt) are not supported in batches");
+        if (p.model.tag < 32) tags |= 1u << p.model.tag;
+    }
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());  // no substep may run while the pool and tables change
+    uint32_t slot = NONE;
+    for (uint32_t s = 0; s < b->max_scenes; ++s)
+        if (!b->slots[s].used) {
+            slot = s;
+            break;
+        }
+    if (slot == NONE) return fail(c, SLOSH_E_CAPACITY, "all %u scene slots are in use", b->max_scenes);
+    cudaStream_t st = pick(c, stream);
+    if (b->body_top + n_bodies > b->max_bodies) {
+        int r = compact_bodies(b);
+        if (r) return r;
+        if (b->body_top + n_bodies > b->max_bodies)
+            return fail(c, SLOSH_E_CAPACITY, "body table full (%u entries)", b->max_bodies);
+    }
+    if (n > b->staging_cap) {
+        CK(cudaStreamSynchronize(st));
+        if (c->staging) {
+            cudaFree(c->staging);
+            c->allocs.erase(std::find(c->allocs.begin(), c->allocs.end(), (void *)c->staging));
+            c->staging = nullptr;
+        }
+        int r = dalloc(c, &c->staging, n);
+        if (r) return r;
+        b->staging_cap = n;
+    }
+    const uint32_t base = b->n_storage;
+    DevScene s = make_batch_scene(b, c->parity);
+    IoBuffers io{};
+    io.in = c->staging;
+    io.mat_hkeys = c->mat_hkeys;
+    io.mat_dense = c->mat_dense;
+    io.n_mat = c->small;
+    io.scene_flags = c->small + 1;
+    CK(cudaMemcpyAsync(c->staging, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice, st));
+    const uint32_t g = grid_for(n, 256, (uint32_t)c->sm_count * 16);
+    k_mat_insert<<<g, 256, 0, st>>>(s, io, n);
+    if (c->dim == 3) k_ingest<3, true><<<g, 256, 0, st>>>(s, io, base, n, slot);
+    else k_ingest<2, true><<<g, 256, 0, st>>>(s, io, base, n, slot);
+    CK(cudaGetLastError());
+    const uint32_t new_n = base + n;
+    CK(cudaMemcpyAsync(b->n_dev, &new_n, 4, cudaMemcpyHostToDevice, st));
+    if (n_bodies) {
+        std::vector<DevBody> db(n_bodies);
+        for (uint32_t k = 0; k < n_bodies; ++k) {
+            to_dev_body(bodies[k], db[k]);
+            db[k].scene = slot;
+        }
+        CK(cudaMemcpyAsync(c->bodies + b->body_top, db.data(), n_bodies * sizeof(DevBody), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    SceneRec &rec = b->scenes[slot];
+    rec = SceneRec{};
+    rec.h = desc->cell_width;
+    rec.inv_h = 1.0f / desc->cell_width;
+    rec.dt = desc->params.dt;
+    for (int k = 0; k < 3; ++k) rec.gravity[k] = desc->params.gravity[k];
+    int ex = 0;
+    rec.h_pow2 = (std::frexp(desc->cell_width, &ex) == 0.5f) ? 1u : 0u;
+    rec.body_first = b->body_top;
+    rec.n_bodies = n_bodies;
+    rec.live = 1u;
+    int r = upload_scene_rec(b, slot, st);
+    if (r) return r;
+    uint32_t small[2] = {0, 0};
+    CK(cudaMemcpy(small, c->small, 8, cudaMemcpyDeviceToHost));
+    c->n_materials = small[0];
+    c->has_damping |= (small[1] & SCENE_DAMPING) ? 1u : 0u;
+    c->has_sand |= (small[1] & SCENE_SAND) ? 1u : 0u;
+    r = batch_check_error(b);
+    if (r) return r;
+    slosh_batch::Slot &sl = b->slots[slot];
+    sl.used = true;
+    sl.live = true;
+    sl.n = n;
+    sl.body_first = b->body_top;
+    sl.n_bodies = n_bodies;
+    sl.tags = tags;
+    sl.r0.resize(n);
+    sl.phase.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        sl.r0[i] = particles[i].init_radius;
+        sl.phase[i] = particles[i].phase;
+    }
+    b->body_top += n_bodies;
+    b->n_storage = new_n;
+    if (b->graphs_valid && (b->graph_flags != (c->has_damping | (c->has_sand << 1)) || n_bodies))
+        destroy_batch_graphs(b);  // captured scene flags or body count changed
+    *slot_out = slot;
+    return SLOSH_OK;
+}
+
+int slosh_batch_remove_scene(slosh_batch *b, uint32_t slot) {
+    if (!b || slot >= b->max_scenes) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    if (!b->slots[slot].live) return fail(c, SLOSH_E_STATE, "scene slot %u is not live", slot);
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());  // no substep may run while the scene table changes
+    b->slots[slot].live = false;
+    b->scenes[slot].live = 0u;
+    int r = upload_scene_rec(b, slot, c->stream);
+    if (r) return r;
+    b->dropped.push_back(slot);
+    return SLOSH_OK;
+}
+
+int slosh_batch_step(slosh_batch *b, uint32_t n_substeps, void *stream) {
+    if (!b) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    for (uint32_t k = 0; k < n_substeps; ++k) {
+        if (b->n_storage == 0) break;
+        if (!b->graphs_valid) {
+            CK(cudaStreamSynchronize(st));
+            int r = build_batch_graphs(b);
+            if (r) return r;
+            CK(cudaStreamSynchronize(c->stream));
+        }
+        CK(cudaGraphLaunch(b->graph[c->parity], st));
+        c->parity ^= 1u;
+        if (!b->dropped.empty()) {  // their particles left storage in this substep
+            for (uint32_t s : b->dropped) {
+                b->n_storage -= b->slots[s].n;
+                b->slots[s] = slosh_batch::Slot{};
+            }
+            b->dropped.clear();
+        }
+    }
+    return SLOSH_OK;
+}
+
+int slosh_batch_download_particles(slosh_batch *b, uint32_t slot, slosh_particle *out, uint32_t n, void *stream) {
+    if (!b || slot >= b->max_scenes || (!out && n)) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    const slosh_batch::Slot &sl = b->slots[slot];
+    if (!sl.live) return fail(c, SLOSH_E_STATE, "scene slot %u is not live", slot);
+    if (n > sl.n) return fail(c, SLOSH_E_INVALID, "asked for %u particles, scene holds %u", n, sl.n);
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    if (n > 0) {
+        DevScene s = make_batch_scene(b, c->parity);
+        IoBuffers io{};
+        io.out = c->staging;
+        const uint32_t g = grid_for(b->n_storage, 256, (uint32_t)c->sm_count * 16);
+        if (c->dim == 3) k_egest<3, true><<<g, 256, 0, st>>>(s, io, slot);
+        else k_egest<2, true><<<g, 256, 0, st>>>(s, io, slot);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, c->staging, (size_t)n * sizeof(slosh_particle), cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < n; ++i) {
+        out[i].init_radius = sl.r0[i];
+        out[i].phase = sl.phase[i];
+    }
+    return batch_check_error(b);
+}
+
+int slosh_batch_download_positions(slosh_batch *b, uint32_t slot, float *out, uint32_t n, void *stream) {
+    if (!b || slot >= b->max_scenes || (!out && n)) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    const slosh_batch::Slot &sl = b->slots[slot];
+    if (!sl.live) return fail(c, SLOSH_E_STATE, "scene slot %u is not live", slot);
+    if (n > sl.n) return fail(c, SLOSH_E_INVALID, "asked for %u particles, scene holds %u", n, sl.n);
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    if (n > 0) {
+        DevScene s = make_batch_scene(b, c->parity);
+        float4 *tmp = (float4 *)c->staging;  // staging holds >= 12 float4 per particle of the largest scene
+        k_positions<true><<<grid_for(b->n_storage, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s, tmp, slot);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, tmp, (size_t)n * 16, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return batch_check_error(b);
+}
+
+int slosh_batch_get_bodies(slosh_batch *b, uint32_t slot, slosh_body *out, uint32_t n) {
+    if (!b || slot >= b->max_scenes || (!out && n)) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    const slosh_batch::Slot &sl = b->slots[slot];
+    if (!sl.live || n > sl.n_bodies) return fail(c, SLOSH_E_INVALID, "scene slot %u: %u bodies", slot, sl.n_bodies);
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<DevBody> db(n);
+    if (n) CK(cudaMemcpy(db.data(), c->bodies + sl.body_first, n * sizeof(DevBody), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) from_dev_body(db[i], out[i]);
+    return SLOSH_OK;
+}
+
+int slosh_batch_sync(slosh_batch *b, void *stream) {
+    if (!b) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(pick(c, stream)));
+    CK(cudaGetLastError());
+    return batch_check_error(b);
+}
+
+int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out) {
+    if (!b || !out) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    Counters ctr;
+    CK(cudaMemcpy(&ctr, c->ctr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    for (const auto &sl : b->slots) out->live_scenes += sl.live ? 1u : 0u;
+    out->n_particles = b->n_storage;
+    out->n_blocks = ctr.last_n_blocks;
+    out->n_materials = c->n_materials;
+    out->n_svd_fp64 = ctr.n_svd_fp64;
+    out->n_bodies = b->body_top;
+    out->tuning = b->tune;
+    return SLOSH_OK;
+}
+
+int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t) {
+    if (!b || !t) return SLOSH_E_INVALID;
+    if ((t->g2p_threads != 64 && t->g2p_threads != 128 && t->g2p_threads != 256) || t->p2g_ctas_per_sm == 0 ||
+        t->p2g_ctas_per_sm > 64 || t->g2p_ctas_per_sm == 0 || t->g2p_ctas_per_sm > 64)
+        return fail(&b->c, SLOSH_E_INVALID, "invalid tuning");
+    b->tune = *t;
+    b->tune.pad = 0;
+    destroy_batch_graphs(b);
+    return SLOSH_OK;
+}
+
+int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream) {
+    if (!b) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    if (b->n_storage == 0) return fail(c, SLOSH_E_STATE, "no scenes");
+    const auto key = tune_key(b);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return slosh_batch_set_tuning(b, &it->second);
+    }
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    const slosh_tuning cands[] = {{8, 128, 8, 0}, {4, 128, 4, 0},  {16, 128, 16, 0},
+                                  {8, 64, 16, 0}, {8, 256, 4, 0},  {4, 64, 8, 0}};
+    const uint32_t reps = std::max<uint32_t>(substeps, 1u);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    slosh_tuning pick_t = b->tune;
+    for (const slosh_tuning &t : cands) {
+        b->tune = t;
+        enqueue_batch_substep_any(b, st, c->parity);  // warm-up of this shape
+        c->parity ^= 1u;
+        CK(cudaEventRecord(e0, st));
+        for (uint32_t k = 0; k < reps; ++k) {
+            enqueue_batch_substep_any(b, st, c->parity);
+            c->parity ^= 1u;
+        }
+        CK(cudaEventRecord(e1, st));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaGetLastError());
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            pick_t = t;
+        }
+        if (!b->dropped.empty()) {
+            for (uint32_t s : b->dropped) {
+                b->n_storage -= b->slots[s].n;
+                b->slots[s] = slosh_batch::Slot{};
+            }
+            b->dropped.clear();
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cache[key] = pick_t;
+    }
+    int r = slosh_batch_set_tuning(b, &pick_t);
+    if (r) return r;
+    return batch_check_error(b);
+}
+
+int slosh_batch_last_error(const slosh_batch *b, char *buf, size_t len) {
+    if (!b || !buf || len == 0) return SLOSH_E_INVALID;
+    std::snprintf(buf, len, "%s", b->c.last_error.c_str());
+    return SLOSH_OK;
+}
+
+}  // extern "C"

@@ -21,6 +21,7 @@ constexpr uint32_t ERR_BLOCK_OVERFLOW = 1u << 1;   // more active blocks than ca
 constexpr uint32_t ERR_MATERIALS = 1u << 2;        // too many distinct materials
 constexpr uint32_t ERR_MATERIAL_HASH = 1u << 3;    // two materials share a 32-bit hash
 constexpr uint32_t ERR_KEY_RANGE = 1u << 4;        // a block coordinate outside the packed-key range
+constexpr uint32_t ERR_SCENE_BLOCKS = 1u << 5;     // a batch scene has more blocks than the per-scene sort holds
 
 // Sparse grid geometry per dimension (shaders/slosh/grid/grid.slang:224-257).
 template <int D> struct Geo;
@@ -154,10 +155,24 @@ struct Material {
     float p[12];
 };
 
-// Flags word of a particle: material id, enabled, fixed.
+// Flags word of a particle: material id, enabled, fixed, and (multi-scene
+// batches) the scene slot in the top 14 bits.
 constexpr uint32_t FLAG_MAT_MASK = 0xffffu;
 constexpr uint32_t FLAG_ENABLED = 1u << 16;
 constexpr uint32_t FLAG_FIXED = 1u << 17;
+constexpr uint32_t FLAG_SCENE_SHIFT = 18;
+constexpr uint32_t MAX_SCENES = 1u << 14;
+__host__ __device__ __forceinline__ uint32_t scene_of(uint32_t flags) { return flags >> FLAG_SCENE_SHIFT; }
+
+// Per-scene parameters of a multi-scene batch (the single-scene context
+// passes the same values as kernel arguments).
+struct SceneRec {
+    float h, inv_h, dt;
+    float gravity[3];
+    uint32_t h_pow2;
+    uint32_t body_first, n_bodies;  // the scene's colliders in the body table
+    uint32_t live;                  // 0: the slot's particles are dropped at the next substep
+};
 
 // Collider body on the device (slosh_body in device form).
 struct DevBody {
@@ -172,6 +187,7 @@ struct DevBody {
     float local_com[3];
     uint32_t bc_type;
     float friction;
+    uint32_t scene;  // owning scene slot (multi-scene batches)
 };
 
 // Per-substep device counters.

@@ -62,6 +62,65 @@ __device__ __forceinline__ uint32_t hash_find(const uint32_t *keys, uint32_t hca
     return NONE;
 }
 
+// Multi-scene maps: 64-bit keys (scene << 32 | packed block key), same
+// linear probing.  With scene 0 the slot sequence is the single-scene one.
+constexpr unsigned long long NONE64 = ~0ull;
+__device__ __forceinline__ uint32_t hash64(unsigned long long k) {
+    return murmur_mix((uint32_t)k ^ murmur_mix((uint32_t)(k >> 32) * 0x9e3779b1u));
+}
+
+__device__ __forceinline__ uint32_t hash_insert64(unsigned long long *keys, uint32_t hcap, unsigned long long key,
+                                                  bool &inserted, uint32_t *err) {
+    uint32_t slot = hash64(key) & (hcap - 1u);
+    for (uint32_t k = 0; k < hcap; ++k) {
+        const unsigned long long old = atomicCAS(&keys[slot], NONE64, key);
+        if (old == NONE64) {
+            inserted = true;
+            return slot;
+        }
+        if (old == key) {
+            inserted = false;
+            return slot;
+        }
+        slot = (slot + 1u) & (hcap - 1u);
+    }
+    atomicOr(err, ERR_HASH_OVERFLOW);
+    inserted = false;
+    return NONE;
+}
+
+__device__ __forceinline__ uint32_t hash_find64(const unsigned long long *keys, uint32_t hcap, unsigned long long key) {
+    uint32_t slot = hash64(key) & (hcap - 1u);
+    for (uint32_t k = 0; k < hcap; ++k) {
+        const unsigned long long kk = keys[slot];
+        if (kk == key) return slot;
+        if (kk == NONE64) return NONE;
+        slot = (slot + 1u) & (hcap - 1u);
+    }
+    return NONE;
+}
+
+// Block map access of the single-scene (B = false: 32-bit keys, scene
+// ignored) and the multi-scene (B = true) contexts.
+template <bool B>
+__device__ __forceinline__ uint32_t map_insert(const DevScene &s, uint32_t key, uint32_t sc, bool &inserted) {
+    if constexpr (B) return hash_insert64(s.hkeys64, s.hcap, ((unsigned long long)sc << 32) | key, inserted, s.err);
+    else return hash_insert(s.hkeys, s.hcap, key, inserted, s.err);
+}
+template <bool B> __device__ __forceinline__ uint32_t map_find(const DevScene &s, uint32_t key, uint32_t sc) {
+    if constexpr (B) return hash_find64(s.hkeys64, s.hcap, ((unsigned long long)sc << 32) | key);
+    else return hash_find(s.hkeys, s.hcap, key);
+}
+template <bool B> __device__ __forceinline__ uint32_t map_find_prev(const DevScene &s, uint32_t key, uint32_t sc) {
+    if constexpr (B) return hash_find64(s.prev_hkeys64, s.hcap, ((unsigned long long)sc << 32) | key);
+    else return hash_find(s.prev_hkeys, s.hcap, key);
+}
+// Particles in storage.
+template <bool B> __device__ __forceinline__ uint32_t n_particles(const DevScene &s) {
+    if constexpr (B) return *s.n_dev;
+    else return s.n;
+}
+
 // Cell index of a local cell inside its block: x + BW y (+ BW^2 z).
 template <int D> __device__ __forceinline__ uint32_t cell_index(const int *a) {
     if constexpr (D == 3) return (uint32_t)(a[0] + 4 * a[1] + 16 * a[2]);
@@ -72,13 +131,16 @@ template <int D> __device__ __forceinline__ uint32_t cell_index(const int *a) {
 // reset_hmap (grid.slang:200-218).  The per-slot cell counts are cleared by
 // k_block_setup after they are read; after a substep that raised an error
 // (blocks left without a rank keep their counts) they are all cleared here.
-__global__ void k_clear(DevScene s) {
+template <bool B = false> __global__ void k_clear(DevScene s) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = tid; i < s.hcap; i += stride) {
-        s.hkeys[i] = NONE;
+        if constexpr (B) s.hkeys64[i] = NONE64;
+        else s.hkeys[i] = NONE;
         s.hvals[i] = NONE;
     }
+    if constexpr (B)
+        for (uint32_t i = tid; i < s.n_scenes; i += stride) s.scene_nblk[i] = 0u;
     if (*s.err != 0u)
         for (size_t i = tid; i < (size_t)s.hcap * CELLS; i += stride) s.slot_counts[i] = 0u;
     for (uint32_t i = tid; i < HIST_BINS; i += stride) {
@@ -95,31 +157,49 @@ __global__ void k_clear(DevScene s) {
 // Per particle: activate the primary block and count the particle in its
 // cell.  Replaces touch_primary_blocks (sort.slang:50-67) and the primary
 // half of update_block_particle_count (sort.slang:208-246).
-template <int D> __global__ void k_touch(DevScene s) {
+// Multi-scene batches (B): the particle's scene comes from its flags, its
+// cell width from the scene table, and particles of a dropped scene get no
+// block (they leave storage at this substep).
+template <int D, bool B = false> __global__ void k_touch(DevScene s) {
     const uint32_t lane = lane_id();
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < s.n; base += stride) {
+    const uint32_t n = n_particles<B>(s);
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
         const uint32_t i = base + lane;
-        const bool valid = i < s.n;
+        const bool valid = i < n;
         const unsigned mask = __ballot_sync(FULL_MASK, valid);
         if (!valid) continue;
         const float4 p = s.pm[i];
         const float x[3] = {p.x, p.y, p.z};
-        const CellLoc<D> c = locate<D>(x, s.h, s.inv_h, s.h_pow2);
+        float h = s.h, inv_h = s.inv_h;
+        uint32_t pow2 = s.h_pow2, sc = 0;
+        bool live = true;
+        if constexpr (B) {
+            sc = scene_of(s.flags[i]);
+            const SceneRec &rec = s.scenes[sc];
+            h = rec.h;
+            inv_h = rec.inv_h;
+            pow2 = rec.h_pow2;
+            live = rec.live != 0u;
+        }
+        const CellLoc<D> c = locate<D>(x, h, inv_h, pow2);
         const uint32_t key = pack_key<D>(c.block);
         const uint32_t cell = cell_index<D>(c.local);
-        const unsigned peers = __match_any_sync(mask, key);
+        unsigned peers;
+        if constexpr (B) peers = __match_any_sync(mask, live ? (((unsigned long long)sc << 32) | key) : NONE64);
+        else peers = __match_any_sync(mask, key);
         const int leader = __ffs(peers) - 1;
         uint32_t slot = NONE;
-        if ((int)lane == leader) {
+        if ((int)lane == leader && live) {
             bool inserted = false;
-            slot = hash_insert(s.hkeys, s.hcap, key, inserted, s.err);
+            slot = map_insert<B>(s, key, sc, inserted);
             if (inserted) {
                 const uint32_t j = atomicAdd(&s.ctr->n_primary, 1u);
                 if (j < s.cap) {
                     s.blist_key[j] = key;
                     s.blist_slot[j] = slot;
-                    atomicAdd(&s.hist[key >> 16], 1u);
+                    if constexpr (B) atomicAdd(&s.scene_nblk[sc], 1u);
+                    else atomicAdd(&s.hist[key >> 16], 1u);
                 } else {
                     atomicOr(s.err, ERR_BLOCK_OVERFLOW);
                 }
@@ -135,7 +215,7 @@ template <int D> __global__ void k_touch(DevScene s) {
 
 // Activates the +1 neighbours of every primary block, one thread per
 // (block, neighbour).  Replaces touch_neighbor_blocks (sort.slang:75-92).
-template <int D> __global__ void k_neighbors(DevScene s) {
+template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t np = min(s.ctr->n_primary, s.cap);
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -147,14 +227,17 @@ template <int D> __global__ void k_neighbors(DevScene s) {
         assoc_offset<D>(sidx, o);
         for (int k = 0; k < D; ++k) b[k] += o[k];
         const uint32_t key = pack_key<D>(b);
+        uint32_t sc = 0;
+        if constexpr (B) sc = (uint32_t)(s.hkeys64[s.blist_slot[j]] >> 32);
         bool inserted = false;
-        const uint32_t slot = hash_insert(s.hkeys, s.hcap, key, inserted, s.err);
+        const uint32_t slot = map_insert<B>(s, key, sc, inserted);
         if (inserted) {
             const uint32_t jj = atomicAdd(&s.ctr->n_extra, 1u);
             if (jj < s.cap) {
                 s.blist2_key[jj] = key;
                 s.blist2_slot[jj] = slot;
-                atomicAdd(&s.hist[key >> 16], 1u);
+                if constexpr (B) atomicAdd(&s.scene_nblk[sc], 1u);
+                else atomicAdd(&s.hist[key >> 16], 1u);
             } else {
                 atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             }
@@ -317,11 +400,97 @@ __global__ void k_rank(DevScene s) {
     }
 }
 
+// ---- multi-scene block ranking ----------------------------------------------
+// Blocks are ranked scene-major and by ascending packed key within a scene,
+// so each scene gets the block order (and hence the particle storage order)
+// it would have alone.  Per-scene block counts were taken when the blocks
+// were inserted; one CTA scans them into per-scene rank bases.
+template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s) {
+    const uint32_t total = cta_scan_vec16<NT>(s.scene_nblk, s.scene_bbase, s.n_scenes);
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < s.n_scenes; q += NT) s.scene_fill[q] = s.scene_bbase[q];
+    if (threadIdx.x == 0) {
+        if (total > s.cap) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+        s.ctr->n_blocks = min(total, s.cap);
+    }
+}
+
+// Groups the appended blocks by scene (unordered within a scene).
+__global__ void k_scene_scatter(DevScene s) {
+    const uint32_t n1 = min(s.ctr->n_primary, s.cap), n2 = min(s.ctr->n_extra, s.cap);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n1 + n2; t += stride) {
+        const uint32_t key = t < n1 ? s.blist_key[t] : s.blist2_key[t - n1];
+        const uint32_t slot = t < n1 ? s.blist_slot[t] : s.blist2_slot[t - n1];
+        const uint32_t sc = (uint32_t)(s.hkeys64[slot] >> 32);
+        const uint32_t pos = atomicAdd(&s.scene_fill[sc], 1u);
+        if (pos < 2u * s.cap) {
+            s.tmp_key[pos] = key;
+            s.tmp_slot[pos] = slot;
+        }
+    }
+}
+
+// Bitonic sort of P (a power of two) 64-bit values in shared memory.
+template <int NT> __device__ __forceinline__ void bitonic_sort_smem(unsigned long long *a, uint32_t P) {
+    for (uint32_t k = 2; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < P / 2; i += NT) {
+                const uint32_t lo = 2u * j * (i / j) + (i % j), hi = lo + j;
+                const bool up = (lo & k) == 0u;
+                const unsigned long long x = a[lo], y = a[hi];
+                if ((x > y) == up) {
+                    a[lo] = y;
+                    a[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// One CTA per scene whose block count m has PMIN < nextpow2(m) <= PMAX:
+// sorts (key << 32 | slot) in shared memory (PMAX * 8 bytes, dynamic) and
+// writes the ranked block arrays and the map's rank values.  Scenes beyond
+// SCENE_SORT_MAX blocks raise ERR_SCENE_BLOCKS.
+constexpr uint32_t SCENE_SORT_SMALL = 2048;
+constexpr uint32_t SCENE_SORT_MAX = 16384;
+template <int NT, uint32_t PMIN, uint32_t PMAX> __global__ void __launch_bounds__(NT) k_scene_sort(DevScene s) {
+    extern __shared__ unsigned long long sbuf[];
+    for (uint32_t sc = blockIdx.x; sc < s.n_scenes; sc += gridDim.x) {
+        const uint32_t m = s.scene_nblk[sc];
+        if (m == 0) continue;
+        uint32_t P = 1;
+        while (P < m) P <<= 1;
+        if (P <= PMIN) continue;
+        if (P > PMAX) {
+            if (PMAX == SCENE_SORT_MAX && threadIdx.x == 0) atomicOr(s.err, ERR_SCENE_BLOCKS);
+            continue;
+        }
+        const uint32_t base = s.scene_bbase[sc];
+        if (base + m > 2u * s.cap) continue;  // overflow, already flagged
+        for (uint32_t q = threadIdx.x; q < P; q += NT)
+            sbuf[q] = q < m ? (((unsigned long long)s.tmp_key[base + q] << 32) | s.tmp_slot[base + q]) : NONE64;
+        __syncthreads();
+        bitonic_sort_smem<NT>(sbuf, P);
+        for (uint32_t q = threadIdx.x; q < m; q += NT) {
+            const uint32_t r = base + q;
+            if (r >= s.cap) break;
+            const unsigned long long v = sbuf[q];
+            const uint32_t slot = (uint32_t)v;
+            s.bkey[r] = (uint32_t)(v >> 32);
+            s.bslot[r] = slot;
+            s.bscene[r] = sc;
+            s.hvals[slot] = r;
+        }
+        __syncthreads();
+    }
+}
+
 // One warp per block: per-cell counts (cleared in the hash-slot array once
 // read) with their in-block exclusive scan, the block total, the +1 and -1
 // neighbour ranks (update_nbh_block_ids, sort.slang:100-117) and, for the
 // atomic P2G variants, zeroed nodes (reset, grid.slang:455-485).
-template <int D> __global__ void k_block_setup(DevScene s) {
+template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t lane = lane_id();
@@ -358,7 +527,7 @@ template <int D> __global__ void k_block_setup(DevScene s) {
             unpack_key<D>(s.bkey[r], b);
             assoc_offset<D>(q + 1, o);
             for (int k = 0; k < D; ++k) b[k] += fwd ? o[k] : -o[k];
-            const uint32_t slot = hash_find(s.hkeys, s.hcap, pack_key<D>(b));
+            const uint32_t slot = map_find<B>(s, pack_key<D>(b), B ? s.bscene[r] : 0u);
             const uint32_t rank = (slot == NONE) ? NONE : s.hvals[slot];
             if (fwd) s.bnbh[r * NN + q] = rank;
             else s.bnbh_rev[r * NN + q] = rank;
@@ -375,12 +544,13 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
 
 // Per particle: claim its slot in the block's cell range (the primary part
 // of finalize_particles_sort, sort.slang:304-357), warp-aggregated.
-__global__ void k_scatter(DevScene s) {
+template <bool B = false> __global__ void k_scatter(DevScene s) {
     const uint32_t lane = lane_id();
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < s.n; base += stride) {
+    const uint32_t n = n_particles<B>(s);
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
         const uint32_t i = base + lane;
-        const bool valid = i < s.n;
+        const bool valid = i < n;
         const unsigned mask = __ballot_sync(FULL_MASK, valid);
         if (!valid) continue;
         const uint32_t bin = s.pslot[i];

@@ -39,13 +39,14 @@ __device__ __forceinline__ uint32_t material_hash(const uint32_t *w) {
     return h == NONE ? 0x7fffffffu : h;
 }
 
-// Pass 1 of the upload: distinct materials into the material table.
-__global__ void k_mat_insert(DevScene s, IoBuffers io) {
+// Pass 1 of the upload: distinct materials of `count` staged records into
+// the material table.
+__global__ void k_mat_insert(DevScene s, IoBuffers io, uint32_t count) {
     const uint32_t lane = lane_id();
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < s.n; base += stride) {
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
         const uint32_t i = base + lane;
-        const bool valid = i < s.n;
+        const bool valid = i < count;
         const unsigned mask = __ballot_sync(FULL_MASK, valid);
         if (!valid) continue;
         uint32_t w[13];
@@ -76,13 +77,18 @@ __global__ void k_mat_insert(DevScene s, IoBuffers io) {
     }
 }
 
-// Pass 2 of the upload: record -> structure of arrays.
-template <int D> __global__ void k_ingest(DevScene s, IoBuffers io) {
+// Pass 2 of the upload: record i -> structure of arrays at storage index
+// base + i, original id i.  Multi-scene batches (B) tag the particle with its
+// scene slot and keep no upload-order side arrays (forces are rejected on
+// the host; radius and phase stay with the host).
+template <int D, bool B = false>
+__global__ void k_ingest(DevScene s, IoBuffers io, uint32_t base, uint32_t count, uint32_t scene) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const size_t n = s.n;
     uint32_t sflags = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
-        const slosh_particle &p = io.in[i];
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < count; i0 += stride) {
+        const uint32_t i = base + i0;
+        const slosh_particle &p = io.in[i0];
         uint32_t w[13];
         material_key(p.model, w);
         const uint32_t hsh = material_hash(w);
@@ -108,8 +114,10 @@ template <int D> __global__ void k_ingest(DevScene s, IoBuffers io) {
         s.pm[i] = make_float4(p.position[0], p.position[1], D == 3 ? p.position[2] : 0.f, p.mass);
         for (int k = 0; k < D; ++k) {
             s.vel[k * n + i] = p.velocity[k];
-            s.fdt[k * n + i] = p.force_dt[k];
-            if (p.force_dt[k] != 0.f) sflags |= SCENE_FORCE;
+            if constexpr (!B) {
+                s.fdt[k * n + i] = p.force_dt[k];
+                if (p.force_dt[k] != 0.f) sflags |= SCENE_FORCE;
+            }
         }
         for (int r = 0; r < D; ++r)
             for (int c = 0; c < D; ++c) {
@@ -118,11 +126,14 @@ template <int D> __global__ void k_ingest(DevScene s, IoBuffers io) {
             }
         s.V0[i] = p.init_volume;
         s.damping[i] = p.damping;
-        s.oid[i] = i;
+        s.oid[i] = i0;
         if (p.damping != 0.f) sflags |= SCENE_DAMPING;
-        io.r0[i] = p.init_radius;
-        io.phase[i] = p.phase;
-        s.flags[i] = (dense & FLAG_MAT_MASK) | (p.enabled ? FLAG_ENABLED : 0u) | (p.fixed ? FLAG_FIXED : 0u);
+        if constexpr (!B) {
+            io.r0[i] = p.init_radius;
+            io.phase[i] = p.phase;
+        }
+        s.flags[i] = (dense & FLAG_MAT_MASK) | (p.enabled ? FLAG_ENABLED : 0u) | (p.fixed ? FLAG_FIXED : 0u) |
+                     (scene << FLAG_SCENE_SHIFT);
         const bool sand = p.model.tag == SLOSH_MODEL_SAND_LINEAR || p.model.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN;
         for (int k = 0; k < 3; ++k) s.plastic[k * n + i] = sand ? p.model.data[k] : 0.f;
         if (sand) sflags |= SCENE_SAND;
@@ -132,11 +143,15 @@ template <int D> __global__ void k_ingest(DevScene s, IoBuffers io) {
 }
 
 // Structure of arrays -> records, back in upload order (stored particle i is
-// record oid[i]).
-template <int D> __global__ void k_egest(DevScene s, IoBuffers io) {
+// record oid[i]).  Multi-scene batches (B) export the particles of one scene;
+// radius and phase are filled in by the host.
+template <int D, bool B = false> __global__ void k_egest(DevScene s, IoBuffers io, uint32_t scene) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const size_t n = s.n;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+    const uint32_t count = n_particles<B>(s);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        if constexpr (B)
+            if (scene_of(s.flags[i]) != scene) continue;
         const uint32_t orig = s.oid[i];
         slosh_particle p;
         const float4 pm = s.pm[i];
@@ -159,10 +174,10 @@ template <int D> __global__ void k_egest(DevScene s, IoBuffers io) {
         if (D == 2) p.def_grad[8] = 0.f;
         p.vel_grad_det = 0.f;
         p.init_volume = s.V0[i];
-        p.init_radius = io.r0[orig];
+        p.init_radius = B ? 0.f : io.r0[orig];
         p.mass = pm.w;
         p.damping = s.has_damping ? s.damping[i] : 0.f;
-        p.phase = io.phase[orig];
+        p.phase = B ? 0.f : io.phase[orig];
         const uint32_t fl = s.flags[i];
         p.enabled = (fl & FLAG_ENABLED) ? 1u : 0u;
         p.fixed = (fl & FLAG_FIXED) ? 1u : 0u;
@@ -175,10 +190,13 @@ template <int D> __global__ void k_egest(DevScene s, IoBuffers io) {
     }
 }
 
-// Positions as vec4 (x, y, z, 0) in upload order.
-__global__ void k_positions(DevScene s, float4 *out) {
+// Positions as vec4 (x, y, z, 0) in upload order (of one scene in B).
+template <bool B = false> __global__ void k_positions(DevScene s, float4 *out, uint32_t scene) {
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+    const uint32_t count = n_particles<B>(s);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        if constexpr (B)
+            if (scene_of(s.flags[i]) != scene) continue;
         const float4 p = s.pm[i];
         out[s.oid[i]] = make_float4(p.x, p.y, p.z, 0.f);
     }

@@ -83,6 +83,21 @@ struct DevScene {
 
     Counters *ctr;
     uint32_t *err;
+
+    // ---- multi-scene batch (unused by the single-scene context) -------------
+    // `n` is then the plane stride (pool capacity) and the particle count in
+    // storage is *n_dev; blocks are hashed by (scene << 32 | key) in 64-bit
+    // maps and ranked scene-major, ascending key within a scene.
+    const SceneRec *scenes;
+    uint32_t n_scenes;               // scene slots
+    uint32_t *n_dev;
+    unsigned long long *hkeys64;
+    const unsigned long long *prev_hkeys64;
+    unsigned long long *clr_hkeys64;
+    uint32_t *bscene;                // scene of each ranked block
+    uint32_t *scene_nblk;            // blocks per scene this substep
+    uint32_t *scene_bbase;           // first block rank of each scene
+    uint32_t *scene_fill;            // scatter cursors
 };
 
 }  // namespace slosh

@@ -362,6 +362,36 @@ void to_dev_body(const slosh_body &b, DevBody &d) {
     d.friction = b.bc_friction;
 }
 
+void from_dev_body(const DevBody &d, slosh_body &b) {
+    std::memset(&b, 0, sizeof(b));
+    for (int k = 0; k < 4; ++k) {
+        b.shape_a[k] = d.sa[k];
+        b.rotation[k] = d.rot[k];
+    }
+    std::memcpy(&b.shape_a[3], &d.shape_type, 4);
+    for (int k = 0; k < 3; ++k) {
+        b.translation[k] = d.tra[k];
+        b.linvel[k] = d.linvel[k];
+        b.angvel[k] = d.angvel[k];
+        b.inv_mass[k] = d.inv_mass[k];
+        b.local_com[k] = d.local_com[k];
+    }
+    b.translation[3] = d.scale;
+    b.bc_type = d.bc_type;
+    b.bc_friction = d.friction;
+}
+
+// Frees the device resources of a context (not the object itself).
+void release_ctx(slosh_ctx *c) {
+    cudaSetDevice(c->device);
+    destroy_graphs(c);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void *p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    c->stream = nullptr;
+}
+
 }  // namespace
 
 extern "C" {
@@ -441,11 +471,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
 
 void slosh_ctx_destroy(slosh_ctx *c) {
     if (!c) return;
-    cudaSetDevice(c->device);
-    destroy_graphs(c);
-    if (c->stream) cudaStreamSynchronize(c->stream);
-    for (void *p : c->allocs) cudaFree(p);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    release_ctx(c);
     delete c;
 }
 
@@ -487,9 +513,9 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
         io.r0 = c->r0;
         io.phase = c->phase;
         const uint32_t g = grid_for(n, 256, (uint32_t)c->sm_count * 16);
-        k_mat_insert<<<g, 256, 0, st>>>(s, io);
-        if (c->dim == 3) k_ingest<3><<<g, 256, 0, st>>>(s, io);
-        else k_ingest<2><<<g, 256, 0, st>>>(s, io);
+        k_mat_insert<<<g, 256, 0, st>>>(s, io, n);
+        if (c->dim == 3) k_ingest<3><<<g, 256, 0, st>>>(s, io, 0u, n, 0u);
+        else k_ingest<2><<<g, 256, 0, st>>>(s, io, 0u, n, 0u);
         CK(cudaGetLastError());
     }
     uint32_t small[2] = {0, 0};
@@ -514,8 +540,8 @@ int slosh_download_particles(slosh_ctx *c, slosh_particle *out, uint32_t n, void
         io.r0 = c->r0;
         io.phase = c->phase;
         const uint32_t g = grid_for(c->n, 256, (uint32_t)c->sm_count * 16);
-        if (c->dim == 3) k_egest<3><<<g, 256, 0, st>>>(s, io);
-        else k_egest<2><<<g, 256, 0, st>>>(s, io);
+        if (c->dim == 3) k_egest<3><<<g, 256, 0, st>>>(s, io, 0u);
+        else k_egest<2><<<g, 256, 0, st>>>(s, io, 0u);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out, c->staging, (size_t)n * sizeof(slosh_particle), cudaMemcpyDeviceToHost, st));
     }
@@ -531,7 +557,7 @@ int slosh_download_positions(slosh_ctx *c, float *out, uint32_t n, void *stream)
     if (n > 0) {
         DevScene s = make_scene(c, c->parity, false);
         float4 *tmp = (float4 *)c->staging;  // staging holds >= 12 float4 per particle
-        k_positions<<<grid_for(c->n, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s, tmp);
+        k_positions<<<grid_for(c->n, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s, tmp, 0u);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out, tmp, (size_t)n * 16, cudaMemcpyDeviceToHost, st));
     }
@@ -563,25 +589,7 @@ int slosh_get_bodies(slosh_ctx *c, slosh_body *out, uint32_t n) {
     CK(cudaStreamSynchronize(c->stream));
     std::vector<DevBody> db(n);
     if (n) CK(cudaMemcpy(db.data(), c->bodies, n * sizeof(DevBody), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) {
-        slosh_body &b = out[i];
-        const DevBody &d = db[i];
-        for (int k = 0; k < 4; ++k) {
-            b.shape_a[k] = d.sa[k];
-            b.rotation[k] = d.rot[k];
-        }
-        std::memcpy(&b.shape_a[3], &d.shape_type, 4);
-        for (int k = 0; k < 3; ++k) {
-            b.translation[k] = d.tra[k];
-            b.linvel[k] = d.linvel[k];
-            b.angvel[k] = d.angvel[k];
-            b.inv_mass[k] = d.inv_mass[k];
-            b.local_com[k] = d.local_com[k];
-        }
-        b.translation[3] = d.scale;
-        b.bc_type = d.bc_type;
-        b.bc_friction = d.friction;
-    }
+    for (uint32_t i = 0; i < n; ++i) from_dev_body(db[i], out[i]);
     return SLOSH_OK;
 }
 
@@ -818,3 +826,5 @@ int slosh_last_error(const slosh_ctx *c, char *buf, size_t len) {
 }
 
 }  // extern "C"
+
+#include "batch.cuh"

@@ -5,6 +5,7 @@
 //   k_rigid        rigid-body pose integration
 #pragma once
 
+#include "grid_build.cuh"
 #include "models.cuh"
 #include "scene.cuh"
 
@@ -381,7 +382,7 @@ template <> struct SlabTile<2> {
     static constexpr int PY = 10, PZ = 0, SIZE = 100;
 };
 
-template <int D, bool DET> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScene s) {
+template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
     constexpr int NT = P2G_THREADS;
@@ -394,7 +395,7 @@ template <int D, bool DET> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p
     __shared__ float sp_v[2][D][NT];
     __shared__ float sp_c[2][D * D][NT];
     const uint32_t nb = s.ctr->n_blocks;
-    const float h = s.h, inv_h = 1.0f / s.h;
+    float h = s.h, inv_h = 1.0f / s.h;
     const size_t n = s.n;
     const uint32_t tid = threadIdx.x;
     const int mycell = (int)(threadIdx.x & 63u), myslab = (int)(threadIdx.x >> 6);
@@ -418,6 +419,10 @@ template <int D, bool DET> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p
         }
         if constexpr (!DET)
             for (int t = threadIdx.x; t < 4 * TILE; t += P2G_THREADS) (&tile[0][0])[t] = 0.f;
+        if constexpr (B) {
+            h = s.scenes[s.bscene[r]].h;
+            inv_h = 1.0f / h;
+        }
         int bv[D];
         unpack_key<D>(s.bkey[r], bv);
         const uint32_t lo = s.bcell[(size_t)r * CELLS + mycell];
@@ -677,15 +682,16 @@ __device__ __forceinline__ bool project_on_boundary(const DevBody &b, const floa
 // collide (shaders/slosh/collision/collide.slang:87-153).  Returns the
 // collider id or NONE; `nd` = (normal, dot(point_node - proj, normal)).
 template <int D>
-__device__ __forceinline__ uint32_t collide(const DevScene &s, const float *pt, float4 &nd) {
-    const float cap = s.h * 1.5f;
+__device__ __forceinline__ uint32_t collide(const DevBody *bodies, uint32_t n_bodies, float h, const float *pt,
+                                            float4 &nd) {
+    const float cap = h * 1.5f;
     float best = 1.0e10f;
     uint32_t id = NONE;
     float bn[D] = {}, bp[D] = {};
-    for (uint32_t i = 0; i < s.n_bodies && i < MAX_BODIES; ++i) {
+    for (uint32_t i = 0; i < n_bodies && i < MAX_BODIES; ++i) {
         float proj[D];
         bool inside = false;
-        if (!project_on_boundary<D>(s.bodies[i], pt, proj, inside)) continue;
+        if (!project_on_boundary<D>(bodies[i], pt, proj, inside)) continue;
         float dpt[D], n2 = 0.f;
         bool within = true;
 #pragma unroll
@@ -761,14 +767,25 @@ __device__ __forceinline__ void project_velocity(uint32_t type, float friction, 
 // node.  The collision of a node is reused from the previous substep when
 // its block was active there (slosh's cache, which assumes static colliders),
 // otherwise collide() runs; both are recorded for the next substep.
-template <int D> __global__ void k_grid_update(DevScene s) {
+template <int D, bool B = false> __global__ void k_grid_update(DevScene s) {
     constexpr int BW = Geo<D>::BW;
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const float h = s.h, dt = s.dt;
-    const float vlim = h / dt;
+    float h = s.h, dt = s.dt, grav[3] = {s.gravity[0], s.gravity[1], s.gravity[2]};
+    const DevBody *bodies = s.bodies;
+    uint32_t n_bodies = s.n_bodies, sc = 0;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * 64u; t += stride) {
         const uint32_t r = t >> 6, node = t & 63u;
+        if constexpr (B) {
+            sc = s.bscene[r];
+            const SceneRec &rec = s.scenes[sc];
+            h = rec.h;
+            dt = rec.dt;
+            for (int k = 0; k < 3; ++k) grav[k] = rec.gravity[k];
+            bodies = s.bodies + rec.body_first;
+            n_bodies = rec.n_bodies;
+        }
+        const float vlim = h / dt;
         const uint32_t key = s.bkey[r];
         int bv[D], lc[D];
         unpack_key<D>(key, bv);
@@ -826,24 +843,24 @@ template <int D> __global__ void k_grid_update(DevScene s) {
         float vel[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) {
-            const float v = (pm[k] + mass * s.gravity[k] * dt) * inv_mass;
+            const float v = (pm[k] + mass * grav[k] * dt) * inv_mass;
             vel[k] = fminf(fmaxf(v, -vlim), vlim);
         }
         float4 cn;
         uint32_t cid;
-        const uint32_t pslot = hash_find(s.prev_hkeys, s.hcap, key);
+        const uint32_t pslot = map_find_prev<B>(s, key, sc);
         const uint32_t prank = (pslot == NONE) ? NONE : s.prev_hvals[pslot];
         if (prank != NONE) {
             cn = s.prev_coll[(size_t)prank * 64u + node];
             cid = s.prev_coll_id[(size_t)prank * 64u + node];
         } else {
-            cid = collide<D>(s, cell_pos, cn);
+            cid = collide<D>(bodies, n_bodies, h, cell_pos, cn);
         }
         s.coll[t] = cn;
         s.coll_id[t] = cid;
         if (cid != NONE) {
             const float n[3] = {cn.x, cn.y, cn.z};
-            project_velocity<D>(s.bodies[cid].bc_type, s.bodies[cid].friction, vel, n, cn.w - h, dt);
+            project_velocity<D>(bodies[cid].bc_type, bodies[cid].friction, vel, n, cn.w - h, dt);
         }
         s.nodes[t] = make_float4(vel[0], vel[1], D == 3 ? vel[D - 1] : 0.f, mass);
     }
@@ -859,7 +876,7 @@ template <int D> __global__ void k_grid_update(DevScene s) {
 // staged into shared memory with cp.async while the current particle is
 // computed; each thread consumes only its own staged slot, so the particle
 // loop has no barrier.
-template <int D, int NT> __global__ void __launch_bounds__(NT, 4) k_g2p_update(DevScene s) {
+template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float tv[D][TILE];
     __shared__ float4 st_pm[2][NT];
@@ -870,22 +887,28 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 4) k_g2p_update(D
     __shared__ uint32_t st_fl[2][NT];
     __shared__ uint32_t st_oid[2][NT];
     const uint32_t nb = s.ctr->n_blocks;
-    const float h = s.h, dt = s.dt;
-    const float inv_d = 4.0f / (h * h);
-    const float vmax = h / dt;
+    float h = s.h, dt = s.dt, inv_h = s.inv_h;
+    uint32_t h_pow2 = s.h_pow2;
+    float inv_d = 4.0f / (h * h);
+    float vmax = h / dt;
     const size_t n = s.n;
     const uint32_t tid = threadIdx.x;
     if (s.clear_tail) {
-        // Clear the next substep's hash map and the key histogram (their
-        // readers in this substep have all run).
+        // Clear the next substep's hash map and the key histogram / per-scene
+        // block counts (their readers in this substep have all run).
         const uint32_t g0 = blockIdx.x * NT + tid, gs = gridDim.x * NT;
         for (uint32_t q = g0; q < s.hcap; q += gs) {
-            s.clr_hkeys[q] = NONE;
+            if constexpr (B) s.clr_hkeys64[q] = NONE64;
+            else s.clr_hkeys[q] = NONE;
             s.clr_hvals[q] = NONE;
         }
-        for (uint32_t q = g0; q < HIST_BINS; q += gs) {
-            s.hist[q] = 0u;
-            s.hist_fill[q] = 0u;
+        if constexpr (B) {
+            for (uint32_t q = g0; q < s.n_scenes; q += gs) s.scene_nblk[q] = 0u;
+        } else {
+            for (uint32_t q = g0; q < HIST_BINS; q += gs) {
+                s.hist[q] = 0u;
+                s.hist_fill[q] = 0u;
+            }
         }
         if (*s.err != 0u)
             for (size_t q = g0; q < (size_t)s.hcap * CELLS; q += gs) s.slot_counts[q] = 0u;
@@ -913,6 +936,15 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 4) k_g2p_update(D
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
         stage(0, first, tid, np);
+        if constexpr (B) {
+            const SceneRec &rec = s.scenes[s.bscene[r]];
+            h = rec.h;
+            dt = rec.dt;
+            inv_h = rec.inv_h;
+            h_pow2 = rec.h_pow2;
+            inv_d = 4.0f / (h * h);
+            vmax = h / dt;
+        }
         for (int t = threadIdx.x; t < TILE; t += NT) {
             uint32_t rank, local;
             float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -946,11 +978,11 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 4) k_g2p_update(D
                 bool in_block = true;
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
-                    const float assoc = rintf(div_h(x[k], h, s.inv_h, s.h_pow2)) - 1.0f;
+                    const float assoc = rintf(div_h(x[k], h, inv_h, h_pow2)) - 1.0f;
                     a[k] = (int)assoc - bv[k] * BW;
                     in_block = in_block && a[k] >= 0 && a[k] < BW;
                     d0[k] = assoc * h - x[k];
-                    bspline_weights(div_h(-d0[k], h, s.inv_h, s.h_pow2), w[k]);
+                    bspline_weights(div_h(-d0[k], h, inv_h, h_pow2), w[k]);
                 }
                 if (!in_block) {  // packed-key aliasing: gather nothing
                     atomicOr(s.err, ERR_KEY_RANGE);
@@ -1144,18 +1176,29 @@ template <int D, int NT> __global__ void __launch_bounds__(NT, 4) k_g2p_update(D
 // kernels, so velocity capping (guarded by a non-zero impulse) never runs.
 // The last kernel of the substep: it also resets the grid-build counters for
 // the next substep.
-template <int D> __global__ void k_rigid(DevScene s) {
-    const uint32_t id = threadIdx.x;
+// Multi-scene batches (B): bodies of all scenes in one table, each with its
+// scene's dt and gravity (bodies of dropped scenes are left alone), and the
+// particle count in storage becomes this substep's sorted count.
+template <int D, bool B = false> __global__ void k_rigid(DevScene s) {
+    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id == 0 && s.clear_tail) {
-        s.ctr->last_n_blocks = s.ctr->n_blocks;
+        const uint32_t nb = s.ctr->n_blocks;
+        s.ctr->last_n_blocks = nb;
         s.ctr->last_n_primary = min(s.ctr->n_primary, s.cap);
         s.ctr->n_primary = 0u;
         s.ctr->n_extra = 0u;
         s.ctr->n_blocks = 0u;
+        if constexpr (B) *s.n_dev = nb ? s.bfirst[nb - 1] + s.bnp[nb - 1] : 0u;
     }
     if (id >= s.n_bodies) return;
     DevBody b = s.bodies[id];
-    const float dt = s.dt;
+    float dt = s.dt, grav[3] = {s.gravity[0], s.gravity[1], s.gravity[2]};
+    if constexpr (B) {
+        const SceneRec &rec = s.scenes[b.scene];
+        if (!rec.live) return;
+        dt = rec.dt;
+        for (int k = 0; k < 3; ++k) grav[k] = rec.gravity[k];
+    }
     float init_com[3] = {0.f, 0.f, 0.f};
     pose_mul_pt<D>(b, b.local_com, init_com);
     if constexpr (D == 3) {
@@ -1193,7 +1236,7 @@ template <int D> __global__ void k_rigid(DevScene s) {
         b.rot[0] = nc;
         b.rot[1] = ns;
     }
-    for (int k = 0; k < D; ++k) b.linvel[k] = b.linvel[k] + s.gravity[k] * ((b.inv_mass[k] != 0.f) ? 1.f : 0.f) * dt;
+    for (int k = 0; k < D; ++k) b.linvel[k] = b.linvel[k] + grav[k] * ((b.inv_mass[k] != 0.f) ? 1.f : 0.f) * dt;
     s.bodies[id] = b;
 }
 

@@ -1,0 +1,153 @@
+"""Multi-scene batches (slosh_batch_* C ABI) on the GPU.
+
+- a batch holding one scene reproduces the single-scene context;
+- a scene's results are bit-identical alone and in a mix, also while other
+  scenes join and leave (continuous batching);
+- every scene of a mix matches the oracle within the FP32 tolerance of the
+  single-scene parity tests;
+- every launch shape the autotuner tries gives identical bits;
+- capacity, state and unsupported-input errors are reported, not faulted.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from slosh_b200 import scenes
+from slosh_b200._lib import SLOSH_E_CAPACITY, SLOSH_E_INVALID, SLOSH_E_STATE, SloshError
+from slosh_b200.batch import MpmBatch
+from slosh_b200.pipeline import MpmPipeline
+
+pytestmark = pytest.mark.gpu
+
+
+def close(name, got, exp, atol, rtol):
+    got = np.asarray(got, np.float64)
+    exp = np.asarray(exp, np.float64)
+    err = np.abs(got - exp).max() if got.size else 0.0
+    bound = atol + rtol * (np.abs(exp).max() if exp.size else 0.0)
+    print(f"{name}: max err {err:.3e} bound {bound:.3e}")
+    assert err <= bound, f"{name}: max err {err:.3e} > {bound:.3e}"
+
+
+def mix_scenes():
+    return [
+        scenes.random_scene_3d(6000, "sand", 1 / 64, seed=11),
+        scenes.random_scene_3d(9000, "elastic", 1 / 128, seed=12),
+        scenes.random_scene_3d(4000, "fluid", 1 / 64, seed=13),
+        scenes.random_scene_3d(12000, "sand", 1 / 128, seed=14),
+    ]
+
+
+def new_batch(**kw):
+    args = dict(max_particles=1 << 17, grid_capacity=1 << 13, max_scenes=64, max_bodies=256)
+    args.update(kw)
+    return MpmBatch(3, **args)
+
+
+def fields(p):
+    return {k: p[k] for k in ("position", "velocity", "def_grad", "affine", "mass", "model")}
+
+
+def test_batch_of_one_matches_single_context(cuda_lib):
+    sc = scenes.sand_column_3d(h=1 / 32, substeps=10)
+    data = scenes.build_mpm_data(sc)
+    MpmPipeline().launch_step(data, 10)
+    single = data.download_particles()
+    data.close()
+    b = new_batch()
+    slot = b.add(sc)
+    b.step(10)
+    got = b.download_particles(slot)
+    b.close()
+    for k, v in fields(single).items():
+        close(f"batch of one vs context {k}", got[k], v, 1e-7, 1e-6)
+    assert np.array_equal(got["init_radius"], single["init_radius"])
+
+
+def test_alone_vs_mix_bit_identical(cuda_lib):
+    target = scenes.random_scene_3d(8000, "sand", 1 / 64, seed=21)
+    alone = new_batch()
+    s0 = alone.add(target)
+    alone.step(30)
+    ref = alone.download_particles(s0)
+    alone.close()
+
+    others = mix_scenes()
+    mix = new_batch()
+    mix.add(others[0])
+    a = mix.add(others[1])
+    st = mix.add(target)
+    mix.step(10)
+    mix.remove_scene(a)  # leaves at the next substep
+    mix.add(others[2])
+    mix.step(10)
+    mix.add(others[3])
+    mix.step(10)
+    got = mix.download_particles(st)
+    mix.close()
+    assert got.tobytes() == ref.tobytes()
+
+
+def test_mix_matches_oracle(cuda_lib):
+    scs = mix_scenes()
+    b = new_batch()
+    slots = [b.add(sc) for sc in scs]
+    b.step(5)
+    loose = 5.0  # the single-scene parity tests' factor for multi-substep runs
+    for sc, sl in zip(scs, slots):
+        orc = O.from_scene(sc, threads=8)
+        orc.step(5)
+        o = orc.get_particles()
+        g = b.download_particles(sl)
+        tag = sc.name
+        close(f"{tag} position", g["position"], o["position"], 1e-6 * loose, 0)
+        close(f"{tag} velocity", g["velocity"], o["velocity"], 1e-6 * loose, 1e-4 * loose)
+        close(f"{tag} def_grad", g["def_grad"], o["def_grad"], 2e-6 * loose, 2e-6 * loose)
+        close(f"{tag} mass", g["mass"], o["mass"], 0, 0)
+    b.close()
+
+
+def test_launch_shapes_give_identical_bits(cuda_lib):
+    scs = mix_scenes()
+    results = []
+    for shape in [(8, 128, 8), (4, 64, 8), (16, 256, 4)]:
+        b = new_batch()
+        slots = [b.add(sc) for sc in scs]
+        b.set_tuning(*shape)
+        b.step(8)
+        results.append([b.download_particles(s).tobytes() for s in slots])
+        b.close()
+    assert results[0] == results[1] == results[2]
+    b = new_batch()
+    for sc in scs:
+        b.add(sc)
+    tuned = b.autotune(1)
+    assert tuned["g2p_threads"] in (64, 128, 256)
+    b.step(2)
+    b.sync()
+    b.close()
+
+
+def test_batch_errors_reported(cuda_lib):
+    b = new_batch(max_particles=5000, max_scenes=2)
+    sc = scenes.random_scene_3d(4000, "fluid", 1 / 64, seed=31)
+    s0 = b.add(sc)
+    with pytest.raises(SloshError) as e:
+        b.add(sc)  # pool of 5000 particles
+    assert e.value.code == SLOSH_E_CAPACITY
+    forced = sc.particles.copy()[:100]
+    forced["force_dt"][:, 0] = 1.0
+    with pytest.raises(SloshError) as e:
+        b.add_scene(forced, sc.cell_width, sc.params, sc.bodies)
+    assert e.value.code == SLOSH_E_INVALID
+    b.remove_scene(s0)
+    with pytest.raises(SloshError) as e:
+        b.remove_scene(s0)
+    assert e.value.code == SLOSH_E_STATE
+    b.step(1)  # the removed scene leaves storage
+    assert b.stats()["n_particles"] == 0
+    s1 = b.add(sc)  # the pool and the slot are free again
+    b.step(2)
+    assert b.stats()["live_scenes"] == 1 and b.stats()["n_particles"] == sc.n
+    b.positions(s1)
+    b.close()

@@ -57,6 +57,8 @@ def test_record_layouts_match_c_structs(tmp_path):
                  offsetof(slosh_particle, enabled), sizeof(slosh_body), offsetof(slosh_body, bc_type),
                  sizeof(slosh_model));
           printf("%zu %zu\\n", sizeof(slosh_grid_dump), offsetof(slosh_grid_dump, neighbors));
+          printf("%zu %zu %zu %zu %zu\\n", sizeof(slosh_batch_config), sizeof(slosh_scene_desc),
+                 sizeof(slosh_tuning), sizeof(slosh_batch_stats), offsetof(slosh_batch_stats, tuning));
           return 0;
         }
         """
@@ -77,6 +79,13 @@ def test_record_layouts_match_c_structs(tmp_path):
 
     assert vals[6] == ctypes.sizeof(_lib.SloshGridDump)
     assert vals[7] == _lib.SloshGridDump.neighbors.offset
+    assert vals[8:13] == [
+        ctypes.sizeof(_lib.SloshBatchConfig),
+        ctypes.sizeof(_lib.SloshSceneDesc),
+        ctypes.sizeof(_lib.SloshTuning),
+        ctypes.sizeof(_lib.SloshBatchStats),
+        _lib.SloshBatchStats.tuning.offset,
+    ]
 
 
 def test_lame_parameters():
