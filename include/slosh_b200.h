@@ -367,6 +367,73 @@ int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream);
 int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t);
 int slosh_batch_last_error(const slosh_batch *b, char *buf, size_t len);
 
+/* ---- Serving loop -----------------------------------------------------------
+ * A request is one scene to advance by a number of substeps.  A worker
+ * thread owns a batch: it admits queued requests in arrival order while their
+ * device footprint fits the HBM budget (particle pool, block capacity, scene
+ * slots), advances all in-flight scenes together (continuous batching:
+ * scenes join and leave between batched steps), and on completion writes the
+ * scene's final positions to the request's output buffer and frees its slot.
+ * No reference counterpart: slosh's frame loops (src_testbed/step.rs:208-224)
+ * step one scene at a time. */
+typedef struct slosh_server slosh_server;
+
+typedef struct slosh_server_config {
+    int32_t dim;
+    int32_t device;
+    uint64_t hbm_budget_bytes;  /* the batch's pool is carved from this      */
+    uint32_t max_scenes;        /* in-flight scenes                            */
+    uint32_t max_bodies;
+    uint32_t tick_substeps;     /* substeps per batched step, at most          */
+    uint32_t max_in_flight;     /* 0: no limit; 1: one request at a time       */
+    uint32_t autotune;          /* 1: tune the launch shape once under load    */
+    uint32_t pad;
+} slosh_server_config;
+
+typedef struct slosh_request {
+    slosh_scene_desc desc;
+    uint32_t n;                      /* particles                                  */
+    uint32_t n_bodies;
+    uint32_t substeps;
+    uint32_t pad;
+    const slosh_particle *particles; /* caller-owned until completion            */
+    const slosh_body *bodies;        /* caller-owned until completion            */
+    float *out_positions;            /* n x 4 floats, written at completion      */
+} slosh_request;
+
+typedef struct slosh_completion {
+    uint64_t id;
+    int32_t status;  /* SLOSH_OK or the error that ended the request         */
+    uint32_t n;
+    uint32_t substeps;
+    uint32_t pad;
+    double submit_s, admit_s, done_s;  /* server clock, seconds                */
+} slosh_completion;
+
+typedef struct slosh_server_stats {
+    uint64_t submitted, admitted, completed;
+    uint64_t particle_substeps;  /* work done                                   */
+    uint64_t in_flight_bytes;    /* footprint of the admitted scenes            */
+    uint64_t pool_bytes;         /* device memory the batch holds               */
+    double busy_s;               /* time with at least one scene in flight      */
+    double now_s;
+    uint32_t in_flight, queued;
+    uint32_t max_in_flight_seen, pad;
+} slosh_server_stats;
+
+int slosh_server_create(const slosh_server_config *cfg, slosh_server **out);
+/* Stops the worker; queued and in-flight requests are dropped. */
+void slosh_server_destroy(slosh_server *s);
+/* Queues a request (thread-safe, non-blocking); SLOSH_E_CAPACITY when it
+ * can never fit the budget's pool. */
+int slosh_server_submit(slosh_server *s, const slosh_request *req, uint64_t *id);
+/* Takes up to `cap` completions (non-blocking). */
+int slosh_server_poll(slosh_server *s, slosh_completion *out, uint32_t cap, uint32_t *n_out);
+/* Waits until nothing is queued or in flight; SLOSH_E_STATE on timeout. */
+int slosh_server_wait_idle(slosh_server *s, double timeout_s);
+int slosh_server_get_stats(slosh_server *s, slosh_server_stats *out);
+int slosh_server_last_error(const slosh_server *s, char *buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -164,6 +164,63 @@ class SloshBatchStats(ctypes.Structure):
     ]
 
 
+class SloshServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("hbm_budget_bytes", ctypes.c_uint64),
+        ("max_scenes", ctypes.c_uint32),
+        ("max_bodies", ctypes.c_uint32),
+        ("tick_substeps", ctypes.c_uint32),
+        ("max_in_flight", ctypes.c_uint32),
+        ("autotune", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+    ]
+
+
+class SloshRequest(ctypes.Structure):
+    _fields_ = [
+        ("desc", SloshSceneDesc),
+        ("n", ctypes.c_uint32),
+        ("n_bodies", ctypes.c_uint32),
+        ("substeps", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("particles", ctypes.c_void_p),
+        ("bodies", ctypes.c_void_p),
+        ("out_positions", ctypes.c_void_p),
+    ]
+
+
+class SloshCompletion(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_uint64),
+        ("status", ctypes.c_int32),
+        ("n", ctypes.c_uint32),
+        ("substeps", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("submit_s", ctypes.c_double),
+        ("admit_s", ctypes.c_double),
+        ("done_s", ctypes.c_double),
+    ]
+
+
+class SloshServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64),
+        ("admitted", ctypes.c_uint64),
+        ("completed", ctypes.c_uint64),
+        ("particle_substeps", ctypes.c_uint64),
+        ("in_flight_bytes", ctypes.c_uint64),
+        ("pool_bytes", ctypes.c_uint64),
+        ("busy_s", ctypes.c_double),
+        ("now_s", ctypes.c_double),
+        ("in_flight", ctypes.c_uint32),
+        ("queued", ctypes.c_uint32),
+        ("max_in_flight_seen", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+    ]
+
+
 # Every symbol include/slosh_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
@@ -203,6 +260,13 @@ SIGNATURES = {
     "slosh_batch_autotune": (ctypes.c_int, [_P, _U32, _P]),
     "slosh_batch_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(SloshTuning)]),
     "slosh_batch_last_error": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "slosh_server_create": (ctypes.c_int, [ctypes.POINTER(SloshServerConfig), ctypes.POINTER(_P)]),
+    "slosh_server_destroy": (None, [_P]),
+    "slosh_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(SloshRequest), ctypes.POINTER(ctypes.c_uint64)]),
+    "slosh_server_poll": (ctypes.c_int, [_P, _P, _U32, ctypes.POINTER(_U32)]),
+    "slosh_server_wait_idle": (ctypes.c_int, [_P, ctypes.c_double]),
+    "slosh_server_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(SloshServerStats)]),
+    "slosh_server_last_error": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t]),
 }
 
 _lib = None

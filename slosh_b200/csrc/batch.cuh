@@ -521,9 +521,15 @@ int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t) {
     return SLOSH_OK;
 }
 
-int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream) {
-    if (!b) return SLOSH_E_INVALID;
+}  // extern "C"
+
+namespace {
+
+// Autotuner body; *ran = substeps the timing advanced the scenes by (0 when
+// a cached shape was applied).
+int batch_autotune(slosh_batch *b, uint32_t substeps, void *stream, uint32_t *ran) {
     slosh_ctx *c = &b->c;
+    *ran = 0;
     if (b->n_storage == 0) return fail(c, SLOSH_E_STATE, "no scenes");
     const auto key = tune_key(b);
     {
@@ -550,6 +556,7 @@ int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream) {
             enqueue_batch_substep_any(b, st, c->parity);
             c->parity ^= 1u;
         }
+        *ran += reps + 1;
         CK(cudaEventRecord(e1, st));
         CK(cudaEventSynchronize(e1));
         CK(cudaGetLastError());
@@ -576,6 +583,16 @@ int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream) {
     int r = slosh_batch_set_tuning(b, &pick_t);
     if (r) return r;
     return batch_check_error(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream) {
+    if (!b) return SLOSH_E_INVALID;
+    uint32_t ran = 0;
+    return batch_autotune(b, substeps, stream, &ran);
 }
 
 int slosh_batch_last_error(const slosh_batch *b, char *buf, size_t len) {

@@ -828,3 +828,4 @@ int slosh_last_error(const slosh_ctx *c, char *buf, size_t len) {
 }  // extern "C"
 
 #include "batch.cuh"
+#include "server.cuh"

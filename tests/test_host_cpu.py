@@ -59,6 +59,8 @@ def test_record_layouts_match_c_structs(tmp_path):
           printf("%zu %zu\\n", sizeof(slosh_grid_dump), offsetof(slosh_grid_dump, neighbors));
           printf("%zu %zu %zu %zu %zu\\n", sizeof(slosh_batch_config), sizeof(slosh_scene_desc),
                  sizeof(slosh_tuning), sizeof(slosh_batch_stats), offsetof(slosh_batch_stats, tuning));
+          printf("%zu %zu %zu %zu %zu\\n", sizeof(slosh_server_config), sizeof(slosh_request),
+                 offsetof(slosh_request, particles), sizeof(slosh_completion), sizeof(slosh_server_stats));
           return 0;
         }
         """
@@ -85,6 +87,13 @@ def test_record_layouts_match_c_structs(tmp_path):
         ctypes.sizeof(_lib.SloshTuning),
         ctypes.sizeof(_lib.SloshBatchStats),
         _lib.SloshBatchStats.tuning.offset,
+    ]
+    assert vals[13:18] == [
+        ctypes.sizeof(_lib.SloshServerConfig),
+        ctypes.sizeof(_lib.SloshRequest),
+        _lib.SloshRequest.particles.offset,
+        ctypes.sizeof(_lib.SloshCompletion),
+        ctypes.sizeof(_lib.SloshServerStats),
     ]
 
 
