@@ -50,10 +50,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument(
         "--workload",
-        choices=["sand", "batched", "served"],
+        choices=["sand", "dam_break_2d", "elastic_drop_3d", "batched", "served", "precision"],
         default="sand",
-        help="sand: the 4.74 M-particle sand column (default); batched: 256 independent scenes in one "
-        "batch vs the plain per-scene loop; served: Poisson request stream through the serving loop",
+        help="sand: the 4.74 M-particle sand column (default); dam_break_2d, elastic_drop_3d: the other "
+        "plain scenes; batched: 256 independent scenes in one batch vs the plain per-scene loop; served: "
+        "Poisson request stream through the serving loop; precision: sand column vs the FP64 oracle",
     )
     ap.add_argument("--scenes", type=int, default=256, help="batched: number of scenes")
     ap.add_argument("--requests", type=int, default=200, help="served: requests in the trace")
@@ -721,10 +722,202 @@ def main_served(args):
     return 0
 
 
+def plain_alg_bytes(dim: int, sand: bool, n: int, n_nodes: int) -> dict:
+    """Algorithmic bytes per launch of the two transfer kernels."""
+    d2 = dim * dim
+    pl = 12 if sand else 0
+    return {
+        # x+m, perm, V0, flags, F, plastic read; x, v, C, F, plastic written; node velocities read
+        "k_g2p_update": n * (16 + 4 + 4 + 4 + 4 * d2 + pl + 4 * dim + 4 * dim + 4 * d2 + 4 * d2 + pl)
+        + n_nodes * 4 * dim,
+        # perm, x+m, v, C read; node partial tiles written
+        "k_p2g": n * (4 + 16 + 4 * dim + 4 * d2) + n_nodes * 16,
+    }
+
+
+def main_plain(args):
+    """The other plain single-scene configurations: the 2D dam break
+    (62.6 k particles, Tait fluid) and the 3D elastic drop (524 k particles,
+    two fixed-corotated cubes), timed like the sand column."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+    from slosh_b200 import scenes
+    from slosh_b200._lib import PARTICLE_DTYPE
+    from slosh_b200.pipeline import MpmPipeline
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if args.workload == "dam_break_2d":
+        sc = scenes.dam_break_2d()
+        desc = "dam_break_2d: Tait fluid column 0.4x0.6 at 2x2 ppc, dx=1/256, stick walls, dt=1e-4"
+        b_alg, sand = 129.0, False
+    else:
+        sc = scenes.elastic_drop_3d()
+        desc = "elastic_drop_3d: two fixed-corotated cubes (E=1e5, nu=0.3) at 8 ppc, dx=1/128, slip floor, dt=5e-5"
+        b_alg, sand = 230.0, False
+    n = sc.n
+    data = scenes.build_mpm_data(sc, device=local)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    pipe = MpmPipeline()
+    pipe.launch_step(data, max(args.warmup, 3), sptr)
+    data.sync(sptr)
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    pipe.launch_step(data, args.steps, sptr)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ck = clocks.stop()
+    data.sync(sptr)
+    ms = ev0.elapsed_time(ev1)
+    value = n * args.steps / (ms / 1e3)
+    prof = data.profile_substeps(args.profile_steps, sptr)
+    per_substep = {k: v / args.profile_steps for k, v in prof.items()}
+    dom = max(per_substep, key=per_substep.get)
+    peak, peak_kind = measured_peaks()
+    nb = data.stats()["n_blocks"]
+    ab = plain_alg_bytes(sc.dim, sand, n, nb * 64).get(dom)
+    roof = None
+    if ab is not None:
+        achieved = ab / (per_substep[dom] / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None}
+    launches = data.kernels_per_substep * args.steps
+    # e2e: upload + K substeps + positions through the public API
+    buf = torch.empty(n * PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+    host = buf.numpy().view(PARTICLE_DTYPE)
+    host[:] = sc.particles
+    outbuf = torch.empty(n * 16, dtype=torch.uint8, pin_memory=True)
+    out = outbuf.numpy().view(np.float32).reshape(n, 4)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    data.upload(host, sptr)
+    pipe.launch_step(data, args.steps, sptr)
+    data.positions(out, sptr)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e = n * args.steps / (e0.elapsed_time(e1) / 1e3)
+    data.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        orc = O.from_scene(sc, threads=os.cpu_count() or 1)
+        orc.step(1)
+        done, t0 = 0, time.perf_counter()
+        while done < 2 or (time.perf_counter() - t0 < args.cpu_seconds and done < sc.substeps):
+            orc.step(1)
+            done += 1
+        el = time.perf_counter() - t0
+        orc.close()
+        cpu = {"value": n * done / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"full scene, {done} substeps after 1 warm-up"}
+    line = {
+        "metric": f"particle-substeps/s ({args.workload})",
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded lattice + jitter; no dataset)",
+        "config": {"workload": desc, "particles": n, "dim": sc.dim, "active_blocks": nb},
+        "roofline": roof,
+        "substep_roofline": {"bytes_per_particle_substep": b_alg, "achieved_gbs": value * b_alg / 1e9,
+                             "frac_of_peak": value * b_alg / 1e9 / peak},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * 192, "d2h_bytes_per_step": n * 16},
+        "gpu_launches": launches,
+        "clocks": ck,
+        "kernel_ms_per_substep": per_substep,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main_precision(args):
+    """Precision study of the sand column: the FP32 GPU substep and the FP32
+    oracle against the FP64 oracle after K substeps, on the column at
+    dx = 1/64 (the FP64 oracle cannot run the 4.74 M-particle column for 500
+    substeps in minutes; the material, geometry, bodies and dt are those of
+    the full configuration)."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+    from slosh_b200 import scenes
+    from slosh_b200.pipeline import MpmPipeline
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    sc = scenes.sand_column_3d(h=args.h if args.h > 1.0 / 100 else 1.0 / 64, substeps=args.steps)
+    data = scenes.build_mpm_data(sc, device=local)
+    MpmPipeline().launch_step(data, args.steps)
+    g = data.download_particles()
+    fp64_fallbacks = data.stats()["n_svd_fp64"]
+    data.close()
+    threads = os.cpu_count() or 1
+    o32 = O.from_scene(sc, threads=threads)
+    o64 = O.from_scene(sc, double=True, threads=threads)
+    t0 = time.perf_counter()
+    o32.step(args.steps)
+    o64.step(args.steps)
+    cpu_s = time.perf_counter() - t0
+    r32, r64 = o32.get_particles(), o64.get_particles()
+    o32.close()
+    o64.close()
+
+    def err(a, b, k, cols=None):
+        x = np.asarray(a[k], np.float64)
+        y = np.asarray(b[k], np.float64)
+        if cols is not None:
+            x, y = x[:, cols], y[:, cols]
+        d = np.abs(x - y)
+        return {"max": float(d.max()), "rms": float(np.sqrt((d**2).mean())), "scale": float(np.abs(y).max())}
+
+    res = {}
+    for name, a in (("gpu_fp32", g), ("oracle_fp32", r32)):
+        res[name] = {
+            "position": err(a, r64, "position"),
+            "velocity": err(a, r64, "velocity"),
+            "def_grad": err(a, r64, "def_grad"),
+            "plastic_q": err(a, r64, "model", [1]),
+        }
+    line = {
+        "metric": "error vs FP64 oracle (sand column)",
+        "workload": f"sand_column_3d at dx={sc.cell_width:.6g}: {sc.n} particles, {args.steps} substeps, dt=2e-5",
+        "particles": sc.n,
+        "substeps": args.steps,
+        "cell_width": sc.cell_width,
+        "errors": res,
+        "position_max_err_in_cells": res["gpu_fp32"]["position"]["max"] / sc.cell_width,
+        "gpu_svd_fp64_fallbacks": fp64_fallbacks,
+        "oracle_cpu_seconds": cpu_s,
+        "oracle_threads": threads,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.ncu_case:
         return main_ncu_case(args)
+    if args.workload in ("dam_break_2d", "elastic_drop_3d"):
+        return main_plain(args)
+    if args.workload == "precision":
+        return main_precision(args)
     if args.workload == "batched":
         return main_batched(args)
     if args.workload == "served":

@@ -279,6 +279,14 @@ int slosh_prefix_sum(slosh_ctx *ctx, const uint32_t *in, uint32_t *out,
 int slosh_prefix_sum_noalloc(const uint32_t *d_in, uint32_t *d_out, uint32_t n,
                              void *stream);
 
+/* Largest stable timestep of the current particles, in seconds, for
+ * adaptive substepping: per enabled particle the model's sound-speed bound
+ * CFL * h / max(|v|, c) and the velocity bound h / |v|, quantised to whole
+ * picoseconds (u32, saturating at ~4.29e-3 s), minimum over particles.
+ * Replaces WgTimestepBounds::compute_bounds (src/solver/timestep_bound.rs:58-81;
+ * shader shaders/slosh/solver/timestep_bound.slang:37-91).  Synchronous. */
+int slosh_timestep_bound(slosh_ctx *ctx, float *dt_out, void *stream);
+
 /* Copies the last error message of the context into `buf`. */
 int slosh_last_error(const slosh_ctx *ctx, char *buf, size_t len);
 
@@ -353,6 +361,9 @@ int slosh_batch_download_particles(slosh_batch *b, uint32_t slot, slosh_particle
                                    void *stream);
 int slosh_batch_download_positions(slosh_batch *b, uint32_t slot, float *out_xyzw, uint32_t n, void *stream);
 int slosh_batch_get_bodies(slosh_batch *b, uint32_t slot, slosh_body *out, uint32_t n);
+
+/* slosh_timestep_bound for one scene of the batch. */
+int slosh_batch_timestep_bound(slosh_batch *b, uint32_t slot, float *dt_out, void *stream);
 
 /* Waits for the batch's work; reports device-side errors. */
 int slosh_batch_sync(slosh_batch *b, void *stream);

@@ -64,6 +64,7 @@ def load() -> ctypes.CDLL:
             "orc_prefix_sum": (None, [_P, ctypes.c_uint32]),
             "orc_svd": (None, [ctypes.c_uint32, _P, _P, _P, _P]),
             "orc_model_stress": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
+            "orc_timestep_bound": (ctypes.c_uint32, [_P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(lib, name)
@@ -197,6 +198,12 @@ class Oracle:
         out = np.zeros(4)
         self.lib.orc_totals(self.ctx, _p(out))
         return out
+
+    def timestep_bound(self) -> tuple[int, float]:
+        """(picosecond count, seconds as f32) of estimate_timestep_bound
+        (shaders/slosh/solver/timestep_bound.slang:37-91)."""
+        u = int(self.lib.orc_timestep_bound(self.ctx))
+        return u, float(np.float32(u) / np.float32(1.0e12))
 
     def close(self):
         if self.ctx:

@@ -1270,7 +1270,32 @@ struct AnyCtx {
     virtual int nodes_get(float *out) = 0;
     virtual void totals(double *out) = 0;
     virtual void node_totals(double *out) = 0;
+    virtual uint32_t timestep_bound() = 0;
 };
+
+// GpuTimestepBounds::secs_to_int (shaders/slosh/solver/timestep_bound.slang:20-27):
+// floor(secs * 1e12) as u32, saturating.
+template <typename T> inline uint32_t secs_to_int(T secs) {
+    const T x = std::floor(secs * T(1.0e12));
+    if (!(x > T(0))) return 0u;
+    return x >= T(4294967296.0) ? 0xffffffffu : (uint32_t)x;
+}
+
+// ElasticitySoundSpeedTimestepBound::timestep_bound (models/utils.slang:119-136).
+template <typename T>
+inline T sound_speed_bound(T alpha, T bulk, T shear, T density0, T det_f, T vlen, T h) {
+    const T rho = density0 / std::max(det_f, T(1.0e-6));
+    const T c = std::sqrt((bulk + shear * T(4.0) / T(3.0)) / rho);
+    return alpha * h / std::max(vlen, c);
+}
+
+// LinearElasticModel / NeoHookeanModel::timestep_bound
+// (linear_elasticity.slang:117-133, neo_hookean_elasticity.slang:29-45):
+// bulk = lambda + 2 mu / 3, shear = mu (models/utils.slang:22-28).
+template <typename T> inline T elastic_bound(const T *p, T density0, T det_f, T vlen, T h) {
+    const T bulk = p[0] + T(2.0) * p[1] / T(3.0);
+    return sound_speed_bound(p[2], bulk, p[1], density0, det_f, vlen, h);
+}
 
 template <typename T, int D> struct CtxImpl : AnyCtx {
     Ctx<T, D> c;
@@ -1355,6 +1380,50 @@ template <typename T, int D> struct CtxImpl : AnyCtx {
             for (int k = 0; k < D; ++k) out[1 + k] += (double)c.p.mass[i] * (double)c.p.v[i * D + k];
         }
     }
+    // estimate_timestep_bound (timestep_bound.slang:37-91) over all particles,
+    // as the u32 picosecond count; DefaultParticleModel::timestep_bound
+    // (models/default.slang:94-127) per model, and for the Tait fluid the
+    // sound speed c^2 = K J^-gamma / rho with CFL 0.5.
+    uint32_t timestep_bound() override {
+        uint32_t best = 0xffffffffu;
+        const T h = c.h;
+        for (size_t i = 0; i < c.p.n; ++i) {
+            if (!c.p.enabled[i]) continue;
+            const T density0 = c.p.mass[i] / c.p.V0[i];
+            Mat<T, D> F;
+            for (int r = 0; r < D; ++r)
+                for (int q = 0; q < D; ++q) F.m[r][q] = c.p.F[i * D * D + r * D + q];
+            const T det_f = det<T, D>(F);
+            T v2 = T(0);
+            for (int k = 0; k < D; ++k) v2 = v2 + c.p.v[i * D + k] * c.p.v[i * D + k];
+            const T vlen = std::sqrt(v2);
+            const T *p = &c.p.model[i * 12];
+            T dt;
+            switch (c.p.tag[i]) {
+                case SLOSH_MODEL_ELASTIC_LINEAR:
+                case SLOSH_MODEL_ELASTIC_NEO_HOOKEAN:
+                    dt = elastic_bound<T>(p, density0, det_f, vlen, h);
+                    break;
+                case SLOSH_MODEL_SAND_LINEAR:
+                case SLOSH_MODEL_SAND_NEO_HOOKEAN:
+                    dt = elastic_bound<T>(p + 9, density0, det_f, vlen, h);
+                    break;
+                case SLOSH_MODEL_FLUID_TAIT: {
+                    const T J = F.m[0][0];
+                    const T rho = density0 / std::max(J, T(1.0e-6));
+                    const T cs = std::sqrt(p[1] * std::pow(std::max(J, T(1.0e-6)), -p[2]) / rho);
+                    dt = T(0.5) * h / std::max(vlen, cs);
+                    break;
+                }
+                default:
+                    dt = T(0);
+                    break;
+            }
+            dt = std::min(dt, h / vlen);
+            best = std::min(best, secs_to_int<T>(dt));
+        }
+        return best;
+    }
     Grid<T, D> scratch;
 };
 
@@ -1391,6 +1460,7 @@ void *orc_create(uint32_t dim, uint32_t use_double, float cell_width, uint32_t g
 }
 
 void orc_destroy(void *c) { delete (orc::AnyCtx *)c; }
+uint32_t orc_timestep_bound(void *c) { return ((orc::AnyCtx *)c)->timestep_bound(); }
 void orc_set_params(void *c, const float *gravity, float dt) { ((orc::AnyCtx *)c)->set_params(gravity, dt); }
 int orc_set_particles(void *c, const slosh_particle *p, uint32_t n) {
     return ((orc::AnyCtx *)c)->set_particles(p, n);

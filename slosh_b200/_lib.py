@@ -243,6 +243,7 @@ SIGNATURES = {
     "slosh_debug_nodes": (ctypes.c_int, [_P, ctypes.c_int, _P, _U32, ctypes.POINTER(_U32)]),
     "slosh_prefix_sum": (ctypes.c_int, [_P, _P, _P, _U32]),
     "slosh_prefix_sum_noalloc": (ctypes.c_int, [_P, _P, _U32, _P]),
+    "slosh_timestep_bound": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), _P]),
     "slosh_last_error": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     "slosh_batch_create": (ctypes.c_int, [ctypes.POINTER(SloshBatchConfig), ctypes.POINTER(_P)]),
     "slosh_batch_destroy": (None, [_P]),
@@ -255,6 +256,7 @@ SIGNATURES = {
     "slosh_batch_download_particles": (ctypes.c_int, [_P, _U32, _P, _U32, _P]),
     "slosh_batch_download_positions": (ctypes.c_int, [_P, _U32, _P, _U32, _P]),
     "slosh_batch_get_bodies": (ctypes.c_int, [_P, _U32, _P, _U32]),
+    "slosh_batch_timestep_bound": (ctypes.c_int, [_P, _U32, ctypes.POINTER(ctypes.c_float), _P]),
     "slosh_batch_sync": (ctypes.c_int, [_P, _P]),
     "slosh_batch_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(SloshBatchStats)]),
     "slosh_batch_autotune": (ctypes.c_int, [_P, _U32, _P]),

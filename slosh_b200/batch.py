@@ -122,6 +122,12 @@ class MpmBatch:
         _check(self._lib, self._b, self._lib.slosh_batch_get_bodies(self._b, slot, ptr(out) if n else None, n))
         return out
 
+    def timestep_bound(self, slot: int, stream=None) -> float:
+        """Largest stable dt of one scene (as MpmData.timestep_bound)."""
+        dt = ctypes.c_float()
+        _check(self._lib, self._b, self._lib.slosh_batch_timestep_bound(self._b, slot, ctypes.byref(dt), stream))
+        return float(dt.value)
+
     def stats(self) -> dict:
         st = SloshBatchStats()
         _check(self._lib, self._b, self._lib.slosh_batch_get_stats(self._b, ctypes.byref(st)))

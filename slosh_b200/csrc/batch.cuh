@@ -483,6 +483,26 @@ int slosh_batch_get_bodies(slosh_batch *b, uint32_t slot, slosh_body *out, uint3
     return SLOSH_OK;
 }
 
+int slosh_batch_timestep_bound(slosh_batch *b, uint32_t slot, float *dt_out, void *stream) {
+    if (!b || slot >= b->max_scenes || !dt_out) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    if (!b->slots[slot].live) return fail(c, SLOSH_E_STATE, "scene slot %u is not live", slot);
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    const DevScene s = make_batch_scene(b, c->parity);
+    uint32_t *out = c->small + 3;
+    CK(cudaMemsetAsync(out, 0xff, 4, st));
+    const uint32_t g = grid_for(b->n_storage, 256, (uint32_t)c->sm_count * 16);
+    if (c->dim == 3) k_timestep_bound<3, true><<<g, 256, 0, st>>>(s, slot, out);
+    else k_timestep_bound<2, true><<<g, 256, 0, st>>>(s, slot, out);
+    CK(cudaGetLastError());
+    uint32_t u = 0;
+    CK(cudaMemcpyAsync(&u, out, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *dt_out = (float)u / TIMESTEP_FLOAT_TO_INT;
+    return SLOSH_OK;
+}
+
 int slosh_batch_sync(slosh_batch *b, void *stream) {
     if (!b) return SLOSH_E_INVALID;
     slosh_ctx *c = &b->c;

@@ -16,6 +16,7 @@
 #include "grid_build.cuh"
 #include "io.cuh"
 #include "transfer.cuh"
+#include "timestep.cuh"
 
 using namespace slosh;
 
@@ -816,6 +817,25 @@ int slosh_prefix_sum(slosh_ctx *c, const uint32_t *in, uint32_t *out, uint32_t n
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, c->tmp_slot, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    return SLOSH_OK;
+}
+
+int slosh_timestep_bound(slosh_ctx *c, float *dt_out, void *stream) {
+    if (!c || !dt_out) return SLOSH_E_INVALID;
+    if (c->n == 0) return fail(c, SLOSH_E_STATE, "no particles uploaded");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    const DevScene s = make_scene(c, c->parity, false);
+    uint32_t *slot = c->small + 3;
+    CK(cudaMemsetAsync(slot, 0xff, 4, st));
+    const uint32_t g = grid_for(c->n, 256, (uint32_t)c->sm_count * 16);
+    if (c->dim == 3) k_timestep_bound<3><<<g, 256, 0, st>>>(s, 0u, slot);
+    else k_timestep_bound<2><<<g, 256, 0, st>>>(s, 0u, slot);
+    CK(cudaGetLastError());
+    uint32_t u = 0;
+    CK(cudaMemcpyAsync(&u, slot, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *dt_out = (float)u / TIMESTEP_FLOAT_TO_INT;  // GpuTimestepBounds::computed_dt
     return SLOSH_OK;
 }
 

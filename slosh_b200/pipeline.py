@@ -340,6 +340,13 @@ class MpmData:
     def sync(self, stream=None):
         _check(self._lib, self._ctx, self._lib.slosh_sync(self._ctx, stream))
 
+    def timestep_bound(self, stream=None) -> float:
+        """Largest stable dt of the current particles (seconds), as
+        ``WgTimestepBounds::compute_bounds`` (src/solver/timestep_bound.rs:58-81)."""
+        dt = ctypes.c_float()
+        _check(self._lib, self._ctx, self._lib.slosh_timestep_bound(self._ctx, ctypes.byref(dt), stream))
+        return float(dt.value)
+
     @property
     def kernels_per_substep(self) -> int:
         return int(self._lib.slosh_kernels_per_substep(self._ctx))
@@ -428,3 +435,15 @@ class MpmPipeline:
 
     def launch_step(self, data: MpmData, n_substeps: int = 1, stream=None):
         _check(self._lib, data._ctx, self._lib.slosh_step(data._ctx, int(n_substeps), stream))
+
+    def compute_timestep_bound(self, data: MpmData, stream=None) -> float:
+        """``pipeline.timestep_bounds.compute_bounds`` (src/solver/timestep_bound.rs:58-81)."""
+        return data.timestep_bound(stream)
+
+
+def adaptive_substeps(base_dt: float, bound: float, min_substeps: int, max_substeps: int) -> int:
+    """Number of substeps per frame of the testbed's adaptive stepping
+    (src_testbed/step.rs:104-134): ceil(base_dt / bound) clamped to
+    [min_substeps, max_substeps]; each substep then uses base_dt / n."""
+    est = math.ceil(base_dt / bound) if bound > 0 else max_substeps
+    return int(min(max(est, min_substeps), max_substeps))

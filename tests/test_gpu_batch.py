@@ -151,3 +151,15 @@ def test_batch_errors_reported(cuda_lib):
     assert b.stats()["live_scenes"] == 1 and b.stats()["n_particles"] == sc.n
     b.positions(s1)
     b.close()
+
+
+def test_batch_timestep_bound_per_scene(cuda_lib):
+    """Each scene's bound in a batch equals the single-scene context's."""
+    scs = mix_scenes()
+    b = new_batch()
+    slots = [b.add(sc) for sc in scs]
+    for sc, sl in zip(scs, slots):
+        data = scenes.build_mpm_data(sc)
+        assert b.timestep_bound(sl) == data.timestep_bound()
+        data.close()
+    b.close()

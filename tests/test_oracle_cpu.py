@@ -218,3 +218,52 @@ def test_rigid_update_integrates_pose(oracle_lib):
     assert abs(q[1] - math.sin(0.1)) < 1e-4 and abs(q[3] - math.cos(0.1)) < 1e-4
     # one-way coupling: zero inverse mass, no gravity on the body
     assert b["linvel"][1] == 0.0
+
+
+def test_timestep_bound_closed_form(oracle_lib):
+    """estimate_timestep_bound (timestep_bound.slang:37-91): at rest the bound
+    is cfl h / c with c^2 = (lambda + 2 mu / 3 + 4 mu / 3) / rho; a fast
+    particle bounds it by h / |v|; disabled particles do not count; the
+    result is a whole number of picoseconds."""
+    h = 1 / 64
+    model = ParticleModel.elastic(1e5, 0.3)
+    lam, mu, cfl = model.data[:3]
+    o = _oracle_from(oracle_lib, [[0.5, 0.5, 0.5]], h, 3, model=model)
+    u, dt = o.timestep_bound()
+    rho = 1000.0
+    c = math.sqrt((lam + 2 * mu / 3 + 4 * mu / 3) / rho)
+    expect = cfl * h / c
+    assert abs(u - expect * 1e12) <= 1e-6 * expect * 1e12  # FP32 arithmetic, like the shader
+    assert dt == np.float32(np.float32(u) / np.float32(1e12))
+    # velocity-limited: |v| far above the sound speed
+    recs = make_particles(np.array([[0.5, 0.5, 0.5], [0.2, 0.2, 0.2]]), h / 4, 1000.0, model, dim=3)
+    recs["velocity"][0] = (300.0, 0.0, 400.0)  # |v| = 500
+    recs["velocity"][1] = (5000.0, 0.0, 0.0)
+    recs["enabled"][1] = 0  # ignored
+    o.set_particles(recs)
+    u2, _ = o.timestep_bound()
+    fast = min(cfl * h / max(500.0, c), h / 500.0)  # the model bound takes max(|v|, c)
+    assert abs(u2 - fast * 1e12) <= 1e-6 * fast * 1e12
+    o.close()
+
+
+def test_timestep_bound_models(oracle_lib):
+    """Sand uses its elastic part's moduli; the Tait fluid its own sound
+    speed c^2 = K J^-gamma / rho; bounds beyond the u32 picosecond range
+    (4.29e-3 s) saturate."""
+    h = 1 / 32
+    sand = ParticleModel.sand(3.5e5, 0.3, friction_angle_deg=30.0)
+    o = _oracle_from(oracle_lib, [[0.5, 0.5, 0.5]], h, 3, model=sand)
+    lam, mu, cfl = sand.data[9:12]
+    c = math.sqrt((lam + 2 * mu) / 1000.0)
+    assert abs(o.timestep_bound()[0] - cfl * h / c * 1e12) <= 1e-6 * cfl * h / c * 1e12
+    o.close()
+    fluid = ParticleModel.fluid_tait(1000.0, 1.0e4, 7.0)
+    o = _oracle_from(oracle_lib, [[0.5, 0.5]], h, 2, model=fluid)
+    assert o.timestep_bound()[0] == 0xFFFFFFFF  # 0.5 h / c = 4.9e-3 s saturates
+    o.close()
+    h = 1 / 256
+    o = _oracle_from(oracle_lib, [[0.5, 0.5]], h, 2, model=fluid)
+    c = math.sqrt(1.0e4 / 1000.0)
+    assert abs(o.timestep_bound()[0] - 0.5 * h / c * 1e12) <= 1e-6 * 0.5 * h / c * 1e12
+    o.close()
