@@ -91,7 +91,7 @@ template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uin
     k_block_setup<D, true><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
     k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     k_scatter<true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
-    k_canon_cells<<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
+    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
     k_p2g<D, true, true><<<std::min<uint32_t>(c->cap, sm * b->tune.p2g_ctas_per_sm), P2G_THREADS, 0, st>>>(s);
     k_grid_update<D, true><<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
     if (b->tune.g2p_threads == 64) launch_batch_g2p<D, 64>(b, s, st);
@@ -236,6 +236,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||
+        (st = dalloc(c, &c->skey, N)) ||
         (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, b->max_bodies)) ||

@@ -161,14 +161,24 @@ template <bool B = false> __global__ void k_clear(DevScene s) {
 // cell width from the scene table, and particles of a dropped scene get no
 // block (they leave storage at this substep).
 template <int D, bool B = false> __global__ void k_touch(DevScene s) {
+    // Each warp takes a contiguous chunk of storage.  Storage is in the
+    // previous substep's canonical order (block by block), so successive
+    // iterations of a warp mostly hit the block of the last one: the warp
+    // remembers its last (key -> slot) and skips the hash CAS round trip.
     const uint32_t lane = lane_id();
-    const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t n = n_particles<B>(s);
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t chunk = (((n + warps - 1) / warps) + 31u) & ~31u;
+    const uint32_t begin = wid * chunk;
+    const uint32_t end = min(n, begin + chunk);
+    unsigned long long last_key = NONE64;
+    uint32_t last_slot = NONE;
+    for (uint32_t base = begin; base < end; base += 32) {
         const uint32_t i = base + lane;
-        const bool valid = i < n;
+        const bool valid = i < end;
         const unsigned mask = __ballot_sync(FULL_MASK, valid);
-        if (!valid) continue;
+        if (!valid) break;
         const float4 p = s.pm[i];
         const float x[3] = {p.x, p.y, p.z};
         float h = s.h, inv_h = s.inv_h;
@@ -185,27 +195,33 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
         const CellLoc<D> c = locate<D>(x, h, inv_h, pow2);
         const uint32_t key = pack_key<D>(c.block);
         const uint32_t cell = cell_index<D>(c.local);
-        unsigned peers;
-        if constexpr (B) peers = __match_any_sync(mask, live ? (((unsigned long long)sc << 32) | key) : NONE64);
-        else peers = __match_any_sync(mask, key);
+        const unsigned long long ckey = live ? (((unsigned long long)sc << 32) | key) : NONE64;
+        const unsigned peers = __match_any_sync(mask, ckey);
         const int leader = __ffs(peers) - 1;
         uint32_t slot = NONE;
         if ((int)lane == leader && live) {
-            bool inserted = false;
-            slot = map_insert<B>(s, key, sc, inserted);
-            if (inserted) {
-                const uint32_t j = atomicAdd(&s.ctr->n_primary, 1u);
-                if (j < s.cap) {
-                    s.blist_key[j] = key;
-                    s.blist_slot[j] = slot;
-                    if constexpr (B) atomicAdd(&s.scene_nblk[sc], 1u);
-                    else atomicAdd(&s.hist[key >> 16], 1u);
-                } else {
-                    atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+            if (ckey == last_key) {
+                slot = last_slot;
+            } else {
+                bool inserted = false;
+                slot = map_insert<B>(s, key, sc, inserted);
+                if (inserted) {
+                    const uint32_t j = atomicAdd(&s.ctr->n_primary, 1u);
+                    if (j < s.cap) {
+                        s.blist_key[j] = key;
+                        s.blist_slot[j] = slot;
+                        if constexpr (B) atomicAdd(&s.scene_nblk[sc], 1u);
+                        else atomicAdd(&s.hist[key >> 16], 1u);
+                    } else {
+                        atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+                    }
                 }
             }
         }
         slot = __shfl_sync(mask, slot, leader);
+        const int top = 31 - __clz(mask);  // last valid lane: its block is the likeliest next
+        last_key = __shfl_sync(mask, ckey, top);
+        last_slot = __shfl_sync(mask, slot, top);
         const uint32_t bin = (slot == NONE) ? NONE : (slot << 6) | cell;
         const unsigned peers2 = __match_any_sync(mask, bin);
         if (bin != NONE && (int)lane == __ffs(peers2) - 1) atomicAdd(&s.slot_counts[bin], (uint32_t)__popc(peers2));
@@ -357,8 +373,63 @@ template <int NT> __device__ __forceinline__ uint32_t cta_scan_vec16(const uint3
 }
 
 // Exclusive scan of the key histogram (one CTA) and the final block count.
+// Warp w owns HIST_BINS / (NT / 32) consecutive bins, read as rows of 32
+// uint4 (one coalesced 512-byte load per row, BATCH rows in flight).  Pass 1
+// sums each warp's bins and scans the warp totals across the CTA; pass 2
+// re-reads the rows (L2 hits) and writes the prefix, a warp scan per row
+// with a running carry.
 template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) {
-    cta_scan_vec16<NT>(s.hist, s.hist_start, HIST_BINS);
+    constexpr uint32_t NW = NT / 32, SEG = HIST_BINS / NW, ROWS = SEG / 128, BATCH = 8;
+    static_assert(SEG % 128 == 0 && ROWS % BATCH == 0, "bins per warp");
+    __shared__ uint32_t wtot[NW];
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const uint4 *in = reinterpret_cast<const uint4 *>(s.hist + (size_t)w * SEG);
+    uint32_t part = 0;
+    for (uint32_t q0 = 0; q0 < ROWS; q0 += BATCH) {
+        uint4 v[BATCH];
+#pragma unroll
+        for (uint32_t q = 0; q < BATCH; ++q) v[q] = in[(q0 + q) * 32 + lane];
+#pragma unroll
+        for (uint32_t q = 0; q < BATCH; ++q) part += v[q].x + v[q].y + v[q].z + v[q].w;
+    }
+    part = __reduce_add_sync(FULL_MASK, part);
+    if (lane == 0) wtot[w] = part;
+    __syncthreads();
+    if (w == 0) {
+        const uint32_t t = lane < NW ? wtot[lane] : 0u;
+        uint32_t incl = t;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
+            if (lane >= (uint32_t)off) incl += y;
+        }
+        if (lane < NW) wtot[lane] = incl - t;
+    }
+    __syncthreads();
+    uint32_t carry = wtot[w];
+    uint4 *out = reinterpret_cast<uint4 *>(s.hist_start + (size_t)w * SEG);
+    for (uint32_t q0 = 0; q0 < ROWS; q0 += BATCH) {
+        uint4 v[BATCH];
+#pragma unroll
+        for (uint32_t q = 0; q < BATCH; ++q) v[q] = in[(q0 + q) * 32 + lane];
+#pragma unroll
+        for (uint32_t q = 0; q < BATCH; ++q) {
+            const uint32_t sum = v[q].x + v[q].y + v[q].z + v[q].w;
+            uint32_t incl = sum;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
+                if (lane >= (uint32_t)off) incl += y;
+            }
+            uint4 o;
+            o.x = carry + incl - sum;
+            o.y = o.x + v[q].x;
+            o.z = o.y + v[q].y;
+            o.w = o.z + v[q].z;
+            out[(q0 + q) * 32 + lane] = o;
+            carry += __shfl_sync(FULL_MASK, incl, 31);
+        }
+    }
     if (threadIdx.x == 0) {
         const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
         if (total > s.cap) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
@@ -565,71 +636,66 @@ template <bool B = false> __global__ void k_scatter(DevScene s) {
         pos = __shfl_sync(mask, pos, leader);
         if (pos != NONE) {
             const uint32_t at = pos + __popc(peers & lanemask_lt());
-            if (at < s.n) s.perm[at] = i;
-            else atomicOr(s.err, ERR_BLOCK_OVERFLOW);  // stale counts after an earlier overflow
+            if (at < s.n) {
+                s.perm[at] = i;
+                s.skey[at] = ((unsigned long long)(bin & 63u) << 32) | s.oid[i];
+            } else {
+                atomicOr(s.err, ERR_BLOCK_OVERFLOW);  // stale counts after an earlier overflow
+            }
         }
     }
 }
 
-// Orders each (block, cell) range of the permutation by original particle
-// id, in place: the canonical order.  One thread per (block, cell).  perm
-// holds storage indices and the order key is oid[storage index].  Storage is
-// already in the previous substep's canonical order, so the warp-aggregated
-// scatter usually leaves a cell sorted; unsorted cells get an insertion sort
-// (in registers up to 16 particles, in global memory beyond).
-constexpr int CANON_REG = 16;
-__global__ void k_canon_cells(DevScene s) {
+// Canonical order inside each (block, cell) range of the permutation:
+// ascending original id.  k_scatter stores beside every permutation entry
+// its sort key (cell << 32 | original id).  Storage is already in the
+// previous substep's canonical order and the scatter keeps a warp's lanes in
+// storage order, so most cells come out sorted; the ones that do not are
+// cells whose particles were scattered by two different warps.  One warp per
+// block compares neighbouring keys (coalesced loads of the block's
+// contiguous entries), and the lanes owning an out-of-order cell
+// insertion-sort it, keys and permutation together.
+__device__ __forceinline__ void sort_cell_keys(unsigned long long *key, uint32_t *perm, uint32_t m) {
+    for (uint32_t j = 1; j < m; ++j) {
+        const unsigned long long kj = key[j];
+        const uint32_t pj = perm[j];
+        int q = (int)j - 1;
+        while (q >= 0 && key[q] > kj) {
+            key[q + 1] = key[q];
+            perm[q + 1] = perm[q];
+            --q;
+        }
+        key[q + 1] = kj;
+        perm[q + 1] = pj;
+    }
+}
+
+__global__ void k_canon(DevScene s) {
     const uint32_t nb = s.ctr->n_blocks;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * CELLS; t += stride) {
-        const uint32_t r = t >> 6, c = t & 63u;
-        const uint32_t np = s.bnp[r];
-        const uint32_t first = s.bfirst[r];
-        const uint32_t b0 = s.bcell[(size_t)r * CELLS + c];
-        const uint32_t b1 = (c < CELLS - 1) ? s.bcell[(size_t)r * CELLS + c + 1] : np;
-        if (b1 <= b0 + 1) continue;
-        if ((size_t)first + b1 > s.n) {  // only after an earlier overflow left stale counts
-            atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
+        const uint32_t first = s.bfirst[r], np = s.bnp[r];
+        if (np < 2) continue;
+        if ((size_t)first + np > s.n) {  // only after an earlier overflow left stale counts
+            if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
         }
-        uint32_t *seg = s.perm + first + b0;
-        const uint32_t m = b1 - b0;
-        bool sorted = true;
-        uint32_t prev = s.oid[seg[0]];
-        for (uint32_t j = 1; j < m; ++j) {
-            const uint32_t k = s.oid[seg[j]];
-            sorted = sorted && (prev < k);
-            prev = k;
+        const unsigned long long *k = s.skey + first;
+        unsigned long long bad = 0ull;  // cells holding an inversion
+        for (uint32_t e = lane; e + 1 < np; e += 32) {
+            const unsigned long long k0 = k[e], k1 = k[e + 1];
+            if (k0 > k1 && (k0 >> 32) == (k1 >> 32)) bad |= 1ull << (uint32_t)(k0 >> 32);
         }
-        if (sorted) continue;
-        if (m <= (uint32_t)CANON_REG) {
-            uint32_t ids[CANON_REG], keys[CANON_REG];
-            for (uint32_t j = 0; j < m; ++j) {
-                ids[j] = seg[j];
-                keys[j] = s.oid[ids[j]];
-            }
-            for (uint32_t j = 1; j < m; ++j) {
-                const uint32_t ki = keys[j], ii = ids[j];
-                int q = (int)j - 1;
-                while (q >= 0 && keys[q] > ki) {
-                    keys[q + 1] = keys[q];
-                    ids[q + 1] = ids[q];
-                    --q;
-                }
-                keys[q + 1] = ki;
-                ids[q + 1] = ii;
-            }
-            for (uint32_t j = 0; j < m; ++j) seg[j] = ids[j];
-        } else {
-            for (uint32_t j = 1; j < m; ++j) {
-                const uint32_t ii = seg[j], ki = s.oid[ii];
-                int q = (int)j - 1;
-                while (q >= 0 && s.oid[seg[q]] > ki) {
-                    seg[q + 1] = seg[q];
-                    --q;
-                }
-                seg[q + 1] = ii;
-            }
+        const uint32_t lo = __reduce_or_sync(FULL_MASK, (uint32_t)bad);
+        const uint32_t hi = __reduce_or_sync(FULL_MASK, (uint32_t)(bad >> 32));
+        if ((lo | hi) == 0u) continue;
+        for (uint32_t c = lane; c < CELLS; c += 32) {
+            const uint32_t word = c < 32 ? lo : hi;
+            if (!((word >> (c & 31u)) & 1u)) continue;
+            const uint32_t b0 = s.bcell[(size_t)r * CELLS + c];
+            const uint32_t b1 = (c < CELLS - 1) ? s.bcell[(size_t)r * CELLS + c + 1] : np;
+            if (b1 > b0 + 1) sort_cell_keys(s.skey + first + b0, s.perm + first + b0, b1 - b0);
         }
     }
 }

@@ -67,6 +67,7 @@ struct DevScene {
     uint32_t *bnbh;        // (NASSOC - 1) neighbour ranks per block, NONE if inactive
     uint32_t *pslot;       // per particle: (hash slot << 6) | cell
     uint32_t *perm;        // primary order: scatter output, canonicalised in place
+    unsigned long long *skey;  // beside perm: (cell << 32 | original id), the canonical sort key
     uint32_t *bnbh_rev;    // (NASSOC - 1) ranks of the blocks b - o (the -1 neighbours), NONE if inactive
     float4 *nodes;         // 64 nodes per block: (momentum | velocity, mass)
     float4 *partial;       // TILE nodes per block: the block's own P2G sums over its (block + 2)^D tile

@@ -53,6 +53,7 @@ struct slosh_ctx {
     // shared-memory staging, 3 "direct" cell-owner with float atomics.
     int p2g_variant = 0;
     uint32_t *pslot = nullptr, *perm = nullptr;
+    unsigned long long *skey = nullptr;
     float4 *nodes = nullptr, *partial = nullptr, *coll[2] = {nullptr, nullptr};
     uint32_t *coll_id[2] = {nullptr, nullptr};
 
@@ -176,6 +177,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.bnbh_rev = c->bnbh_rev;
     s.pslot = c->pslot;
     s.perm = c->perm;
+    s.skey = c->skey;
     s.nodes = c->nodes;
     s.partial = c->partial;
     s.use_partial = (c->p2g_variant == 0) ? 1u : 0u;
@@ -255,7 +257,7 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
     k_scatter<<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(7);
     PROF_BEGIN(8);
-    k_canon_cells<<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
+    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(8);
 }
 
@@ -443,6 +445,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||
+        (st = dalloc(c, &c->skey, N)) ||
         (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, MAX_BODIES)) ||
