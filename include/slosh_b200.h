@@ -86,6 +86,9 @@ typedef struct slosh_particle {
 /* Collider shape types: shaders/slosh/rbd/shapes/shape.slang:19-25. */
 #define SLOSH_SHAPE_BALL 0u
 #define SLOSH_SHAPE_CUBOID 1u
+#define SLOSH_SHAPE_CAPSULE 2u   /* 2D and 3D */
+#define SLOSH_SHAPE_CONE 3u      /* 3D, axis along local y */
+#define SLOSH_SHAPE_CYLINDER 4u  /* 3D, axis along local y */
 
 /* Boundary conditions: src/solver/boundary_condition.rs:14-19. */
 #define SLOSH_BC_STICK 0u
@@ -99,8 +102,12 @@ typedef struct slosh_particle {
  * slosh's GpuBodySet (src/rbd/dynamics/body.rs:74-90) plus its
  * GpuBoundaryCondition (src/solver/boundary_condition.rs:8-12).  192 bytes.
  * Shape layout as shaders/slosh/rbd/shapes/shape.slang:44-62:
- *   ball:   shape_a = (radius, -, -, type)
- *   cuboid: shape_a = (hx, hy, hz, type)
+ *   ball:     shape_a = (radius, -, -, type)
+ *   cuboid:   shape_a = (hx, hy, hz, type)
+ *   capsule:  shape_a = (ax, ay, az, type), shape_b = (bx, by, bz, radius):
+ *             the segment a-b inflated by the radius
+ *   cone, cylinder: shape_a = (half_height, radius, -, type); a cone's apex
+ *             is at +half_height, its base disc at -half_height
  * where `type` is the shape type stored as uint32 bits.  The pose is a
  * similarity: rotation (3D unit quaternion i,j,k,w; 2D cos,sin), translation
  * xyz and uniform scale in translation[3].  Bodies coupled one-way (the

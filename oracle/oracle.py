@@ -65,6 +65,7 @@ def load() -> ctypes.CDLL:
             "orc_svd": (None, [ctypes.c_uint32, _P, _P, _P, _P]),
             "orc_model_stress": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
             "orc_timestep_bound": (ctypes.c_uint32, [_P]),
+            "orc_project": (ctypes.c_int, [ctypes.c_uint32, _P, _P, _P, _P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(lib, name)
@@ -76,6 +77,19 @@ def load() -> ctypes.CDLL:
 
 def _p(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+def project_on_boundary(dim: int, body_record, point) -> tuple[np.ndarray, bool] | None:
+    """Shape::project_point_on_boundary of one body record (FP32); None
+    when the shape is not supported in `dim`."""
+    lib = load()
+    rec = np.ascontiguousarray(np.asarray(body_record).reshape(1))
+    pt = np.zeros(3, np.float32)
+    pt[:dim] = np.asarray(point, np.float32)[:dim]
+    out = np.zeros(3, np.float32)
+    inside = ctypes.c_int(0)
+    ok = lib.orc_project(dim, _p(rec), _p(pt), _p(out), ctypes.byref(inside))
+    return (out[:dim].copy(), bool(inside.value)) if ok else None
 
 
 def prefix_sum(values) -> np.ndarray:

@@ -445,6 +445,128 @@ template <typename T, int D> struct Pose {
 
 // Shape::project_point_on_boundary for ball and cuboid
 // (shaders/slosh/rbd/shapes/ball.slang, cuboid.slang:34-63).
+// Segment::project_local_point (rbd/shapes/segment.slang:9-28).
+template <typename T, int D> void segment_project(const T *a, const T *b, const T *p, T *q) {
+    T ab[D], ab_ap = 0, sqn = 0;
+    for (int k = 0; k < D; ++k) {
+        ab[k] = b[k] - a[k];
+        ab_ap += ab[k] * (p[k] - a[k]);
+        sqn += ab[k] * ab[k];
+    }
+    if (ab_ap <= T(0)) {
+        for (int k = 0; k < D; ++k) q[k] = a[k];
+    } else if (ab_ap >= sqn) {
+        for (int k = 0; k < D; ++k) q[k] = b[k];
+    } else {
+        T u = ab_ap / sqn;
+        for (int k = 0; k < D; ++k) q[k] = a[k] + ab[k] * u;
+    }
+}
+
+// Capsule::project_local_point_on_boundary (rbd/shapes/capsule.slang:38-55),
+// any_orthogonal_vector / orthonormal_basis3 (capsule.slang:66-95).
+template <typename T, int D> bool capsule_project(const T *a, const T *b, T radius, const T *p, T *out) {
+    T q[D], d[D], n2 = 0;
+    segment_project<T, D>(a, b, p, q);
+    for (int k = 0; k < D; ++k) {
+        d[k] = p[k] - q[k];
+        n2 += d[k] * d[k];
+    }
+    T dist = std::sqrt(n2);
+    if (dist > T(0)) {
+        for (int k = 0; k < D; ++k) out[k] = q[k] + d[k] * (radius / dist);
+        return dist <= radius;
+    }
+    T ax[D], l2 = 0;
+    for (int k = 0; k < D; ++k) {
+        ax[k] = b[k] - a[k];
+        l2 += ax[k] * ax[k];
+    }
+    T len = std::sqrt(l2);
+    for (int k = 0; k < D; ++k) ax[k] = ax[k] / len;
+    T o[D];
+    if constexpr (D == 2) {
+        o[0] = ax[1];
+        o[1] = -ax[0];
+    } else {
+        T sg = ax[2] >= T(0) ? T(1) : T(-1);
+        T aa = T(-1) / (sg + ax[2]);
+        T bb = ax[0] * ax[1] * aa;
+        o[0] = T(1) + sg * ax[0] * ax[0] * aa;
+        o[1] = sg * bb;
+        o[2] = -sg * ax[0];
+    }
+    for (int k = 0; k < D; ++k) out[k] = q[k] + o[k] * radius;
+    return true;
+}
+
+// Cylinder::project_local_point_on_boundary (rbd/shapes/cylinder.slang:72-125).
+template <typename T> bool cylinder_project(T hh, T r, const T *p, T *out) {
+    T rxz = std::sqrt(p[0] * p[0] + p[2] * p[2]);
+    T dx = rxz > T(0) ? p[0] / rxz : T(1), dz = rxz > T(0) ? p[2] / rxz : T(0);
+    T px = dx * r, pz = dz * r;
+    if (p[1] >= -hh && p[1] <= hh && rxz <= r) {
+        T top = hh - p[1], bottom = p[1] - (-hh), side = r - rxz;
+        if (top < bottom && top < side) {
+            out[0] = p[0], out[1] = hh, out[2] = p[2];
+        } else if (bottom < top && bottom < side) {
+            out[0] = p[0], out[1] = -hh, out[2] = p[2];
+        } else {
+            out[0] = px, out[1] = p[1], out[2] = pz;
+        }
+        return true;
+    }
+    if (p[1] > hh) {
+        if (rxz <= r) out[0] = p[0], out[1] = hh, out[2] = p[2];
+        else out[0] = px, out[1] = hh, out[2] = pz;
+    } else if (p[1] < -hh) {
+        if (rxz <= r) out[0] = p[0], out[1] = -hh, out[2] = p[2];
+        else out[0] = px, out[1] = -hh, out[2] = pz;
+    } else {
+        out[0] = px, out[1] = p[1], out[2] = pz;
+    }
+    return false;
+}
+
+// Cone::project_local_point_on_boundary (rbd/shapes/cone.slang:82-131).
+template <typename T> bool cone_project(T hh, T r, const T *p, T *out) {
+    T rxz = std::sqrt(p[0] * p[0] + p[2] * p[2]);
+    T dx = rxz > T(0) ? p[0] / rxz : T(1), dz = rxz > T(0) ? p[2] / rxz : T(0);
+    T basis[3] = {p[0], -hh, p[2]};
+    if (p[1] < -hh && rxz <= r) {
+        for (int k = 0; k < 3; ++k) out[k] = basis[k];
+        return false;
+    }
+    T circle[3] = {dx * r, -hh, dz * r};
+    T apex[3] = {T(0), hh, T(0)};
+    T seg_dir[3] = {circle[0] - apex[0], circle[1] - apex[1], circle[2] - apex[2]};
+    T proj[3];
+    segment_project<T, 3>(apex, circle, p, proj);
+    T rel[3] = {p[0] - apex[0], p[1] - apex[1], p[2] - apex[2]};
+    T down[3] = {T(0), T(-2) * hh, T(0)};
+    auto cross = [](const T *u, const T *v, T *w) {
+        w[0] = u[1] * v[2] - u[2] * v[1];
+        w[1] = u[2] * v[0] - u[0] * v[2];
+        w[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    T c1[3], c2[3];
+    cross(seg_dir, rel, c1);
+    cross(seg_dir, down, c2);
+    bool in = p[1] >= -hh && p[1] <= hh && (c1[0] * c2[0] + c1[1] * c2[1] + c1[2] * c2[2]) >= T(0);
+    if (in) {
+        T dp = 0, db = 0;
+        for (int k = 0; k < 3; ++k) {
+            dp += (proj[k] - p[k]) * (proj[k] - p[k]);
+            db += (basis[k] - p[k]) * (basis[k] - p[k]);
+        }
+        const T *src = dp > db ? basis : proj;
+        for (int k = 0; k < 3; ++k) out[k] = src[k];
+        return true;
+    }
+    for (int k = 0; k < 3; ++k) out[k] = proj[k];
+    return false;
+}
+
 template <typename T, int D>
 bool project_on_boundary(const Body<T, D> &b, const T *pt, T *proj, bool *is_inside) {
     T local[D];
@@ -489,6 +611,12 @@ bool project_on_boundary(const Body<T, D> &b, const T *pt, T *proj, bool *is_ins
         for (int i = 0; i < D; ++i) lp[i] = (dist != T(0)) ? local[i] * (r / dist) : T(0);
         if (dist == T(0)) lp[1] = r;
         *is_inside = dist <= r;
+    } else if (b.shape_type == SLOSH_SHAPE_CAPSULE) {
+        *is_inside = capsule_project<T, D>(b.sa, b.sb, b.sb[3], local, lp);
+    } else if (D == 3 && b.shape_type == SLOSH_SHAPE_CYLINDER) {
+        if constexpr (D == 3) *is_inside = cylinder_project<T>(b.sa[0], b.sa[1], local, lp);
+    } else if (D == 3 && b.shape_type == SLOSH_SHAPE_CONE) {
+        if constexpr (D == 3) *is_inside = cone_project<T>(b.sa[0], b.sa[1], local, lp);
     } else {
         return false;
     }
@@ -1461,6 +1589,22 @@ void *orc_create(uint32_t dim, uint32_t use_double, float cell_width, uint32_t g
 
 void orc_destroy(void *c) { delete (orc::AnyCtx *)c; }
 uint32_t orc_timestep_bound(void *c) { return ((orc::AnyCtx *)c)->timestep_bound(); }
+
+// Shape::project_point_on_boundary of one body record (FP32), for tests:
+// returns 1 when the shape is supported, with the projection and "inside".
+int orc_project(uint32_t dim, const slosh_body *body, const float *pt, float *out, int *inside) {
+    bool in = false;
+    bool ok;
+    if (dim == 3) {
+        const orc::Body<float, 3> b = orc::load_body<float, 3>(*body);
+        ok = orc::project_on_boundary<float, 3>(b, pt, out, &in);
+    } else {
+        const orc::Body<float, 2> b = orc::load_body<float, 2>(*body);
+        ok = orc::project_on_boundary<float, 2>(b, pt, out, &in);
+    }
+    *inside = in ? 1 : 0;
+    return ok ? 1 : 0;
+}
 void orc_set_params(void *c, const float *gravity, float dt) { ((orc::AnyCtx *)c)->set_params(gravity, dt); }
 int orc_set_particles(void *c, const slosh_particle *p, uint32_t n) {
     return ((orc::AnyCtx *)c)->set_particles(p, n);

@@ -43,6 +43,9 @@ MODEL_FLUID_TAIT = 4
 
 SHAPE_BALL = 0
 SHAPE_CUBOID = 1
+SHAPE_CAPSULE = 2
+SHAPE_CONE = 3
+SHAPE_CYLINDER = 4
 
 BC_STICK = 0
 BC_SLIP = 1

@@ -286,6 +286,12 @@ int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const sl
     if (n_bodies > MAX_BODIES) return fail(c, SLOSH_E_CAPACITY, "%u bodies exceed %u per scene", n_bodies, MAX_BODIES);
     if ((uint64_t)b->n_storage + n > c->max_n)
         return fail(c, SLOSH_E_CAPACITY, "%u + %u particles exceed the pool of %u", b->n_storage, n, c->max_n);
+    for (uint32_t k = 0; k < n_bodies; ++k) {
+        DevBody d;
+        to_dev_body(bodies[k], d);
+        if (!(d.scale > 0.f) || !shape_supported(d.shape_type, c->dim))
+            return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u or scale", k, d.shape_type);
+    }
     uint32_t tags = 0;
     for (uint32_t i = 0; i < n; ++i) {
         const slosh_particle &p = particles[i];

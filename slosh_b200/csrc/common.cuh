@@ -178,6 +178,7 @@ struct SceneRec {
 struct DevBody {
     uint32_t shape_type;
     float sa[4];
+    float sb[4];
     float rot[4];
     float tra[3];
     float scale;

@@ -351,6 +351,7 @@ void to_dev_body(const slosh_body &b, DevBody &d) {
     std::memcpy(&d.shape_type, &b.shape_a[3], 4);
     for (int k = 0; k < 4; ++k) {
         d.sa[k] = b.shape_a[k];
+        d.sb[k] = b.shape_b[k];
         d.rot[k] = b.rotation[k];
     }
     for (int k = 0; k < 3; ++k) {
@@ -365,10 +366,18 @@ void to_dev_body(const slosh_body &b, DevBody &d) {
     d.friction = b.bc_friction;
 }
 
+// Collider shapes the projection handles: ball, cuboid and capsule in 2D and
+// 3D; cylinder and cone in 3D (shaders/slosh/rbd/shapes/shape.slang:99-125).
+bool shape_supported(uint32_t ty, int dim) {
+    if (ty == SLOSH_SHAPE_BALL || ty == SLOSH_SHAPE_CUBOID || ty == SLOSH_SHAPE_CAPSULE) return true;
+    return dim == 3 && (ty == SLOSH_SHAPE_CYLINDER || ty == SLOSH_SHAPE_CONE);
+}
+
 void from_dev_body(const DevBody &d, slosh_body &b) {
     std::memset(&b, 0, sizeof(b));
     for (int k = 0; k < 4; ++k) {
         b.shape_a[k] = d.sa[k];
+        b.shape_b[k] = d.sb[k];
         b.rotation[k] = d.rot[k];
     }
     std::memcpy(&b.shape_a[3], &d.shape_type, 4);
@@ -576,8 +585,8 @@ int slosh_set_bodies(slosh_ctx *c, const slosh_body *bodies, uint32_t n) {
     for (uint32_t i = 0; i < n; ++i) {
         to_dev_body(bodies[i], db[i]);
         if (!(db[i].scale > 0.f)) return fail(c, SLOSH_E_INVALID, "body %u: scale must be > 0", i);
-        if (db[i].shape_type != SLOSH_SHAPE_BALL && db[i].shape_type != SLOSH_SHAPE_CUBOID)
-            return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u", i, db[i].shape_type);
+        if (!shape_supported(db[i].shape_type, c->dim))
+            return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u in %dD", i, db[i].shape_type, c->dim);
     }
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));

@@ -631,8 +631,149 @@ template <int D> __device__ __forceinline__ void pose_inv_mul_pt(const DevBody &
     }
 }
 
-// Shape::project_point_on_boundary for balls and cuboids
-// (shaders/slosh/rbd/shapes/ball.slang:39-52, cuboid.slang:14-63).
+// Closest point of the segment a-b (shaders/slosh/rbd/shapes/segment.slang:9-28):
+// an end point in its Voronoi region, else the orthogonal projection.
+template <int D> __device__ __forceinline__ void segment_closest(const float *a, const float *b, const float *p,
+                                                                 float *q) {
+    float ab[D], ap_ab = 0.f, ab2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        ab[k] = b[k] - a[k];
+        ap_ab += ab[k] * (p[k] - a[k]);
+        ab2 += ab[k] * ab[k];
+    }
+    if (ap_ab <= 0.f) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) q[k] = a[k];
+    } else if (ap_ab >= ab2) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) q[k] = b[k];
+    } else {
+        const float u = ap_ab / ab2;
+#pragma unroll
+        for (int k = 0; k < D; ++k) q[k] = a[k] + ab[k] * u;
+    }
+}
+
+// Capsule = segment a-b inflated by `radius` (capsule.slang:38-55): the
+// closest axis point pushed out by the radius.  A point exactly on the axis
+// goes out along a fixed unit vector orthogonal to the axis: in 3D the first
+// vector of the branchless orthonormal basis of Duff et al., "Building an
+// Orthonormal Basis, Revisited" (JCGT 2017).  Returns "inside".
+template <int D>
+__device__ __forceinline__ bool capsule_boundary(const float *a, const float *b, float radius, const float *p,
+                                                 float *out) {
+    float q[D], d[D], n2 = 0.f;
+    segment_closest<D>(a, b, p, q);
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        d[k] = p[k] - q[k];
+        n2 += d[k] * d[k];
+    }
+    const float dist = sqrtf(n2);
+    if (dist > 0.f) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) out[k] = q[k] + d[k] * (radius / dist);
+        return dist <= radius;
+    }
+    float ax[D], l2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        ax[k] = b[k] - a[k];
+        l2 += ax[k] * ax[k];
+    }
+    const float len = sqrtf(l2);
+#pragma unroll
+    for (int k = 0; k < D; ++k) ax[k] /= len;
+    float o[D];
+    if constexpr (D == 2) {
+        o[0] = ax[1];
+        o[1] = -ax[0];
+    } else {
+        const float sg = ax[2] >= 0.f ? 1.f : -1.f;
+        const float aa = -1.0f / (sg + ax[2]);
+        const float bb = ax[0] * ax[1] * aa;
+        o[0] = 1.0f + sg * ax[0] * ax[0] * aa;
+        o[1] = sg * bb;
+        o[2] = -sg * ax[0];
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) out[k] = q[k] + o[k] * radius;
+    return true;
+}
+
+// Cylinder of half height hh and radius r around the local y axis
+// (cylinder.slang:72-125): inside, the nearest of the two caps and the
+// side; outside, the cap disc, the cap rim or the side.  Returns "inside".
+__device__ __forceinline__ bool cylinder_boundary(float hh, float r, const float *p, float *out) {
+    const float rxz = sqrtf(p[0] * p[0] + p[2] * p[2]);
+    const float dx = rxz > 0.f ? p[0] / rxz : 1.f, dz = rxz > 0.f ? p[2] / rxz : 0.f;
+    const float sx = dx * r, sz = dz * r;
+    if (p[1] >= -hh && p[1] <= hh && rxz <= r) {
+        const float to_top = hh - p[1], to_bottom = p[1] + hh, to_side = r - rxz;
+        if (to_top < to_bottom && to_top < to_side) {
+            out[0] = p[0], out[1] = hh, out[2] = p[2];
+        } else if (to_bottom < to_top && to_bottom < to_side) {
+            out[0] = p[0], out[1] = -hh, out[2] = p[2];
+        } else {
+            out[0] = sx, out[1] = p[1], out[2] = sz;
+        }
+        return true;
+    }
+    if (p[1] > hh || p[1] < -hh) {
+        const float y = p[1] > hh ? hh : -hh;
+        if (rxz <= r) out[0] = p[0], out[1] = y, out[2] = p[2];
+        else out[0] = sx, out[1] = y, out[2] = sz;
+    } else {
+        out[0] = sx, out[1] = p[1], out[2] = sz;
+    }
+    return false;
+}
+
+// Cone of half height hh and base radius r, apex at +hh on the local y axis
+// (cone.slang:82-131): below the base disc, the disc; otherwise the closest
+// point of the generatrix through the point's azimuth, or (inside) the base
+// when that is nearer.  Returns "inside".
+__device__ __forceinline__ bool cone_boundary(float hh, float r, const float *p, float *out) {
+    const float rxz = sqrtf(p[0] * p[0] + p[2] * p[2]);
+    const float dx = rxz > 0.f ? p[0] / rxz : 1.f, dz = rxz > 0.f ? p[2] / rxz : 0.f;
+    const float base[3] = {p[0], -hh, p[2]};
+    if (p[1] < -hh && rxz <= r) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) out[k] = base[k];
+        return false;
+    }
+    const float rim[3] = {dx * r, -hh, dz * r};
+    const float apex[3] = {0.f, hh, 0.f};
+    float proj[3];
+    segment_closest<3>(apex, rim, p, proj);
+    const float gen[3] = {rim[0] - apex[0], rim[1] - apex[1], rim[2] - apex[2]};
+    const float ap[3] = {p[0] - apex[0], p[1] - apex[1], p[2] - apex[2]};
+    const float axis[3] = {0.f, -2.0f * hh, 0.f};
+    const float c1[3] = {gen[1] * ap[2] - gen[2] * ap[1], gen[2] * ap[0] - gen[0] * ap[2], gen[0] * ap[1] - gen[1] * ap[0]};
+    const float c2[3] = {gen[1] * axis[2] - gen[2] * axis[1], gen[2] * axis[0] - gen[0] * axis[2],
+                         gen[0] * axis[1] - gen[1] * axis[0]};
+    const bool in = p[1] >= -hh && p[1] <= hh && (c1[0] * c2[0] + c1[1] * c2[1] + c1[2] * c2[2]) >= 0.f;
+    if (in) {
+        float d_side = 0.f, d_base = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            d_side += (proj[k] - p[k]) * (proj[k] - p[k]);
+            d_base += (base[k] - p[k]) * (base[k] - p[k]);
+        }
+        const float *src = d_side > d_base ? base : proj;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) out[k] = src[k];
+        return true;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = proj[k];
+    return false;
+}
+
+// Shape::project_point_on_boundary for balls, cuboids, capsules, cylinders
+// and cones (shaders/slosh/rbd/shapes/shape.slang:152-175; ball.slang:39-52,
+// cuboid.slang:14-63, capsule.slang, cylinder.slang, cone.slang).
 template <int D>
 __device__ __forceinline__ bool project_on_boundary(const DevBody &b, const float *pt, float *proj, bool &inside) {
     float local[D], lp[D];
@@ -672,6 +813,12 @@ __device__ __forceinline__ bool project_on_boundary(const DevBody &b, const floa
         for (int i = 0; i < D; ++i) lp[i] = (dist != 0.f) ? local[i] * (rad / dist) : 0.f;
         if (dist == 0.f) lp[1] = rad;
         inside = dist <= rad;
+    } else if (b.shape_type == SLOSH_SHAPE_CAPSULE) {
+        inside = capsule_boundary<D>(b.sa, b.sb, b.sb[3], local, lp);
+    } else if constexpr (D == 3) {
+        if (b.shape_type == SLOSH_SHAPE_CYLINDER) inside = cylinder_boundary(b.sa[0], b.sa[1], local, lp);
+        else if (b.shape_type == SLOSH_SHAPE_CONE) inside = cone_boundary(b.sa[0], b.sa[1], local, lp);
+        else return false;
     } else {
         return false;
     }

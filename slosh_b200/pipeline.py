@@ -203,8 +203,11 @@ class GpuBoundaryCondition:
 @dataclass
 class RigidBody:
     """One body with its collider (a GpuBodySet entry).  ``shape`` is
-    ("cuboid", half_extents) or ("ball", radius).  Rotation is a unit
-    quaternion (i, j, k, w) in 3D or an angle in radians in 2D."""
+    ("cuboid", half_extents), ("ball", radius), ("capsule", (a, b, radius))
+    with a, b the segment end points, or in 3D ("cylinder", (half_height,
+    radius)) or ("cone", (half_height, radius)) around the local y axis
+    (GpuShape layouts, shaders/slosh/rbd/shapes/shape.slang:37-80).  Rotation
+    is a unit quaternion (i, j, k, w) in 3D or an angle in radians in 2D."""
 
     shape: tuple
     translation: Sequence[float] = (0.0, 0.0, 0.0)
@@ -226,6 +229,19 @@ class RigidBody:
         elif kind == "ball":
             r["shape_a"][0] = float(param)
             r["shape_a"].view(np.uint32)[3] = _lib.SHAPE_BALL
+        elif kind == "capsule":
+            a, b, radius = param
+            a = list(a) + [0.0] * (3 - len(a))
+            b = list(b) + [0.0] * (3 - len(b))
+            r["shape_a"][:3] = a[:3]
+            r["shape_a"].view(np.uint32)[3] = _lib.SHAPE_CAPSULE
+            r["shape_b"][:3] = b[:3]
+            r["shape_b"][3] = float(radius)
+        elif kind in ("cylinder", "cone") and dim == 3:
+            hh, radius = param
+            r["shape_a"][0] = float(hh)
+            r["shape_a"][1] = float(radius)
+            r["shape_a"].view(np.uint32)[3] = _lib.SHAPE_CYLINDER if kind == "cylinder" else _lib.SHAPE_CONE
         else:
             raise ValueError(f"unsupported shape {kind!r}")
         if dim == 3:

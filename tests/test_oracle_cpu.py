@@ -267,3 +267,55 @@ def test_timestep_bound_models(oracle_lib):
     c = math.sqrt(1.0e4 / 1000.0)
     assert abs(o.timestep_bound()[0] - 0.5 * h / c * 1e12) <= 1e-6 * 0.5 * h / c * 1e12
     o.close()
+
+
+def test_collider_shape_projections(oracle_lib):
+    """Capsule, cylinder and cone boundary projections
+    (rbd/shapes/capsule.slang, cylinder.slang, cone.slang): the projection
+    lies on the analytic surface, the inside flag matches the analytic
+    inside test, and outside points project to their nearest surface point
+    (checked against the analytic distance)."""
+    rng = np.random.default_rng(7)
+    a, b, rc = np.array([-0.1, -0.05, 0.02]), np.array([0.15, 0.1, -0.03]), 0.07
+    hh, r = 0.12, 0.09
+
+    def seg_dist(p):
+        ab = b - a
+        t = np.clip(np.dot(p - a, ab) / np.dot(ab, ab), 0.0, 1.0)
+        return np.linalg.norm(p - (a + t * ab))
+
+    def cone_radius(y):
+        return r * (hh - y) / (2 * hh)
+
+    def cyl_dist(p):  # signed Euclidean distance to the cylinder surface
+        dy, dr = abs(p[1]) - hh, math.hypot(p[0], p[2]) - r
+        return math.hypot(dy, dr) if dy > 0 and dr > 0 else max(dy, dr)
+
+    shapes = {
+        "capsule": (RigidBody(("capsule", (a, b, rc))).record(3), lambda p: seg_dist(p) - rc),
+        "cylinder": (RigidBody(("cylinder", (hh, r))).record(3), lambda p: cyl_dist(p)),
+        "cone": (RigidBody(("cone", (hh, r))).record(3), None),
+    }
+    for name, (rec, sdf) in shapes.items():
+        for _ in range(400):
+            p = rng.uniform(-0.3, 0.3, 3)
+            proj, inside = oracle_lib.project_on_boundary(3, rec, p)
+            proj = proj.astype(np.float64)
+            if name == "cone":
+                rxz, y = math.hypot(p[0], p[2]), p[1]
+                exp_inside = -hh <= y <= hh and rxz <= cone_radius(y)
+                on_base = abs(proj[1] + hh) < 1e-5 and math.hypot(proj[0], proj[2]) <= r + 1e-5
+                on_side = abs(math.hypot(proj[0], proj[2]) - cone_radius(proj[1])) < 1e-5
+                assert on_base or on_side, (name, p, proj)
+            else:
+                exp_inside = sdf(p) <= 0
+                assert abs(sdf(proj)) < 1e-5, (name, p, proj)
+                if not exp_inside:  # outside: the projection is the nearest surface point
+                    assert abs(np.linalg.norm(proj - p) - sdf(p)) < 1e-5, (name, p, proj)
+            if abs(sdf(p) if sdf else 1.0) > 1e-4:
+                assert inside == exp_inside, (name, p)
+    # 2D capsule
+    rec2 = RigidBody(("capsule", ((-0.1, 0.0), (0.2, 0.05), 0.05))).record(2)
+    proj, inside = oracle_lib.project_on_boundary(2, rec2, (0.05, 0.3))
+    assert not inside and abs(np.linalg.norm(proj - np.array([0.05, 0.3])) - (0.3 - 0.025 - 0.05)) < 0.02
+    assert oracle_lib.project_on_boundary(2, RigidBody(("cone", (0.1, 0.1))).record(3), (0.0, 0.0)) is None
