@@ -165,6 +165,19 @@ int slosh_set_params(slosh_ctx *ctx, const slosh_params *params);
 int slosh_upload_particles(slosh_ctx *ctx, const slosh_particle *particles,
                            uint32_t n, void *stream);
 
+/* Appends `n` particles from HOST memory behind the current ones; they take
+ * the insertion-order indices [old count, old count + n).  Replaces
+ * GpuParticles::append (src/solver/particle.rs:536-572). */
+int slosh_append_particles(slosh_ctx *ctx, const slosh_particle *particles,
+                           uint32_t n, void *stream);
+
+/* Removes the particles with insertion-order indices [start, start + count)
+ * (clamped to the current count); later particles move down to close the
+ * gap.  `*removed` receives the number removed.  Replaces
+ * GpuParticles::shift_remove (src/solver/particle.rs:505-534). */
+int slosh_remove_particles(slosh_ctx *ctx, uint32_t start, uint32_t count,
+                           uint32_t *removed, void *stream);
+
 /* Reads the particles back into the record layout above (in upload order).
  * Replaces the staging readbacks of src_testbed/step.rs:260-334.
  * `vel_grad_det` is transient inside the fused G2P/update and reads as 0. */

@@ -232,6 +232,8 @@ SIGNATURES = {
     "slosh_ctx_destroy": (None, [_P]),
     "slosh_set_params": (ctypes.c_int, [_P, ctypes.POINTER(SloshParams)]),
     "slosh_upload_particles": (ctypes.c_int, [_P, _P, _U32, _P]),
+    "slosh_append_particles": (ctypes.c_int, [_P, _P, _U32, _P]),
+    "slosh_remove_particles": (ctypes.c_int, [_P, _U32, _U32, ctypes.POINTER(_U32), _P]),
     "slosh_download_particles": (ctypes.c_int, [_P, _P, _U32, _P]),
     "slosh_download_positions": (ctypes.c_int, [_P, _P, _U32, _P]),
     "slosh_set_bodies": (ctypes.c_int, [_P, _P, _U32]),

@@ -52,6 +52,7 @@ DevScene make_batch_scene(slosh_batch *b, uint32_t parity) {
     slosh_ctx *c = &b->c;
     DevScene s = make_scene(c, parity, false);
     s.n = c->max_n;  // plane stride; the count is *n_dev
+    s.count = 0u;
     s.force_pending = 0u;
     s.scenes = b->scenes_dev;
     s.n_scenes = b->max_scenes;

@@ -118,7 +118,7 @@ template <bool B> __device__ __forceinline__ uint32_t map_find_prev(const DevSce
 // Particles in storage.
 template <bool B> __device__ __forceinline__ uint32_t n_particles(const DevScene &s) {
     if constexpr (B) return *s.n_dev;
-    else return s.n;
+    else return s.count;
 }
 
 // Cell index of a local cell inside its block: x + BW y (+ BW^2 z).

@@ -78,11 +78,12 @@ __global__ void k_mat_insert(DevScene s, IoBuffers io, uint32_t count) {
 }
 
 // Pass 2 of the upload: record i -> structure of arrays at storage index
-// base + i, original id i.  Multi-scene batches (B) tag the particle with its
-// scene slot and keep no upload-order side arrays (forces are rejected on
-// the host; radius and phase stay with the host).
+// base + i, original id oid_base + i.  Multi-scene batches (B) tag the
+// particle with its scene slot and keep no upload-order side arrays (forces
+// are rejected on the host; radius and phase stay with the host).
 template <int D, bool B = false>
-__global__ void k_ingest(DevScene s, IoBuffers io, uint32_t base, uint32_t count, uint32_t scene) {
+__global__ void k_ingest(DevScene s, IoBuffers io, uint32_t base, uint32_t count, uint32_t scene,
+                         uint32_t oid_base = 0u) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const size_t n = s.n;
     uint32_t sflags = 0;
@@ -126,11 +127,11 @@ __global__ void k_ingest(DevScene s, IoBuffers io, uint32_t base, uint32_t count
             }
         s.V0[i] = p.init_volume;
         s.damping[i] = p.damping;
-        s.oid[i] = i0;
+        s.oid[i] = oid_base + i0;
         if (p.damping != 0.f) sflags |= SCENE_DAMPING;
         if constexpr (!B) {
-            io.r0[i] = p.init_radius;
-            io.phase[i] = p.phase;
+            io.r0[oid_base + i0] = p.init_radius;
+            io.phase[oid_base + i0] = p.phase;
         }
         s.flags[i] = (dense & FLAG_MAT_MASK) | (p.enabled ? FLAG_ENABLED : 0u) | (p.fixed ? FLAG_FIXED : 0u) |
                      (scene << FLAG_SCENE_SHIFT);
@@ -190,6 +191,55 @@ template <int D, bool B = false> __global__ void k_egest(DevScene s, IoBuffers i
     }
 }
 
+// GpuParticles::shift_remove (src/solver/particle.rs:505-534) of the
+// original ids [start, end): every other stored particle is copied from
+// storage A to storage B at its new insertion-order index (ids past the
+// range move down by end - start), so B holds the survivors in insertion
+// order, like right after an upload.  The upload-order side arrays (radius,
+// phase) and the pending forces move to the same new indices through
+// `tmp` (3 + D floats a particle, plane stride s.n).
+template <int D>
+__global__ void k_remove(DevScene s, IoBuffers io, uint32_t start, uint32_t end, float *tmp) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const size_t n = s.n;
+    const uint32_t removed = end - start;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.count; i += stride) {
+        const uint32_t o = s.oid[i];
+        if (o >= start && o < end) continue;
+        const uint32_t j = o >= end ? o - removed : o;
+        s.out_pm[j] = s.pm[i];
+#pragma unroll
+        for (int k = 0; k < D; ++k) s.out_vel[k * n + j] = s.vel[k * n + i];
+#pragma unroll
+        for (int q = 0; q < D * D; ++q) {
+            s.out_C[q * n + j] = s.C[q * n + i];
+            s.out_F[q * n + j] = s.F[q * n + i];
+        }
+        s.out_V0[j] = s.V0[i];
+        s.out_flags[j] = s.flags[i];
+        s.out_damping[j] = s.damping[i];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s.out_plastic[q * n + j] = s.plastic[q * n + i];
+        s.out_oid[j] = j;
+        tmp[j] = io.r0[o];
+        tmp[n + j] = io.phase[o];
+#pragma unroll
+        for (int k = 0; k < D; ++k) tmp[(2 + k) * n + j] = s.force_pending ? s.fdt[k * n + i] : 0.0f;
+    }
+}
+
+// Second pass of the removal: the side arrays and forces back from `tmp`.
+template <int D> __global__ void k_remove_sides(DevScene s, IoBuffers io, uint32_t count, const float *tmp) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const size_t n = s.n;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += stride) {
+        io.r0[j] = tmp[j];
+        io.phase[j] = tmp[n + j];
+#pragma unroll
+        for (int k = 0; k < D; ++k) s.fdt[k * n + j] = tmp[(2 + k) * n + j];
+    }
+}
+
 // Positions as vec4 (x, y, z, 0) in upload order (of one scene in B).
 template <bool B = false> __global__ void k_positions(DevScene s, float4 *out, uint32_t scene) {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -205,7 +255,7 @@ template <bool B = false> __global__ void k_positions(DevScene s, float4 *out, u
 // Debug: the hot path's primary permutation in original ids.
 __global__ void k_perm_to_oid(DevScene s, uint32_t *out) {
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < s.n; e += stride) out[e] = s.oid[s.perm[e]];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < s.count; e += stride) out[e] = s.oid[s.perm[e]];
 }
 
 // ---------------------------------------------------------------------------
@@ -252,7 +302,7 @@ template <int D> __device__ __forceinline__ uint32_t extra_bucket(const int *a, 
 template <int D> __global__ void k_dbg_count(DevScene s, DebugBuffers d) {
     constexpr int NB = Geo<D>::NB, NN = Geo<D>::NASSOC - 1;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.count; i += stride) {
         uint32_t r0;
         int a[D];
         if (!particle_rank_local<D>(s, i, r0, a)) continue;
@@ -294,7 +344,7 @@ template <int D, int NT> __global__ void __launch_bounds__(NT) k_dbg_scan(DevSce
 template <int D> __global__ void k_dbg_scatter(DevScene s, DebugBuffers d) {
     constexpr int NB = Geo<D>::NB, NN = Geo<D>::NASSOC - 1;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += stride) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.count; i += stride) {
         uint32_t r0;
         int a[D];
         if (!particle_rank_local<D>(s, i, r0, a)) continue;

@@ -11,7 +11,8 @@ struct DevScene {
     // Storage is double-buffered: the substep reads the arrays below (in the
     // canonical order of the previous substep) and the fused G2P/update
     // writes the `out_*` arrays in this substep's canonical order.
-    uint32_t n;            // particle count
+    uint32_t n;            // plane stride of the particle arrays (pool capacity)
+    uint32_t count;        // particles in storage (single-scene context; batches read *n_dev)
     float h;               // cell width
     float inv_h;           // 1 / h (exact when h_pow2)
     uint32_t h_pow2;       // h is a power of two

@@ -117,7 +117,8 @@ int nbk(int dim) { return dim == 3 ? Geo<3>::NB : Geo<2>::NB; }
 
 DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     DevScene s{};
-    s.n = c->n;
+    s.n = c->max_n;
+    s.count = c->n;
     s.h = c->h;
     s.inv_h = 1.0f / c->h;
     {
@@ -538,6 +539,84 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     c->has_damping = (small[1] & SCENE_DAMPING) ? 1u : 0u;
     c->force_pending = (small[1] & SCENE_FORCE) ? 1u : 0u;
     c->has_sand = (small[1] & SCENE_SAND) ? 1u : 0u;
+    return check_device_error(c);
+}
+
+int slosh_append_particles(slosh_ctx *c, const slosh_particle *particles, uint32_t n, void *stream) {
+    if (!c || (!particles && n)) return SLOSH_E_INVALID;
+    if ((uint64_t)c->n + n > c->max_n)
+        return fail(c, SLOSH_E_CAPACITY, "%u + %u particles exceed max_particles %u", c->n, n, c->max_n);
+    if (n == 0) return SLOSH_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    CK(cudaStreamSynchronize(c->stream));
+    destroy_graphs(c);
+    bool forces = false;
+    for (uint32_t i = 0; i < n && !forces; ++i)
+        forces = particles[i].force_dt[0] != 0.f || particles[i].force_dt[1] != 0.f || particles[i].force_dt[2] != 0.f;
+    const uint32_t base = c->n;
+    DevScene s = make_scene(c, c->parity, false);
+    if (forces && !c->force_pending && base > 0) {
+        // the stored forces of the earlier particles were consumed by a substep
+        for (int k = 0; k < c->dim; ++k) CK(cudaMemsetAsync(c->fdt + (size_t)k * c->max_n, 0, (size_t)base * 4, st));
+    }
+    CK(cudaMemcpyAsync(c->staging, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice, st));
+    IoBuffers io{};
+    io.in = c->staging;
+    io.mat_hkeys = c->mat_hkeys;
+    io.mat_dense = c->mat_dense;
+    io.n_mat = c->small;
+    io.scene_flags = c->small + 1;
+    io.r0 = c->r0;
+    io.phase = c->phase;
+    const uint32_t g = grid_for(n, 256, (uint32_t)c->sm_count * 16);
+    k_mat_insert<<<g, 256, 0, st>>>(s, io, n);
+    if (c->dim == 3) k_ingest<3><<<g, 256, 0, st>>>(s, io, base, n, 0u, base);
+    else k_ingest<2><<<g, 256, 0, st>>>(s, io, base, n, 0u, base);
+    CK(cudaGetLastError());
+    uint32_t small[2] = {0, 0};
+    CK(cudaMemcpyAsync(small, c->small, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    c->n = base + n;
+    c->n_materials = small[0];
+    c->has_damping = (small[1] & SCENE_DAMPING) ? 1u : 0u;
+    c->has_sand = (small[1] & SCENE_SAND) ? 1u : 0u;
+    c->force_pending = (c->force_pending || forces) ? 1u : 0u;
+    return check_device_error(c);
+}
+
+int slosh_remove_particles(slosh_ctx *c, uint32_t start, uint32_t count, uint32_t *removed, void *stream) {
+    if (!c) return SLOSH_E_INVALID;
+    const uint32_t end = (uint32_t)std::min<uint64_t>((uint64_t)start + count, c->n);
+    const uint32_t nrem = start < end ? end - start : 0u;
+    if (removed) *removed = nrem;
+    if (nrem == 0) return SLOSH_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    CK(cudaStreamSynchronize(c->stream));
+    destroy_graphs(c);
+    const DevScene s = make_scene(c, c->parity, c->force_pending != 0);
+    IoBuffers io{};
+    io.r0 = c->r0;
+    io.phase = c->phase;
+    // the record staging area (192 bytes a particle) holds the (3 + D)-plane temporary
+    float *tmp = reinterpret_cast<float *>(c->staging);
+    const uint32_t g = grid_for(c->n, 256, (uint32_t)c->sm_count * 16);
+    if (c->dim == 3) k_remove<3><<<g, 256, 0, st>>>(s, io, start, end, tmp);
+    else k_remove<2><<<g, 256, 0, st>>>(s, io, start, end, tmp);
+    CK(cudaGetLastError());
+    const uint32_t left = c->n - nrem;
+    // B now holds the survivors in insertion order: make it the current storage
+    std::swap(c->pb[c->parity & 1u], c->pb[(c->parity & 1u) ^ 1u]);
+    c->n = left;
+    const DevScene s2 = make_scene(c, c->parity, false);
+    if (left) {
+        const uint32_t g2 = grid_for(left, 256, (uint32_t)c->sm_count * 16);
+        if (c->dim == 3) k_remove_sides<3><<<g2, 256, 0, st>>>(s2, io, left, tmp);
+        else k_remove_sides<2><<<g2, 256, 0, st>>>(s2, io, left, tmp);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(st));
     return check_device_error(c);
 }
 

@@ -335,6 +335,26 @@ class MpmData:
             self._lib.slosh_upload_particles(self._ctx, ptr(particles), self.n, stream),
         )
 
+    def append(self, particles: np.ndarray, stream=None):
+        """``GpuParticles::append`` (src/solver/particle.rs:536-572)."""
+        particles = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        _check(self._lib, self._ctx, self._lib.slosh_append_particles(self._ctx, ptr(particles), len(particles), stream))
+        self.n += len(particles)
+
+    def shift_remove(self, start: int, end: int, stream=None) -> int:
+        """``GpuParticles::shift_remove`` of the insertion-order range
+        [start, end) (src/solver/particle.rs:505-534); returns the number
+        removed."""
+        removed = ctypes.c_uint32(0)
+        count = max(int(end) - int(start), 0)
+        _check(
+            self._lib,
+            self._ctx,
+            self._lib.slosh_remove_particles(self._ctx, int(start), count, ctypes.byref(removed), stream),
+        )
+        self.n -= removed.value
+        return removed.value
+
     def download_particles(self, out: np.ndarray | None = None, stream=None) -> np.ndarray:
         if out is None:
             out = np.zeros(self.n, dtype=PARTICLE_DTYPE)

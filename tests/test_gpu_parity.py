@@ -354,3 +354,41 @@ def test_collider_shapes_parity(cuda_lib, name):
     orc.step(5)
     compare_particles(f"{name} 5 steps", data.download_particles(), orc.get_particles(), d, loose=5.0)
     data.close()
+
+
+def test_append_and_shift_remove(cuda_lib):
+    """GpuParticles::append / shift_remove (src/solver/particle.rs:505-572):
+    appended particles take the next insertion-order indices, a removed range
+    closes up, and stepping afterwards matches the oracle given the same
+    record edits."""
+    sc = small_scenes()["elastic3d"]
+    parts = sc.particles
+    half = len(parts) // 2
+    sc.particles = parts[:half].copy()
+    data = scenes.build_mpm_data(sc, max_particles=len(parts))
+    orc = O.from_scene(sc, threads=8)
+    pipe = MpmPipeline()
+    pipe.launch_step(data, 4)
+    orc.step(4)
+    data.append(parts[half:])
+    orc.set_particles(np.concatenate([orc.get_particles(), parts[half:]]))
+    got = data.download_particles()
+    assert len(got) == len(parts)
+    assert np.array_equal(got[half:]["position"], parts[half:]["position"])
+    pipe.launch_step(data, 3)
+    orc.step(3)
+    compare_particles("after append", data.download_particles(), orc.get_particles(), 3, loose=5.0)
+    before = data.download_particles()
+    start, end = len(parts) // 5, len(parts) // 5 + 777
+    assert data.shift_remove(start, end) == 777
+    after = data.download_particles()
+    expect = np.concatenate([before[:start], before[end:]])
+    for k in ("position", "velocity", "def_grad", "affine", "mass", "init_radius", "phase"):
+        assert np.array_equal(after[k], expect[k]), k
+    o = orc.get_particles()
+    orc.set_particles(np.concatenate([o[:start], o[end:]]))
+    pipe.launch_step(data, 3)
+    orc.step(3)
+    compare_particles("after shift_remove", data.download_particles(), orc.get_particles(), 3, loose=10.0)
+    assert data.shift_remove(len(after) - 10, len(after) + 50) == 10  # clamped to the count
+    data.close()
