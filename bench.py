@@ -90,6 +90,24 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(ms: float, pg, device=None) -> float:
+    """The slowest rank's time: every rank passes its own timed region and
+    gets the maximum (all ranks take this collective at the same point)."""
+    if pg is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, units_per_rank: float, ms: float) -> float:
+    """Whole-job throughput of replicas: units of all ranks over the slowest
+    rank's time (weak scaling: every rank runs the full workload)."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -310,12 +328,8 @@ def main_ours(args):
     barrier()
     ck = clocks.stop()
     data.sync(sptr)
-    ms = ev0.elapsed_time(ev1)
-    if pg is not None:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), pg, dev)
+    value = aggregate_rate(world, n * args.steps, ms)
     launches = data.kernels_per_substep * args.steps
 
     # per-kernel device time (direct launches with events around each kernel)
@@ -377,13 +391,9 @@ def main_ours(args):
             data.positions(out, sptr)
         e1.record(stream)
         barrier()
-        ems = e0.elapsed_time(e1)
-        if pg is not None:
-            t = torch.tensor([ems], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(e0.elapsed_time(e1), pg, dev)
         e2e = {
-            "value": world * n * args.e2e_substeps * args.e2e_steps / (ems / 1e3),
+            "value": aggregate_rate(world, n * args.e2e_substeps * args.e2e_steps, ems),
             "unit": UNIT,
             "h2d_bytes_per_step": int(n * PARTICLE_DTYPE.itemsize),
             "d2h_bytes_per_step": int(n * 16),
