@@ -40,6 +40,18 @@ struct slosh_batch {
     uint32_t n_storage = 0;         // particles in storage (mirror of *n_dev)
     uint32_t body_top = 0;          // body table entries in use
     uint32_t staging_cap = 0;       // records in c.staging
+    // Two-phase admission: a staged scene's records sit in `up` (copied on
+    // `up_stream`, possibly while substeps run); activation converts them
+    // into the pool between substeps.
+    struct Staged {
+        uint32_t slot, n, offset, tags;
+        slosh_scene_desc desc;
+        std::vector<DevBody> bodies;
+    };
+    std::vector<Staged> staged;
+    slosh_particle *up = nullptr;
+    uint32_t up_cap = 0, up_used = 0, staged_n = 0;
+    cudaStream_t up_stream = nullptr;
     slosh_tuning tune{8, 128, 8, 0};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
@@ -159,7 +171,7 @@ int compact_bodies(slosh_batch *b) {
     std::vector<DevBody> kept;
     for (uint32_t s = 0; s < b->max_scenes; ++s) {
         slosh_batch::Slot &sl = b->slots[s];
-        if (!sl.used) continue;
+        if (!sl.live) continue;  // dropped scenes no longer read bodies; staged ones have none yet
         const uint32_t first = (uint32_t)kept.size();
         for (uint32_t k = 0; k < sl.n_bodies; ++k) kept.push_back(all[sl.body_first + k]);
         sl.body_first = first;
@@ -212,6 +224,8 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     if (cudaSetDevice(c->device) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
+    if (cudaStreamCreateWithFlags(&b->up_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail_create(SLOSH_E_CUDA);
     const size_t N = c->max_n;
     const int D = c->dim;
     const uint32_t cap = c->cap, hcap = c->hcap;
@@ -273,35 +287,60 @@ void slosh_batch_destroy(slosh_batch *b) {
     if (!b) return;
     cudaSetDevice(b->c.device);
     destroy_batch_graphs(b);
+    if (b->up_stream) {
+        cudaStreamSynchronize(b->up_stream);
+        cudaStreamDestroy(b->up_stream);
+    }
     release_ctx(&b->c);
     delete b;
 }
 
-int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles, uint32_t n,
-                          const slosh_body *bodies, uint32_t n_bodies, uint32_t *slot_out, void *stream) {
-    if (!b || !desc || (!particles && n) || (!bodies && n_bodies) || !slot_out) return SLOSH_E_INVALID;
+}  // extern "C"
+
+namespace {
+
+// Checks a scene before anything is claimed; returns its model-tag mask.
+int batch_validate(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles, uint32_t n,
+                   const slosh_body *bodies, uint32_t n_bodies, uint32_t *tags) {
     slosh_ctx *c = &b->c;
     if (n == 0) return fail(c, SLOSH_E_INVALID, "a scene needs particles");
     if (!(desc->cell_width > 0.f) || !(desc->params.dt > 0.f))
         return fail(c, SLOSH_E_INVALID, "cell width and dt must be > 0");
     if (n_bodies > MAX_BODIES) return fail(c, SLOSH_E_CAPACITY, "%u bodies exceed %u per scene", n_bodies, MAX_BODIES);
-    if ((uint64_t)b->n_storage + n > c->max_n)
-        return fail(c, SLOSH_E_CAPACITY, "%u + %u particles exceed the pool of %u", b->n_storage, n, c->max_n);
     for (uint32_t k = 0; k < n_bodies; ++k) {
         DevBody d;
         to_dev_body(bodies[k], d);
         if (!(d.scale > 0.f) || !shape_supported(d.shape_type, c->dim))
             return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u or scale", k, d.shape_type);
     }
-    uint32_t tags = 0;
+    uint32_t m = 0;
     for (uint32_t i = 0; i < n; ++i) {
         const slosh_particle &p = particles[i];
         if (p.force_dt[0] != 0.f || p.force_dt[1] != 0.f || p.force_dt[2] != 0.f)
             return fail(c, SLOSH_E_INVALID, "external forces (force_dt) are not supported in batches");
-        if (p.model.tag < 32) tags |= 1u << p.model.tag;
+        if (p.model.tag < 32) m |= 1u << p.model.tag;
     }
-    CK(cudaSetDevice(c->device));
-    CK(cudaDeviceSynchronize());  // no substep may run while the pool and tables change
+    *tags = m;
+    return SLOSH_OK;
+}
+
+// Phase 1 of an admission: claims a slot and copies the records into the
+// upload buffer on the upload stream (the host returns when they are on the
+// device).  Nothing a substep reads changes, so substeps may be in flight.
+// SLOSH_E_CAPACITY when the pool, the slots, the body table or the upload
+// buffer cannot take the scene now.
+int batch_stage(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles, uint32_t n,
+                const slosh_body *bodies, uint32_t n_bodies, uint32_t tags, uint32_t *slot_out) {
+    slosh_ctx *c = &b->c;
+    if ((uint64_t)b->n_storage + b->staged_n + n > c->max_n)
+        return fail(c, SLOSH_E_CAPACITY, "%u + %u particles exceed the pool of %u", b->n_storage + b->staged_n, n,
+                    c->max_n);
+    uint32_t bodies_in_use = n_bodies;
+    for (const auto &sl : b->slots) bodies_in_use += sl.used ? sl.n_bodies : 0u;
+    for (const auto &sg : b->staged) bodies_in_use += (uint32_t)sg.bodies.size();
+    if (bodies_in_use > b->max_bodies) return fail(c, SLOSH_E_CAPACITY, "body table full (%u entries)", b->max_bodies);
+    if ((uint64_t)b->up_used + n > b->up_cap)
+        return fail(c, SLOSH_E_CAPACITY, "upload buffer full (%u + %u records of %u)", b->up_used, n, b->up_cap);
     uint32_t slot = NONE;
     for (uint32_t s = 0; s < b->max_scenes; ++s)
         if (!b->slots[s].used) {
@@ -309,74 +348,24 @@ int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const sl
             break;
         }
     if (slot == NONE) return fail(c, SLOSH_E_CAPACITY, "all %u scene slots are in use", b->max_scenes);
-    cudaStream_t st = pick(c, stream);
-    if (b->body_top + n_bodies > b->max_bodies) {
-        int r = compact_bodies(b);
-        if (r) return r;
-        if (b->body_top + n_bodies > b->max_bodies)
-            return fail(c, SLOSH_E_CAPACITY, "body table full (%u entries)", b->max_bodies);
+    CK(cudaMemcpyAsync(b->up + b->up_used, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice,
+                       b->up_stream));
+    CK(cudaStreamSynchronize(b->up_stream));
+    slosh_batch::Staged sg;
+    sg.slot = slot;
+    sg.n = n;
+    sg.offset = b->up_used;
+    sg.tags = tags;
+    sg.desc = *desc;
+    sg.bodies.resize(n_bodies);
+    for (uint32_t k = 0; k < n_bodies; ++k) {
+        to_dev_body(bodies[k], sg.bodies[k]);
+        sg.bodies[k].scene = slot;
     }
-    if (n > b->staging_cap) {
-        CK(cudaStreamSynchronize(st));
-        if (c->staging) {
-            cudaFree(c->staging);
-            c->allocs.erase(std::find(c->allocs.begin(), c->allocs.end(), (void *)c->staging));
-            c->staging = nullptr;
-        }
-        int r = dalloc(c, &c->staging, n);
-        if (r) return r;
-        b->staging_cap = n;
-    }
-    const uint32_t base = b->n_storage;
-    DevScene s = make_batch_scene(b, c->parity);
-    IoBuffers io{};
-    io.in = c->staging;
-    io.mat_hkeys = c->mat_hkeys;
-    io.mat_dense = c->mat_dense;
-    io.n_mat = c->small;
-    io.scene_flags = c->small + 1;
-    CK(cudaMemcpyAsync(c->staging, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice, st));
-    const uint32_t g = grid_for(n, 256, (uint32_t)c->sm_count * 16);
-    k_mat_insert<<<g, 256, 0, st>>>(s, io, n);
-    if (c->dim == 3) k_ingest<3, true><<<g, 256, 0, st>>>(s, io, base, n, slot);
-    else k_ingest<2, true><<<g, 256, 0, st>>>(s, io, base, n, slot);
-    CK(cudaGetLastError());
-    const uint32_t new_n = base + n;
-    CK(cudaMemcpyAsync(b->n_dev, &new_n, 4, cudaMemcpyHostToDevice, st));
-    if (n_bodies) {
-        std::vector<DevBody> db(n_bodies);
-        for (uint32_t k = 0; k < n_bodies; ++k) {
-            to_dev_body(bodies[k], db[k]);
-            db[k].scene = slot;
-        }
-        CK(cudaMemcpyAsync(c->bodies + b->body_top, db.data(), n_bodies * sizeof(DevBody), cudaMemcpyHostToDevice, st));
-        CK(cudaStreamSynchronize(st));
-    }
-    SceneRec &rec = b->scenes[slot];
-    rec = SceneRec{};
-    rec.h = desc->cell_width;
-    rec.inv_h = 1.0f / desc->cell_width;
-    rec.dt = desc->params.dt;
-    for (int k = 0; k < 3; ++k) rec.gravity[k] = desc->params.gravity[k];
-    int ex = 0;
-    rec.h_pow2 = (std::frexp(desc->cell_width, &ex) == 0.5f) ? 1u : 0u;
-    rec.body_first = b->body_top;
-    rec.n_bodies = n_bodies;
-    rec.live = 1u;
-    int r = upload_scene_rec(b, slot, st);
-    if (r) return r;
-    uint32_t small[2] = {0, 0};
-    CK(cudaMemcpy(small, c->small, 8, cudaMemcpyDeviceToHost));
-    c->n_materials = small[0];
-    c->has_damping |= (small[1] & SCENE_DAMPING) ? 1u : 0u;
-    c->has_sand |= (small[1] & SCENE_SAND) ? 1u : 0u;
-    r = batch_check_error(b);
-    if (r) return r;
     slosh_batch::Slot &sl = b->slots[slot];
+    sl = slosh_batch::Slot{};
     sl.used = true;
-    sl.live = true;
     sl.n = n;
-    sl.body_first = b->body_top;
     sl.n_bodies = n_bodies;
     sl.tags = tags;
     sl.r0.resize(n);
@@ -385,12 +374,123 @@ int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const sl
         sl.r0[i] = particles[i].init_radius;
         sl.phase[i] = particles[i].phase;
     }
-    b->body_top += n_bodies;
-    b->n_storage = new_n;
-    if (b->graphs_valid && (b->graph_flags != (c->has_damping | (c->has_sand << 1)) || n_bodies))
-        destroy_batch_graphs(b);  // captured scene flags or body count changed
+    b->up_used += n;
+    b->staged_n += n;
+    b->staged.push_back(std::move(sg));
     *slot_out = slot;
     return SLOSH_OK;
+}
+
+// Phase 2: converts every staged scene into the pool behind the live
+// particles, writes its bodies and scene record, and makes them live.  No
+// substep may be in flight.
+int batch_activate(slosh_batch *b, cudaStream_t st) {
+    slosh_ctx *c = &b->c;
+    if (b->staged.empty()) return SLOSH_OK;
+    uint32_t new_bodies = 0;
+    for (const auto &sg : b->staged) new_bodies += (uint32_t)sg.bodies.size();
+    if (b->body_top + new_bodies > b->max_bodies) {
+        int r = compact_bodies(b);
+        if (r) return r;
+    }
+    DevScene s = make_batch_scene(b, c->parity);
+    IoBuffers io{};
+    io.mat_hkeys = c->mat_hkeys;
+    io.mat_dense = c->mat_dense;
+    io.n_mat = c->small;
+    io.scene_flags = c->small + 1;
+    uint32_t base = b->n_storage;
+    for (auto &sg : b->staged) {
+        io.in = b->up + sg.offset;
+        const uint32_t g = grid_for(sg.n, 256, (uint32_t)c->sm_count * 16);
+        k_mat_insert<<<g, 256, 0, st>>>(s, io, sg.n);
+        if (c->dim == 3) k_ingest<3, true><<<g, 256, 0, st>>>(s, io, base, sg.n, sg.slot);
+        else k_ingest<2, true><<<g, 256, 0, st>>>(s, io, base, sg.n, sg.slot);
+        CK(cudaGetLastError());
+        if (!sg.bodies.empty())
+            CK(cudaMemcpyAsync(c->bodies + b->body_top, sg.bodies.data(), sg.bodies.size() * sizeof(DevBody),
+                               cudaMemcpyHostToDevice, st));
+        SceneRec &rec = b->scenes[sg.slot];
+        rec = SceneRec{};
+        rec.h = sg.desc.cell_width;
+        rec.inv_h = 1.0f / sg.desc.cell_width;
+        rec.dt = sg.desc.params.dt;
+        for (int k = 0; k < 3; ++k) rec.gravity[k] = sg.desc.params.gravity[k];
+        int ex = 0;
+        rec.h_pow2 = (std::frexp(sg.desc.cell_width, &ex) == 0.5f) ? 1u : 0u;
+        rec.body_first = b->body_top;
+        rec.n_bodies = (uint32_t)sg.bodies.size();
+        rec.live = 1u;
+        CK(cudaMemcpyAsync(b->scenes_dev + sg.slot, &rec, sizeof(SceneRec), cudaMemcpyHostToDevice, st));
+        slosh_batch::Slot &sl = b->slots[sg.slot];
+        sl.live = true;
+        sl.body_first = b->body_top;
+        b->body_top += rec.n_bodies;
+        base += sg.n;
+    }
+    const uint32_t new_n = base;
+    CK(cudaMemcpyAsync(b->n_dev, &new_n, 4, cudaMemcpyHostToDevice, st));
+    uint32_t small[2] = {0, 0};
+    CK(cudaMemcpyAsync(small, c->small, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));  // the host-side sources above are released after this
+    c->n_materials = small[0];
+    c->has_damping |= (small[1] & SCENE_DAMPING) ? 1u : 0u;
+    c->has_sand |= (small[1] & SCENE_SAND) ? 1u : 0u;
+    b->n_storage = new_n;
+    if (b->graphs_valid && (b->graph_flags != (c->has_damping | (c->has_sand << 1)) || new_bodies))
+        destroy_batch_graphs(b);  // captured scene flags or body count changed
+    b->staged.clear();
+    b->up_used = 0;
+    b->staged_n = 0;
+    return batch_check_error(b);
+}
+
+// Grows the upload buffer to `n` records (device idle).
+int batch_reserve_upload(slosh_batch *b, uint32_t n) {
+    slosh_ctx *c = &b->c;
+    if (n <= b->up_cap) return SLOSH_OK;
+    if (b->up) {
+        cudaFree(b->up);
+        c->allocs.erase(std::find(c->allocs.begin(), c->allocs.end(), (void *)b->up));
+        b->up = nullptr;
+        b->up_cap = 0;
+    }
+    int r = dalloc(c, &b->up, n);
+    if (r) return r;
+    b->up_cap = n;
+    return SLOSH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles, uint32_t n,
+                          const slosh_body *bodies, uint32_t n_bodies, uint32_t *slot_out, void *stream) {
+    if (!b || !desc || (!particles && n) || (!bodies && n_bodies) || !slot_out) return SLOSH_E_INVALID;
+    slosh_ctx *c = &b->c;
+    uint32_t tags = 0;
+    int r = batch_validate(b, desc, particles, n, bodies, n_bodies, &tags);
+    if (r) return r;
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());  // no substep may run while the pool and tables change
+    if (b->staged.empty()) {
+        r = batch_reserve_upload(b, n);
+        if (r) return r;
+    }
+    if (n > b->staging_cap) {  // downloads of this scene go through c.staging
+        if (c->staging) {
+            cudaFree(c->staging);
+            c->allocs.erase(std::find(c->allocs.begin(), c->allocs.end(), (void *)c->staging));
+            c->staging = nullptr;
+        }
+        r = dalloc(c, &c->staging, n);
+        if (r) return r;
+        b->staging_cap = n;
+    }
+    r = batch_stage(b, desc, particles, n, bodies, n_bodies, tags, slot_out);
+    if (r) return r;
+    return batch_activate(b, pick(c, stream));
 }
 
 int slosh_batch_remove_scene(slosh_batch *b, uint32_t slot) {

@@ -16,7 +16,10 @@
 // Steps.  A batched step advances every in-flight scene by the smallest
 // remaining substep count (at most tick_substeps), so every request gets
 // exactly its own number of substeps and leaves the batch right after its
-// last one.
+// last one.  Admission has two phases: while a tick runs on the GPU, queued
+// requests are staged (their records copied into the batch's upload
+// buffer); between ticks the staged scenes are activated (converted into
+// the pool) and join the next tick.
 #pragma once
 
 #include <condition_variable>
@@ -40,6 +43,7 @@ struct slosh_server {
     std::condition_variable cv, idle_cv;
     bool stop = false;
     std::deque<Req> queue;
+    std::vector<Req> staging;  // staged in the batch, joining at the next activation
     std::vector<Req> flight;
     std::deque<slosh_completion> done;
     uint64_t next_id = 1, submitted = 0, admitted = 0, completed = 0, work = 0, in_flight_bytes = 0;
@@ -74,53 +78,79 @@ void retire(slosh_server *s, slosh_server::Req &q, int status, uint32_t done_sub
     s->blocks_in_flight -= q.blocks;
 }
 
+// Stages queued requests, in arrival order, while they fit.  Called both
+// between ticks and while a tick runs: staging only copies records into the
+// batch's upload buffer.
+void stage_pending(slosh_server *s, std::unique_lock<std::mutex> &lk) {
+    slosh_batch *b = s->batch;
+    while (!s->queue.empty()) {
+        const slosh_server::Req &q = s->queue.front();
+        uint32_t free_slots = 0;
+        for (const auto &sl : b->slots) free_slots += sl.used ? 0u : 1u;
+        const size_t active = s->flight.size() + s->staging.size();
+        const bool fits = (s->cfg.max_in_flight == 0 || active < s->cfg.max_in_flight) && free_slots > 0 &&
+                          (uint64_t)b->n_storage + b->staged_n + q.r.n <= s->pool_particles &&
+                          (uint64_t)b->up_used + q.r.n <= b->up_cap &&
+                          (uint64_t)s->blocks_in_flight + q.blocks <= s->pool_blocks;
+        if (!fits) return;
+        slosh_server::Req r = q;
+        s->queue.pop_front();
+        lk.unlock();
+        uint32_t tags = 0, slot = 0;
+        int st = batch_validate(b, &r.r.desc, r.r.particles, r.r.n, r.r.bodies, r.r.n_bodies, &tags);
+        if (st == SLOSH_OK)
+            st = batch_stage(b, &r.r.desc, r.r.particles, r.r.n, r.r.bodies, r.r.n_bodies, tags, &slot);
+        lk.lock();
+        s->admitted += 1;
+        s->in_flight_bytes += r.bytes;
+        s->blocks_in_flight += r.blocks;
+        r.admit_s = s->now();
+        if (st != SLOSH_OK) {
+            s->last_error = b->c.last_error;
+            retire(s, r, st, 0);
+            continue;
+        }
+        r.slot = slot;
+        r.remaining = r.r.substeps;
+        s->staging.push_back(r);
+    }
+}
+
 void server_loop(slosh_server *s) {
     cudaSetDevice(s->cfg.device);
     slosh_batch *b = s->batch;
     std::unique_lock<std::mutex> lk(s->mu);
     while (!s->stop) {
-        // admissions, in arrival order (the batch is touched by this thread only)
-        while (!s->queue.empty()) {
-            const slosh_server::Req &q = s->queue.front();
-            uint32_t free_slots = 0;
-            for (const auto &sl : b->slots) free_slots += sl.used ? 0u : 1u;
-            const bool fits = (s->cfg.max_in_flight == 0 || s->flight.size() < s->cfg.max_in_flight) &&
-                              free_slots > 0 && (uint64_t)b->n_storage + q.r.n <= s->pool_particles &&
-                              (uint64_t)s->blocks_in_flight + q.blocks <= s->pool_blocks;
-            if (!fits) break;
-            slosh_server::Req r = q;
-            s->queue.pop_front();
-            lk.unlock();
-            uint32_t slot = 0;
-            const int st = slosh_batch_add_scene(b, &r.r.desc, r.r.particles, r.r.n, r.r.bodies, r.r.n_bodies, &slot,
-                                                 nullptr);
-            lk.lock();
-            r.admit_s = s->now();
-            s->admitted += 1;
-            s->in_flight_bytes += r.bytes;
-            s->blocks_in_flight += r.blocks;
-            if (st != SLOSH_OK) {
-                s->last_error = b->c.last_error;
-                retire(s, r, st, 0);
+        stage_pending(s, lk);
+        if (s->flight.empty() && s->staging.empty()) {
+            if (!b->dropped.empty()) {
+                // retired scenes hold pool space and slots until a substep compacts them
+                lk.unlock();
+                slosh_batch_step(b, 1, nullptr);
+                slosh_batch_sync(b, nullptr);
+                lk.lock();
                 continue;
             }
-            r.slot = slot;
-            r.remaining = r.r.substeps;
-            s->flight.push_back(r);
-            s->max_seen = std::max<uint32_t>(s->max_seen, (uint32_t)s->flight.size());
-        }
-        if (s->flight.empty() && !b->dropped.empty()) {
-            // retired scenes hold pool space and slots until a substep compacts them
-            lk.unlock();
-            slosh_batch_step(b, 1, nullptr);
-            slosh_batch_sync(b, nullptr);
-            lk.lock();
-            continue;
-        }
-        if (s->flight.empty()) {
             if (s->queue.empty()) s->idle_cv.notify_all();
             s->cv.wait(lk, [&] { return s->stop || !s->queue.empty(); });
             continue;
+        }
+        // activation: the staged scenes join the batch (no tick in flight)
+        if (!s->staging.empty()) {
+            lk.unlock();
+            const int st = batch_activate(b, b->c.stream);
+            lk.lock();
+            for (auto &r : s->staging) {
+                if (st == SLOSH_OK) {
+                    s->flight.push_back(r);
+                } else {
+                    s->last_error = b->c.last_error;
+                    retire(s, r, st, 0);
+                }
+            }
+            s->staging.clear();
+            s->max_seen = std::max<uint32_t>(s->max_seen, (uint32_t)s->flight.size());
+            if (s->flight.empty()) continue;
         }
         uint32_t tick = std::max<uint32_t>(s->cfg.tick_substeps, 1u);
         for (const auto &r : s->flight) tick = std::min(tick, r.remaining);
@@ -136,6 +166,10 @@ void server_loop(slosh_server *s) {
         }
         if (st == SLOSH_OK && ran == 0) st = slosh_batch_step(b, tick, nullptr);
         else if (ran) tick = ran;
+        lk.lock();
+        // while the tick runs on the GPU: copy the next requests' records up
+        if (st == SLOSH_OK) stage_pending(s, lk);
+        lk.unlock();
         if (st == SLOSH_OK) st = slosh_batch_sync(b, nullptr);
         const double tb = s->now();
         lk.lock();
@@ -172,7 +206,8 @@ void server_loop(slosh_server *s) {
             retire(s, r, st2, r.r.substeps);
             s->flight.erase(s->flight.begin() + (long)k);
         }
-        if (s->flight.empty() && s->queue.empty() && b->dropped.empty()) s->idle_cv.notify_all();
+        if (s->flight.empty() && s->queue.empty() && s->staging.empty() && b->dropped.empty())
+            s->idle_cv.notify_all();
     }
 }
 
@@ -189,11 +224,16 @@ int slosh_server_create(const slosh_server_config *cfg, slosh_server **out) {
     slosh_server *s = new slosh_server();
     s->cfg = *cfg;
     const double budget = (double)cfg->hbm_budget_bytes;
-    s->pool_particles = (uint32_t)std::min<double>(0.7 * budget / POOL_BYTES_PER_PARTICLE, 2147483648.0);
+    // upload buffer for staged records: a quarter of the pool, at most 4 M records
+    const double pool0 = std::min<double>(0.7 * budget / POOL_BYTES_PER_PARTICLE, 2147483648.0);
+    const uint32_t up_records = (uint32_t)std::min<double>(pool0 / 4.0, 4194304.0);
+    s->pool_particles = (uint32_t)((0.7 * budget - (double)up_records * sizeof(slosh_particle)) /
+                                   POOL_BYTES_PER_PARTICLE);
     uint32_t blocks = 1;
     while ((double)blocks * 2.0 * POOL_BYTES_PER_BLOCK <= 0.3 * budget && blocks < (1u << 24)) blocks <<= 1;
     s->pool_blocks = blocks;
-    s->pool_bytes = (uint64_t)s->pool_particles * POOL_BYTES_PER_PARTICLE + (uint64_t)blocks * POOL_BYTES_PER_BLOCK;
+    s->pool_bytes = (uint64_t)s->pool_particles * POOL_BYTES_PER_PARTICLE + (uint64_t)blocks * POOL_BYTES_PER_BLOCK +
+                    (uint64_t)up_records * sizeof(slosh_particle);
     slosh_batch_config bc{};
     bc.dim = cfg->dim;
     bc.max_particles = s->pool_particles;
@@ -201,8 +241,16 @@ int slosh_server_create(const slosh_server_config *cfg, slosh_server **out) {
     bc.max_scenes = cfg->max_scenes;
     bc.max_bodies = std::max<uint32_t>(cfg->max_bodies, 16u);
     bc.device = cfg->device;
-    const int st = slosh_batch_create(&bc, &s->batch);
+    int st = slosh_batch_create(&bc, &s->batch);
+    if (st == SLOSH_OK) st = batch_reserve_upload(s->batch, up_records);
+    if (st == SLOSH_OK) {
+        // downloads of completed scenes go through the batch's record staging
+        slosh_ctx *c = &s->batch->c;
+        st = dalloc(c, &c->staging, up_records);
+        if (st == SLOSH_OK) s->batch->staging_cap = up_records;
+    }
     if (st != SLOSH_OK) {
+        if (s->batch) slosh_batch_destroy(s->batch);
         delete s;
         return st;
     }
@@ -231,7 +279,7 @@ int slosh_server_submit(slosh_server *s, const slosh_request *req, uint64_t *id)
     q.blocks = request_blocks(req->n);
     q.bytes = (uint64_t)req->n * POOL_BYTES_PER_PARTICLE + (uint64_t)q.blocks * POOL_BYTES_PER_BLOCK;
     std::lock_guard<std::mutex> lk(s->mu);
-    if (req->n > s->pool_particles || q.blocks > s->pool_blocks) {
+    if (req->n > s->pool_particles || q.blocks > s->pool_blocks || req->n > s->batch->up_cap) {
         s->last_error = "request larger than the budget's particle pool or block capacity";
         return SLOSH_E_CAPACITY;
     }
@@ -260,7 +308,7 @@ int slosh_server_wait_idle(slosh_server *s, double timeout_s) {
     if (!s) return SLOSH_E_INVALID;
     std::unique_lock<std::mutex> lk(s->mu);
     const bool ok = s->idle_cv.wait_for(lk, std::chrono::duration<double>(timeout_s),
-                                        [&] { return s->queue.empty() && s->flight.empty(); });
+                                        [&] { return s->queue.empty() && s->flight.empty() && s->staging.empty(); });
     if (!ok) {
         s->last_error = "timeout waiting for the queue to drain";
         return SLOSH_E_STATE;
@@ -280,7 +328,7 @@ int slosh_server_get_stats(slosh_server *s, slosh_server_stats *out) {
     out->pool_bytes = s->pool_bytes;
     out->busy_s = s->busy;
     out->now_s = s->now();
-    out->in_flight = (uint32_t)s->flight.size();
+    out->in_flight = (uint32_t)(s->flight.size() + s->staging.size());
     out->queued = (uint32_t)s->queue.size();
     out->max_in_flight_seen = s->max_seen;
     return SLOSH_OK;
