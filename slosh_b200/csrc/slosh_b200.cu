@@ -47,10 +47,9 @@ struct slosh_ctx {
              *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_fill = nullptr, *tmp_key = nullptr,
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
              *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr, *bnbh_rev = nullptr;
-    // P2G variant for A/B measurements (environment SLOSH_P2G at creation):
-    // 0 cell-owner with the fixed-order (bit-reproducible) reduction
-    // (default), 1 "atomic" per-particle shared atomics, 2 "staged"
-    // shared-memory staging, 3 "direct" cell-owner with float atomics.
+    // P2G reduction (environment SLOSH_P2G at creation): 0 fixed-order,
+    // bit-reproducible (default); 3 "direct": the same cell-owner kernel with
+    // shared-memory and global float atomics, kept for A/B comparison.
     int p2g_variant = 0;
     uint32_t *pslot = nullptr, *perm = nullptr;
     unsigned long long *skey = nullptr;
@@ -265,11 +264,7 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
 template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
     PROF_BEGIN(9);
     const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
-    if (c->p2g_variant == 1)
-        k_p2g_atomic<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 12), 128, 0, st>>>(s);
-    else if (c->p2g_variant == 2)
-        k_p2g_staged<D><<<g, P2G_THREADS, 0, st>>>(s);
-    else if (c->p2g_variant == 3)
+    if (c->p2g_variant == 3)
         k_p2g<D, false><<<g, P2G_THREADS, 0, st>>>(s);
     else
         k_p2g<D, true><<<g, P2G_THREADS, 0, st>>>(s);
@@ -472,9 +467,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     cudaMemset(c->pb[1].damping, 0, N * 4);
     cudaMemset(c->slot_counts, 0, (size_t)hcap * CELLS * 4);
     if (const char *variant = std::getenv("SLOSH_P2G")) {
-        if (std::strcmp(variant, "atomic") == 0) c->p2g_variant = 1;
-        else if (std::strcmp(variant, "staged") == 0) c->p2g_variant = 2;
-        else if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;
+        if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;
     }
     if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     c->params.gravity[1] = -9.81f;

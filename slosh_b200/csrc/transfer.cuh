@@ -39,317 +39,7 @@ __device__ __forceinline__ bool tile_node_owner(const DevScene &s, uint32_t r, i
     return rank != NONE;
 }
 
-// Particle-to-grid, shared-memory-atomic variant (kept for comparison).  One
-// CTA per active block with primaries; each thread scatters whole particles
-// into a shared (block + 2)^D tile of node momentum/mass with shared-memory
-// float atomics, then the tile is added to the global nodes of the block and
-// its +1 neighbours with 16-byte vector atomics.
-template <int D, int NT> __global__ void __launch_bounds__(NT) k_p2g_atomic(DevScene s) {
-    constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
-    __shared__ float tile[4][TILE];
-    const uint32_t nb = s.ctr->n_blocks;
-    const float h = s.h;
-    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
-        const uint32_t np = s.bnp[r];
-        if (np == 0) continue;
-        for (int t = threadIdx.x; t < 4 * TILE; t += NT) (&tile[0][0])[t] = 0.f;
-        __syncthreads();
-        int bv[D];
-        unpack_key<D>(s.bkey[r], bv);
-        const uint32_t first = s.bfirst[r];
-        for (uint32_t e = threadIdx.x; e < np; e += NT) {
-            const uint32_t i = s.perm[first + e];
-            const float4 p = s.pm[i];
-            const float x[3] = {p.x, p.y, p.z};
-            const float m = p.w;
-            float d0[D], w[D][3];
-            int a[D];
-            bool in_block = true;
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                const float assoc = rintf(div_h(x[k], h, s.inv_h, s.h_pow2)) - 1.0f;
-                a[k] = (int)assoc - bv[k] * BW;
-                in_block = in_block && a[k] >= 0 && a[k] < BW;
-                d0[k] = assoc * h - x[k];
-                bspline_weights(div_h(-d0[k], h, s.inv_h, s.h_pow2), w[k]);
-            }
-            if (!in_block) {  // packed-key aliasing far outside the key range
-                atomicOr(s.err, ERR_KEY_RANGE);
-                continue;
-            }
-            float q[D], Cm[D][D];
-#pragma unroll
-            for (int j = 0; j < D; ++j) {
-                q[j] = s.vel[j * s.n + i] * m;
-                if (s.force_pending) q[j] += s.fdt[j * s.n + i];
-#pragma unroll
-                for (int k = 0; k < D; ++k) Cm[j][k] = s.C[(j * D + k) * s.n + i];
-            }
-            float base[D], hc[D][D];  // hc[k] = h * column k of C
-#pragma unroll
-            for (int j = 0; j < D; ++j) {
-                float acc = q[j];
-#pragma unroll
-                for (int k = 0; k < D; ++k) {
-                    acc += Cm[j][k] * d0[k];
-                    hc[k][j] = h * Cm[j][k];
-                }
-                base[j] = acc;
-            }
-            if constexpr (D == 3) {
-#pragma unroll
-                for (int sz = 0; sz < 3; ++sz) {
-                    float mz[3];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) mz[j] = base[j] + (float)sz * hc[2][j];
-#pragma unroll
-                    for (int sy = 0; sy < 3; ++sy) {
-                        float my[3];
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) my[j] = mz[j] + (float)sy * hc[1][j];
-                        const float wyz = w[1][sy] * w[2][sz];
-#pragma unroll
-                        for (int sx = 0; sx < 3; ++sx) {
-                            const float wt = w[0][sx] * wyz;
-                            const int idx = (a[0] + sx) + TW * ((a[1] + sy) + TW * (a[2] + sz));
-                            atomicAdd(&tile[0][idx], wt * (my[0] + (float)sx * hc[0][0]));
-                            atomicAdd(&tile[1][idx], wt * (my[1] + (float)sx * hc[0][1]));
-                            atomicAdd(&tile[2][idx], wt * (my[2] + (float)sx * hc[0][2]));
-                            atomicAdd(&tile[3][idx], wt * m);
-                        }
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int sy = 0; sy < 3; ++sy) {
-                    float my[2];
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) my[j] = base[j] + (float)sy * hc[1][j];
-#pragma unroll
-                    for (int sx = 0; sx < 3; ++sx) {
-                        const float wt = w[0][sx] * w[1][sy];
-                        const int idx = (a[0] + sx) + TW * (a[1] + sy);
-                        atomicAdd(&tile[0][idx], wt * (my[0] + (float)sx * hc[0][0]));
-                        atomicAdd(&tile[1][idx], wt * (my[1] + (float)sx * hc[0][1]));
-                        atomicAdd(&tile[3][idx], wt * m);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        for (int t = threadIdx.x; t < TILE; t += NT) {
-            const float4 val = make_float4(tile[0][t], tile[1][t], tile[2][t], tile[3][t]);
-            if (val.x == 0.f && val.y == 0.f && val.z == 0.f && val.w == 0.f) continue;
-            uint32_t rank, local;
-            if (!tile_node_owner<D>(s, r, t, rank, local)) continue;
-            atomicAdd(&s.nodes[(size_t)rank * 64u + local], val);
-        }
-        __syncthreads();
-    }
-}
-
-// Particle-to-grid without atomics inside the block.
-//
-// Node momentum/mass match slosh's p2g_scatter_style
-// (shaders/slosh/solver/p2g_scatter_style.slang:84-154):
-//   acc_i = sum_p w_ip [ C_p (x_i - x_p) + m_p v_p + f_p dt ,  m_p ],
-// with w_ip the product of the quadratic B-spline weights per axis.
-//
-// One CTA of 192 threads per active block with primaries.  The block's
-// particles arrive in canonical (cell, id) order, so every cell is a
-// contiguous range:
-//  1. stage: each thread loads a particle, computes its three weights per
-//     axis, its momentum at the base node (q + C d0) and h C, and stores
-//     them in shared memory (six float4 per particle in 3D);
-//  2. accumulate: thread (cell c, slab) owns the particles of cell c and the
-//     stencil offsets of one slab (sz in 3D, sy in 2D): 9 nodes in 3D, 3 in
-//     2D, accumulated in registers across the cell's particles and chunks,
-//     sharing the weight and momentum sub-expressions between the offsets;
-//     the sums land in a shared (cell, offset) array with plain stores (one
-//     owner per entry);
-//  3. reduce: each tile node sums its (cell, offset) entries in a fixed
-//     order, and the (block + 2)^D tile is added to the global nodes of the
-//     block and its +1 neighbours with 16-byte vector atomics.
-template <int D> struct P2GLayout;
-template <> struct P2GLayout<3> {
-    // stencil offsets, float4 per staged particle, chunk
-    static constexpr int NOFF = 27, F4 = 6, CH = 128;
-};
-template <> struct P2GLayout<2> {
-    static constexpr int NOFF = 9, F4 = 4, CH = 256;
-};
-
 constexpr int P2G_THREADS = 192;  // 64 cells x 3 slabs
-
-template <int D> __global__ void __launch_bounds__(P2G_THREADS) k_p2g_staged(DevScene s) {
-    constexpr int NT = P2G_THREADS;
-    constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
-    constexpr int NOFF = P2GLayout<D>::NOFF, F4 = P2GLayout<D>::F4;
-    constexpr int CH = P2GLayout<D>::CH;  // particles staged per chunk
-    __shared__ float4 pd[CH * F4];
-    __shared__ float4 stage[64 * NOFF];
-    __shared__ uint32_t cstart[65];
-    const uint32_t nb = s.ctr->n_blocks;
-    const float h = s.h, inv_h = 1.0f / s.h;
-    // thread -> (cell, slab offset along the slowest axis)
-    const int mycell = (int)(threadIdx.x & 63u), myslab = (int)(threadIdx.x >> 6);
-    const float fsl = (float)myslab;
-    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
-        const uint32_t np = s.bnp[r];
-        if (np == 0) continue;
-        const uint32_t first = s.bfirst[r];
-        if (first + np > s.n) {  // only after an earlier overflow left stale counts
-            if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
-            continue;
-        }
-        int bv[D];
-        unpack_key<D>(s.bkey[r], bv);
-        for (int c = threadIdx.x; c < 64; c += NT) cstart[c] = s.bcell[(size_t)r * CELLS + c];
-        if (threadIdx.x == 0) cstart[64] = np;
-        __syncthreads();
-        const uint32_t clo = cstart[mycell], chi = cstart[mycell + 1];
-        constexpr int NACC = NOFF / 3;  // offsets owned by one thread
-        float4 acc[NACC];
-#pragma unroll
-        for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (uint32_t base = 0; base < np; base += CH) {
-            const uint32_t cnt = min((uint32_t)CH, np - base);
-            // ---- 1. stage ----
-            for (uint32_t e = threadIdx.x; e < cnt; e += NT) {
-                const uint32_t i = s.perm[first + base + e];
-                const float4 p = s.pm[i];
-                const float x[3] = {p.x, p.y, p.z};
-                float m = p.w;
-                float d0[D], w[D][3];
-                bool in_block = true;
-#pragma unroll
-                for (int k = 0; k < D; ++k) {
-                    const float assoc = rintf(div_h(x[k], h, s.inv_h, s.h_pow2)) - 1.0f;
-                    const int a = (int)assoc - bv[k] * BW;
-                    in_block = in_block && a >= 0 && a < BW;
-                    d0[k] = assoc * h - x[k];
-                    bspline_weights(-d0[k] * inv_h, w[k]);
-                }
-                float q[D], Cm[D][D];
-#pragma unroll
-                for (int j = 0; j < D; ++j) {
-                    q[j] = s.vel[j * s.n + i] * m;
-                    if (s.force_pending) q[j] += s.fdt[j * s.n + i];
-#pragma unroll
-                    for (int k = 0; k < D; ++k) Cm[j][k] = s.C[(j * D + k) * s.n + i];
-                }
-                if (!in_block) {  // packed-key aliasing far outside the key range: contributes nothing
-                    atomicOr(s.err, ERR_KEY_RANGE);
-                    m = 0.f;
-#pragma unroll
-                    for (int k = 0; k < D; ++k) w[k][0] = w[k][1] = w[k][2] = 0.f;
-                }
-                float bm[D];
-#pragma unroll
-                for (int j = 0; j < D; ++j) {
-                    float acc = q[j];
-#pragma unroll
-                    for (int k = 0; k < D; ++k) acc += Cm[j][k] * d0[k];
-                    bm[j] = acc;
-                }
-                float4 *o = &pd[e * F4];
-                if constexpr (D == 3) {
-                    o[0] = make_float4(w[0][0], w[0][1], w[0][2], m);
-                    o[1] = make_float4(w[1][0], w[1][1], w[1][2], bm[0]);
-                    o[2] = make_float4(w[2][0], w[2][1], w[2][2], bm[1]);
-                    o[3] = make_float4(h * Cm[0][0], h * Cm[1][0], h * Cm[2][0], bm[2]);
-                    o[4] = make_float4(h * Cm[0][1], h * Cm[1][1], h * Cm[2][1], 0.f);
-                    o[5] = make_float4(h * Cm[0][2], h * Cm[1][2], h * Cm[2][2], 0.f);
-                } else {
-                    o[0] = make_float4(w[0][0], w[0][1], w[0][2], m);
-                    o[1] = make_float4(w[1][0], w[1][1], w[1][2], 0.f);
-                    o[2] = make_float4(bm[0], bm[1], h * Cm[0][0], h * Cm[1][0]);
-                    o[3] = make_float4(h * Cm[0][1], h * Cm[1][1], 0.f, 0.f);
-                }
-            }
-            __syncthreads();
-            // ---- 2. accumulate: this thread's cell, its slab of offsets ----
-            const uint32_t lo = max(clo, base), hi = min(chi, base + cnt);
-            for (uint32_t j = lo; j < hi; ++j) {
-                const float4 *pp = &pd[(j - base) * F4];
-                const float4 q0 = pp[0], q1 = pp[1];
-                if constexpr (D == 3) {
-                    const float4 q2 = pp[2], q3 = pp[3], q4 = pp[4], q5 = pp[5];
-                    const float wz = myslab == 0 ? q2.x : (myslab == 1 ? q2.y : q2.z);
-                    const float mz0 = q1.w + fsl * q5.x, mz1 = q2.w + fsl * q5.y, mz2 = q3.w + fsl * q5.z;
-                    const float wy[3] = {q1.x, q1.y, q1.z};
-                    const float wx[3] = {q0.x, q0.y, q0.z};
-#pragma unroll
-                    for (int sy = 0; sy < 3; ++sy) {
-                        const float wyz = wy[sy] * wz;
-                        const float my0 = mz0 + (float)sy * q4.x, my1 = mz1 + (float)sy * q4.y,
-                                    my2 = mz2 + (float)sy * q4.z;
-#pragma unroll
-                        for (int sx = 0; sx < 3; ++sx) {
-                            const float wt = wx[sx] * wyz;
-                            float4 &a = acc[sx + 3 * sy];
-                            a.x += wt * (my0 + (float)sx * q3.x);
-                            a.y += wt * (my1 + (float)sx * q3.y);
-                            a.z += wt * (my2 + (float)sx * q3.z);
-                            a.w += wt * q0.w;
-                        }
-                    }
-                } else {
-                    const float4 q2 = pp[2], q3 = pp[3];
-                    const float wy = myslab == 0 ? q1.x : (myslab == 1 ? q1.y : q1.z);
-                    const float my0 = q2.x + fsl * q3.x, my1 = q2.y + fsl * q3.y;
-                    const float wx[3] = {q0.x, q0.y, q0.z};
-#pragma unroll
-                    for (int sx = 0; sx < 3; ++sx) {
-                        const float wt = wx[sx] * wy;
-                        float4 &a = acc[sx];
-                        a.x += wt * (my0 + (float)sx * q2.z);
-                        a.y += wt * (my1 + (float)sx * q2.w);
-                        a.w += wt * q0.w;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        // offsets of this thread: sx + 3 sy + 9 slab (3D), sx + 3 slab (2D)
-#pragma unroll
-        for (int k = 0; k < NACC; ++k) stage[mycell * NOFF + NACC * myslab + k] = acc[k];
-        __syncthreads();
-        // ---- 3. reduce per tile node, then add to the global nodes ----
-        for (int t = threadIdx.x; t < TILE; t += NT) {
-            int nc[D];
-            nc[0] = t % TW;
-            if constexpr (D == 3) {
-                nc[1] = (t / TW) % TW;
-                nc[2] = t / (TW * TW);
-            } else {
-                nc[1] = t / TW;
-            }
-            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int so = 0; so < NOFF; ++so) {
-                const int sx = so % 3, sy = (so / 3) % 3, sz = so / 9;
-                const int cx = nc[0] - sx, cy = nc[1] - sy;
-                int cz = 0;
-                if constexpr (D == 3) cz = nc[2] - sz;
-                bool ok = cx >= 0 && cx < BW && cy >= 0 && cy < BW;
-                if constexpr (D == 3) ok = ok && cz >= 0 && cz < BW;
-                if (!ok) continue;
-                const int cell = (D == 3) ? cx + 4 * cy + 16 * cz : cx + 8 * cy;
-                const float4 v = stage[cell * NOFF + so];
-                sum.x += v.x;
-                sum.y += v.y;
-                sum.z += v.z;
-                sum.w += v.w;
-            }
-            if (sum.x == 0.f && sum.y == 0.f && sum.z == 0.f && sum.w == 0.f) continue;
-            uint32_t rank, local;
-            if (!tile_node_owner<D>(s, r, t, rank, local)) continue;
-            atomicAdd(&s.nodes[(size_t)rank * 64u + local], sum);
-        }
-        __syncthreads();
-    }
-}
 
 // Particle-to-grid, direct cell-owner kernel.
 //

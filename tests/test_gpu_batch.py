@@ -163,3 +163,31 @@ def test_batch_timestep_bound_per_scene(cuda_lib):
         assert b.timestep_bound(sl) == data.timestep_bound()
         data.close()
     b.close()
+
+
+def test_batch_2d_alone_vs_mix_and_context(cuda_lib):
+    """2D batches: a dam break alone in a batch equals the single-scene
+    context, and stays bit-identical next to other 2D scenes of different
+    cell widths."""
+    a = scenes.dam_break_2d(h=1 / 64, substeps=10)
+    b_sc = scenes.dam_break_2d(h=1 / 128, substeps=10)
+    data = scenes.build_mpm_data(a)
+    MpmPipeline().launch_step(data, 12)
+    single = data.download_particles()
+    data.close()
+    alone = MpmBatch(2, max_particles=1 << 17, grid_capacity=1 << 12, max_scenes=8, max_bodies=64)
+    s0 = alone.add(a)
+    alone.step(12)
+    ref = alone.download_particles(s0)
+    alone.close()
+    for k, v in fields(single).items():
+        close(f"2D batch of one vs context {k}", ref[k], v, 1e-7, 1e-6)
+    mix = MpmBatch(2, max_particles=1 << 17, grid_capacity=1 << 12, max_scenes=8, max_bodies=64)
+    mix.add(b_sc)
+    s1 = mix.add(a)
+    mix.step(5)
+    mix.add(b_sc)
+    mix.step(7)
+    got = mix.download_particles(s1)
+    mix.close()
+    assert got.tobytes() == ref.tobytes()
