@@ -615,15 +615,26 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
 
 // Per particle: claim its slot in the block's cell range (the primary part
 // of finalize_particles_sort, sort.slang:304-357), warp-aggregated.
+//
+// Each warp takes a contiguous chunk of storage and walks it in order; a
+// warp's next claim waits for the previous one's result, so a cell's
+// particles handled by one warp land in storage order, which is already the
+// canonical order for particles that stayed in their cell.  Only cells split
+// between two chunks (and cells entered from another cell) need k_canon's
+// fix-up.
 template <bool B = false> __global__ void k_scatter(DevScene s) {
     const uint32_t lane = lane_id();
-    const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t n = n_particles<B>(s);
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t chunk = (((n + warps - 1) / warps) + 31u) & ~31u;
+    const uint32_t begin = wid * chunk;
+    const uint32_t end = min(n, begin + chunk);
+    for (uint32_t base = begin; base < end; base += 32) {
         const uint32_t i = base + lane;
-        const bool valid = i < n;
+        const bool valid = i < end;
         const unsigned mask = __ballot_sync(FULL_MASK, valid);
-        if (!valid) continue;
+        if (!valid) break;
         const uint32_t bin = s.pslot[i];
         const unsigned peers = __match_any_sync(mask, bin);
         const int leader = __ffs(peers) - 1;
