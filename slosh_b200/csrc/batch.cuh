@@ -232,10 +232,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     int st = SLOSH_OK;
     for (int k = 0; k < 2; ++k) {
         slosh_ctx::Storage &S = c->pb[k];
-        if ((st = dalloc(c, &S.pm, N)) || (st = dalloc(c, &S.vel, N * D)) || (st = dalloc(c, &S.C, N * D * D)) ||
-            (st = dalloc(c, &S.F, N * D * D)) || (st = dalloc(c, &S.V0, N)) || (st = dalloc(c, &S.flags, N)) ||
-            (st = dalloc(c, &S.damping, N)) || (st = dalloc(c, &S.plastic, N * 3)) || (st = dalloc(c, &S.oid, N)))
-            return fail_create(st);
+        if ((st = alloc_storage(c, S, N, D))) return fail_create(st);
     }
     if ((st = dalloc(c, &c->materials, MAX_MATERIALS)) || (st = dalloc(c, &c->mat_hkeys, MAT_HASH)) ||
         (st = dalloc(c, &c->mat_dense, MAT_HASH)) || (st = dalloc(c, &b->hkeys64[0], hcap)) ||
@@ -269,8 +266,6 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     cudaMemset(c->err, 0, 4);
     cudaMemset(c->small, 0, 16);
     cudaMemset(c->mat_hkeys, 0xff, MAT_HASH * 4);
-    cudaMemset(c->pb[0].damping, 0, N * 4);
-    cudaMemset(c->pb[1].damping, 0, N * 4);
     cudaMemset(b->scene_nblk, 0, b->max_scenes * 4);
     cudaMemset(b->scenes_dev, 0, b->max_scenes * sizeof(SceneRec));
     cudaMemset(b->n_dev, 0, 4);

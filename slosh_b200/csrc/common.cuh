@@ -136,6 +136,10 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
@@ -147,6 +151,41 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+// D x D matrices of the particle state (C, F) are stored as MQ<D> float4
+// planes holding the row-major elements 0-3 (and 4-7); in 3D element 8 rides
+// in the spare fourth lane of another per-particle vector (C22 with the
+// velocity, F22 with the flags), so every particle access is a 16-byte one.
+template <int D> struct MQ;
+template <> struct MQ<3> {
+    static constexpr int Q = 2;
+};
+template <> struct MQ<2> {
+    static constexpr int Q = 1;
+};
+
+template <int D>
+__device__ __forceinline__ void mat_from(const float4 *q, float e8, float (&M)[D][D]) {
+    if constexpr (D == 3) {
+        M[0][0] = q[0].x, M[0][1] = q[0].y, M[0][2] = q[0].z, M[1][0] = q[0].w;
+        M[1][1] = q[1].x, M[1][2] = q[1].y, M[2][0] = q[1].z, M[2][1] = q[1].w;
+        M[2][2] = e8;
+    } else {
+        M[0][0] = q[0].x, M[0][1] = q[0].y, M[1][0] = q[0].z, M[1][1] = q[0].w;
+    }
+}
+
+// Inverse of mat_from: fills the MQ<D> vectors and returns element 8 (0 in 2D).
+template <int D> __device__ __forceinline__ float mat_split(const float (&M)[D][D], float4 *q) {
+    if constexpr (D == 3) {
+        q[0] = make_float4(M[0][0], M[0][1], M[0][2], M[1][0]);
+        q[1] = make_float4(M[1][1], M[1][2], M[2][0], M[2][1]);
+        return M[2][2];
+    } else {
+        q[0] = make_float4(M[0][0], M[0][1], M[1][0], M[1][1]);
+        return 0.f;
+    }
 }
 
 // Material record: GpuParticleModel without the per-particle plastic state.

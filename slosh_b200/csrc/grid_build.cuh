@@ -185,7 +185,7 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
         uint32_t pow2 = s.h_pow2, sc = 0;
         bool live = true;
         if constexpr (B) {
-            sc = scene_of(s.flags[i]);
+            sc = scene_of(s.fo[i].x);
             const SceneRec &rec = s.scenes[sc];
             h = rec.h;
             inv_h = rec.inv_h;

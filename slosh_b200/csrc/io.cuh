@@ -113,30 +113,38 @@ __global__ void k_ingest(DevScene s, IoBuffers io, uint32_t base, uint32_t count
             if (!same) atomicOr(s.err, ERR_MATERIAL_HASH);
         }
         s.pm[i] = make_float4(p.position[0], p.position[1], D == 3 ? p.position[2] : 0.f, p.mass);
-        for (int k = 0; k < D; ++k) {
-            s.vel[k * n + i] = p.velocity[k];
-            if constexpr (!B) {
+        if constexpr (!B) {
+            for (int k = 0; k < D; ++k) {
                 s.fdt[k * n + i] = p.force_dt[k];
                 if (p.force_dt[k] != 0.f) sflags |= SCENE_FORCE;
             }
         }
+        float Fm[D][D], Cm[D][D];
         for (int r = 0; r < D; ++r)
             for (int c = 0; c < D; ++c) {
-                s.F[(r * D + c) * n + i] = p.def_grad[c * 3 + r];
-                s.C[(r * D + c) * n + i] = p.affine[c * 3 + r];
+                Fm[r][c] = p.def_grad[c * 3 + r];
+                Cm[r][c] = p.affine[c * 3 + r];
             }
-        s.V0[i] = p.init_volume;
-        s.damping[i] = p.damping;
-        s.oid[i] = oid_base + i0;
+        float4 fv[MQ<D>::Q], cv[MQ<D>::Q];
+        const float f22 = mat_split<D>(Fm, fv), c22 = mat_split<D>(Cm, cv);
+#pragma unroll
+        for (int q = 0; q < MQ<D>::Q; ++q) {
+            s.fq[q * n + i] = fv[q];
+            s.cq[q * n + i] = cv[q];
+        }
+        s.vv[i] = make_float4(p.velocity[0], p.velocity[1], D == 3 ? p.velocity[2] : 0.f, c22);
         if (p.damping != 0.f) sflags |= SCENE_DAMPING;
         if constexpr (!B) {
             io.r0[oid_base + i0] = p.init_radius;
             io.phase[oid_base + i0] = p.phase;
         }
-        s.flags[i] = (dense & FLAG_MAT_MASK) | (p.enabled ? FLAG_ENABLED : 0u) | (p.fixed ? FLAG_FIXED : 0u) |
-                     (scene << FLAG_SCENE_SHIFT);
+        const uint32_t flags = (dense & FLAG_MAT_MASK) | (p.enabled ? FLAG_ENABLED : 0u) |
+                               (p.fixed ? FLAG_FIXED : 0u) | (scene << FLAG_SCENE_SHIFT);
+        s.fo[i] = make_uint4(flags, oid_base + i0, __float_as_uint(p.init_volume), __float_as_uint(f22));
+        s.oid[i] = oid_base + i0;
         const bool sand = p.model.tag == SLOSH_MODEL_SAND_LINEAR || p.model.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN;
-        for (int k = 0; k < 3; ++k) s.plastic[k * n + i] = sand ? p.model.data[k] : 0.f;
+        s.ps[i] = sand ? make_float4(p.model.data[0], p.model.data[1], p.model.data[2], p.damping)
+                       : make_float4(0.f, 0.f, 0.f, p.damping);
         if (sand) sflags |= SCENE_SAND;
     }
     sflags = __reduce_or_sync(FULL_MASK, sflags);
@@ -151,42 +159,56 @@ template <int D, bool B = false> __global__ void k_egest(DevScene s, IoBuffers i
     const size_t n = s.n;
     const uint32_t count = n_particles<B>(s);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const uint4 fo = s.fo[i];
         if constexpr (B)
-            if (scene_of(s.flags[i]) != scene) continue;
-        const uint32_t orig = s.oid[i];
+            if (scene_of(fo.x) != scene) continue;
+        const uint32_t orig = fo.y;
         slosh_particle p;
-        const float4 pm = s.pm[i];
+        const float4 pm = s.pm[i], vv = s.vv[i], ps = s.ps[i];
         p.position[0] = pm.x;
         p.position[1] = pm.y;
         p.position[2] = D == 3 ? pm.z : 0.f;
-        for (int k = 0; k < 3; ++k) {
-            p.velocity[k] = k < D ? s.vel[k * n + i] : 0.f;
-            p.force_dt[k] = (k < D && s.force_pending) ? s.fdt[k * n + i] : 0.f;
-        }
+        p.velocity[0] = vv.x;
+        p.velocity[1] = vv.y;
+        p.velocity[2] = D == 3 ? vv.z : 0.f;
+        for (int k = 0; k < 3; ++k) p.force_dt[k] = (k < D && s.force_pending) ? s.fdt[k * n + i] : 0.f;
         for (int q = 0; q < 9; ++q) {
             p.def_grad[q] = 0.f;
             p.affine[q] = 0.f;
         }
+        float Fm[D][D], Cm[D][D];
+        {
+            float4 fv[MQ<D>::Q], cv[MQ<D>::Q];
+#pragma unroll
+            for (int q = 0; q < MQ<D>::Q; ++q) {
+                fv[q] = s.fq[q * n + i];
+                cv[q] = s.cq[q * n + i];
+            }
+            mat_from<D>(fv, __uint_as_float(fo.w), Fm);
+            mat_from<D>(cv, vv.w, Cm);
+        }
         for (int r = 0; r < D; ++r)
             for (int c = 0; c < D; ++c) {
-                p.def_grad[c * 3 + r] = s.F[(r * D + c) * n + i];
-                p.affine[c * 3 + r] = s.C[(r * D + c) * n + i];
+                p.def_grad[c * 3 + r] = Fm[r][c];
+                p.affine[c * 3 + r] = Cm[r][c];
             }
-        if (D == 2) p.def_grad[8] = 0.f;
         p.vel_grad_det = 0.f;
-        p.init_volume = s.V0[i];
+        p.init_volume = __uint_as_float(fo.z);
         p.init_radius = B ? 0.f : io.r0[orig];
         p.mass = pm.w;
-        p.damping = s.has_damping ? s.damping[i] : 0.f;
+        p.damping = s.has_damping ? ps.w : 0.f;
         p.phase = B ? 0.f : io.phase[orig];
-        const uint32_t fl = s.flags[i];
+        const uint32_t fl = fo.x;
         p.enabled = (fl & FLAG_ENABLED) ? 1u : 0u;
         p.fixed = (fl & FLAG_FIXED) ? 1u : 0u;
         const Material &m = s.materials[fl & FLAG_MAT_MASK];
         p.model.tag = m.tag;
         for (int q = 0; q < 12; ++q) p.model.data[q] = m.p[q];
-        if (m.tag == SLOSH_MODEL_SAND_LINEAR || m.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN)
-            for (int q = 0; q < 3; ++q) p.model.data[q] = s.plastic[q * n + i];
+        if (m.tag == SLOSH_MODEL_SAND_LINEAR || m.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN) {
+            p.model.data[0] = ps.x;
+            p.model.data[1] = ps.y;
+            p.model.data[2] = ps.z;
+        }
         io.out[orig] = p;
     }
 }
@@ -204,22 +226,19 @@ __global__ void k_remove(DevScene s, IoBuffers io, uint32_t start, uint32_t end,
     const size_t n = s.n;
     const uint32_t removed = end - start;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.count; i += stride) {
-        const uint32_t o = s.oid[i];
+        const uint4 fo = s.fo[i];
+        const uint32_t o = fo.y;
         if (o >= start && o < end) continue;
         const uint32_t j = o >= end ? o - removed : o;
         s.out_pm[j] = s.pm[i];
+        s.out_vv[j] = s.vv[i];
 #pragma unroll
-        for (int k = 0; k < D; ++k) s.out_vel[k * n + j] = s.vel[k * n + i];
-#pragma unroll
-        for (int q = 0; q < D * D; ++q) {
-            s.out_C[q * n + j] = s.C[q * n + i];
-            s.out_F[q * n + j] = s.F[q * n + i];
+        for (int q = 0; q < MQ<D>::Q; ++q) {
+            s.out_cq[q * n + j] = s.cq[q * n + i];
+            s.out_fq[q * n + j] = s.fq[q * n + i];
         }
-        s.out_V0[j] = s.V0[i];
-        s.out_flags[j] = s.flags[i];
-        s.out_damping[j] = s.damping[i];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) s.out_plastic[q * n + j] = s.plastic[q * n + i];
+        s.out_ps[j] = s.ps[i];
+        s.out_fo[j] = make_uint4(fo.x, j, fo.z, fo.w);
         s.out_oid[j] = j;
         tmp[j] = io.r0[o];
         tmp[n + j] = io.phase[o];
@@ -245,17 +264,18 @@ template <bool B = false> __global__ void k_positions(DevScene s, float4 *out, u
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t count = n_particles<B>(s);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const uint2 fo = make_uint2(s.fo[i].x, s.fo[i].y);
         if constexpr (B)
-            if (scene_of(s.flags[i]) != scene) continue;
+            if (scene_of(fo.x) != scene) continue;
         const float4 p = s.pm[i];
-        out[s.oid[i]] = make_float4(p.x, p.y, p.z, 0.f);
+        out[fo.y] = make_float4(p.x, p.y, p.z, 0.f);
     }
 }
 
 // Debug: the hot path's primary permutation in original ids.
 __global__ void k_perm_to_oid(DevScene s, uint32_t *out) {
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < s.count; e += stride) out[e] = s.oid[s.perm[e]];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < s.count; e += stride) out[e] = s.fo[s.perm[e]].y;
 }
 
 // ---------------------------------------------------------------------------
@@ -366,11 +386,11 @@ template <int D> __global__ void k_dbg_scatter(DevScene s, DebugBuffers d) {
 // original id), extras by original id.
 template <int D>
 __device__ __forceinline__ uint64_t dbg_order_key(const DevScene &s, uint32_t j, uint32_t b) {
-    if (b >= (uint32_t)Geo<D>::NPB) return s.oid[j];
+    if (b >= (uint32_t)Geo<D>::NPB) return s.fo[j].y;
     const float4 p = s.pm[j];
     const float x[3] = {p.x, p.y, p.z};
     const CellLoc<D> c = locate<D>(x, s.h, s.inv_h, s.h_pow2);
-    return ((uint64_t)cell_index<D>(c.local) << 32) | s.oid[j];
+    return ((uint64_t)cell_index<D>(c.local) << 32) | s.fo[j].y;
 }
 
 // One thread per (block, bucket) segment: rank each entry by its canonical
@@ -390,7 +410,7 @@ template <int D> __global__ void k_dbg_canon(DevScene s, DebugBuffers d) {
             const uint64_t key = dbg_order_key<D>(s, id, b);
             uint32_t rank = 0;
             for (uint32_t j = lo; j < hi; ++j) rank += (dbg_order_key<D>(s, d.sorted[j], b) < key) ? 1u : 0u;
-            d.sorted2[lo + rank] = s.oid[id];
+            d.sorted2[lo + rank] = s.fo[id].y;
         }
     }
 }

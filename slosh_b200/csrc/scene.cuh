@@ -19,17 +19,16 @@ struct DevScene {
     float dt;
     float gravity[3];
     float4 *pm;            // (x, y, z, mass); 2D: (x, y, 0, mass)
-    float *vel;            // D planes of n floats
-    float *C;              // D*D planes: APIC affine matrix, row-major math
-    float *F;              // D*D planes: deformation gradient
-    float *V0;             // initial volume
-    uint32_t *flags;       // material id | enabled | fixed
-    float *damping;        // read only when has_damping
-    float *plastic;        // 3 planes (det_p, q, log_vol_gain) for sand models
-    uint32_t *oid;         // original (upload) index of each stored particle
-    float4 *out_pm;
-    float *out_vel, *out_C, *out_F, *out_V0, *out_damping, *out_plastic;
-    uint32_t *out_flags, *out_oid;
+    float4 *vv;            // (vx, vy, vz, C22); 2D: (vx, vy, 0, 0)
+    float4 *cq;            // APIC matrix C, row-major elements 0-7 (0-3): MQ<D> float4 planes
+    float4 *fq;            // deformation gradient F, same layout
+    uint4 *fo;             // (flags: material id | enabled | fixed | scene slot, original index,
+                           //  V0 bits, F22 bits (3D))
+    float4 *ps;            // (plastic det, hardening q, log_vol_gain, damping)
+    uint32_t *oid;         // copy of fo.y as its own plane for the grid build's sort keys
+    float4 *out_pm, *out_vv, *out_cq, *out_fq, *out_ps;
+    uint4 *out_fo;
+    uint32_t *out_oid;
     float *fdt;            // D planes of force*dt in upload order, read by P2G while force_pending
     uint32_t has_damping;
     uint32_t has_sand;

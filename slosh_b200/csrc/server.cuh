@@ -4,11 +4,12 @@
 // Included at the end of slosh_b200.cu after batch.cuh.
 //
 // Footprint accounting.  The batch is allocated once from the HBM budget:
-// 70 % as particle pool (264 bytes a particle: two copies of the 128-byte
-// particle state plus the sort key and permutation) and up to 30 % as block
+// 70 % as particle pool (280 bytes a particle: two copies of the 128-byte
+// particle state and of the original-index plane, the sort key, the
+// permutation and the cell slot) and up to 30 % as block
 // capacity (8240 bytes a block: hash slots, per-cell counts and cursors,
 // neighbour ranks, the P2G partial tile, nodes and the collision caches).  A
-// request's footprint is n * 264 + blocks * 8240 with blocks estimated as
+// request's footprint is n * 280 + blocks * 8240 with blocks estimated as
 // 2.5 n / 512 + 64 (8 particles per cell fill 512 per block; the factor
 // covers the +1 neighbour blocks and partly filled blocks).  Admission needs
 // the pool's free particles, the estimated blocks and a free scene slot.
@@ -57,7 +58,7 @@ struct slosh_server {
 
 namespace {
 
-constexpr uint64_t POOL_BYTES_PER_PARTICLE = 264;
+constexpr uint64_t POOL_BYTES_PER_PARTICLE = 280;
 constexpr uint64_t POOL_BYTES_PER_BLOCK = 8240;
 constexpr uint32_t AUTOTUNE_SUBSTEPS = 12;  // 6 launch shapes x (1 warm-up + 1 timed)
 

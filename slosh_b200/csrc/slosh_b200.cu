@@ -32,9 +32,9 @@ struct slosh_ctx {
     // particles: double-buffered storage in canonical order (buffer `parity`
     // holds the state the next substep reads) + upload-order side arrays
     struct Storage {
-        float4 *pm = nullptr;
-        float *vel = nullptr, *C = nullptr, *F = nullptr, *V0 = nullptr, *damping = nullptr, *plastic = nullptr;
-        uint32_t *flags = nullptr, *oid = nullptr;
+        float4 *pm = nullptr, *vv = nullptr, *cq = nullptr, *fq = nullptr, *ps = nullptr;
+        uint4 *fo = nullptr;
+        uint32_t *oid = nullptr;
     } pb[2];
     float *fdt = nullptr, *r0 = nullptr, *phase = nullptr;
     Material *materials = nullptr;
@@ -105,6 +105,18 @@ template <typename T> int dalloc(slosh_ctx *c, T **p, size_t count) {
     return SLOSH_OK;
 }
 
+// One particle storage buffer (128 bytes a particle in 3D).
+int alloc_storage(slosh_ctx *c, slosh_ctx::Storage &S, size_t N, int D) {
+    const size_t Q = D == 3 ? 2 : 1;
+    int st;
+    if ((st = dalloc(c, &S.pm, N)) || (st = dalloc(c, &S.vv, N)) || (st = dalloc(c, &S.cq, N * Q)) ||
+        (st = dalloc(c, &S.fq, N * Q)) || (st = dalloc(c, &S.ps, N)) || (st = dalloc(c, &S.fo, N)) ||
+        (st = dalloc(c, &S.oid, N)))
+        return st;
+    cudaMemset(S.ps, 0, N * sizeof(float4));
+    return SLOSH_OK;
+}
+
 uint32_t next_pow2(uint32_t v) {
     uint32_t p = 1;
     while (p < v) p <<= 1;
@@ -128,22 +140,18 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     for (int k = 0; k < 3; ++k) s.gravity[k] = c->params.gravity[k];
     const slosh_ctx::Storage &A = c->pb[parity & 1u], &B = c->pb[(parity & 1u) ^ 1u];
     s.pm = A.pm;
-    s.vel = A.vel;
-    s.C = A.C;
-    s.F = A.F;
-    s.V0 = A.V0;
-    s.flags = A.flags;
-    s.damping = A.damping;
-    s.plastic = A.plastic;
+    s.vv = A.vv;
+    s.cq = A.cq;
+    s.fq = A.fq;
+    s.ps = A.ps;
+    s.fo = A.fo;
     s.oid = A.oid;
     s.out_pm = B.pm;
-    s.out_vel = B.vel;
-    s.out_C = B.C;
-    s.out_F = B.F;
-    s.out_V0 = B.V0;
-    s.out_flags = B.flags;
-    s.out_damping = B.damping;
-    s.out_plastic = B.plastic;
+    s.out_vv = B.vv;
+    s.out_cq = B.cq;
+    s.out_fq = B.fq;
+    s.out_ps = B.ps;
+    s.out_fo = B.fo;
     s.out_oid = B.oid;
     s.fdt = c->fdt;
     s.has_damping = c->has_damping;
@@ -430,10 +438,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     const uint32_t cap = c->cap, hcap = c->hcap;
     for (int b = 0; b < 2; ++b) {
         slosh_ctx::Storage &S = c->pb[b];
-        if ((st = dalloc(c, &S.pm, N)) || (st = dalloc(c, &S.vel, N * D)) || (st = dalloc(c, &S.C, N * D * D)) ||
-            (st = dalloc(c, &S.F, N * D * D)) || (st = dalloc(c, &S.V0, N)) || (st = dalloc(c, &S.flags, N)) ||
-            (st = dalloc(c, &S.damping, N)) || (st = dalloc(c, &S.plastic, N * 3)) || (st = dalloc(c, &S.oid, N)))
-            return fail_create(st);
+        if ((st = alloc_storage(c, S, N, D))) return fail_create(st);
     }
     if ((st = dalloc(c, &c->fdt, N * D)) || (st = dalloc(c, &c->r0, N)) || (st = dalloc(c, &c->phase, N)) ||
         (st = dalloc(c, &c->materials, MAX_MATERIALS)) || (st = dalloc(c, &c->mat_hkeys, MAT_HASH)) ||
@@ -463,8 +468,6 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     cudaMemset(c->hvals[1], 0xff, hcap * 4);
     cudaMemset(c->ctr, 0, sizeof(Counters));
     cudaMemset(c->err, 0, 4);
-    cudaMemset(c->pb[0].damping, 0, N * 4);
-    cudaMemset(c->pb[1].damping, 0, N * 4);
     cudaMemset(c->slot_counts, 0, (size_t)hcap * CELLS * 4);
     if (const char *variant = std::getenv("SLOSH_P2G")) {
         if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;

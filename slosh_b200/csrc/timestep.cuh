@@ -67,24 +67,25 @@ template <int D, bool B = false> __global__ void k_timestep_bound(DevScene s, ui
     float h = s.h;
     if constexpr (B) h = s.scenes[scene].h;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t fl = s.flags[i];
+        const uint4 fo = s.fo[i];
+        const uint32_t fl = fo.x;
         if (!(fl & FLAG_ENABLED)) continue;
         if constexpr (B)
             if (scene_of(fl) != scene) continue;
-        const float4 pm = s.pm[i];
-        const float density0 = __fdiv_rn(pm.w, s.V0[i]);
+        const float4 pm = s.pm[i], vv = s.vv[i];
+        const float density0 = __fdiv_rn(pm.w, __uint_as_float(fo.z));
         float F[D][D];
+        {
+            float4 fv[MQ<D>::Q];
 #pragma unroll
-        for (int r = 0; r < D; ++r)
-#pragma unroll
-            for (int c = 0; c < D; ++c) F[r][c] = s.F[(r * D + c) * ps + i];
+            for (int q = 0; q < MQ<D>::Q; ++q) fv[q] = s.fq[q * ps + i];
+            mat_from<D>(fv, __uint_as_float(fo.w), F);
+        }
         const float det_f = det_rn<D>(F);
+        const float vel[3] = {vv.x, vv.y, vv.z};
         float v2 = 0.0f;
 #pragma unroll
-        for (int k = 0; k < D; ++k) {
-            const float vk = s.vel[k * ps + i];
-            v2 = __fadd_rn(v2, __fmul_rn(vk, vk));
-        }
+        for (int k = 0; k < D; ++k) v2 = __fadd_rn(v2, __fmul_rn(vel[k], vel[k]));
         const float vlen = __fsqrt_rn(v2);
         const Material &m = s.materials[fl & FLAG_MAT_MASK];
         float dt;

@@ -81,9 +81,10 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
     __shared__ float4 stile[DET ? 3 : 1][DET ? SlabTile<D>::SIZE : 1];
     // per-thread double buffer: the next particle of the cell is copied in
     // (cp.async) while the current one is accumulated
+    constexpr int Q = MQ<D>::Q;
     __shared__ float4 sp_pm[2][NT];
-    __shared__ float sp_v[2][D][NT];
-    __shared__ float sp_c[2][D * D][NT];
+    __shared__ float4 sp_vv[2][NT];
+    __shared__ float4 sp_cq[2][Q][NT];
     const uint32_t nb = s.ctr->n_blocks;
     float h = s.h, inv_h = 1.0f / s.h;
     const size_t n = s.n;
@@ -127,10 +128,9 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
             if (j < hi) {
                 const uint32_t i = s.perm[first + j];
                 cp_async16(&sp_pm[b][tid], &s.pm[i]);
+                cp_async16(&sp_vv[b][tid], &s.vv[i]);
 #pragma unroll
-                for (int k = 0; k < D; ++k) cp_async4(&sp_v[b][k][tid], &s.vel[k * n + i]);
-#pragma unroll
-                for (int q = 0; q < D * D; ++q) cp_async4(&sp_c[b][q][tid], &s.C[q * n + i]);
+                for (int q = 0; q < Q; ++q) cp_async16(&sp_cq[b][q][tid], &s.cq[q * n + i]);
             }
             cp_async_commit();
         };
@@ -157,14 +157,22 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
                 atomicOr(s.err, ERR_KEY_RANGE);
                 continue;
             }
-            float bm[D], hc[D][D];
+            float bm[D], hc[D][D], Cm[D][D];
+            {
+                float4 cv[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) cv[q] = sp_cq[buf][q][tid];
+                mat_from<D>(cv, sp_vv[buf][tid].w, Cm);
+            }
+            const float4 vv = sp_vv[buf][tid];
+            const float vel[3] = {vv.x, vv.y, vv.z};
 #pragma unroll
             for (int jj = 0; jj < D; ++jj) {
-                float q = sp_v[buf][jj][tid] * m;
+                float q = vel[jj] * m;
                 if (s.force_pending) q += s.fdt[jj * n + i];
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
-                    const float c = sp_c[buf][jj * D + k][tid];
+                    const float c = Cm[jj][k];
                     q += c * d0[k];
                     hc[k][jj] = h * c;
                 }
@@ -716,13 +724,11 @@ template <int D, bool B = false> __global__ void k_grid_update(DevScene s) {
 template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float tv[D][TILE];
+    constexpr int Q = MQ<D>::Q;
     __shared__ float4 st_pm[2][NT];
-    __shared__ float st_F[2][D * D][NT];
-    __shared__ float st_pl[2][3][NT];
-    __shared__ float st_v0[2][NT];
-    __shared__ float st_dmp[2][NT];
-    __shared__ uint32_t st_fl[2][NT];
-    __shared__ uint32_t st_oid[2][NT];
+    __shared__ float4 st_fq[2][Q][NT];
+    __shared__ uint4 st_fo[2][NT];
+    __shared__ float4 st_ps[2][NT];
     const uint32_t nb = s.ctr->n_blocks;
     float h = s.h, dt = s.dt, inv_h = s.inv_h;
     uint32_t h_pow2 = s.h_pow2;
@@ -757,14 +763,9 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
             const uint32_t i = s.perm[first + e];
             cp_async16(&st_pm[b][tid], &s.pm[i]);
 #pragma unroll
-            for (int q = 0; q < D * D; ++q) cp_async4(&st_F[b][q][tid], &s.F[q * n + i]);
-            cp_async4(&st_v0[b][tid], &s.V0[i]);
-            cp_async4(&st_fl[b][tid], &s.flags[i]);
-            cp_async4(&st_oid[b][tid], &s.oid[i]);
-            if (s.has_sand)
-#pragma unroll
-                for (int q = 0; q < 3; ++q) cp_async4(&st_pl[b][q][tid], &s.plastic[q * n + i]);
-            if (s.has_damping) cp_async4(&st_dmp[b][tid], &s.damping[i]);
+            for (int q = 0; q < Q; ++q) cp_async16(&st_fq[b][q][tid], &s.fq[q * n + i]);
+            cp_async16(&st_fo[b][tid], &s.fo[i]);
+            if (s.has_sand | s.has_damping) cp_async16(&st_ps[b][tid], &s.ps[i]);
         }
         cp_async_commit();
     };
@@ -800,7 +801,8 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
             const float4 p = st_pm[buf][tid];
             const float x[3] = {p.x, p.y, p.z};
             float m = p.w;
-            uint32_t fl = st_fl[buf][tid];
+            const uint4 fo = st_fo[buf][tid];
+            uint32_t fl = fo.x;
             // ---- G2P ----
             float vel[D], grad[D][D], div = 0.f;
 #pragma unroll
@@ -903,8 +905,9 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
             if (len > vmax)
 #pragma unroll
                 for (int k = 0; k < D; ++k) vel[k] = vel[k] / len * h / dt;
+            const float4 ps = (s.has_sand | s.has_damping) ? st_ps[buf][tid] : make_float4(0.f, 0.f, 0.f, 0.f);
             if (s.has_damping) {
-                const float dmp = 1.0f + st_dmp[buf][tid] * dt;
+                const float dmp = 1.0f + ps.w * dt;
 #pragma unroll
                 for (int k = 0; k < D; ++k) vel[k] = vel[k] / dmp;
             }
@@ -916,10 +919,12 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
 #pragma unroll
             for (int k = 0; k < D; ++k) nx[k] = x[k] + vel[k] * dt;
             float F[D][D];
+            {
+                float4 fv[Q];
 #pragma unroll
-            for (int rr = 0; rr < D; ++rr)
-#pragma unroll
-                for (int c = 0; c < D; ++c) F[rr][c] = st_F[buf][rr * D + c][tid];
+                for (int q = 0; q < Q; ++q) fv[q] = st_fq[buf][q][tid];
+                mat_from<D>(fv, __uint_as_float(fo.w), F);
+            }
             if (!fluid) {
                 float Fn[D][D];
 #pragma unroll
@@ -949,12 +954,14 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
 #pragma unroll
                     for (int c = 0; c < D; ++c) grad[rr][c] = 0.f;
             float st[3] = {0.f, 0.f, 0.f};
-            if (sand)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) st[k] = st_pl[buf][k][tid];
+            if (sand) {
+                st[0] = ps.x;
+                st[1] = ps.y;
+                st[2] = ps.z;
+            }
             float tau[D][D];
             model_update<D>(mat, F, st, tau, &s.ctr->n_svd_fp64);
-            const float v0 = st_v0[buf][tid];
+            const float v0 = __uint_as_float(fo.z);
             const float coef = v0 * inv_d * dt;
             bool finite = true;
 #pragma unroll
@@ -962,45 +969,42 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
             // The particle is stored at its canonical position o in the
             // output buffers (contiguous, coalesced writes).
             const size_t o = (size_t)first + e;
+            float Cn[D][D];
+            float4 np4 = p;
             if (finite && det<D>(F) > 0.f) {
-                float4 np4 = p;
                 np4.x = nx[0];
                 np4.y = nx[1];
                 if constexpr (D == 3) np4.z = nx[2];
-                s.out_pm[o] = np4;
 #pragma unroll
                 for (int rr = 0; rr < D; ++rr)
 #pragma unroll
-                    for (int c = 0; c < D; ++c) s.out_C[(rr * D + c) * n + o] = grad[rr][c] * m - tau[rr][c] * coef;
-#pragma unroll
-                for (int k = 0; k < D; ++k) s.out_vel[k * n + o] = vel[k];
+                    for (int c = 0; c < D; ++c) Cn[rr][c] = grad[rr][c] * m - tau[rr][c] * coef;
             } else {
                 fl &= ~FLAG_ENABLED;
                 m = 0.f;
-                float4 np4 = p;
                 np4.w = 0.f;
-                s.out_pm[o] = np4;
 #pragma unroll
                 for (int rr = 0; rr < D; ++rr)
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
                         F[rr][c] = (rr == c) ? 1.f : 0.f;
-                        s.out_C[(rr * D + c) * n + o] = 0.f;
+                        Cn[rr][c] = 0.f;
                     }
 #pragma unroll
-                for (int k = 0; k < D; ++k) s.out_vel[k * n + o] = 0.f;
+                for (int k = 0; k < D; ++k) vel[k] = 0.f;
             }
+            float4 cv[Q], fv[Q];
+            const float c22 = mat_split<D>(Cn, cv), f22 = mat_split<D>(F, fv);
+            s.out_pm[o] = np4;
+            s.out_vv[o] = make_float4(vel[0], vel[1], D == 3 ? vel[D - 1] : 0.f, c22);
 #pragma unroll
-            for (int rr = 0; rr < D; ++rr)
-#pragma unroll
-                for (int c = 0; c < D; ++c) s.out_F[(rr * D + c) * n + o] = F[rr][c];
-            if (s.has_sand)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) s.out_plastic[k * n + o] = st[k];
-            if (s.has_damping) s.out_damping[o] = st_dmp[buf][tid];
-            s.out_flags[o] = fl;
-            s.out_V0[o] = v0;
-            s.out_oid[o] = st_oid[buf][tid];
+            for (int q = 0; q < Q; ++q) {
+                s.out_cq[q * n + o] = cv[q];
+                s.out_fq[q * n + o] = fv[q];
+            }
+            s.out_fo[o] = make_uint4(fl, fo.y, fo.z, __float_as_uint(f22));
+            s.out_oid[o] = fo.y;
+            if (s.has_sand | s.has_damping) s.out_ps[o] = make_float4(st[0], st[1], st[2], ps.w);
         }
         cp_async_wait<0>();
         __syncthreads();
