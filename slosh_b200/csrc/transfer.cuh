@@ -756,11 +756,11 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
         if (*s.err != 0u)
             for (size_t q = g0; q < (size_t)s.hcap * CELLS; q += gs) s.slot_counts[q] = 0u;
     }
-    // Issues the copies of sorted entry e of the block into buffer b (an
-    // empty group when e is past the block's particles).
-    auto stage = [&](int b, uint32_t first, uint32_t e, uint32_t np) {
+    // Issues the copies of sorted entry e (storage index i) of the block into
+    // buffer b (an empty group when e is past the block's particles).  The
+    // storage index is loaded one iteration before the copies that need it.
+    auto stage = [&](int b, uint32_t e, uint32_t np, uint32_t i) {
         if (e < np) {
-            const uint32_t i = s.perm[first + e];
             cp_async16(&st_pm[b][tid], &s.pm[i]);
 #pragma unroll
             for (int q = 0; q < Q; ++q) cp_async16(&st_fq[b][q][tid], &s.fq[q * n + i]);
@@ -773,7 +773,8 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
-        stage(0, first, tid, np);
+        stage(0, tid, np, tid < np ? s.perm[first + tid] : 0u);
+        uint32_t i_next = tid + NT < np ? s.perm[first + tid + NT] : 0u;
         if constexpr (B) {
             const SceneRec &rec = s.scenes[s.bscene[r]];
             h = rec.h;
@@ -796,7 +797,8 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
         unpack_key<D>(s.bkey[r], bv);
         int buf = 0;
         for (uint32_t e = tid; e < np; e += NT, buf ^= 1) {
-            stage(buf ^ 1, first, e + NT, np);
+            stage(buf ^ 1, e + NT, np, i_next);
+            i_next = e + 2 * NT < np ? s.perm[first + e + 2 * NT] : 0u;
             cp_async_wait<1>();
             const float4 p = st_pm[buf][tid];
             const float x[3] = {p.x, p.y, p.z};
