@@ -21,6 +21,7 @@ constexpr uint32_t ERR_BLOCK_OVERFLOW = 1u << 1;   // more active blocks than ca
 constexpr uint32_t ERR_MATERIALS = 1u << 2;        // too many distinct materials
 constexpr uint32_t ERR_MATERIAL_HASH = 1u << 3;    // two materials share a 32-bit hash
 constexpr uint32_t ERR_KEY_RANGE = 1u << 4;        // a block coordinate outside the packed-key range
+constexpr uint32_t ERR_BLOCK_PARTICLES = 1u << 6;  // a block holds 2^26 particles or more
 constexpr uint32_t ERR_SCENE_BLOCKS = 1u << 5;     // a batch scene has more blocks than the per-scene sort holds
 
 // Sparse grid geometry per dimension (shaders/slosh/grid/grid.slang:224-257).
@@ -146,6 +147,17 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Named CTA barriers (ids 1-15; 0 is __syncthreads) over n threads, a
+// multiple of 32: `arrive` signals without waiting, `sync` waits for n.
+// Both order the shared-memory accesses made before them for the threads
+// that complete the barrier.
+__device__ __forceinline__ void named_bar_sync(uint32_t id, uint32_t n) {
+    asm volatile("barrier.sync %0, %1;\n" ::"r"(id), "r"(n) : "memory");
+}
+__device__ __forceinline__ void named_bar_arrive(uint32_t id, uint32_t n) {
+    asm volatile("barrier.arrive %0, %1;\n" ::"r"(id), "r"(n) : "memory");
+}
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;

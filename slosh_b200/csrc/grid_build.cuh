@@ -558,7 +558,8 @@ template <int NT, uint32_t PMIN, uint32_t PMAX> __global__ void __launch_bounds_
 }
 
 // One warp per block: per-cell counts (cleared in the hash-slot array once
-// read) with their in-block exclusive scan, the block total, the +1 and -1
+// read) with their in-block exclusive scan, the block total, the cells in
+// decreasing count order for P2G's thread assignment, the +1 and -1
 // neighbour ranks (update_nbh_block_ids, sort.slang:100-117) and, for the
 // atomic P2G variants, zeroed nodes (reset, grid.slang:455-485).
 template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
@@ -584,7 +585,25 @@ template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
         s.bcell[(size_t)r * CELLS + 2 * lane + 1] = ex + c0;
         s.bcur[(size_t)r * CELLS + 2 * lane] = ex;
         s.bcur[(size_t)r * CELLS + 2 * lane + 1] = ex + c0;
-        if (lane == 31) s.bnp[r] = incl;
+        if (lane == 31) {
+            s.bnp[r] = incl;
+            if (incl >= (1u << 26)) atomicOr(s.err, ERR_BLOCK_PARTICLES);  // beyond the 26-bit first in bord
+        }
+        {
+            // rank of each cell among the 64 by (count desc, cell asc): the
+            // number of keys above its own, keys being distinct
+            const uint32_t k0 = (min(c0, 0x3ffffffu) << 6) | (63u - 2u * lane);
+            const uint32_t k1 = (min(c1, 0x3ffffffu) << 6) | (62u - 2u * lane);
+            uint32_t r0 = 0, r1 = 0;
+#pragma unroll 8
+            for (int q = 0; q < 32; ++q) {
+                const uint32_t a = __shfl_sync(FULL_MASK, k0, q), b = __shfl_sync(FULL_MASK, k1, q);
+                r0 += (a > k0) + (b > k0);
+                r1 += (a > k1) + (b > k1);
+            }
+            s.bord[(size_t)r * CELLS + r0] = make_uint2((2u * lane) | (ex << 6), c0);
+            s.bord[(size_t)r * CELLS + r1] = make_uint2((2u * lane + 1u) | ((ex + c0) << 6), c1);
+        }
         if (!s.use_partial) {  // the atomic P2G variants accumulate into the nodes
             s.nodes[(size_t)r * 64 + 2 * lane] = make_float4(0.f, 0.f, 0.f, 0.f);
             s.nodes[(size_t)r * 64 + 2 * lane + 1] = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -80,26 +80,25 @@ __device__ __forceinline__ void recompose(const float (&U)[D][D], const float *s
         }
 }
 
+// With F = U S V^T and R = U V^T, (F - R) F^T = U (S - I) S U^T, so the
+// stress needs U and the singular values only: a symmetric product.
 template <int D>
-__device__ __forceinline__ void fixed_corotated(const float (&F)[D][D], const SvdD<D> &sv, float lambda, float mu,
-                                                float (&tau)[D][D]) {
+__device__ __forceinline__ void fixed_corotated(const SvdD<D> &sv, float lambda, float mu, float (&tau)[D][D]) {
     float j = sv.s[0] * sv.s[1];
     if constexpr (D == 3) j = j * sv.s[2];
-    float sm1[D];
+    float d[D];
 #pragma unroll
-    for (int k = 0; k < D; ++k) sm1[k] = sv.s[k] - 1.f;
-    float rec[D][D];
-    recompose<D>(sv.U, sm1, sv.V, rec);  // F - R
+    for (int k = 0; k < D; ++k) d[k] = 2.f * mu * (sv.s[k] - 1.f) * sv.s[k];
     const float diag = lambda * (j - 1.f) * j;
-    const float two_mu = 2.f * mu;
 #pragma unroll
     for (int i = 0; i < D; ++i)
 #pragma unroll
-        for (int k = 0; k < D; ++k) {
+        for (int k = i; k < D; ++k) {
             float acc = 0.f;
 #pragma unroll
-            for (int l = 0; l < D; ++l) acc += F[k][l] * rec[i][l];
-            tau[i][k] = acc * two_mu;
+            for (int l = 0; l < D; ++l) acc += (sv.U[i][l] * d[l]) * sv.U[k][l];
+            tau[i][k] = acc;
+            tau[k][i] = acc;
         }
 #pragma unroll
     for (int i = 0; i < D; ++i) tau[i][i] += diag;
@@ -201,7 +200,7 @@ __device__ __forceinline__ void model_update(const Material &mat, float (&F)[D][
         case SLOSH_MODEL_ELASTIC_LINEAR: {
             SvdD<D> sv;
             sv.compute(F, fp64);
-            fixed_corotated<D>(F, sv, mat.p[0], mat.p[1], tau);
+            fixed_corotated<D>(sv, mat.p[0], mat.p[1], tau);
             break;
         }
         case SLOSH_MODEL_ELASTIC_NEO_HOOKEAN:
@@ -211,7 +210,7 @@ __device__ __forceinline__ void model_update(const Material &mat, float (&F)[D][
             SvdD<D> sv;
             sv.compute(F, fp64);
             if (mat.p[7] != 0.f) drucker_prager<D>(st, mat.p + 3, sv, F);
-            fixed_corotated<D>(F, sv, mat.p[9], mat.p[10], tau);
+            fixed_corotated<D>(sv, mat.p[9], mat.p[10], tau);
             break;
         }
         case SLOSH_MODEL_SAND_NEO_HOOKEAN: {

@@ -47,6 +47,7 @@ struct slosh_ctx {
              *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_fill = nullptr, *tmp_key = nullptr,
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
              *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr, *bnbh_rev = nullptr;
+    uint2 *bord = nullptr;
     // P2G reduction (environment SLOSH_P2G at creation): 0 fixed-order,
     // bit-reproducible (default); 3 "direct": the same cell-owner kernel with
     // shared-memory and global float atomics, kept for A/B comparison.
@@ -180,6 +181,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.bfirst = c->bfirst;
     s.bnp = c->bnp;
     s.bcell = c->bcell;
+    s.bord = c->bord;
     s.bcur = c->bcur;
     s.bnbh = c->bnbh;
     s.bnbh_rev = c->bnbh_rev;
@@ -341,6 +343,8 @@ int check_device_error(slosh_ctx *c) {
     CK(cudaMemset(c->err, 0, 4));
     if (e & (ERR_HASH_OVERFLOW | ERR_BLOCK_OVERFLOW))
         return fail(c, SLOSH_E_OVERFLOW, "active blocks exceed the grid capacity %u (error bits 0x%x)", c->cap, e);
+    if (e & ERR_BLOCK_PARTICLES)
+        return fail(c, SLOSH_E_OVERFLOW, "a block holds 2^26 particles or more (error bits 0x%x)", e);
     if (e & ERR_KEY_RANGE)
         return fail(c, SLOSH_E_OVERFLOW, "a particle left the packed block-key range (error bits 0x%x)", e);
     if (e & (ERR_MATERIALS | ERR_MATERIAL_HASH))
@@ -452,6 +456,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) || (st = dalloc(c, &c->bkey, cap)) ||
         (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
+        (st = dalloc(c, &c->bord, (size_t)cap * CELLS)) ||
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||

@@ -89,16 +89,11 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
     float h = s.h, inv_h = 1.0f / s.h;
     const size_t n = s.n;
     const uint32_t tid = threadIdx.x;
-    const int mycell = (int)(threadIdx.x & 63u), myslab = (int)(threadIdx.x >> 6);
-    int ca[D];
-    if constexpr (D == 3) {
-        ca[0] = mycell & 3;
-        ca[1] = (mycell >> 2) & 3;
-        ca[2] = mycell >> 4;
-    } else {
-        ca[0] = mycell & 7;
-        ca[1] = mycell >> 3;
-    }
+    // Thread (rank, slab): the block's cells sorted by decreasing particle
+    // count (bord), three slab threads each, so a warp holds about 11 cells
+    // of similar count and its lanes finish their particle loops together.
+    const uint32_t myrank = tid / 3u;
+    const int myslab = (int)(tid - 3u * myrank);
     const float fsl = (float)myslab;
     for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
         const uint32_t np = s.bnp[r];
@@ -108,16 +103,41 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
             if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
         }
-        if constexpr (!DET)
+        if constexpr (!DET) {
             for (int t = threadIdx.x; t < 4 * TILE; t += P2G_THREADS) (&tile[0][0])[t] = 0.f;
+        } else {
+            // zero the nodes each slab tile receives: 3D z planes sl .. sl + 3
+            // of 6 x 6, 2D rows sl .. sl + 7 of 10
+            if constexpr (D == 3) {
+                for (uint32_t q = tid; q < 432u; q += NT) {
+                    const uint32_t sl = q / 144u, rr = q - 144u * sl, pl = rr / 36u, rem = rr - 36u * pl;
+                    stile[sl][(rem % 6u) + PY * (rem / 6u) + PZ * (sl + pl)] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            } else {
+                for (uint32_t q = tid; q < 240u; q += NT) {
+                    const uint32_t sl = q / 80u, rr = q - 80u * sl;
+                    stile[sl][(rr % 10u) + PY * (sl + rr / 10u)] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+        }
         if constexpr (B) {
             h = s.scenes[s.bscene[r]].h;
             inv_h = 1.0f / h;
         }
         int bv[D];
         unpack_key<D>(s.bkey[r], bv);
-        const uint32_t lo = s.bcell[(size_t)r * CELLS + mycell];
-        const uint32_t hi = (mycell < 63) ? s.bcell[(size_t)r * CELLS + mycell + 1] : np;
+        const uint2 ord = s.bord[(size_t)r * CELLS + myrank];
+        const int mycell = (int)(ord.x & 63u);
+        const uint32_t lo = ord.x >> 6, hi = lo + ord.y;
+        int ca[D];
+        if constexpr (D == 3) {
+            ca[0] = mycell & 3;
+            ca[1] = (mycell >> 2) & 3;
+            ca[2] = mycell >> 4;
+        } else {
+            ca[0] = mycell & 7;
+            ca[1] = mycell >> 3;
+        }
         float assoc[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) assoc[k] = (float)(bv[k] * BW + ca[k]);
@@ -211,20 +231,15 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
         }
         cp_async_wait<0>();
         if constexpr (DET) {
+            // Warps add their cells' nodes into the slab tiles one after the
+            // other, lightest (last) warp first: for a fixed k the lanes of a
+            // warp hit distinct nodes, and the named-barrier chain orders the
+            // warps, so every node sums in the same order on every run.
             float4 *pt = stile[myslab];
-            const uint32_t lane = tid & 31u, w = (tid & 63u) >> 5;
-            // zero the slab-tile planes this warp writes: 3D z planes
-            // 2w + slab .. +1 (6 x 6 nodes each), 2D rows 4w + slab .. +3
-            if constexpr (D == 3) {
-                for (uint32_t q = lane; q < 72u; q += 32u) {
-                    const uint32_t pl = 2u * w + (uint32_t)myslab + q / 36u, rem = q % 36u;
-                    pt[(rem % 6u) + PY * (rem / 6u) + PZ * pl] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            } else {
-                for (uint32_t q = lane; q < 40u; q += 32u)
-                    pt[(q % 10u) + PY * (4u * w + (uint32_t)myslab + q / 10u)] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+            const uint32_t warp = tid >> 5;
+            constexpr uint32_t NW = NT / 32;
             __syncwarp();
+            if (warp + 1 < NW) named_bar_sync(1 + warp, 64);
 #pragma unroll
             for (int k = 0; k < NACC; ++k) {
                 const int sx = k % 3, sy = (D == 3) ? k / 3 : myslab, sz = (D == 3) ? myslab : 0;
@@ -238,6 +253,7 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
                 pt[idx] = v;
                 __syncwarp();
             }
+            if (warp > 0) named_bar_arrive(warp, 64);
             __syncthreads();
             for (int t = threadIdx.x; t < TILE; t += P2G_THREADS) {
                 int tc[D];
@@ -723,7 +739,7 @@ template <int D, bool B = false> __global__ void k_grid_update(DevScene s) {
 // loop has no barrier.
 template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
-    __shared__ float tv[D][TILE];
+    __shared__ float4 tv[TILE];  // node (velocity, mass): one 16-byte load per node
     constexpr int Q = MQ<D>::Q;
     __shared__ float4 st_pm[2][NT];
     __shared__ float4 st_fq[2][Q][NT];
@@ -788,9 +804,7 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
             uint32_t rank, local;
             float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
             if (tile_node_owner<D>(s, r, t, rank, local)) v = s.nodes[(size_t)rank * 64u + local];
-            tv[0][t] = v.x;
-            tv[1][t] = v.y;
-            if constexpr (D == 3) tv[2][t] = v.z;
+            tv[t] = v;
         }
         __syncthreads();
         int bv[D];
@@ -852,9 +866,12 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
                         for (int sy = 0; sy < 3; ++sy) {
                             const int idx = a[0] + TW * ((a[1] + sy) + TW * (a[2] + sz));
                             const float wy = w[1][sy], wys = (float)sy * w[1][sy];
+                            const float4 n0 = tv[idx], n1 = tv[idx + 1], n2 = tv[idx + 2];
+                            const float a0[3] = {n0.x, n0.y, n0.z}, a1[3] = {n1.x, n1.y, n1.z},
+                                        a2[3] = {n2.x, n2.y, n2.z};
 #pragma unroll
                             for (int c = 0; c < 3; ++c) {
-                                const float v0 = tv[c][idx], v1 = tv[c][idx + 1], v2 = tv[c][idx + 2];
+                                const float v0 = a0[c], v1 = a1[c], v2 = a2[c];
                                 const float R0 = wx0 * v0 + wx1 * v1 + wx2 * v2;
                                 const float Rx = wx1 * v1 + wx2b * v2;
                                 S0[c] += wy * R0;
@@ -876,9 +893,11 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
                     for (int sy = 0; sy < 3; ++sy) {
                         const int idx = a[0] + TW * (a[1] + sy);
                         const float wy = w[1][sy], wys = (float)sy * w[1][sy];
+                        const float4 n0 = tv[idx], n1 = tv[idx + 1], n2 = tv[idx + 2];
+                        const float a0[2] = {n0.x, n0.y}, a1[2] = {n1.x, n1.y}, a2[2] = {n2.x, n2.y};
 #pragma unroll
                         for (int c = 0; c < 2; ++c) {
-                            const float v0 = tv[c][idx], v1 = tv[c][idx + 1], v2 = tv[c][idx + 2];
+                            const float v0 = a0[c], v1 = a1[c], v2 = a2[c];
                             const float R0 = wx0 * v0 + wx1 * v1 + wx2 * v2;
                             const float Rx = wx1 * v1 + wx2b * v2;
                             M0[c] += wy * R0;
