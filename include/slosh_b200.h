@@ -343,7 +343,7 @@ typedef struct slosh_scene_desc {
 
 /* Launch shape of the batched substep (no effect on results). */
 typedef struct slosh_tuning {
-    uint32_t p2g_ctas_per_sm;  /* P2G grid = SMs x this (4, 8, 16)          */
+    uint32_t p2g_ctas_per_sm;  /* P2G grid = SMs x this CTAs of 4 warps (5 fit an SM) */
     uint32_t g2p_threads;      /* G2P CTA size: 64, 128 or 256              */
     uint32_t g2p_ctas_per_sm;  /* G2P grid = SMs x this                     */
     uint32_t pad;

@@ -52,7 +52,7 @@ struct slosh_batch {
     slosh_particle *up = nullptr;
     uint32_t up_cap = 0, up_used = 0, staged_n = 0;
     cudaStream_t up_stream = nullptr;
-    slosh_tuning tune{8, 128, 8, 0};
+    slosh_tuning tune{5, 128, 8, 0};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
     uint32_t graph_flags = 0;       // has_damping | has_sand << 1 the graphs were captured with
@@ -105,7 +105,8 @@ template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uin
     k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     k_scatter<true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
     k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
-    k_p2g<D, true, true><<<std::min<uint32_t>(c->cap, sm * b->tune.p2g_ctas_per_sm), P2G_THREADS, 0, st>>>(s);
+    k_p2g<D, true><<<std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, sm * b->tune.p2g_ctas_per_sm),
+                     32 * P2G_WARPS, 0, st>>>(s);
     k_grid_update<D, true><<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
     if (b->tune.g2p_threads == 64) launch_batch_g2p<D, 64>(b, s, st);
     else if (b->tune.g2p_threads == 256) launch_batch_g2p<D, 256>(b, s, st);
@@ -663,8 +664,8 @@ int batch_autotune(slosh_batch *b, uint32_t substeps, void *stream, uint32_t *ra
     }
     CK(cudaSetDevice(c->device));
     cudaStream_t st = pick(c, stream);
-    const slosh_tuning cands[] = {{8, 128, 8, 0}, {4, 128, 4, 0},  {16, 128, 16, 0},
-                                  {8, 64, 16, 0}, {8, 256, 4, 0},  {4, 64, 8, 0}};
+    const slosh_tuning cands[] = {{5, 128, 8, 0}, {4, 128, 4, 0},  {10, 128, 16, 0},
+                                  {5, 64, 16, 0}, {5, 256, 4, 0},  {4, 64, 8, 0}};
     const uint32_t reps = std::max<uint32_t>(substeps, 1u);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));

@@ -273,11 +273,13 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
 
 template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
     PROF_BEGIN(9);
-    const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
-    if (c->p2g_variant == 3)
-        k_p2g<D, false><<<g, P2G_THREADS, 0, st>>>(s);
-    else
-        k_p2g<D, true><<<g, P2G_THREADS, 0, st>>>(s);
+    if (c->p2g_variant == 3) {
+        const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
+        k_p2g_atomic<D><<<g, P2G_ATOMIC_THREADS, 0, st>>>(s);
+    } else {
+        const uint32_t g = std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, (uint32_t)c->sm_count * 5);
+        k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
+    }
     PROF_END(9);
 }
 

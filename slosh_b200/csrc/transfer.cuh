@@ -39,86 +39,127 @@ __device__ __forceinline__ bool tile_node_owner(const DevScene &s, uint32_t r, i
     return rank != NONE;
 }
 
-constexpr int P2G_THREADS = 192;  // 64 cells x 3 slabs
+// Adds one particle to a thread's stencil sums.  The thread owns cell `assoc`
+// (its base node, in cells) and one slab of the 3^D stencil: 3D the nodes
+// (sx, sy, slab), 2D (sx, slab).  p = (x, m), vv = (v, C22), cq = C rows,
+// fdt = the pending force impulse (zeros when none).  The weights use
+// -d0 / h = -d0 * (1/h) like slosh's p2g (dpt * inv_cell_width) with
+// d0 = assoc h - x exact from the sorted cell.  Returns false for a
+// particle outside the cell (packed-key aliasing far outside the key range).
+template <int D>
+__device__ __forceinline__ bool p2g_particle(const float4 p, const float4 vv, const float4 *cq, const float (&fdt)[3],
+                                             const float (&assoc)[D], float h, float inv_h, int slab,
+                                             float4 (&acc)[D == 3 ? 9 : 3]) {
+    const float x[3] = {p.x, p.y, p.z};
+    const float m = p.w;
+    float d0[D], w[D][3];
+    bool in_cell = true;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        d0[k] = assoc[k] * h - x[k];
+        const float f = -d0[k] * inv_h;
+        in_cell = in_cell && f >= 0.49f && f <= 1.51f;
+        bspline_weights(f, w[k]);
+    }
+    if (!in_cell) return false;
+    float bm[D], hc[D][D], Cm[D][D];
+    mat_from<D>(cq, vv.w, Cm);
+    const float vel[3] = {vv.x, vv.y, vv.z};
+#pragma unroll
+    for (int jj = 0; jj < D; ++jj) {
+        float q = vel[jj] * m + fdt[jj];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const float c = Cm[jj][k];
+            q += c * d0[k];
+            hc[k][jj] = h * c;
+        }
+        bm[jj] = q;
+    }
+    const float fsl = (float)slab;
+    if constexpr (D == 3) {
+        const float wz = slab == 0 ? w[2][0] : (slab == 1 ? w[2][1] : w[2][2]);
+        const float mz0 = bm[0] + fsl * hc[2][0], mz1 = bm[1] + fsl * hc[2][1], mz2 = bm[2] + fsl * hc[2][2];
+#pragma unroll
+        for (int sy = 0; sy < 3; ++sy) {
+            const float wyz = w[1][sy] * wz;
+            const float my0 = mz0 + (float)sy * hc[1][0], my1 = mz1 + (float)sy * hc[1][1],
+                        my2 = mz2 + (float)sy * hc[1][2];
+#pragma unroll
+            for (int sx = 0; sx < 3; ++sx) {
+                const float wt = w[0][sx] * wyz;
+                float4 &a = acc[sx + 3 * sy];
+                a.x += wt * (my0 + (float)sx * hc[0][0]);
+                a.y += wt * (my1 + (float)sx * hc[0][1]);
+                a.z += wt * (my2 + (float)sx * hc[0][2]);
+                a.w += wt * m;
+            }
+        }
+    } else {
+        const float wy = slab == 0 ? w[1][0] : (slab == 1 ? w[1][1] : w[1][2]);
+        const float my0 = bm[0] + fsl * hc[1][0], my1 = bm[1] + fsl * hc[1][1];
+#pragma unroll
+        for (int sx = 0; sx < 3; ++sx) {
+            const float wt = w[0][sx] * wy;
+            float4 &a = acc[sx];
+            a.x += wt * (my0 + (float)sx * hc[0][0]);
+            a.y += wt * (my1 + (float)sx * hc[0][1]);
+            a.w += wt * m;
+        }
+    }
+    return true;
+}
 
-// Particle-to-grid, direct cell-owner kernel.
+// Particle-to-grid, one warp per active block (P2G_WARPS warps a CTA, each
+// on its own blocks, no CTA barrier).
 //
-// One CTA of 192 threads per active block with primaries; thread (cell c,
-// slab) owns cell c and the 9 (3D) or 3 (2D) stencil offsets of one slab.
-// It reads the particles of its cell straight from global memory -- they
-// are contiguous in the canonical storage order -- and accumulates its nodes
-// in registers.  The cell comes from the sort, so the base node position is
-// exact and no division is needed: d0 = (block origin + cell) h - x, and the
-// weights use -d0 / h = -d0 * (1/h) like slosh's p2g (dpt * inv_cell_width).
+// The block's 64 cells x 3 stencil slabs are 192 (cell, slab) items, taken
+// in bord's order (cells by decreasing particle count) in 6 passes of 32:
+// the lanes of a pass hold cells of similar count, so they finish their
+// particle loops together, and a pass whose first (largest) cell is empty
+// ends the block.  A lane owns cell c and the 9 (3D) or 3 (2D) stencil nodes
+// of one slab, reads the particles of c -- contiguous in the canonical order
+// -- double-buffered through cp.async, and sums its nodes in registers.
 //
-// DET (default): the per-thread sums are reduced in a fixed order, so the
-// whole substep is bit-reproducible.  Each slab has its own (block + 2)^D
-// tile in shared memory; the 9 (3) offsets of a slab are added in 9 (3)
-// phases, one offset per phase, and since all contributors of a slab-tile
-// node lie in one warp (same cell z in 3D, same cell row group in 2D) the
-// phases only need __syncwarp.  The three slab tiles are then summed in slab
-// order and the block's tile is stored to its own `partial` slot with plain
-// stores; k_grid_update adds the (up to 2^D) tiles overlapping each node in
-// a fixed order.  Without DET the sums go through shared-memory atomics and
-// 16-byte global atomics into the nodes (kept for comparison).
-// Slab-tile layout of the deterministic reduction: pitches chosen so that a
-// quarter-warp's 16-byte accesses hit distinct bank groups (3D: x 1, y 12,
-// z 72; 2D: x 1, y 10).
+// Reduction, fixed order (the substep is bit-reproducible): each slab has a
+// tile of the nodes its cells reach (3D: 6 x 6 x 4, z relative to the slab;
+// 2D: 10 x 8).  After each pass the lanes add their 9 (3) sums, one stencil
+// offset at a time; for a fixed offset the lanes of a pass hit distinct
+// nodes (one item per (cell, slab)), so only __syncwarp is needed.  The
+// slab tiles are then summed in slab order into the block's (block + 2)^D
+// tile, stored to its own `partial` slot; k_grid_update adds the (up to 2^D)
+// tiles overlapping each node in a fixed order.
+constexpr int P2G_WARPS = 4;
 template <int D> struct SlabTile;
 template <> struct SlabTile<3> {
-    static constexpr int PY = 12, PZ = 72, SIZE = 432;
+    static constexpr int PY = 6, PZ = 36, SIZE = 144;  // x 6, y 6, z 4
 };
 template <> struct SlabTile<2> {
-    static constexpr int PY = 10, PZ = 0, SIZE = 100;
+    static constexpr int PY = 10, PZ = 0, SIZE = 80;  // x 10, y 8
 };
 
-template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(DevScene s) {
+template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
-    constexpr int NT = P2G_THREADS;
-    constexpr int PY = SlabTile<D>::PY, PZ = SlabTile<D>::PZ;
-    __shared__ float tile[4][DET ? 1 : TILE];
-    __shared__ float4 stile[DET ? 3 : 1][DET ? SlabTile<D>::SIZE : 1];
-    // per-thread double buffer: the next particle of the cell is copied in
-    // (cp.async) while the current one is accumulated
+    constexpr int PY = SlabTile<D>::PY, PZ = SlabTile<D>::PZ, SSZ = SlabTile<D>::SIZE;
     constexpr int Q = MQ<D>::Q;
-    __shared__ float4 sp_pm[2][NT];
-    __shared__ float4 sp_vv[2][NT];
-    __shared__ float4 sp_cq[2][Q][NT];
+    __shared__ float4 stile[P2G_WARPS][3 * SSZ];
+    __shared__ float4 sp_pm[P2G_WARPS][2][32];
+    __shared__ float4 sp_vv[P2G_WARPS][2][32];
+    __shared__ float4 sp_cq[P2G_WARPS][2][Q][32];
     const uint32_t nb = s.ctr->n_blocks;
-    float h = s.h, inv_h = 1.0f / s.h;
     const size_t n = s.n;
-    const uint32_t tid = threadIdx.x;
-    // Thread (rank, slab): the block's cells sorted by decreasing particle
-    // count (bord), three slab threads each, so a warp holds about 11 cells
-    // of similar count and its lanes finish their particle loops together.
-    const uint32_t myrank = tid / 3u;
-    const int myslab = (int)(tid - 3u * myrank);
-    const float fsl = (float)myslab;
-    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
+    const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
+    float4 *tiles = stile[wl];
+    float h = s.h, inv_h = 1.0f / s.h;
+    const uint32_t nwarps = gridDim.x * P2G_WARPS;
+    for (uint32_t r = blockIdx.x * P2G_WARPS + wl; r < nb; r += nwarps) {
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
         if (first + np > s.n) {  // only after an earlier overflow left stale counts
-            if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+            if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
-        }
-        if constexpr (!DET) {
-            for (int t = threadIdx.x; t < 4 * TILE; t += P2G_THREADS) (&tile[0][0])[t] = 0.f;
-        } else {
-            // zero the nodes each slab tile receives: 3D z planes sl .. sl + 3
-            // of 6 x 6, 2D rows sl .. sl + 7 of 10
-            if constexpr (D == 3) {
-                for (uint32_t q = tid; q < 432u; q += NT) {
-                    const uint32_t sl = q / 144u, rr = q - 144u * sl, pl = rr / 36u, rem = rr - 36u * pl;
-                    stile[sl][(rem % 6u) + PY * (rem / 6u) + PZ * (sl + pl)] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            } else {
-                for (uint32_t q = tid; q < 240u; q += NT) {
-                    const uint32_t sl = q / 80u, rr = q - 80u * sl;
-                    stile[sl][(rr % 10u) + PY * (sl + rr / 10u)] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
         }
         if constexpr (B) {
             h = s.scenes[s.bscene[r]].h;
@@ -126,18 +167,147 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
         }
         int bv[D];
         unpack_key<D>(s.bkey[r], bv);
-        const uint2 ord = s.bord[(size_t)r * CELLS + myrank];
-        const int mycell = (int)(ord.x & 63u);
-        const uint32_t lo = ord.x >> 6, hi = lo + ord.y;
-        int ca[D];
-        if constexpr (D == 3) {
-            ca[0] = mycell & 3;
-            ca[1] = (mycell >> 2) & 3;
-            ca[2] = mycell >> 4;
-        } else {
-            ca[0] = mycell & 7;
-            ca[1] = mycell >> 3;
+        for (uint32_t q = lane; q < 3u * SSZ; q += 32u) tiles[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint2 ord = s.bord[(size_t)r * CELLS + lane / 3u];
+        for (uint32_t pass = 0; pass < 6u; ++pass) {
+            const uint32_t item = 32u * pass + lane;
+            const int slab = (int)(item % 3u);
+            const uint32_t lo = ord.x >> 6, hi = lo + ord.y;
+            const int cell = (int)(ord.x & 63u);
+            if (__shfl_sync(FULL_MASK, ord.y, 0) == 0u) break;  // this and later passes hold empty cells
+            if (pass < 5u) ord = s.bord[(size_t)r * CELLS + (item + 32u) / 3u];
+            int ca[D];
+            if constexpr (D == 3) {
+                ca[0] = cell & 3;
+                ca[1] = (cell >> 2) & 3;
+                ca[2] = cell >> 4;
+            } else {
+                ca[0] = cell & 7;
+                ca[1] = cell >> 3;
+            }
+            float assoc[D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) assoc[k] = (float)(bv[k] * BW + ca[k]);
+            float4 acc[NACC];
+#pragma unroll
+            for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            auto stage = [&](int b, uint32_t j) {
+                if (j < hi) {
+                    const uint32_t i = s.perm[first + j];
+                    cp_async16(&sp_pm[wl][b][lane], &s.pm[i]);
+                    cp_async16(&sp_vv[wl][b][lane], &s.vv[i]);
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) cp_async16(&sp_cq[wl][b][q][lane], &s.cq[q * n + i]);
+                }
+                cp_async_commit();
+            };
+            stage(0, lo);
+            int buf = 0;
+            for (uint32_t j = lo; j < hi; ++j, buf ^= 1) {
+                stage(buf ^ 1, j + 1);
+                cp_async_wait<1>();
+                float fdt[3] = {0.f, 0.f, 0.f};
+                if (s.force_pending) {
+                    const uint32_t i = s.perm[first + j];
+#pragma unroll
+                    for (int k = 0; k < D; ++k) fdt[k] = s.fdt[k * n + i];
+                }
+                float4 cv[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) cv[q] = sp_cq[wl][buf][q][lane];
+                if (!p2g_particle<D>(sp_pm[wl][buf][lane], sp_vv[wl][buf][lane], cv, fdt, assoc, h, inv_h, slab, acc))
+                    atomicOr(s.err, ERR_KEY_RANGE);
+            }
+            cp_async_wait<0>();
+            __syncwarp();
+            // node (cell + stencil offset) in the slab's tile, whose slab-axis
+            // coordinate is relative to the slab: 3D z - slab = ca[2], 2D
+            // y - slab = ca[1]
+            float4 *pt = tiles + slab * SSZ;
+#pragma unroll
+            for (int k = 0; k < NACC; ++k) {
+                const int sx = k % 3;
+                int idx;
+                if constexpr (D == 3) idx = (ca[0] + sx) + PY * (ca[1] + k / 3) + PZ * ca[2];
+                else idx = (ca[0] + sx) + PY * ca[1];
+                float4 v = pt[idx];
+                v.x += acc[k].x;
+                v.y += acc[k].y;
+                v.z += acc[k].z;
+                v.w += acc[k].w;
+                pt[idx] = v;
+                __syncwarp();
+            }
         }
+        for (int t = (int)lane; t < TILE; t += 32) {
+            int tc[D];
+            tc[0] = t % TW;
+            if constexpr (D == 3) {
+                tc[1] = (t / TW) % TW;
+                tc[2] = t / (TW * TW);
+            } else {
+                tc[1] = t / TW;
+            }
+            const int along = tc[D - 1];  // slab axis: z in 3D, y in 2D
+            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int sl = 0; sl < 3; ++sl) {
+                const int rel = along - sl;  // node plane within slab sl's tile
+                if (rel < 0 || rel >= BW) continue;
+                const int lay = (D == 3) ? tc[0] + PY * tc[1] + PZ * rel : tc[0] + PY * rel;
+                const float4 v = tiles[sl * SSZ + lay];
+                sum.x += v.x;
+                sum.y += v.y;
+                sum.z += v.z;
+                sum.w += v.w;
+            }
+            s.partial[(size_t)r * TILE + t] = sum;
+        }
+        __syncwarp();
+    }
+}
+
+// Particle-to-grid with float atomics, kept for comparison (SLOSH_P2G=direct):
+// one CTA of 192 threads a block, thread (cell, slab) sums its nodes like
+// k_p2g and adds them through shared-memory atomics into the block's tile,
+// then 16-byte global atomics into the nodes.  Not bit-reproducible.
+constexpr int P2G_ATOMIC_THREADS = 192;
+template <int D> __global__ void __launch_bounds__(P2G_ATOMIC_THREADS, 4) k_p2g_atomic(DevScene s) {
+    constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
+    constexpr int NACC = (D == 3) ? 9 : 3;
+    constexpr int NT = P2G_ATOMIC_THREADS;
+    constexpr int Q = MQ<D>::Q;
+    __shared__ float tile[4][TILE];
+    __shared__ float4 sp_pm[2][NT];
+    __shared__ float4 sp_vv[2][NT];
+    __shared__ float4 sp_cq[2][Q][NT];
+    const uint32_t nb = s.ctr->n_blocks;
+    const float h = s.h, inv_h = 1.0f / s.h;
+    const size_t n = s.n;
+    const uint32_t tid = threadIdx.x;
+    const int mycell = (int)(tid & 63u), myslab = (int)(tid >> 6);
+    int ca[D];
+    if constexpr (D == 3) {
+        ca[0] = mycell & 3;
+        ca[1] = (mycell >> 2) & 3;
+        ca[2] = mycell >> 4;
+    } else {
+        ca[0] = mycell & 7;
+        ca[1] = mycell >> 3;
+    }
+    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
+        const uint32_t np = s.bnp[r];
+        if (np == 0) continue;
+        const uint32_t first = s.bfirst[r];
+        if (first + np > s.n) {
+            if (tid == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+            continue;
+        }
+        for (int t = tid; t < 4 * TILE; t += NT) (&tile[0][0])[t] = 0.f;
+        int bv[D];
+        unpack_key<D>(s.bkey[r], bv);
+        const uint32_t lo = s.bcell[(size_t)r * CELLS + mycell];
+        const uint32_t hi = (mycell < 63) ? s.bcell[(size_t)r * CELLS + mycell + 1] : np;
         float assoc[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) assoc[k] = (float)(bv[k] * BW + ca[k]);
@@ -160,127 +330,19 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
         for (uint32_t j = lo; j < hi; ++j, buf ^= 1) {
             stage(buf ^ 1, j + 1);
             cp_async_wait<1>();
-            const uint32_t i = s.force_pending ? s.perm[first + j] : 0u;
-            const float4 p = sp_pm[buf][tid];
-            const float x[3] = {p.x, p.y, p.z};
-            const float m = p.w;
-            float d0[D], w[D][3];
-            bool in_cell = true;
+            float fdt[3] = {0.f, 0.f, 0.f};
+            if (s.force_pending) {
+                const uint32_t i = s.perm[first + j];
 #pragma unroll
-            for (int k = 0; k < D; ++k) {
-                d0[k] = assoc[k] * h - x[k];
-                const float f = -d0[k] * inv_h;
-                in_cell = in_cell && f >= 0.49f && f <= 1.51f;
-                bspline_weights(f, w[k]);
+                for (int k = 0; k < D; ++k) fdt[k] = s.fdt[k * n + i];
             }
-            if (!in_cell) {  // packed-key aliasing far outside the key range
+            float4 cv[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) cv[q] = sp_cq[buf][q][tid];
+            if (!p2g_particle<D>(sp_pm[buf][tid], sp_vv[buf][tid], cv, fdt, assoc, h, inv_h, myslab, acc))
                 atomicOr(s.err, ERR_KEY_RANGE);
-                continue;
-            }
-            float bm[D], hc[D][D], Cm[D][D];
-            {
-                float4 cv[Q];
-#pragma unroll
-                for (int q = 0; q < Q; ++q) cv[q] = sp_cq[buf][q][tid];
-                mat_from<D>(cv, sp_vv[buf][tid].w, Cm);
-            }
-            const float4 vv = sp_vv[buf][tid];
-            const float vel[3] = {vv.x, vv.y, vv.z};
-#pragma unroll
-            for (int jj = 0; jj < D; ++jj) {
-                float q = vel[jj] * m;
-                if (s.force_pending) q += s.fdt[jj * n + i];
-#pragma unroll
-                for (int k = 0; k < D; ++k) {
-                    const float c = Cm[jj][k];
-                    q += c * d0[k];
-                    hc[k][jj] = h * c;
-                }
-                bm[jj] = q;
-            }
-            if constexpr (D == 3) {
-                const float wz = myslab == 0 ? w[2][0] : (myslab == 1 ? w[2][1] : w[2][2]);
-                const float mz0 = bm[0] + fsl * hc[2][0], mz1 = bm[1] + fsl * hc[2][1], mz2 = bm[2] + fsl * hc[2][2];
-#pragma unroll
-                for (int sy = 0; sy < 3; ++sy) {
-                    const float wyz = w[1][sy] * wz;
-                    const float my0 = mz0 + (float)sy * hc[1][0], my1 = mz1 + (float)sy * hc[1][1],
-                                my2 = mz2 + (float)sy * hc[1][2];
-#pragma unroll
-                    for (int sx = 0; sx < 3; ++sx) {
-                        const float wt = w[0][sx] * wyz;
-                        float4 &a = acc[sx + 3 * sy];
-                        a.x += wt * (my0 + (float)sx * hc[0][0]);
-                        a.y += wt * (my1 + (float)sx * hc[0][1]);
-                        a.z += wt * (my2 + (float)sx * hc[0][2]);
-                        a.w += wt * m;
-                    }
-                }
-            } else {
-                const float wy = myslab == 0 ? w[1][0] : (myslab == 1 ? w[1][1] : w[1][2]);
-                const float my0 = bm[0] + fsl * hc[1][0], my1 = bm[1] + fsl * hc[1][1];
-#pragma unroll
-                for (int sx = 0; sx < 3; ++sx) {
-                    const float wt = w[0][sx] * wy;
-                    float4 &a = acc[sx];
-                    a.x += wt * (my0 + (float)sx * hc[0][0]);
-                    a.y += wt * (my1 + (float)sx * hc[0][1]);
-                    a.w += wt * m;
-                }
-            }
         }
         cp_async_wait<0>();
-        if constexpr (DET) {
-            // Warps add their cells' nodes into the slab tiles one after the
-            // other, lightest (last) warp first: for a fixed k the lanes of a
-            // warp hit distinct nodes, and the named-barrier chain orders the
-            // warps, so every node sums in the same order on every run.
-            float4 *pt = stile[myslab];
-            const uint32_t warp = tid >> 5;
-            constexpr uint32_t NW = NT / 32;
-            __syncwarp();
-            if (warp + 1 < NW) named_bar_sync(1 + warp, 64);
-#pragma unroll
-            for (int k = 0; k < NACC; ++k) {
-                const int sx = k % 3, sy = (D == 3) ? k / 3 : myslab, sz = (D == 3) ? myslab : 0;
-                int idx = (ca[0] + sx) + PY * (ca[1] + sy);
-                if constexpr (D == 3) idx += PZ * (ca[2] + sz);
-                float4 v = pt[idx];
-                v.x += acc[k].x;
-                v.y += acc[k].y;
-                v.z += acc[k].z;
-                v.w += acc[k].w;
-                pt[idx] = v;
-                __syncwarp();
-            }
-            if (warp > 0) named_bar_arrive(warp, 64);
-            __syncthreads();
-            for (int t = threadIdx.x; t < TILE; t += P2G_THREADS) {
-                int tc[D];
-                tc[0] = t % TW;
-                if constexpr (D == 3) {
-                    tc[1] = (t / TW) % TW;
-                    tc[2] = t / (TW * TW);
-                } else {
-                    tc[1] = t / TW;
-                }
-                const int lay = (D == 3) ? tc[0] + PY * tc[1] + PZ * tc[2] : tc[0] + PY * tc[1];
-                const int along = tc[D - 1];  // slab axis: z in 3D, y in 2D
-                float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-                for (int sl = 0; sl < 3; ++sl) {
-                    if (along - sl < 0 || along - sl >= BW) continue;
-                    const float4 v = stile[sl][lay];
-                    sum.x += v.x;
-                    sum.y += v.y;
-                    sum.z += v.z;
-                    sum.w += v.w;
-                }
-                s.partial[(size_t)r * TILE + t] = sum;
-            }
-            __syncthreads();
-            continue;
-        }
         if (hi > lo) {
 #pragma unroll
             for (int k = 0; k < NACC; ++k) {
@@ -294,7 +356,7 @@ template <int D, bool DET, bool B = false> __global__ void __launch_bounds__(P2G
             }
         }
         __syncthreads();
-        for (int t = threadIdx.x; t < TILE; t += P2G_THREADS) {
+        for (int t = tid; t < TILE; t += NT) {
             const float4 val = make_float4(tile[0][t], tile[1][t], tile[2][t], tile[3][t]);
             if (val.x == 0.f && val.y == 0.f && val.z == 0.f && val.w == 0.f) continue;
             uint32_t rank, local;
