@@ -191,9 +191,10 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
             float4 acc[NACC];
 #pragma unroll
             for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-            auto stage = [&](int b, uint32_t j) {
+            // copies of entry j (storage index i); the index of entry j + 2 is
+            // loaded one iteration ahead of the copies that need it
+            auto stage = [&](int b, uint32_t j, uint32_t i) {
                 if (j < hi) {
-                    const uint32_t i = s.perm[first + j];
                     cp_async16(&sp_pm[wl][b][lane], &s.pm[i]);
                     cp_async16(&sp_vv[wl][b][lane], &s.vv[i]);
 #pragma unroll
@@ -201,17 +202,20 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
                 }
                 cp_async_commit();
             };
-            stage(0, lo);
+            uint32_t i_cur = lo < hi ? s.perm[first + lo] : 0u;
+            uint32_t i_next = lo + 1 < hi ? s.perm[first + lo + 1] : 0u;
+            stage(0, lo, i_cur);
             int buf = 0;
             for (uint32_t j = lo; j < hi; ++j, buf ^= 1) {
-                stage(buf ^ 1, j + 1);
+                stage(buf ^ 1, j + 1, i_next);
+                const uint32_t i = i_cur;
+                i_cur = i_next;
+                i_next = j + 2 < hi ? s.perm[first + j + 2] : 0u;
                 cp_async_wait<1>();
                 float fdt[3] = {0.f, 0.f, 0.f};
-                if (s.force_pending) {
-                    const uint32_t i = s.perm[first + j];
+                if (s.force_pending)
 #pragma unroll
                     for (int k = 0; k < D; ++k) fdt[k] = s.fdt[k * n + i];
-                }
                 float4 cv[Q];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) cv[q] = sp_cq[wl][buf][q][lane];
