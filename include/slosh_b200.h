@@ -98,6 +98,25 @@ typedef struct slosh_particle {
 #define SLOSH_BC_NON_REFLECTING 4u
 #define SLOSH_BC_DISABLED 5u
 
+/* Body coupling (BodyCoupling, src/rbd/dynamics/body.rs:124-138).
+ * ONE_WAY: the reference's behaviour on the GPU.  The body moves by its own
+ *   velocity (plus gravity when it has inverse mass); the particles never
+ *   push it, and the grid reuses cached collisions (colliders assumed still).
+ * TWO_WAY: the grid pushes back.  Each grid node projected by the body's
+ *   boundary condition is projected in the body's frame (the node velocity
+ *   relative to the body velocity at the node), and the momentum the node
+ *   loses is added to the body as an impulse at the node: linear and angular
+ *   sums in 64-bit fixed point (2^-40 N s), so the total does not depend on
+ *   the order of the additions.  The rigid update applies the impulse with
+ *   the body's inverse mass and world inverse inertia and caps the velocities
+ *   as rigid_impulses.slang:72-121 does.  While any body is TWO_WAY the grid
+ *   runs collision detection on every node instead of the cache.  slosh
+ *   declares the impulse buffer (rigid_impulses.slang:8-52) but no kernel of
+ *   it fills the buffer, so this mode has no reference output to match; the
+ *   oracle restates it for the parity tests. */
+#define SLOSH_COUPLING_ONE_WAY 0u
+#define SLOSH_COUPLING_TWO_WAY 1u
+
 /* One rigid body with its collider shape and boundary condition: an entry of
  * slosh's GpuBodySet (src/rbd/dynamics/body.rs:74-90) plus its
  * GpuBoundaryCondition (src/solver/boundary_condition.rs:8-12).  192 bytes.
@@ -121,10 +140,12 @@ typedef struct slosh_body {
     float angvel[4];
     float inv_mass[4];
     float local_com[4];
-    float inv_inertia[12]; /* world-space, 3 padded columns */
+    float inv_inertia[12]; /* world-space inverse inertia at this pose, 3 padded
+                              columns (2D: the scalar in [0]) */
     uint32_t bc_type;
     float bc_friction;
-    uint32_t pad[2];
+    uint32_t coupling;     /* SLOSH_COUPLING_* */
+    uint32_t pad;
 } slosh_body;
 
 /* Context creation parameters: the arguments of MpmData::new that size the

@@ -395,7 +395,42 @@ template <typename T, int D> struct Body {
     float inv_inertia[12];
     uint32_t bc_type;
     T friction;
+    uint32_t coupling;  // SLOSH_COUPLING_*
+    T inv_inertia_local[9];  // body-frame inverse inertia, row-major (2D: [0])
 };
+
+// Rotation matrix of a unit quaternion (i, j, k, w), and R M R^T / R^T M R.
+template <typename T> inline void quat_to_mat(const T *q, T (&R)[3][3]) {
+    const T x = q[0], y = q[1], z = q[2], w = q[3];
+    R[0][0] = T(1) - T(2) * (y * y + z * z);
+    R[0][1] = T(2) * (x * y - z * w);
+    R[0][2] = T(2) * (x * z + y * w);
+    R[1][0] = T(2) * (x * y + z * w);
+    R[1][1] = T(1) - T(2) * (x * x + z * z);
+    R[1][2] = T(2) * (y * z - x * w);
+    R[2][0] = T(2) * (x * z - y * w);
+    R[2][1] = T(2) * (y * z + x * w);
+    R[2][2] = T(1) - T(2) * (x * x + y * y);
+}
+template <typename T> inline void conjugate(const T (&R)[3][3], const T *M, T *out, bool forward) {
+    T A[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            T a = 0;
+            for (int k = 0; k < 3; ++k) a += (forward ? R[i][k] : R[k][i]) * M[k * 3 + j];
+            A[i][j] = a;
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            T a = 0;
+            for (int k = 0; k < 3; ++k) a += A[i][k] * (forward ? R[j][k] : R[k][j]);
+            out[i * 3 + j] = a;
+        }
+}
+
+// Two-way coupling impulse sums: 64-bit fixed point, 2^40 units per N s.
+constexpr double IMPULSE_UNITS = 1099511627776.0;
+inline long long impulse_units(double v) { return std::llrint(v * IMPULSE_UNITS); }
 
 // Quaternion helpers (stensor Quat / Sim3, restated from their definitions:
 // rotation of v by q, Hamilton product).
@@ -742,8 +777,15 @@ template <typename T, int D> struct Ctx {
     uint32_t capacity;
     Particles<T, D> p;
     std::vector<Body<T, D>> bodies;
+    std::vector<long long> impulses;  // 6 fixed-point sums per body (two-way coupling)
     Grid<T, D> grid, prev;
     int nthreads = 1;
+
+    bool coll_dynamic() const {
+        for (const auto &b : bodies)
+            if (b.coupling == SLOSH_COUPLING_TWO_WAY) return true;
+        return false;
+    }
 
     // block_associated_to_point and associated_cell_index_in_block_off_by_one
     // (grid.slang:346-354; particle.slang:79-87).
@@ -980,11 +1022,18 @@ template <typename T, int D> struct Ctx {
         }
     }
 
-    // grid_update (shaders/slosh/solver/grid_update.slang:38-163).
+    // grid_update (shaders/slosh/solver/grid_update.slang:38-163).  Bodies
+    // coupled two-way (an extension: slosh's GPU never fills its impulse
+    // buffer) project the node velocity relative to the body velocity at the
+    // node and receive the momentum the node loses as an impulse at the
+    // node, summed in 64-bit fixed point; while one exists, every node runs
+    // collision detection instead of the cache.
     void grid_update(Grid<T, D> &g, const Grid<T, D> &pg) {
         const size_t nb = g.keys.size();
         g.coll.assign(nb * 64, NodeCollision<T, D>{});
         const T vel_limit = h / dt;
+        const bool dynamic = coll_dynamic();
+        impulses.assign(bodies.size() * 6, 0);
 #pragma omp parallel for num_threads(nthreads) schedule(static)
         for (long long rb = 0; rb < (long long)nb; ++rb) {
             const size_t r = (size_t)rb;
@@ -1004,7 +1053,7 @@ template <typename T, int D> struct Ctx {
                     vel[k] = std::min(std::max(v, -vel_limit), vel_limit);
                 }
                 NodeCollision<T, D> c;
-                if (pit != pg.rank.end() && !pg.coll.empty()) {
+                if (pit != pg.rank.end() && !pg.coll.empty() && !dynamic) {
                     c = pg.coll[(size_t)pit->second * 64 + tid];
                 } else {
                     c = collide<T, D>(bodies, h, cell_pos);
@@ -1015,7 +1064,48 @@ template <typename T, int D> struct Ctx {
                     T dd = 0;
                     for (int k = 0; k < D; ++k) dd += (cell_pos[k] - c.point[k]) * c.normal[k];
                     T dist = dd - h;
-                    project_velocity<T, D>(b.bc_type, b.friction, vel, c.normal, dist, dt);
+                    if (b.coupling == SLOSH_COUPLING_TWO_WAY) {
+                        T com[3] = {0, 0, 0}, r[3] = {0, 0, 0}, vb[3] = {0, 0, 0};
+                        Pose<T, D>::mul_pt(b, b.local_com, com);
+                        for (int k = 0; k < D; ++k) r[k] = cell_pos[k] - com[k];
+                        if constexpr (D == 3) {
+                            vb[0] = b.linvel[0] + b.angvel[1] * r[2] - b.angvel[2] * r[1];
+                            vb[1] = b.linvel[1] + b.angvel[2] * r[0] - b.angvel[0] * r[2];
+                            vb[2] = b.linvel[2] + b.angvel[0] * r[1] - b.angvel[1] * r[0];
+                        } else {
+                            vb[0] = b.linvel[0] - b.angvel[0] * r[1];
+                            vb[1] = b.linvel[1] + b.angvel[0] * r[0];
+                        }
+                        T rel[D];
+                        for (int k = 0; k < D; ++k) rel[k] = vel[k] - vb[k];
+                        project_velocity<T, D>(b.bc_type, b.friction, rel, c.normal, dist, dt);
+                        T J[3] = {0, 0, 0};
+                        for (int k = 0; k < D; ++k) {
+                            const T nv = rel[k] + vb[k];
+                            J[k] = mass * (vel[k] - nv);
+                            vel[k] = nv;
+                        }
+                        if (mass > T(0)) {
+                            T A[3] = {0, 0, 0};
+                            if constexpr (D == 3) {
+                                A[0] = r[1] * J[2] - r[2] * J[1];
+                                A[1] = r[2] * J[0] - r[0] * J[2];
+                                A[2] = r[0] * J[1] - r[1] * J[0];
+                            } else {
+                                A[0] = r[0] * J[1] - r[1] * J[0];
+                            }
+                            long long *acc = &impulses[(size_t)c.collider_id * 6];
+                            for (int k = 0; k < 3; ++k) {
+                                const long long jl = impulse_units((double)J[k]), ja = impulse_units((double)A[k]);
+#pragma omp atomic
+                                acc[k] += jl;
+#pragma omp atomic
+                                acc[3 + k] += ja;
+                            }
+                        }
+                    } else {
+                        project_velocity<T, D>(b.bc_type, b.friction, vel, c.normal, dist, dt);
+                    }
                 }
                 for (int k = 0; k < D; ++k) node[k] = vel[k];
                 node[D] = mass;
@@ -1209,9 +1299,42 @@ template <typename T, int D> struct Ctx {
     // update (shaders/slosh/solver/rigid_impulses.slang:72-121) with
     // integrate_velocity (shaders/slosh/rbd/dynamics/body.slang:117-130).
     // The incremental impulse is always zero in the reference (no kernel
-    // writes it), so the impulse and the velocity cap it guards are no-ops.
+    // writes it); bodies coupled two-way apply the grid's impulse sums here
+    // (apply_impulse, body.slang:62-70) followed by the velocity caps.
     void rigid_update() {
-        for (auto &b : bodies) {
+        for (size_t bi = 0; bi < bodies.size(); ++bi) {
+            Body<T, D> &b = bodies[bi];
+            if (b.coupling == SLOSH_COUPLING_TWO_WAY && impulses.size() >= (bi + 1) * 6) {
+                T jl[3], ja[3];
+                for (int k = 0; k < 3; ++k) {
+                    jl[k] = (T)((double)impulses[bi * 6 + k] / IMPULSE_UNITS);
+                    ja[k] = (T)((double)impulses[bi * 6 + 3 + k] / IMPULSE_UNITS);
+                }
+                for (int k = 0; k < D; ++k) b.linvel[k] += b.inv_mass[k] * jl[k];
+                if constexpr (D == 3) {
+                    T R[3][3], Iw[9];
+                    quat_to_mat(b.rot, R);
+                    conjugate(R, b.inv_inertia_local, Iw, true);
+                    for (int i = 0; i < 3; ++i)
+                        b.angvel[i] += Iw[i * 3] * ja[0] + Iw[i * 3 + 1] * ja[1] + Iw[i * 3 + 2] * ja[2];
+                } else {
+                    b.angvel[0] += b.inv_inertia_local[0] * ja[0];
+                }
+                bool pushed = false;
+                for (int k = 0; k < 3; ++k) pushed = pushed || jl[k] != T(0) || ja[k] != T(0);
+                if (pushed) {
+                    const T lin_limit = T(0.1) * h / dt, ang_limit = T(1);
+                    const int na = D == 3 ? 3 : 1;
+                    T l2 = 0, a2 = 0;
+                    for (int k = 0; k < D; ++k) l2 += b.linvel[k] * b.linvel[k];
+                    for (int k = 0; k < na; ++k) a2 += b.angvel[k] * b.angvel[k];
+                    const T ln = std::sqrt(l2), an = std::sqrt(a2);
+                    if (ln > lin_limit)
+                        for (int k = 0; k < D; ++k) b.linvel[k] = b.linvel[k] * (lin_limit / ln);
+                    if (an > ang_limit)
+                        for (int k = 0; k < na; ++k) b.angvel[k] = b.angvel[k] * (ang_limit / an);
+                }
+            }
             T init_com[3] = {0, 0, 0};
             Pose<T, D>::mul_pt(b, b.local_com, init_com);
             if constexpr (D == 3) {
@@ -1358,6 +1481,16 @@ template <typename T, int D> Body<T, D> load_body(const slosh_body &s) {
     std::memcpy(b.inv_inertia, s.inv_inertia, sizeof(b.inv_inertia));
     b.bc_type = s.bc_type;
     b.friction = s.bc_friction;
+    b.coupling = s.coupling;
+    if constexpr (D == 3) {  // the world-space record taken to the body frame
+        T W[9], R[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) W[r * 3 + c] = (T)s.inv_inertia[c * 4 + r];
+        quat_to_mat(b.rot, R);
+        conjugate(R, W, b.inv_inertia_local, false);
+    } else {
+        b.inv_inertia_local[0] = (T)s.inv_inertia[0];
+    }
     return b;
 }
 
@@ -1380,6 +1513,16 @@ template <typename T, int D> void store_body(const Body<T, D> &b, slosh_body &s)
     std::memcpy(s.inv_inertia, b.inv_inertia, sizeof(s.inv_inertia));
     s.bc_type = b.bc_type;
     s.bc_friction = (float)b.friction;
+    s.coupling = b.coupling;
+    if constexpr (D == 3) {  // world-space inverse inertia at the current pose
+        T W[9], R[3][3];
+        quat_to_mat(b.rot, R);
+        conjugate(R, b.inv_inertia_local, W, true);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) s.inv_inertia[c * 4 + r] = (float)W[r * 3 + c];
+    } else {
+        s.inv_inertia[0] = (float)b.inv_inertia_local[0];
+    }
 }
 
 // Type-erased context.

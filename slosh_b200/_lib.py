@@ -47,6 +47,8 @@ SHAPE_CAPSULE = 2
 SHAPE_CONE = 3
 SHAPE_CYLINDER = 4
 
+COUPLING_ONE_WAY = 0
+COUPLING_TWO_WAY = 1
 BC_STICK = 0
 BC_SLIP = 1
 BC_SEPARATE = 2
@@ -90,7 +92,8 @@ BODY_DTYPE = np.dtype(
         ("inv_inertia", "<f4", 12),
         ("bc_type", "<u4"),
         ("bc_friction", "<f4"),
-        ("pad", "<u4", 2),
+        ("coupling", "<u4"),
+        ("pad", "<u4"),
     ]
 )
 assert BODY_DTYPE.itemsize == 192

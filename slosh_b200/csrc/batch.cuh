@@ -254,6 +254,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
         (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, b->max_bodies)) ||
+        (st = dalloc(c, &c->body_imp, (size_t)b->max_bodies * 6)) ||
         (st = dalloc(c, &c->ctr, 1)) || (st = dalloc(c, &c->err, 1)) || (st = dalloc(c, &c->small, 4)) ||
         (st = dalloc(c, &b->scene_nblk, b->max_scenes)) || (st = dalloc(c, &b->scene_bbase, b->max_scenes)) ||
         (st = dalloc(c, &b->scene_fill, b->max_scenes)) || (st = dalloc(c, &b->scenes_dev, b->max_scenes)) ||
@@ -267,6 +268,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     cudaMemset(c->ctr, 0, sizeof(Counters));
     cudaMemset(c->err, 0, 4);
     cudaMemset(c->small, 0, 16);
+    cudaMemset(c->body_imp, 0, (size_t)b->max_bodies * 6 * sizeof(unsigned long long));
     cudaMemset(c->mat_hkeys, 0xff, MAT_HASH * 4);
     cudaMemset(b->scene_nblk, 0, b->max_scenes * 4);
     cudaMemset(b->scenes_dev, 0, b->max_scenes * sizeof(SceneRec));
@@ -306,9 +308,11 @@ int batch_validate(slosh_batch *b, const slosh_scene_desc *desc, const slosh_par
     if (n_bodies > MAX_BODIES) return fail(c, SLOSH_E_CAPACITY, "%u bodies exceed %u per scene", n_bodies, MAX_BODIES);
     for (uint32_t k = 0; k < n_bodies; ++k) {
         DevBody d;
-        to_dev_body(bodies[k], d);
+        to_dev_body(bodies[k], d, c->dim);
         if (!(d.scale > 0.f) || !shape_supported(d.shape_type, c->dim))
             return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u or scale", k, d.shape_type);
+        if (d.coupling > SLOSH_COUPLING_TWO_WAY)
+            return fail(c, SLOSH_E_INVALID, "body %u: unknown coupling %u", k, d.coupling);
     }
     uint32_t m = 0;
     for (uint32_t i = 0; i < n; ++i) {
@@ -356,7 +360,7 @@ int batch_stage(slosh_batch *b, const slosh_scene_desc *desc, const slosh_partic
     sg.desc = *desc;
     sg.bodies.resize(n_bodies);
     for (uint32_t k = 0; k < n_bodies; ++k) {
-        to_dev_body(bodies[k], sg.bodies[k]);
+        to_dev_body(bodies[k], sg.bodies[k], c->dim);
         sg.bodies[k].scene = slot;
     }
     slosh_batch::Slot &sl = b->slots[slot];
@@ -404,6 +408,7 @@ int batch_activate(slosh_batch *b, cudaStream_t st) {
         if (c->dim == 3) k_ingest<3, true><<<g, 256, 0, st>>>(s, io, base, sg.n, sg.slot);
         else k_ingest<2, true><<<g, 256, 0, st>>>(s, io, base, sg.n, sg.slot);
         CK(cudaGetLastError());
+        for (const DevBody &db : sg.bodies) c->coll_dynamic |= db.coupling == SLOSH_COUPLING_TWO_WAY ? 1u : 0u;
         if (!sg.bodies.empty())
             CK(cudaMemcpyAsync(c->bodies + b->body_top, sg.bodies.data(), sg.bodies.size() * sizeof(DevBody),
                                cudaMemcpyHostToDevice, st));
@@ -584,7 +589,7 @@ int slosh_batch_get_bodies(slosh_batch *b, uint32_t slot, slosh_body *out, uint3
     CK(cudaStreamSynchronize(c->stream));
     std::vector<DevBody> db(n);
     if (n) CK(cudaMemcpy(db.data(), c->bodies + sl.body_first, n * sizeof(DevBody), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) from_dev_body(db[i], out[i]);
+    for (uint32_t i = 0; i < n; ++i) from_dev_body(db[i], out[i], c->dim);
     return SLOSH_OK;
 }
 

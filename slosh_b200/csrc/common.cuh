@@ -239,8 +239,45 @@ struct DevBody {
     float local_com[3];
     uint32_t bc_type;
     float friction;
-    uint32_t scene;  // owning scene slot (multi-scene batches)
+    uint32_t scene;         // owning scene slot (multi-scene batches)
+    uint32_t coupling;      // SLOSH_COUPLING_*
+    float inv_inertia[9];   // body-frame inverse inertia, row-major (2D: [0])
 };
+
+// Two-way coupling impulses: 64-bit fixed point, 2^40 units per N s, six
+// sums per body (linear xyz, angular xyz; 2D: linear xy, angular in [3]).
+constexpr double IMPULSE_UNITS = 1099511627776.0;  // 2^40
+
+// Rotation matrix of the unit quaternion q = (i, j, k, w).
+__host__ __device__ inline void quat_matrix(const float *q, float (&R)[3][3]) {
+    const float x = q[0], y = q[1], z = q[2], w = q[3];
+    R[0][0] = 1.f - 2.f * (y * y + z * z);
+    R[0][1] = 2.f * (x * y - z * w);
+    R[0][2] = 2.f * (x * z + y * w);
+    R[1][0] = 2.f * (x * y + z * w);
+    R[1][1] = 1.f - 2.f * (x * x + z * z);
+    R[1][2] = 2.f * (y * z - x * w);
+    R[2][0] = 2.f * (x * z - y * w);
+    R[2][1] = 2.f * (y * z + x * w);
+    R[2][2] = 1.f - 2.f * (x * x + y * y);
+}
+
+// out = R M R^T (rot = true) or R^T M R (rot = false) for 3 x 3 M.
+__host__ __device__ inline void rotate_tensor(const float (&R)[3][3], const float *M, float *out, bool rot) {
+    float T[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float a = 0.f;
+            for (int k = 0; k < 3; ++k) a += (rot ? R[i][k] : R[k][i]) * M[k * 3 + j];
+            T[i][j] = a;
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float a = 0.f;
+            for (int k = 0; k < 3; ++k) a += T[i][k] * (rot ? R[j][k] : R[k][j]);
+            out[i * 3 + j] = a;
+        }
+}
 
 // Per-substep device counters.
 struct Counters {

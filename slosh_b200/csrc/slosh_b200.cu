@@ -59,6 +59,8 @@ struct slosh_ctx {
 
     DevBody *bodies = nullptr;
     uint32_t n_bodies = 0;
+    unsigned long long *body_imp = nullptr;  // two-way coupling impulse sums, 6 per body slot
+    uint32_t coll_dynamic = 0;               // some body is coupled two-way
     Counters *ctr = nullptr;
     uint32_t *err = nullptr;
     uint32_t *small = nullptr;  // [0] n_mat, [1] scene flags, [2] debug total
@@ -198,6 +200,8 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.prev_coll_id = c->coll_id[prv];
     s.bodies = c->bodies;
     s.n_bodies = c->n_bodies;
+    s.body_imp = c->body_imp;
+    s.coll_dynamic = c->coll_dynamic;
     s.ctr = c->ctr;
     s.err = c->err;
     s.clr_hkeys = c->hkeys[prv];
@@ -356,7 +360,7 @@ int check_device_error(slosh_ctx *c) {
 
 cudaStream_t pick(slosh_ctx *c, void *stream) { return stream ? (cudaStream_t)stream : c->stream; }
 
-void to_dev_body(const slosh_body &b, DevBody &d) {
+void to_dev_body(const slosh_body &b, DevBody &d, int dim) {
     std::memset(&d, 0, sizeof(d));
     std::memcpy(&d.shape_type, &b.shape_a[3], 4);
     for (int k = 0; k < 4; ++k) {
@@ -374,6 +378,18 @@ void to_dev_body(const slosh_body &b, DevBody &d) {
     d.scale = b.translation[3];
     d.bc_type = b.bc_type;
     d.friction = b.bc_friction;
+    d.coupling = b.coupling;
+    // the record's world-space inverse inertia, taken to the body frame (a
+    // 2D scalar is frame-independent)
+    if (dim == 3) {
+        float W[9], R[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int col = 0; col < 3; ++col) W[r * 3 + col] = b.inv_inertia[col * 4 + r];
+        quat_matrix(b.rotation, R);
+        rotate_tensor(R, W, d.inv_inertia, false);
+    } else {
+        d.inv_inertia[0] = b.inv_inertia[0];
+    }
 }
 
 // Collider shapes the projection handles: ball, cuboid and capsule in 2D and
@@ -383,7 +399,7 @@ bool shape_supported(uint32_t ty, int dim) {
     return dim == 3 && (ty == SLOSH_SHAPE_CYLINDER || ty == SLOSH_SHAPE_CONE);
 }
 
-void from_dev_body(const DevBody &d, slosh_body &b) {
+void from_dev_body(const DevBody &d, slosh_body &b, int dim) {
     std::memset(&b, 0, sizeof(b));
     for (int k = 0; k < 4; ++k) {
         b.shape_a[k] = d.sa[k];
@@ -401,6 +417,16 @@ void from_dev_body(const DevBody &d, slosh_body &b) {
     b.translation[3] = d.scale;
     b.bc_type = d.bc_type;
     b.bc_friction = d.friction;
+    b.coupling = d.coupling;
+    if (dim == 3) {  // world-space inverse inertia at the current pose
+        float W[9], R[3][3];
+        quat_matrix(d.rot, R);
+        rotate_tensor(R, d.inv_inertia, W, true);
+        for (int r = 0; r < 3; ++r)
+            for (int col = 0; col < 3; ++col) b.inv_inertia[col * 4 + r] = W[r * 3 + col];
+    } else {
+        b.inv_inertia[0] = d.inv_inertia[0];
+    }
 }
 
 // Frees the device resources of a context (not the object itself).
@@ -466,6 +492,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->nodes, (size_t)cap * 64)) || (st = dalloc(c, &c->coll[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll[1], (size_t)cap * 64)) || (st = dalloc(c, &c->coll_id[0], (size_t)cap * 64)) ||
         (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, MAX_BODIES)) ||
+        (st = dalloc(c, &c->body_imp, (size_t)MAX_BODIES * 6)) ||
         (st = dalloc(c, &c->ctr, 1)) || (st = dalloc(c, &c->err, 1)) || (st = dalloc(c, &c->small, 4)) ||
         (st = dalloc(c, &c->staging, N)))
         return fail_create(st);
@@ -476,6 +503,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     cudaMemset(c->ctr, 0, sizeof(Counters));
     cudaMemset(c->err, 0, 4);
     cudaMemset(c->slot_counts, 0, (size_t)hcap * CELLS * 4);
+    cudaMemset(c->body_imp, 0, (size_t)MAX_BODIES * 6 * sizeof(unsigned long long));
     if (const char *variant = std::getenv("SLOSH_P2G")) {
         if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;
     }
@@ -665,15 +693,20 @@ int slosh_set_bodies(slosh_ctx *c, const slosh_body *bodies, uint32_t n) {
     if (n > MAX_BODIES) return fail(c, SLOSH_E_CAPACITY, "%u bodies exceed the limit of %u", n, MAX_BODIES);
     std::vector<DevBody> db(n);
     for (uint32_t i = 0; i < n; ++i) {
-        to_dev_body(bodies[i], db[i]);
+        to_dev_body(bodies[i], db[i], c->dim);
         if (!(db[i].scale > 0.f)) return fail(c, SLOSH_E_INVALID, "body %u: scale must be > 0", i);
+        if (db[i].coupling > SLOSH_COUPLING_TWO_WAY)
+            return fail(c, SLOSH_E_INVALID, "body %u: unknown coupling %u", i, db[i].coupling);
         if (!shape_supported(db[i].shape_type, c->dim))
             return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u in %dD", i, db[i].shape_type, c->dim);
     }
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     if (n) CK(cudaMemcpy(c->bodies, db.data(), n * sizeof(DevBody), cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->body_imp, 0, (size_t)MAX_BODIES * 6 * sizeof(unsigned long long)));
     c->n_bodies = n;
+    c->coll_dynamic = 0;
+    for (uint32_t i = 0; i < n; ++i) c->coll_dynamic |= db[i].coupling == SLOSH_COUPLING_TWO_WAY ? 1u : 0u;
     destroy_graphs(c);
     return SLOSH_OK;
 }
@@ -684,7 +717,7 @@ int slosh_get_bodies(slosh_ctx *c, slosh_body *out, uint32_t n) {
     CK(cudaStreamSynchronize(c->stream));
     std::vector<DevBody> db(n);
     if (n) CK(cudaMemcpy(db.data(), c->bodies, n * sizeof(DevBody), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; ++i) from_dev_body(db[i], out[i]);
+    for (uint32_t i = 0; i < n; ++i) from_dev_body(db[i], out[i], c->dim);
     return SLOSH_OK;
 }
 

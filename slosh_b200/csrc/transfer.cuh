@@ -777,7 +777,7 @@ template <int D, bool B = false> __global__ void k_grid_update(DevScene s) {
         uint32_t cid;
         const uint32_t pslot = map_find_prev<B>(s, key, sc);
         const uint32_t prank = (pslot == NONE) ? NONE : s.prev_hvals[pslot];
-        if (prank != NONE) {
+        if (prank != NONE && !s.coll_dynamic) {
             cn = s.prev_coll[(size_t)prank * 64u + node];
             cid = s.prev_coll_id[(size_t)prank * 64u + node];
         } else {
@@ -786,8 +786,57 @@ template <int D, bool B = false> __global__ void k_grid_update(DevScene s) {
         s.coll[t] = cn;
         s.coll_id[t] = cid;
         if (cid != NONE) {
+            const DevBody &bd = bodies[cid];
             const float n[3] = {cn.x, cn.y, cn.z};
-            project_velocity<D>(bodies[cid].bc_type, bodies[cid].friction, vel, n, cn.w - h, dt);
+            if (bd.coupling == SLOSH_COUPLING_TWO_WAY) {
+                // project in the body's frame; the momentum the node loses
+                // goes to the body as an impulse at the node
+                float com[3] = {0.f, 0.f, 0.f}, r[3] = {0.f, 0.f, 0.f}, vb[3] = {0.f, 0.f, 0.f};
+                pose_mul_pt<D>(bd, bd.local_com, com);
+#pragma unroll
+                for (int k = 0; k < D; ++k) r[k] = cell_pos[k] - com[k];
+                if constexpr (D == 3) {
+                    vb[0] = bd.linvel[0] + bd.angvel[1] * r[2] - bd.angvel[2] * r[1];
+                    vb[1] = bd.linvel[1] + bd.angvel[2] * r[0] - bd.angvel[0] * r[2];
+                    vb[2] = bd.linvel[2] + bd.angvel[0] * r[1] - bd.angvel[1] * r[0];
+                } else {
+                    vb[0] = bd.linvel[0] - bd.angvel[0] * r[1];
+                    vb[1] = bd.linvel[1] + bd.angvel[0] * r[0];
+                }
+                float rel[D];
+#pragma unroll
+                for (int k = 0; k < D; ++k) rel[k] = vel[k] - vb[k];
+                project_velocity<D>(bd.bc_type, bd.friction, rel, n, cn.w - h, dt);
+                float J[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    const float nvk = rel[k] + vb[k];
+                    J[k] = mass * (vel[k] - nvk);
+                    vel[k] = nvk;
+                }
+                if (mass > 0.f) {
+                    float A[3];
+                    int na;
+                    if constexpr (D == 3) {
+                        A[0] = r[1] * J[2] - r[2] * J[1];
+                        A[1] = r[2] * J[0] - r[0] * J[2];
+                        A[2] = r[0] * J[1] - r[1] * J[0];
+                        na = 3;
+                    } else {
+                        A[0] = r[0] * J[1] - r[1] * J[0];
+                        na = 1;
+                    }
+                    unsigned long long *acc = s.body_imp + (size_t)(&bd - s.bodies) * 6u;
+#pragma unroll
+                    for (int k = 0; k < D; ++k)
+                        if (J[k] != 0.f) atomicAdd(acc + k, (unsigned long long)__double2ll_rn((double)J[k] * IMPULSE_UNITS));
+                    for (int k = 0; k < na; ++k)
+                        if (A[k] != 0.f)
+                            atomicAdd(acc + 3 + k, (unsigned long long)__double2ll_rn((double)A[k] * IMPULSE_UNITS));
+                }
+            } else {
+                project_velocity<D>(bd.bc_type, bd.friction, vel, n, cn.w - h, dt);
+            }
         }
         s.nodes[t] = make_float4(vel[0], vel[1], D == 3 ? vel[D - 1] : 0.f, mass);
     }
@@ -1126,6 +1175,42 @@ template <int D, bool B = false> __global__ void k_rigid(DevScene s) {
         if (!rec.live) return;
         dt = rec.dt;
         for (int k = 0; k < 3; ++k) grav[k] = rec.gravity[k];
+    }
+    if (b.coupling == SLOSH_COUPLING_TWO_WAY) {
+        // apply_impulse (shaders/slosh/rbd/dynamics/body.slang:62-70) of the
+        // impulse the grid gave this substep, and the velocity caps of
+        // rigid_impulses.slang:99-111; the sums restart at zero
+        float h = s.h;
+        if constexpr (B) h = s.scenes[b.scene].h;
+        unsigned long long *acc = s.body_imp + (size_t)id * 6u;
+        float jl[3] = {0.f, 0.f, 0.f}, ja[3] = {0.f, 0.f, 0.f};
+        for (int k = 0; k < 3; ++k) {
+            jl[k] = (float)((double)(long long)acc[k] / IMPULSE_UNITS);
+            ja[k] = (float)((double)(long long)acc[3 + k] / IMPULSE_UNITS);
+            acc[k] = 0ull;
+            acc[3 + k] = 0ull;
+        }
+        for (int k = 0; k < D; ++k) b.linvel[k] += b.inv_mass[k] * jl[k];
+        if constexpr (D == 3) {
+            float R[3][3], Iw[9];
+            quat_matrix(b.rot, R);
+            rotate_tensor(R, b.inv_inertia, Iw, true);
+            for (int i = 0; i < 3; ++i) b.angvel[i] += Iw[i * 3] * ja[0] + Iw[i * 3 + 1] * ja[1] + Iw[i * 3 + 2] * ja[2];
+        } else {
+            b.angvel[0] += b.inv_inertia[0] * ja[0];
+        }
+        const bool pushed = jl[0] != 0.f || jl[1] != 0.f || jl[2] != 0.f || ja[0] != 0.f || ja[1] != 0.f || ja[2] != 0.f;
+        if (pushed) {
+            const float lin_limit = 0.1f * h / dt, ang_limit = 1.0f;
+            float l2 = 0.f, a2 = 0.f;
+            for (int k = 0; k < D; ++k) l2 += b.linvel[k] * b.linvel[k];
+            for (int k = 0; k < (D == 3 ? 3 : 1); ++k) a2 += b.angvel[k] * b.angvel[k];
+            const float ln = sqrtf(l2), an = sqrtf(a2);
+            if (ln > lin_limit)
+                for (int k = 0; k < D; ++k) b.linvel[k] = b.linvel[k] * (lin_limit / ln);
+            if (an > ang_limit)
+                for (int k = 0; k < (D == 3 ? 3 : 1); ++k) b.angvel[k] = b.angvel[k] * (ang_limit / an);
+        }
     }
     float init_com[3] = {0.f, 0.f, 0.f};
     pose_mul_pt<D>(b, b.local_com, init_com);

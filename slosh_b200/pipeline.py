@@ -207,7 +207,11 @@ class RigidBody:
     with a, b the segment end points, or in 3D ("cylinder", (half_height,
     radius)) or ("cone", (half_height, radius)) around the local y axis
     (GpuShape layouts, shaders/slosh/rbd/shapes/shape.slang:37-80).  Rotation
-    is a unit quaternion (i, j, k, w) in 3D or an angle in radians in 2D."""
+    is a unit quaternion (i, j, k, w) in 3D or an angle in radians in 2D.
+    ``coupling`` is "one_way" (slosh's GPU behaviour: the particles never
+    push the body) or "two_way" (the grid's contact impulses move it; see
+    :meth:`two_way`).  ``inv_inertia`` is the world-space inverse inertia at
+    this pose: a 3x3 matrix in 3D, a scalar in 2D."""
 
     shape: tuple
     translation: Sequence[float] = (0.0, 0.0, 0.0)
@@ -218,6 +222,23 @@ class RigidBody:
     local_com: Sequence[float] = (0.0, 0.0, 0.0)
     boundary_condition: GpuBoundaryCondition = field(default_factory=GpuBoundaryCondition.default)
     scale: float = 1.0
+    inv_inertia: object = None
+    coupling: str = "one_way"
+
+    @classmethod
+    def two_way(cls, shape: tuple, density: float, dim: int, **kw) -> "RigidBody":
+        """A dynamic body coupled two-way, with the mass properties of its
+        shape (cuboid or ball, scaled by ``scale``) at ``density``, centre of
+        mass at the shape's origin."""
+        body = cls(shape, coupling="two_way", **kw)
+        m, inertia = shape_mass_properties(shape, density, dim, body.scale)
+        body.inv_mass = (1.0 / m,) * 3 if dim == 3 else (1.0 / m, 1.0 / m, 0.0)
+        if dim == 3:
+            rot = quat_to_matrix(body.rotation)
+            body.inv_inertia = rot @ np.diag(1.0 / np.asarray(inertia)) @ rot.T
+        else:
+            body.inv_inertia = 1.0 / float(inertia)
+        return body
 
     def record(self, dim: int) -> np.ndarray:
         r = np.zeros((), dtype=BODY_DTYPE)
@@ -258,7 +279,52 @@ class RigidBody:
             r[name][:3] = v[:3]
         r["bc_type"] = self.boundary_condition.ty
         r["bc_friction"] = self.boundary_condition.friction
+        if self.inv_inertia is not None:
+            if dim == 3:
+                m = np.asarray(self.inv_inertia, np.float64).reshape(3, 3)
+                for c in range(3):
+                    r["inv_inertia"][4 * c : 4 * c + 3] = m[:, c]
+            else:
+                r["inv_inertia"][0] = float(self.inv_inertia)
+        modes = {"one_way": _lib.COUPLING_ONE_WAY, "two_way": _lib.COUPLING_TWO_WAY}
+        if self.coupling not in modes:
+            raise ValueError(f"unknown coupling {self.coupling!r}")
+        r["coupling"] = modes[self.coupling]
         return r
+
+
+def shape_mass_properties(shape: tuple, density: float, dim: int, scale: float = 1.0):
+    """Mass and principal inertia (3D: the three moments; 2D: the scalar)
+    of a uniform cuboid or ball about its centre."""
+    kind, param = shape
+    if kind == "cuboid":
+        he = [float(v) * scale for v in list(param)[:dim]]
+        if dim == 3:
+            m = density * 8.0 * he[0] * he[1] * he[2]
+            return m, (m / 3.0 * (he[1] ** 2 + he[2] ** 2), m / 3.0 * (he[0] ** 2 + he[2] ** 2),
+                       m / 3.0 * (he[0] ** 2 + he[1] ** 2))
+        m = density * 4.0 * he[0] * he[1]
+        return m, m / 3.0 * (he[0] ** 2 + he[1] ** 2)
+    if kind == "ball":
+        r = float(param) * scale
+        if dim == 3:
+            m = density * 4.0 / 3.0 * math.pi * r**3
+            return m, (0.4 * m * r * r,) * 3
+        m = density * math.pi * r * r
+        return m, 0.5 * m * r * r
+    raise ValueError(f"mass properties of {kind!r} are not implemented")
+
+
+def quat_to_matrix(q: Sequence[float]) -> np.ndarray:
+    """Rotation matrix of the unit quaternion (i, j, k, w)."""
+    x, y, z, w = (float(v) for v in q)
+    return np.array(
+        [
+            [1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+            [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+            [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)],
+        ]
+    )
 
 
 def quat_from_axis_angle(axis: Sequence[float], angle: float) -> tuple:

@@ -7,6 +7,8 @@ generated from a lattice with seeded jitter).
 * ``sand_column_3d``   Drucker-Prager sand cylinder + a rigid cuboid
 * ``random_scene_3d``  a box-shaped blob of one material on a floor (the
                        batched / served scenes)
+* ``two_way_impact``   an elastic box hitting a free ball coupled two-way
+                       (no gravity: total momentum is conserved)
 
 The cell width is a parameter so tests can build the same scenes at small
 particle counts.
@@ -140,12 +142,13 @@ def elastic_drop_3d(h: float = 1.0 / 128.0, seed: int = 2, substeps: int = 2000)
     )
 
 
-def sand_column_3d(h: float = 1.0 / 256.0, seed: int = 3, substeps: int = 500) -> Scene:
+def sand_column_3d(h: float = 1.0 / 256.0, seed: int = 3, substeps: int = 500, cube_coupling: str = "one_way") -> Scene:
     """Drucker-Prager sand (friction angle 30 deg, E = 3.5e5, nu = 0.3,
     density 2200): a cylinder of radius 0.15 and height 0.5 standing on a
     Separate(1.0) floor at y = 0.05, axis through (0.5, ., 0.5), 8 jittered
     particles per cell, plus a 0.1^3 rigid cuboid (density 500) resting 2h
-    above the column, coupled as a collider (one-way).  dt = 2e-5."""
+    above the column, coupled as a collider (one-way; ``cube_coupling``
+    "two_way" makes it a dynamic body the sand pushes).  dt = 2e-5."""
     rng = np.random.default_rng(seed)
     r, height, base = 0.15, 0.5, 0.05
     sp = h / 2
@@ -157,10 +160,12 @@ def sand_column_3d(h: float = 1.0 / 256.0, seed: int = 3, substeps: int = 500) -
     t = 4.0 * h
     floor = RigidBody(("cuboid", (2.0, t, 2.0)), translation=(0.5, base - t, 0.5))
     cube_half = 0.05
-    cube = RigidBody(
-        ("cuboid", (cube_half, cube_half, cube_half)),
-        translation=(0.5, base + height + 2 * h + cube_half, 0.5),
-    )
+    cube_shape = ("cuboid", (cube_half, cube_half, cube_half))
+    cube_pos = (0.5, base + height + 2 * h + cube_half, 0.5)
+    if cube_coupling == "two_way":
+        cube = RigidBody.two_way(cube_shape, 500.0, 3, translation=cube_pos)
+    else:
+        cube = RigidBody(cube_shape, translation=cube_pos)
     return Scene(
         "sand_column_3d",
         3,
@@ -212,6 +217,33 @@ def random_scene_3d(
     )
 
 
+def two_way_impact(dim: int = 3, h: float = 1.0 / 32.0, seed: int = 6, substeps: int = 100) -> Scene:
+    """A box of fixed-corotated material (E = 1e4, nu = 0.3, density 1000),
+    side 0.12, moving at 1 m/s along +x into a free ball of radius 0.06
+    (density 1000) at (0.5, 0.5[, 0.5]) coupled two-way, its surface 0.02
+    from the box.  No gravity and no other collider, so the total momentum of
+    particles and ball is conserved.  2^D jittered particles per cell,
+    dt = 1e-4."""
+    rng = np.random.default_rng(seed)
+    lo = (0.30,) + (0.44,) * (dim - 1)
+    hi = (0.42,) + (0.56,) * (dim - 1)
+    pts = _jitter(_lattice(lo, hi, h / 2), h / 4, rng)
+    parts = make_particles(pts, h / 4, 1000.0, ParticleModel.elastic(1.0e4, 0.3), dim=dim)
+    parts["velocity"][:, 0] = 1.0
+    centre = (0.5,) * dim
+    ball = RigidBody.two_way(("ball", 0.06), 1000.0, dim, translation=centre, rotation=(0.0, 0.0, 0.0, 1.0) if dim == 3 else 0.0)
+    return Scene(
+        f"two_way_impact_{dim}d",
+        dim,
+        h,
+        SimulationParams((0.0,) * dim, 1.0e-4),
+        parts,
+        [ball],
+        substeps,
+        _grid_capacity(len(parts), 2**dim, dim),
+    )
+
+
 def build_mpm_data(scene: Scene, device: int = 0, max_particles: int | None = None):
     from .pipeline import MpmData
 
@@ -233,6 +265,7 @@ __all__ = [
     "elastic_drop_3d",
     "sand_column_3d",
     "random_scene_3d",
+    "two_way_impact",
     "build_mpm_data",
     "quat_from_axis_angle",
 ]

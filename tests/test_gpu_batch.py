@@ -191,3 +191,24 @@ def test_batch_2d_alone_vs_mix_and_context(cuda_lib):
     got = mix.download_particles(s1)
     mix.close()
     assert got.tobytes() == ref.tobytes()
+
+
+def test_two_way_scene_in_batch_matches_context(cuda_lib):
+    """A scene with a two-way coupled ball advances in a batch next to other
+    scenes as it does in its own context (ball and particles)."""
+    sc = scenes.two_way_impact(3, h=1 / 64)
+    data = scenes.build_mpm_data(sc)
+    MpmPipeline().launch_step(data, 20)
+    single, single_body = data.download_particles(), data.get_bodies()[0]
+    data.close()
+    b = new_batch()
+    b.add(scenes.random_scene_3d(6000, "sand", 1 / 64, seed=11))
+    slot = b.add(sc)
+    b.step(20)
+    got, body = b.download_particles(slot), b.get_bodies(slot)[0]
+    b.close()
+    assert body["linvel"][0] > 1e-3
+    for k in ("linvel", "angvel", "translation", "rotation"):
+        close(f"batched ball {k}", body[k][:3], single_body[k][:3], 1e-7, 1e-5)
+    for k, v in fields(single).items():
+        close(f"batched two-way scene {k}", got[k], v, 1e-7, 1e-6)

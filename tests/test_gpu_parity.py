@@ -392,3 +392,53 @@ def test_append_and_shift_remove(cuda_lib):
     compare_particles("after shift_remove", data.download_particles(), orc.get_particles(), 3, loose=10.0)
     assert data.shift_remove(len(after) - 10, len(after) + 50) == 10  # clamped to the count
     data.close()
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_two_way_coupling_parity(cuda_lib, dim):
+    """Two-way coupling against the oracle's restatement: particles and the
+    pushed ball after 30 substeps of the impact scene."""
+    sc = scenes.two_way_impact(dim, h=1 / 64)
+    data, orc = pair(sc)
+    MpmPipeline().launch_step(data, 30)
+    orc.step(30)
+    gb, ob = data.get_bodies()[0], orc.get_bodies()[0]
+    assert gb["linvel"][0] > 1e-3
+    close("ball linvel", gb["linvel"][:dim], ob["linvel"][:dim], 1e-5, 1e-3)
+    na = 3 if dim == 3 else 1
+    close("ball angvel", gb["angvel"][:na], ob["angvel"][:na], 1e-3, 1e-2)
+    close("ball translation", gb["translation"][:dim], ob["translation"][:dim], 1e-6, 0)
+    compare_particles(f"two-way {dim}D", data.download_particles(), orc.get_particles(), dim, loose=10.0)
+    data.close()
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_two_way_coupling_conserves_momentum(cuda_lib, dim):
+    """No gravity, no other collider: particles + ball keep the initial
+    momentum (FP32 state; the impulse sums are exact integers)."""
+    sc = scenes.two_way_impact(dim, h=1 / 64)
+    p0 = (sc.particles["velocity"][:, :dim].astype(np.float64) * sc.particles["mass"][:, None]).sum(0)
+    data = scenes.build_mpm_data(sc)
+    MpmPipeline().launch_step(data, 100)
+    p = data.download_particles()
+    b = data.get_bodies()[0]
+    part = (p["velocity"][:, :dim].astype(np.float64) * p["mass"].astype(np.float64)[:, None]).sum(0)
+    ball = b["linvel"][:dim].astype(np.float64) / b["inv_mass"][0]
+    err = np.abs(part + ball - p0).max() / np.abs(p0).max()
+    print(f"{dim}D: ball momentum {ball}, relative total error {err:.2e}")
+    assert err < 2e-5
+    assert ball[0] > 0.02 * p0[0]
+    data.close()
+
+
+def test_two_way_coupling_bit_reproducible(cuda_lib):
+    """The fixed-point impulse sums are order independent, so the coupled
+    substep stays bit-reproducible."""
+    sc = scenes.two_way_impact(3, h=1 / 64)
+    runs = []
+    for _ in range(2):
+        data = scenes.build_mpm_data(sc)
+        MpmPipeline().launch_step(data, 40)
+        runs.append((data.download_particles().tobytes(), data.get_bodies().tobytes()))
+        data.close()
+    assert runs[0] == runs[1]

@@ -61,6 +61,7 @@ def test_record_layouts_match_c_structs(tmp_path):
                  sizeof(slosh_tuning), sizeof(slosh_batch_stats), offsetof(slosh_batch_stats, tuning));
           printf("%zu %zu %zu %zu %zu\\n", sizeof(slosh_server_config), sizeof(slosh_request),
                  offsetof(slosh_request, particles), sizeof(slosh_completion), sizeof(slosh_server_stats));
+          printf("%zu\\n", offsetof(slosh_body, coupling));
           return 0;
         }
         """
@@ -77,6 +78,7 @@ def test_record_layouts_match_c_structs(tmp_path):
     assert vals[3] == B.itemsize
     assert vals[4] == B.fields["bc_type"][1]
     assert vals[5] == 52
+    assert vals[-1] == B.fields["coupling"][1]
     import ctypes
 
     assert vals[6] == ctypes.sizeof(_lib.SloshGridDump)

@@ -319,3 +319,40 @@ def test_collider_shape_projections(oracle_lib):
     proj, inside = oracle_lib.project_on_boundary(2, rec2, (0.05, 0.3))
     assert not inside and abs(np.linalg.norm(proj - np.array([0.05, 0.3])) - (0.3 - 0.025 - 0.05)) < 0.02
     assert oracle_lib.project_on_boundary(2, RigidBody(("cone", (0.1, 0.1))).record(3), (0.0, 0.0)) is None
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_two_way_coupling_conserves_momentum(oracle_lib, dim):
+    """Two-way coupling: the momentum a grid node loses at the ball's
+    boundary goes to the ball, so with no gravity and no other collider the
+    total momentum of particles and ball stays that of the initial push,
+    while the ball picks up a share of it."""
+    sc = scenes.two_way_impact(dim)
+    o = oracle_lib.from_scene(sc, double=True, threads=2)
+
+    def momenta():
+        p, b = o.get_particles(), o.get_bodies()[0]
+        m = p["mass"].astype(np.float64)
+        part = (p["velocity"][:, :dim].astype(np.float64) * m[:, None]).sum(0)
+        return part, b["linvel"][:dim].astype(np.float64) / b["inv_mass"][0], b
+
+    p0, b0, _ = momenta()
+    assert np.all(b0 == 0.0)
+    o.step(60)
+    p1, b1, b = momenta()
+    err = np.abs(p1 + b1 - p0).max() / np.abs(p0).max()
+    print(f"{dim}D: particles {p1}, ball {b1}, relative momentum error {err:.2e}")
+    assert err < 1e-7
+    assert b1[0] > 0.05 * p0[0]
+    assert b["translation"][0] > 0.5  # the ball moved along the push
+
+
+def test_one_way_body_is_not_pushed(oracle_lib):
+    """The reference's coupling: the same ball coupled one-way keeps its
+    velocity (zero) whatever hits it."""
+    sc = scenes.two_way_impact(3)
+    sc.bodies[0].coupling = "one_way"
+    o = oracle_lib.from_scene(sc, double=True, threads=2)
+    o.step(30)
+    b = o.get_bodies()[0]
+    assert np.all(b["linvel"][:3] == 0.0) and np.all(b["angvel"][:3] == 0.0)
