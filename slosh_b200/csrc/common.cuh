@@ -288,7 +288,9 @@ struct Counters {
     uint32_t n_svd_fp64;     // particles whose SVD fell back to FP64 (cumulative)
     uint32_t last_n_blocks;  // n_blocks of the last completed substep
     uint32_t last_n_primary; // n_primary of the last completed substep
-    uint32_t pad;
+    uint32_t p2g_next;       // next block for a P2G warp (reset by k_block_setup)
+    uint32_t g2p_next;       // next block for a G2P CTA (reset by k_block_setup)
+    uint32_t pad[3];
 };
 
 }  // namespace slosh

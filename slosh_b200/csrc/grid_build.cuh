@@ -567,6 +567,10 @@ template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t lane = lane_id();
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // the transfer kernels' block queues, read after this kernel
+        s.ctr->p2g_next = 0u;
+        s.ctr->g2p_next = 0u;
+    }
     for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
         const uint32_t sl = s.bslot[r];
         uint32_t *cnt = s.slot_counts + ((size_t)sl << 6);

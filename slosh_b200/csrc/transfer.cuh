@@ -152,8 +152,14 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
     const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
     float4 *tiles = stile[wl];
     float h = s.h, inv_h = 1.0f / s.h;
-    const uint32_t nwarps = gridDim.x * P2G_WARPS;
-    for (uint32_t r = blockIdx.x * P2G_WARPS + wl; r < nb; r += nwarps) {
+    // blocks are taken from a queue (one atomic a block), so warps that get
+    // light blocks take more of them
+    auto next_block = [&]() {
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(&s.ctr->p2g_next, 1u);
+        return __shfl_sync(FULL_MASK, q, 0);
+    };
+    for (uint32_t r = next_block(); r < nb; r = next_block()) {
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
@@ -900,7 +906,14 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
         }
         cp_async_commit();
     };
-    for (uint32_t r = blockIdx.x; r < nb; r += gridDim.x) {
+    // blocks are taken from a queue, one atomic a block
+    __shared__ uint32_t next_r;
+    for (;;) {
+        __syncthreads();  // every thread has read next_r
+        if (tid == 0) next_r = atomicAdd(&s.ctr->g2p_next, 1u);
+        __syncthreads();
+        const uint32_t r = next_r;
+        if (r >= nb) break;
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
