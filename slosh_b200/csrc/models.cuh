@@ -128,9 +128,12 @@ template <int D>
 __device__ __forceinline__ void drucker_prager(float *st, const float *p, SvdD<D> &sv, float (&F)[D][D]) {
     const float ha = p[0], hb = p[1], hc = p[2], hd = p[3], lambda = p[4], mu = p[5];
     const float q = st[1];
-    const float angle = ha + (hb * q - hd) * expf(-hc * q);
-    const float s_angle = sinf(angle);
-    const float alpha = sqrtf(2.0f / 3.0f) * (2.0f * s_angle) / (3.0f - s_angle);
+    // The friction angle and the cone slope only place the yield surface:
+    // the hardware approximations (a few ulp) are used for them; the terms
+    // that enter F and the plastic state keep the correctly rounded forms.
+    const float angle = ha + (hb * q - hd) * __expf(-hc * q);
+    const float s_angle = __sinf(angle);
+    const float alpha = __fdividef(sqrtf(2.0f / 3.0f) * (2.0f * s_angle), 3.0f - s_angle);
     const float d = (float)D;
     float strain[D], ls[D], tr = 0.f;
 #pragma unroll
@@ -165,9 +168,9 @@ __device__ __forceinline__ void drucker_prager(float *st, const float *p, SvdD<D
 #pragma unroll
         for (int i = 0; i < D; ++i) n2 += dev[i] * dev[i];
         const float devn = sqrtf(n2);
-        const float gamma = devn + (d * lambda + 2.0f * mu) / (2.0f * mu) * tr * alpha;
+        const float gamma = devn + __fdividef(d * lambda + 2.0f * mu, 2.0f * mu) * tr * alpha;
         if (gamma <= 0.f) return;
-        const float g = gamma / devn;
+        const float g = __fdividef(gamma, devn);
 #pragma unroll
         for (int i = 0; i < D; ++i) {
             hh[i] = strain[i] - dev[i] * g;
