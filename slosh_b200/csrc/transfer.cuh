@@ -143,10 +143,15 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
     constexpr int NACC = (D == 3) ? 9 : 3;
     constexpr int PY = SlabTile<D>::PY, PZ = SlabTile<D>::PZ, SSZ = SlabTile<D>::SIZE;
     constexpr int Q = MQ<D>::Q;
+    // Staging: the particles of a pass's cells (at most 12: 32 lanes, 3 slab
+    // lanes a cell, the first and last cell possibly shared with the
+    // neighbouring passes) in NBUF buffers; particle k + NBUF - 1 of every
+    // cell is copied while particle k is summed.
+    constexpr int NBUF = 3, CS = 12;
     __shared__ float4 stile[P2G_WARPS][3 * SSZ];
-    __shared__ float4 sp_pm[P2G_WARPS][2][32];
-    __shared__ float4 sp_vv[P2G_WARPS][2][32];
-    __shared__ float4 sp_cq[P2G_WARPS][2][Q][32];
+    __shared__ float4 sp_pm[P2G_WARPS][NBUF][CS];
+    __shared__ float4 sp_vv[P2G_WARPS][NBUF][CS];
+    __shared__ float4 sp_cq[P2G_WARPS][NBUF][Q][CS];
     const uint32_t nb = s.ctr->n_blocks;
     const size_t n = s.n;
     const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
@@ -197,36 +202,49 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
             float4 acc[NACC];
 #pragma unroll
             for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-            // copies of entry j (storage index i); the index of entry j + 2 is
-            // loaded one iteration ahead of the copies that need it
-            auto stage = [&](int b, uint32_t j, uint32_t i) {
-                if (j < hi) {
-                    cp_async16(&sp_pm[wl][b][lane], &s.pm[i]);
-                    cp_async16(&sp_vv[wl][b][lane], &s.vv[i]);
+            // The first lane of each cell in this pass (its slab-0 lane, or
+            // lane 0 for a cell begun in the previous pass) copies the cell's
+            // particles into the cell's staging slot; the three slab lanes
+            // of a cell read the same slot.  The lanes step through particle
+            // k together (k up to the pass's largest count, lane 0's), so the
+            // warp can sync around the copies.
+            const uint32_t cnt = hi - lo, kmax = __shfl_sync(FULL_MASK, cnt, 0);
+            const uint32_t cs = item / 3u - (32u * pass) / 3u;
+            const bool loader = slab == 0 || lane == 0;
+            auto stage = [&](uint32_t k, uint32_t i) {
+                if (loader && k < cnt) {
+                    const int b = (int)(k % NBUF);
+                    cp_async16(&sp_pm[wl][b][cs], &s.pm[i]);
+                    cp_async16(&sp_vv[wl][b][cs], &s.vv[i]);
 #pragma unroll
-                    for (int q = 0; q < Q; ++q) cp_async16(&sp_cq[wl][b][q][lane], &s.cq[q * n + i]);
+                    for (int q = 0; q < Q; ++q) cp_async16(&sp_cq[wl][b][q][cs], &s.cq[q * n + i]);
                 }
                 cp_async_commit();
             };
-            uint32_t i_cur = lo < hi ? s.perm[first + lo] : 0u;
-            uint32_t i_next = lo + 1 < hi ? s.perm[first + lo + 1] : 0u;
-            stage(0, lo, i_cur);
-            int buf = 0;
-            for (uint32_t j = lo; j < hi; ++j, buf ^= 1) {
-                stage(buf ^ 1, j + 1, i_next);
-                const uint32_t i = i_cur;
-                i_cur = i_next;
-                i_next = j + 2 < hi ? s.perm[first + j + 2] : 0u;
-                cp_async_wait<1>();
-                float fdt[3] = {0.f, 0.f, 0.f};
-                if (s.force_pending)
+            auto index = [&](uint32_t k) { return (loader && k < cnt) ? s.perm[first + lo + k] : 0u; };
+            stage(0u, index(0u));
+            stage(1u, index(1u));
+            uint32_t i_next = index(2u);  // loaded one iteration before its copies
+            for (uint32_t k = 0; k < kmax; ++k) {
+                stage(k + 2u, i_next);
+                i_next = index(k + 3u);
+                cp_async_wait<NBUF - 1>();
+                __syncwarp();  // the loaders' copies of particle k have landed
+                if (k < cnt) {
+                    const int b = (int)(k % NBUF);
+                    float fdt[3] = {0.f, 0.f, 0.f};
+                    if (s.force_pending) {
+                        const uint32_t i = s.perm[first + lo + k];
 #pragma unroll
-                    for (int k = 0; k < D; ++k) fdt[k] = s.fdt[k * n + i];
-                float4 cv[Q];
+                        for (int d = 0; d < D; ++d) fdt[d] = s.fdt[d * n + i];
+                    }
+                    float4 cv[Q];
 #pragma unroll
-                for (int q = 0; q < Q; ++q) cv[q] = sp_cq[wl][buf][q][lane];
-                if (!p2g_particle<D>(sp_pm[wl][buf][lane], sp_vv[wl][buf][lane], cv, fdt, assoc, h, inv_h, slab, acc))
-                    atomicOr(s.err, ERR_KEY_RANGE);
+                    for (int q = 0; q < Q; ++q) cv[q] = sp_cq[wl][b][q][cs];
+                    if (!p2g_particle<D>(sp_pm[wl][b][cs], sp_vv[wl][b][cs], cv, fdt, assoc, h, inv_h, slab, acc))
+                        atomicOr(s.err, ERR_KEY_RANGE);
+                }
+                __syncwarp();  // slot k % NBUF is refilled by the next iteration's copies
             }
             cp_async_wait<0>();
             __syncwarp();
