@@ -222,12 +222,12 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
                 cp_async_commit();
             };
             auto index = [&](uint32_t k) { return (loader && k < cnt) ? s.perm[first + lo + k] : 0u; };
-            stage(0u, index(0u));
-            stage(1u, index(1u));
-            uint32_t i_next = index(2u);  // loaded one iteration before its copies
+#pragma unroll
+            for (uint32_t k = 0; k + 1 < (uint32_t)NBUF; ++k) stage(k, index(k));
+            uint32_t i_next = index(NBUF - 1u);  // loaded one iteration before its copies
             for (uint32_t k = 0; k < kmax; ++k) {
-                stage(k + 2u, i_next);
-                i_next = index(k + 3u);
+                stage(k + NBUF - 1u, i_next);
+                i_next = index(k + NBUF);
                 cp_async_wait<NBUF - 1>();
                 __syncwarp();  // the loaders' copies of particle k have landed
                 if (k < cnt) {
