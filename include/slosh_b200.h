@@ -89,6 +89,7 @@ typedef struct slosh_particle {
 #define SLOSH_SHAPE_CAPSULE 2u   /* 2D and 3D */
 #define SLOSH_SHAPE_CONE 3u      /* 3D, axis along local y */
 #define SLOSH_SHAPE_CYLINDER 4u  /* 3D, axis along local y */
+#define SLOSH_SHAPE_TRIMESH 6u   /* 3D triangle mesh, made by slosh_add_trimesh */
 
 /* Boundary conditions: src/solver/boundary_condition.rs:14-19. */
 #define SLOSH_BC_STICK 0u
@@ -127,6 +128,9 @@ typedef struct slosh_particle {
  *             the segment a-b inflated by the radius
  *   cone, cylinder: shape_a = (half_height, radius, -, type); a cone's apex
  *             is at +half_height, its base disc at -half_height
+ *   trimesh:  shape_a = (vertex offset, index offset, BVH nodes, type),
+ *             shape_b = (triangles, vertices, mesh ordinal, -), all uint32
+ *             bits, as slosh_add_trimesh writes them
  * where `type` is the shape type stored as uint32 bits.  The pose is a
  * similarity: rotation (3D unit quaternion i,j,k,w; 2D cos,sin), translation
  * xyz and uniform scale in translation[3].  Bodies coupled one-way (the
@@ -217,6 +221,19 @@ int slosh_set_bodies(slosh_ctx *ctx, const slosh_body *bodies, uint32_t n);
 
 /* Reads the bodies back (poses and velocities after integration). */
 int slosh_get_bodies(slosh_ctx *ctx, slosh_body *out, uint32_t n);
+
+/* Adds a triangle-mesh collider shape (3D).  Replaces GpuShape::from_parry
+ * for a TriMesh with convert_trimesh_to_gpu (src/rbd/shapes.rs:231-239;
+ * src/trimesh.rs:23-103): builds the mesh's BVH and its vertex and edge
+ * pseudo-normals, appends them to the context's mesh buffers and writes the
+ * trimesh shape into body->shape_a / shape_b; the pose, velocities, mass and
+ * boundary condition of `body` are the caller's.  `vertices` holds x, y, z a
+ * vertex; `indices` three vertex indices a triangle, counter-clockwise seen
+ * from outside.  Heightfields are passed as their triangle meshes, as slosh
+ * converts them (src/rbd/shapes.rs:241-269).  The grid update projects a node
+ * on the mesh only within 1.5 cells of its surface (collide.slang:124-134). */
+int slosh_add_trimesh(slosh_ctx *ctx, const float *vertices, uint32_t n_vertices, const uint32_t *indices,
+                      uint32_t n_triangles, slosh_body *body);
 
 /* Enqueues `n_substeps` substeps on `stream` without any host round trip.
  * Replaces MpmPipeline::launch_step (src/pipeline.rs:562-770) called

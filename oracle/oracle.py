@@ -66,6 +66,11 @@ def load() -> ctypes.CDLL:
             "orc_model_stress": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
             "orc_timestep_bound": (ctypes.c_uint32, [_P]),
             "orc_project": (ctypes.c_int, [ctypes.c_uint32, _P, _P, _P, _P]),
+            "orc_add_trimesh": (ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32]),
+            "orc_project_trimesh": (
+                ctypes.c_int,
+                [_P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P, _P],
+            ),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(lib, name)
@@ -90,6 +95,20 @@ def project_on_boundary(dim: int, body_record, point) -> tuple[np.ndarray, bool]
     inside = ctypes.c_int(0)
     ok = lib.orc_project(dim, _p(rec), _p(pt), _p(out), ctypes.byref(inside))
     return (out[:dim].copy(), bool(inside.value)) if ok else None
+
+
+def project_on_trimesh(vertices, triangles, body_record, point, cap: float):
+    """Closest point on a posed triangle mesh within `cap` and the inside
+    flag (FP64 scan of all triangles), or None."""
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+    rec = np.ascontiguousarray(body_record)
+    pt = np.zeros(3, np.float32)
+    pt[: len(point)] = point
+    out = np.zeros(3, np.float32)
+    inside = ctypes.c_int(0)
+    ok = load().orc_project_trimesh(_p(v), len(v), _p(t), len(t), _p(rec), _p(pt), float(cap), _p(out), ctypes.byref(inside))
+    return (out, bool(inside.value)) if ok else None
 
 
 def prefix_sum(values) -> np.ndarray:
@@ -140,7 +159,24 @@ class Oracle:
         self.n = len(recs)
         assert self.lib.orc_set_particles(self.ctx, _p(recs), self.n) == 0
 
-    def set_bodies(self, recs: np.ndarray):
+    def set_bodies(self, recs: np.ndarray, bodies=None):
+        """`bodies`: the RigidBody objects of the records, whose triangle
+        meshes are added here (each record then names its mesh by ordinal)."""
+        recs = np.array(recs, copy=True)
+        if bodies is not None:
+            if not hasattr(self, "_meshes"):
+                self._meshes = {}
+            for i, b in enumerate(bodies):
+                if b.shape[0] != "trimesh":
+                    continue
+                key = id(b.shape[1][0])
+                if key not in self._meshes:
+                    v = np.ascontiguousarray(b.shape[1][0], np.float32).reshape(-1, 3)
+                    t = np.ascontiguousarray(b.shape[1][1], np.uint32).reshape(-1, 3)
+                    ordinal = self.lib.orc_add_trimesh(self.ctx, _p(v), len(v), _p(t), len(t))
+                    assert ordinal >= 0
+                    self._meshes[key] = (ordinal, b.shape[1])
+                recs[i]["shape_b"].view(np.uint32)[2] = self._meshes[key][0]
         recs = np.ascontiguousarray(recs)
         assert recs.dtype.itemsize == BODY_ITEMSIZE
         assert self.lib.orc_set_bodies(self.ctx, _p(recs) if len(recs) else None, len(recs)) == 0
@@ -239,6 +275,6 @@ def from_scene(scene, double: bool = False, threads: int = 0) -> Oracle:
     recs = np.zeros(len(scene.bodies), dtype=BODY_DTYPE)
     for i, b in enumerate(scene.bodies):
         recs[i] = b.record(scene.dim)
-    o.set_bodies(recs)
+    o.set_bodies(recs, scene.bodies)
     o.set_particles(scene.particles)
     return o

@@ -384,8 +384,165 @@ template <typename T, int D> struct Particles {
     std::vector<T> model;  // n * 12 model payload words
 };
 
+// Triangle mesh of a trimesh collider (3D): vertices (3 a vertex), triangles
+// (3 vertex indices), and the pseudo-normals of Baerentzen and Aanaes (2005):
+// per vertex the angle-weighted sum of the incident unit face normals, per
+// edge the sum of its faces' unit normals (3 a triangle: AB, BC, CA).
+template <typename T> struct Mesh {
+    std::vector<T> v, vpn, epn;
+    std::vector<uint32_t> tri;
+};
+
+template <typename T> Mesh<T> make_mesh(const float *v, uint32_t nv, const uint32_t *tri, uint32_t nt) {
+    Mesh<T> m;
+    m.v.assign(v, v + 3 * (size_t)nv);
+    m.tri.assign(tri, tri + 3 * (size_t)nt);
+    m.vpn.assign(3 * (size_t)nv, T(0));
+    m.epn.assign(9 * (size_t)nt, T(0));
+    std::unordered_map<uint64_t, std::array<T, 3>> edge;
+    std::vector<T> fn(3 * (size_t)nt, T(0));
+    for (uint32_t f = 0; f < nt; ++f) {
+        const uint32_t vs[3] = {tri[3 * f], tri[3 * f + 1], tri[3 * f + 2]};
+        T ab[3], ac[3];
+        for (int k = 0; k < 3; ++k) {
+            ab[k] = m.v[3 * vs[1] + k] - m.v[3 * vs[0] + k];
+            ac[k] = m.v[3 * vs[2] + k] - m.v[3 * vs[0] + k];
+        }
+        T n[3] = {ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2], ab[0] * ac[1] - ab[1] * ac[0]};
+        const T nn = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (nn > T(0))
+            for (int k = 0; k < 3; ++k) n[k] /= nn;
+        for (int k = 0; k < 3; ++k) fn[3 * f + k] = n[k];
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t p0 = vs[c], p1 = vs[(c + 1) % 3], p2 = vs[(c + 2) % 3];
+            T e1[3], e2[3], l1 = 0, l2 = 0, d = 0;
+            for (int k = 0; k < 3; ++k) {
+                e1[k] = m.v[3 * p1 + k] - m.v[3 * p0 + k];
+                e2[k] = m.v[3 * p2 + k] - m.v[3 * p0 + k];
+                l1 += e1[k] * e1[k];
+                l2 += e2[k] * e2[k];
+                d += e1[k] * e2[k];
+            }
+            const T den = std::sqrt(l1 * l2);
+            const T ang = den > T(0) ? std::acos(std::max(T(-1), std::min(T(1), d / den))) : T(0);
+            for (int k = 0; k < 3; ++k) m.vpn[3 * (size_t)p0 + k] += ang * n[k];
+            const uint64_t key = ((uint64_t)std::min(p0, p1) << 32) | std::max(p0, p1);
+            auto it = edge.find(key);
+            if (it == edge.end()) it = edge.emplace(key, std::array<T, 3>{T(0), T(0), T(0)}).first;
+            for (int k = 0; k < 3; ++k) it->second[k] += n[k];
+        }
+    }
+    for (uint32_t i = 0; i < nv; ++i) {
+        T *n = &m.vpn[3 * (size_t)i];
+        const T nn = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (nn > T(0))
+            for (int k = 0; k < 3; ++k) n[k] /= nn;
+    }
+    for (uint32_t f = 0; f < nt; ++f)
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t p0 = tri[3 * f + c], p1 = tri[3 * f + (c + 1) % 3];
+            const auto &e = edge[((uint64_t)std::min(p0, p1) << 32) | std::max(p0, p1)];
+            for (int k = 0; k < 3; ++k) m.epn[9 * (size_t)f + 3 * c + k] = e[k];
+        }
+    return m;
+}
+
+// Closest point on triangle abc to p (Ericson, Real-Time Collision
+// Detection, 5.1.5) and its feature: vertex (0; id 0 a, 1 b, 2 c), edge
+// (1; id 0 AB, 1 BC, 2 CA) or face (2), as in trimesh.slang:214-377.
+template <typename T>
+void tri_closest(const T *a, const T *b, const T *c, const T *p, T *q, int &feat, int &fid) {
+    T ab[3], ac[3], ap[3], bp[3], cp[3];
+    for (int k = 0; k < 3; ++k) {
+        ab[k] = b[k] - a[k];
+        ac[k] = c[k] - a[k];
+        ap[k] = p[k] - a[k];
+        bp[k] = p[k] - b[k];
+        cp[k] = p[k] - c[k];
+    }
+    auto dot = [](const T *u, const T *w) { return u[0] * w[0] + u[1] * w[1] + u[2] * w[2]; };
+    const T d1 = dot(ab, ap), d2 = dot(ac, ap);
+    auto set = [&](const T *s, int f, int i) {
+        for (int k = 0; k < 3; ++k) q[k] = s[k];
+        feat = f, fid = i;
+    };
+    if (d1 <= T(0) && d2 <= T(0)) return set(a, 0, 0);
+    const T d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= T(0) && d4 <= d3) return set(b, 0, 1);
+    const T vc = d1 * d4 - d3 * d2;
+    if (vc <= T(0) && d1 >= T(0) && d3 <= T(0)) {
+        const T t = d1 / (d1 - d3);
+        for (int k = 0; k < 3; ++k) q[k] = a[k] + t * ab[k];
+        feat = 1, fid = 0;
+        return;
+    }
+    const T d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= T(0) && d5 <= d6) return set(c, 0, 2);
+    const T vb = d5 * d2 - d1 * d6;
+    if (vb <= T(0) && d2 >= T(0) && d6 <= T(0)) {
+        const T t = d2 / (d2 - d6);
+        for (int k = 0; k < 3; ++k) q[k] = a[k] + t * ac[k];
+        feat = 1, fid = 2;
+        return;
+    }
+    const T va = d3 * d6 - d5 * d4;
+    if (va <= T(0) && (d4 - d3) >= T(0) && (d5 - d6) >= T(0)) {
+        const T t = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        for (int k = 0; k < 3; ++k) q[k] = b[k] + t * (c[k] - b[k]);
+        feat = 1, fid = 1;
+        return;
+    }
+    const T den = va + vb + vc;
+    if (den != T(0)) {
+        const T v = vb / den, w = vc / den;
+        for (int k = 0; k < 3; ++k) q[k] = a[k] + ab[k] * v + ac[k] * w;
+    } else {
+        for (int k = 0; k < 3; ++k) q[k] = a[k];
+    }
+    feat = 2, fid = 0;
+}
+
+// TriMesh::project_local_point (collision/trimesh.slang:116-155), by a scan
+// of every triangle instead of slosh's BVH: the closest surface point within
+// `max_dist` (ties to the later triangle) and the pseudo-normal inside test.
+template <typename T> bool mesh_project(const Mesh<T> &m, const T *p, T max_dist, T *out, bool *inside) {
+    T best = max_dist, bq[3] = {p[0], p[1], p[2]};
+    int bfeat = 0, bfid = 0;
+    size_t btri = 0;
+    bool found = false;
+    const size_t nt = m.tri.size() / 3;
+    for (size_t f = 0; f < nt; ++f) {
+        T q[3];
+        int feat, fid;
+        tri_closest<T>(&m.v[3 * m.tri[3 * f]], &m.v[3 * m.tri[3 * f + 1]], &m.v[3 * m.tri[3 * f + 2]], p, q, feat, fid);
+        const T dist = std::sqrt((q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) + (q[2] - p[2]) * (q[2] - p[2]));
+        if (dist <= best) {
+            best = dist;
+            for (int k = 0; k < 3; ++k) bq[k] = q[k];
+            bfeat = feat, bfid = fid, btri = f, found = true;
+        }
+    }
+    if (!found) return false;
+    T pn[3];
+    if (bfeat == 0) {
+        for (int k = 0; k < 3; ++k) pn[k] = m.vpn[3 * (size_t)m.tri[3 * btri + bfid] + k];
+    } else if (bfeat == 1) {
+        for (int k = 0; k < 3; ++k) pn[k] = m.epn[9 * btri + 3 * bfid + k];
+    } else {
+        const T *a = &m.v[3 * m.tri[3 * btri]], *b = &m.v[3 * m.tri[3 * btri + 1]], *c = &m.v[3 * m.tri[3 * btri + 2]];
+        const T ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, ac[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        pn[0] = ab[1] * ac[2] - ab[2] * ac[1];
+        pn[1] = ab[2] * ac[0] - ab[0] * ac[2];
+        pn[2] = ab[0] * ac[1] - ab[1] * ac[0];
+    }
+    *inside = pn[0] * (p[0] - bq[0]) + pn[1] * (p[1] - bq[1]) + pn[2] * (p[2] - bq[2]) <= T(0);
+    for (int k = 0; k < 3; ++k) out[k] = bq[k];
+    return true;
+}
+
 template <typename T, int D> struct Body {
     uint32_t shape_type;
+    const Mesh<T> *mesh = nullptr;  // trimesh colliders
     T sa[4], sb[4];
     T rot[4];  // 3D quaternion (i, j, k, w); 2D (cos, sin)
     T tra[3];
@@ -603,7 +760,7 @@ template <typename T> bool cone_project(T hh, T r, const T *p, T *out) {
 }
 
 template <typename T, int D>
-bool project_on_boundary(const Body<T, D> &b, const T *pt, T *proj, bool *is_inside) {
+bool project_on_boundary(const Body<T, D> &b, const T *pt, T *proj, bool *is_inside, T cap = T(1e30)) {
     T local[D];
     Pose<T, D>::inv_mul_pt(b, pt, local);
     T lp[D];
@@ -652,6 +809,9 @@ bool project_on_boundary(const Body<T, D> &b, const T *pt, T *proj, bool *is_ins
         if constexpr (D == 3) *is_inside = cylinder_project<T>(b.sa[0], b.sa[1], local, lp);
     } else if (D == 3 && b.shape_type == SLOSH_SHAPE_CONE) {
         if constexpr (D == 3) *is_inside = cone_project<T>(b.sa[0], b.sa[1], local, lp);
+    } else if (D == 3 && b.shape_type == SLOSH_SHAPE_TRIMESH && b.mesh) {
+        if constexpr (D == 3)
+            if (!mesh_project<T>(*b.mesh, local, cap, lp, is_inside)) return false;
     } else {
         return false;
     }
@@ -675,7 +835,7 @@ NodeCollision<T, D> collide(const std::vector<Body<T, D>> &bodies, T cell_width,
     for (size_t i = 0; i < bodies.size() && i < 16; ++i) {
         T proj[D];
         bool inside = false;
-        if (!project_on_boundary<T, D>(bodies[i], point, proj, &inside)) continue;
+        if (!project_on_boundary<T, D>(bodies[i], point, proj, &inside, dist_cap)) continue;
         T dpt[D];
         bool within = true;
         for (int k = 0; k < D; ++k) {
@@ -777,6 +937,7 @@ template <typename T, int D> struct Ctx {
     uint32_t capacity;
     Particles<T, D> p;
     std::vector<Body<T, D>> bodies;
+    std::vector<Mesh<T>> meshes;  // trimesh colliders, by ordinal
     std::vector<long long> impulses;  // 6 fixed-point sums per body (two-way coupling)
     Grid<T, D> grid, prev;
     int nthreads = 1;
@@ -1532,6 +1693,7 @@ struct AnyCtx {
     virtual int set_particles(const slosh_particle *p, uint32_t n) = 0;
     virtual int get_particles(slosh_particle *p, uint32_t n) = 0;
     virtual int set_bodies(const slosh_body *b, uint32_t n) = 0;
+    virtual int add_trimesh(const float *v, uint32_t nv, const uint32_t *tri, uint32_t nt) = 0;
     virtual int get_bodies(slosh_body *b, uint32_t n) = 0;
     virtual int step(uint32_t nsteps, int nthreads) = 0;
     virtual int stages(int last, int nthreads) = 0;
@@ -1587,7 +1749,27 @@ template <typename T, int D> struct CtxImpl : AnyCtx {
     int set_bodies(const slosh_body *b, uint32_t n) override {
         c.bodies.clear();
         for (uint32_t i = 0; i < n; ++i) c.bodies.push_back(load_body<T, D>(b[i]));
+        return link_meshes();
+    }
+    // A trimesh record names its mesh by the ordinal in shape_b[2].
+    int link_meshes() {
+        for (auto &bd : c.bodies) {
+            bd.mesh = nullptr;
+            if (bd.shape_type != SLOSH_SHAPE_TRIMESH) continue;
+            uint32_t ord;
+            const float f = (float)bd.sb[2];
+            std::memcpy(&ord, &f, 4);
+            if (D != 3 || ord >= c.meshes.size()) return SLOSH_E_INVALID;
+            bd.mesh = &c.meshes[ord];
+        }
         return SLOSH_OK;
+    }
+    int add_trimesh(const float *v, uint32_t nv, const uint32_t *tri, uint32_t nt) override {
+        for (size_t k = 0; k < 3 * (size_t)nt; ++k)
+            if (tri[k] >= nv) return SLOSH_E_INVALID;
+        c.meshes.push_back(make_mesh<T>(v, nv, tri, nt));
+        link_meshes();
+        return (int)c.meshes.size() - 1;
     }
     int get_bodies(slosh_body *b, uint32_t n) override {
         for (uint32_t i = 0; i < n && i < c.bodies.size(); ++i) store_body<T, D>(c.bodies[i], b[i]);
@@ -1754,6 +1936,26 @@ int orc_set_particles(void *c, const slosh_particle *p, uint32_t n) {
 }
 int orc_get_particles(void *c, slosh_particle *p, uint32_t n) { return ((orc::AnyCtx *)c)->get_particles(p, n); }
 int orc_set_bodies(void *c, const slosh_body *b, uint32_t n) { return ((orc::AnyCtx *)c)->set_bodies(b, n); }
+// Adds a triangle mesh; returns its ordinal (for shape_b[2] of trimesh
+// records) or SLOSH_E_INVALID.
+int orc_add_trimesh(void *c, const float *v, uint32_t nv, const uint32_t *tri, uint32_t nt) {
+    return ((orc::AnyCtx *)c)->add_trimesh(v, nv, tri, nt);
+}
+// Projection of a world point on a posed triangle mesh (FP64), within `cap`.
+int orc_project_trimesh(const float *v, uint32_t nv, const uint32_t *tri, uint32_t nt, const slosh_body *body,
+                        const float *pt, float cap, float *out, int *inside) {
+    const orc::Mesh<double> m = orc::make_mesh<double>(v, nv, tri, nt);
+    orc::Body<double, 3> b = orc::load_body<double, 3>(*body);
+    b.shape_type = SLOSH_SHAPE_TRIMESH;
+    b.mesh = &m;
+    const double p[3] = {pt[0], pt[1], pt[2]};
+    double q[3];
+    bool in = false;
+    const bool ok = orc::project_on_boundary<double, 3>(b, p, q, &in, (double)cap);
+    for (int k = 0; k < 3; ++k) out[k] = (float)q[k];
+    *inside = in ? 1 : 0;
+    return ok ? 1 : 0;
+}
 int orc_get_bodies(void *c, slosh_body *b, uint32_t n) { return ((orc::AnyCtx *)c)->get_bodies(b, n); }
 int orc_step(void *c, uint32_t nsteps, int nthreads) { return ((orc::AnyCtx *)c)->step(nsteps, nthreads); }
 int orc_stages(void *c, int last, int nthreads) { return ((orc::AnyCtx *)c)->stages(last, nthreads); }

@@ -46,6 +46,7 @@ SHAPE_CUBOID = 1
 SHAPE_CAPSULE = 2
 SHAPE_CONE = 3
 SHAPE_CYLINDER = 4
+SHAPE_TRIMESH = 6
 
 COUPLING_ONE_WAY = 0
 COUPLING_TWO_WAY = 1
@@ -241,6 +242,7 @@ SIGNATURES = {
     "slosh_download_positions": (ctypes.c_int, [_P, _P, _U32, _P]),
     "slosh_set_bodies": (ctypes.c_int, [_P, _P, _U32]),
     "slosh_get_bodies": (ctypes.c_int, [_P, _P, _U32]),
+    "slosh_add_trimesh": (ctypes.c_int, [_P, _P, _U32, _P, _U32, _P]),
     "slosh_step": (ctypes.c_int, [_P, _U32, _P]),
     "slosh_sync": (ctypes.c_int, [_P, _P]),
     "slosh_kernels_per_substep": (_U32, [_P]),

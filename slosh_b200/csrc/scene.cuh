@@ -83,6 +83,8 @@ struct DevScene {
     // ---- bodies -------------------------------------------------------------
     DevBody *bodies;
     uint32_t n_bodies;
+    const float4 *mesh_vtx;        // triangle-mesh colliders: packed vertex and index buffers
+    const uint32_t *mesh_idx;
     unsigned long long *body_imp;  // 6 fixed-point impulse sums per body (two-way coupling)
     uint32_t coll_dynamic;         // a two-way body moves: no collision cache
 

@@ -61,6 +61,13 @@ struct slosh_ctx {
     uint32_t n_bodies = 0;
     unsigned long long *body_imp = nullptr;  // two-way coupling impulse sums, 6 per body slot
     uint32_t coll_dynamic = 0;               // some body is coupled two-way
+    // triangle-mesh colliders: host copies of the packed buffers and their
+    // device copies, re-uploaded whole when a mesh is added
+    std::vector<float4> mesh_vtx_host;
+    std::vector<uint32_t> mesh_idx_host;
+    float4 *mesh_vtx = nullptr;
+    uint32_t *mesh_idx = nullptr;
+    uint32_t n_meshes = 0;
     Counters *ctr = nullptr;
     uint32_t *err = nullptr;
     uint32_t *small = nullptr;  // [0] n_mat, [1] scene flags, [2] debug total
@@ -202,6 +209,8 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.n_bodies = c->n_bodies;
     s.body_imp = c->body_imp;
     s.coll_dynamic = c->coll_dynamic;
+    s.mesh_vtx = c->mesh_vtx;
+    s.mesh_idx = c->mesh_idx;
     s.ctr = c->ctr;
     s.err = c->err;
     s.clr_hkeys = c->hkeys[prv];
@@ -400,6 +409,14 @@ bool shape_supported(uint32_t ty, int dim) {
     return dim == 3 && (ty == SLOSH_SHAPE_CYLINDER || ty == SLOSH_SHAPE_CONE);
 }
 
+// A trimesh shape record names a mesh of this context's buffers.
+bool trimesh_in_range(const slosh_ctx *c, const DevBody &d) {
+    const TriMeshRef m = trimesh_ref(d.sa, d.sb);
+    return m.ordinal < c->n_meshes &&
+           (uint64_t)m.vtx_root + 2ull * m.n_nodes + 2ull * m.n_verts + 3ull * m.n_tris <= c->mesh_vtx_host.size() &&
+           (uint64_t)m.idx_root + 3ull * m.n_nodes + 3ull * m.n_tris <= c->mesh_idx_host.size();
+}
+
 void from_dev_body(const DevBody &d, slosh_body &b, int dim) {
     std::memset(&b, 0, sizeof(b));
     for (int k = 0; k < 4; ++k) {
@@ -437,6 +454,10 @@ void release_ctx(slosh_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void *p : c->allocs) cudaFree(p);
     c->allocs.clear();
+    cudaFree(c->mesh_vtx);
+    cudaFree(c->mesh_idx);
+    c->mesh_vtx = nullptr;
+    c->mesh_idx = nullptr;
     if (c->stream) cudaStreamDestroy(c->stream);
     c->stream = nullptr;
 }
@@ -698,7 +719,10 @@ int slosh_set_bodies(slosh_ctx *c, const slosh_body *bodies, uint32_t n) {
         if (!(db[i].scale > 0.f)) return fail(c, SLOSH_E_INVALID, "body %u: scale must be > 0", i);
         if (db[i].coupling > SLOSH_COUPLING_TWO_WAY)
             return fail(c, SLOSH_E_INVALID, "body %u: unknown coupling %u", i, db[i].coupling);
-        if (!shape_supported(db[i].shape_type, c->dim))
+        const bool mesh = c->dim == 3 && db[i].shape_type == SLOSH_SHAPE_TRIMESH;
+        if (mesh && !trimesh_in_range(c, db[i]))
+            return fail(c, SLOSH_E_INVALID, "body %u: trimesh shape not made by slosh_add_trimesh on this context", i);
+        if (!mesh && !shape_supported(db[i].shape_type, c->dim))
             return fail(c, SLOSH_E_INVALID, "body %u: unsupported shape type %u in %dD", i, db[i].shape_type, c->dim);
     }
     CK(cudaSetDevice(c->device));
@@ -709,6 +733,44 @@ int slosh_set_bodies(slosh_ctx *c, const slosh_body *bodies, uint32_t n) {
     c->coll_dynamic = 0;
     for (uint32_t i = 0; i < n; ++i) c->coll_dynamic |= db[i].coupling == SLOSH_COUPLING_TWO_WAY ? 1u : 0u;
     destroy_graphs(c);
+    return SLOSH_OK;
+}
+
+int slosh_add_trimesh(slosh_ctx *c, const float *vertices, uint32_t n_vertices, const uint32_t *indices,
+                      uint32_t n_triangles, slosh_body *body) {
+    if (!c || !body || (!vertices && n_vertices) || (!indices && n_triangles)) return SLOSH_E_INVALID;
+    if (c->dim != 3) return fail(c, SLOSH_E_INVALID, "triangle meshes are 3D colliders");
+    if (n_triangles == 0 || n_triangles > (1u << 24))
+        return fail(c, SLOSH_E_INVALID, "a mesh needs 1 to 2^24 triangles (got %u)", n_triangles);
+    std::vector<float4> vtx = c->mesh_vtx_host;
+    std::vector<uint32_t> idx = c->mesh_idx_host;
+    TriMeshRef ref{};
+    if (!build_trimesh(vertices, n_vertices, indices, n_triangles, vtx, idx, c->n_meshes, ref))
+        return fail(c, SLOSH_E_INVALID, "triangle vertex index out of range (%u vertices)", n_vertices);
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    float4 *dv = nullptr;
+    uint32_t *di = nullptr;
+    if (cudaMalloc(&dv, vtx.size() * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&di, idx.size() * sizeof(uint32_t)) != cudaSuccess) {
+        cudaFree(dv);
+        cudaFree(di);
+        return fail(c, SLOSH_E_NOMEM, "mesh buffers");
+    }
+    CK(cudaMemcpy(dv, vtx.data(), vtx.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(di, idx.data(), idx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    cudaFree(c->mesh_vtx);
+    cudaFree(c->mesh_idx);
+    c->mesh_vtx = dv;
+    c->mesh_idx = di;
+    c->mesh_vtx_host.swap(vtx);
+    c->mesh_idx_host.swap(idx);
+    c->n_meshes += 1;
+    destroy_graphs(c);  // the graphs hold the buffer pointers
+    const uint32_t ty = SLOSH_SHAPE_TRIMESH;
+    const uint32_t a[4] = {ref.vtx_root, ref.idx_root, ref.n_nodes, ty}, b[4] = {ref.n_tris, ref.n_verts, ref.ordinal, 0u};
+    std::memcpy(body->shape_a, a, sizeof(a));
+    std::memcpy(body->shape_b, b, sizeof(b));
     return SLOSH_OK;
 }
 

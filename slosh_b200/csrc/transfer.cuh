@@ -8,6 +8,7 @@
 #include "grid_build.cuh"
 #include "models.cuh"
 #include "scene.cuh"
+#include "trimesh.cuh"
 
 namespace slosh {
 
@@ -577,9 +578,12 @@ __device__ __forceinline__ bool cone_boundary(float hh, float r, const float *p,
 
 // Shape::project_point_on_boundary for balls, cuboids, capsules, cylinders
 // and cones (shaders/slosh/rbd/shapes/shape.slang:152-175; ball.slang:39-52,
-// cuboid.slang:14-63, capsule.slang, cylinder.slang, cone.slang).
+// cuboid.slang:14-63, capsule.slang, cylinder.slang, cone.slang), and the
+// triangle-mesh query of collide (collision/collide.slang:124-134): a mesh
+// point is returned only within `cap` of the surface.
 template <int D>
-__device__ __forceinline__ bool project_on_boundary(const DevBody &b, const float *pt, float *proj, bool &inside) {
+__device__ __forceinline__ bool project_on_boundary(const DevBody &b, const float *pt, float *proj, bool &inside,
+                                                    const float4 *mvtx, const uint32_t *midx, float cap) {
     float local[D], lp[D];
     pose_inv_mul_pt<D>(b, pt, local);
     if (b.shape_type == SLOSH_SHAPE_CUBOID) {
@@ -622,7 +626,10 @@ __device__ __forceinline__ bool project_on_boundary(const DevBody &b, const floa
     } else if constexpr (D == 3) {
         if (b.shape_type == SLOSH_SHAPE_CYLINDER) inside = cylinder_boundary(b.sa[0], b.sa[1], local, lp);
         else if (b.shape_type == SLOSH_SHAPE_CONE) inside = cone_boundary(b.sa[0], b.sa[1], local, lp);
-        else return false;
+        else if (b.shape_type == SLOSH_SHAPE_TRIMESH && mvtx) {
+            if (!trimesh_project(trimesh_ref(b.sa, b.sb), mvtx, midx, local, cap, lp, inside)) return false;
+        } else
+            return false;
     } else {
         return false;
     }
@@ -634,7 +641,7 @@ __device__ __forceinline__ bool project_on_boundary(const DevBody &b, const floa
 // collider id or NONE; `nd` = (normal, dot(point_node - proj, normal)).
 template <int D>
 __device__ __forceinline__ uint32_t collide(const DevBody *bodies, uint32_t n_bodies, float h, const float *pt,
-                                            float4 &nd) {
+                                            float4 &nd, const float4 *mvtx, const uint32_t *midx) {
     const float cap = h * 1.5f;
     float best = 1.0e10f;
     uint32_t id = NONE;
@@ -642,7 +649,7 @@ __device__ __forceinline__ uint32_t collide(const DevBody *bodies, uint32_t n_bo
     for (uint32_t i = 0; i < n_bodies && i < MAX_BODIES; ++i) {
         float proj[D];
         bool inside = false;
-        if (!project_on_boundary<D>(bodies[i], pt, proj, inside)) continue;
+        if (!project_on_boundary<D>(bodies[i], pt, proj, inside, mvtx, midx, cap)) continue;
         float dpt[D], n2 = 0.f;
         bool within = true;
 #pragma unroll
@@ -718,7 +725,9 @@ __device__ __forceinline__ void project_velocity(uint32_t type, float friction, 
 // node.  The collision of a node is reused from the previous substep when
 // its block was active there (slosh's cache, which assumes static colliders),
 // otherwise collide() runs; both are recorded for the next substep.
-template <int D, bool B = false> __global__ void k_grid_update(DevScene s) {
+// 4 CTAs of 256 per SM: the register cap (64) leaves the rare collision
+// queries (nodes without a cached collision) to spill, not the whole kernel.
+template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_grid_update(DevScene s) {
     constexpr int BW = Geo<D>::BW;
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -805,7 +814,7 @@ template <int D, bool B = false> __global__ void k_grid_update(DevScene s) {
             cn = s.prev_coll[(size_t)prank * 64u + node];
             cid = s.prev_coll_id[(size_t)prank * 64u + node];
         } else {
-            cid = collide<D>(bodies, n_bodies, h, cell_pos, cn);
+            cid = collide<D>(bodies, n_bodies, h, cell_pos, cn, s.mesh_vtx, s.mesh_idx);
         }
         s.coll[t] = cn;
         s.coll_id[t] = cid;

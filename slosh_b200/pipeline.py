@@ -206,7 +206,10 @@ class RigidBody:
     ("cuboid", half_extents), ("ball", radius), ("capsule", (a, b, radius))
     with a, b the segment end points, or in 3D ("cylinder", (half_height,
     radius)) or ("cone", (half_height, radius)) around the local y axis
-    (GpuShape layouts, shaders/slosh/rbd/shapes/shape.slang:37-80).  Rotation
+    (GpuShape layouts, shaders/slosh/rbd/shapes/shape.slang:37-80), or in 3D
+    ("trimesh", (vertices, triangles)) with vertices an (n, 3) array and
+    triangles an (m, 3) array of vertex indices, counter-clockwise seen from
+    outside (``box_mesh``, ``heightfield_mesh``).  Rotation
     is a unit quaternion (i, j, k, w) in 3D or an angle in radians in 2D.
     ``coupling`` is "one_way" (slosh's GPU behaviour: the particles never
     push the body) or "two_way" (the grid's contact impulses move it; see
@@ -263,6 +266,9 @@ class RigidBody:
             r["shape_a"][0] = float(hh)
             r["shape_a"][1] = float(radius)
             r["shape_a"].view(np.uint32)[3] = _lib.SHAPE_CYLINDER if kind == "cylinder" else _lib.SHAPE_CONE
+        elif kind == "trimesh" and dim == 3:
+            # the mesh offsets are filled in by the context the mesh is added to
+            r["shape_a"].view(np.uint32)[3] = _lib.SHAPE_TRIMESH
         else:
             raise ValueError(f"unsupported shape {kind!r}")
         if dim == 3:
@@ -313,6 +319,43 @@ def shape_mass_properties(shape: tuple, density: float, dim: int, scale: float =
         m = density * math.pi * r * r
         return m, 0.5 * m * r * r
     raise ValueError(f"mass properties of {kind!r} are not implemented")
+
+
+def mesh_arrays(shape: tuple) -> tuple[np.ndarray, np.ndarray]:
+    """The (vertices, triangles) of a ("trimesh", ...) shape as contiguous
+    float32 (n, 3) and uint32 (m, 3) arrays."""
+    v, t = shape[1]
+    return np.ascontiguousarray(v, np.float32).reshape(-1, 3), np.ascontiguousarray(t, np.uint32).reshape(-1, 3)
+
+
+def box_mesh(half_extents: Sequence[float]) -> tuple[np.ndarray, np.ndarray]:
+    """A closed box of 12 triangles, outward counter-clockwise."""
+    hx, hy, hz = (float(x) for x in half_extents)
+    v = np.array([[sx * hx, sy * hy, sz * hz] for sz in (-1, 1) for sy in (-1, 1) for sx in (-1, 1)], np.float32)
+    quads = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    t = []
+    for a, b, c, d in quads:
+        t += [(a, b, c), (a, c, d)]
+    return v, np.array(t, np.uint32)
+
+
+def heightfield_mesh(heights: np.ndarray, extent: Sequence[float]) -> tuple[np.ndarray, np.ndarray]:
+    """The triangle mesh of a heightfield (rows along z, columns along x)
+    over [-ex/2, ex/2] x [-ez/2, ez/2], up = +y, as slosh turns heightfields
+    into meshes (src/rbd/shapes.rs:241-269)."""
+    h = np.asarray(heights, np.float32)
+    nz, nx = h.shape
+    ex, ez = float(extent[0]), float(extent[1])
+    xs = np.linspace(-ex / 2, ex / 2, nx, dtype=np.float32)
+    zs = np.linspace(-ez / 2, ez / 2, nz, dtype=np.float32)
+    v = np.stack([np.tile(xs, nz), h.ravel(), np.repeat(zs, nx)], axis=1).astype(np.float32)
+    t = []
+    for iz in range(nz - 1):
+        for ix in range(nx - 1):
+            a, b = iz * nx + ix, iz * nx + ix + 1
+            c, d = a + nx, b + nx
+            t += [(a, c, b), (b, c, d)]
+    return v, np.array(t, np.uint32)
 
 
 def quat_to_matrix(q: Sequence[float]) -> np.ndarray:
@@ -387,8 +430,19 @@ class MpmData:
     def set_bodies(self, bodies: list):
         self.bodies = bodies
         recs = np.zeros(len(bodies), dtype=BODY_DTYPE)
+        if not hasattr(self, "_meshes"):
+            self._meshes = {}  # id of a trimesh shape's vertex array -> its (shape_a, shape_b)
         for i, b in enumerate(bodies):
             recs[i] = b.record(self.dim)
+            if b.shape[0] == "trimesh":
+                key = id(b.shape[1][0])
+                if key not in self._meshes:
+                    v, t = mesh_arrays(b.shape)
+                    tmp = np.zeros(1, dtype=BODY_DTYPE)
+                    _check(self._lib, self._ctx,
+                           self._lib.slosh_add_trimesh(self._ctx, ptr(v), len(v), ptr(t), len(t), ptr(tmp)))
+                    self._meshes[key] = (tmp["shape_a"][0].copy(), tmp["shape_b"][0].copy(), b.shape[1])
+                recs[i]["shape_a"], recs[i]["shape_b"] = self._meshes[key][0], self._meshes[key][1]
         self.n_bodies = len(bodies)
         _check(self._lib, self._ctx, self._lib.slosh_set_bodies(self._ctx, ptr(recs) if len(bodies) else None, len(bodies)))
 

@@ -327,13 +327,28 @@ def collider_scenes():
         RigidBody(("capsule", ((-0.08, 0.0), (0.1, 0.04), 0.03)), translation=(0.15, 0.05), rotation=0.4,
                   boundary_condition=GpuBoundaryCondition.stick())
     ]
-    return {"shapes3d": sc3, "capsule2d": sc2}
+    from slosh_b200.pipeline import box_mesh, heightfield_mesh
+
+    sc4 = scenes.random_scene_3d(6000, "elastic", 1 / 32, seed=52)
+    parts = sc4.particles.copy()
+    parts["velocity"][:, 1] = -1.0
+    sc4.particles = parts
+    y1 = float(parts["position"][:, 1].min())
+    xz = np.linspace(0.0, 1.0, 7)
+    hf = (0.03 * np.sin(6.0 * xz)[None, :] * np.cos(5.0 * xz)[:, None]).astype(np.float32)
+    sc4.bodies = [
+        RigidBody(("trimesh", box_mesh((0.06, 0.04, 0.05))), translation=(0.45, y1 - 0.03, 0.5),
+                  rotation=quat_from_axis_angle((1, 0, 1), 0.5), boundary_condition=GpuBoundaryCondition.slip()),
+        RigidBody(("trimesh", heightfield_mesh(hf, (0.6, 0.6))), translation=(0.5, y1 - 0.05, 0.5)),
+    ]
+    return {"shapes3d": sc3, "capsule2d": sc2, "trimesh3d": sc4}
 
 
-@pytest.mark.parametrize("name", ["shapes3d", "capsule2d"])
+@pytest.mark.parametrize("name", ["shapes3d", "capsule2d", "trimesh3d"])
 def test_collider_shapes_parity(cuda_lib, name):
     """Grid-update nodes (collide + BC projection) and 5 substeps against the
-    oracle with the capsule, cylinder and cone colliders.  A node lying
+    oracle with the capsule, cylinder, cone and triangle-mesh (box,
+    heightfield) colliders.  A node lying
     almost on a curved surface gets its contact normal from
     (projection - node) / |projection - node| with a tiny denominator, so
     rounding (FMA contraction on the GPU, none in the oracle) is amplified
@@ -442,3 +457,25 @@ def test_two_way_coupling_bit_reproducible(cuda_lib):
         runs.append((data.download_particles().tobytes(), data.get_bodies().tobytes()))
         data.close()
     assert runs[0] == runs[1]
+
+
+def test_trimesh_box_matches_cuboid_collider(cuda_lib):
+    """A box mesh floor moves the sand column like the cuboid floor of the
+    same extents: the meshes's projection is the cuboid's closest point."""
+    from slosh_b200.pipeline import box_mesh
+
+    runs = []
+    for mesh in (False, True):
+        sc = scenes.sand_column_3d(h=1 / 32, substeps=10)
+        fl = sc.bodies[0]
+        he = fl.shape[1]
+        if mesh:
+            sc.bodies[0] = RigidBody(("trimesh", box_mesh(he)), translation=fl.translation,
+                                     boundary_condition=fl.boundary_condition)
+        data = scenes.build_mpm_data(sc)
+        MpmPipeline().launch_step(data, 10)
+        runs.append(data.download_particles())
+        data.close()
+    close("mesh vs cuboid floor position", runs[1]["position"], runs[0]["position"], 1e-6, 0)
+    close("mesh vs cuboid floor velocity", runs[1]["velocity"], runs[0]["velocity"], 1e-5, 1e-4)
+

@@ -356,3 +356,55 @@ def test_one_way_body_is_not_pushed(oracle_lib):
     o.step(30)
     b = o.get_bodies()[0]
     assert np.all(b["linvel"][:3] == 0.0) and np.all(b["angvel"][:3] == 0.0)
+
+
+def test_trimesh_box_matches_cuboid(oracle_lib):
+    """A closed box mesh projects points like the cuboid of the same extents
+    (collision/trimesh.slang:116-155 against rbd/shapes/cuboid.slang:14-63):
+    the same closest surface point and inside flag for points within the
+    1.5-cell cap, on faces, edges and corners; nothing beyond the cap."""
+    from slosh_b200.pipeline import box_mesh, quat_from_axis_angle
+
+    he = (0.1, 0.06, 0.08)
+    pose = dict(translation=(0.5, 0.4, 0.45), rotation=quat_from_axis_angle((1, 2, 0.5), 0.6))
+    cub = RigidBody(("cuboid", he), **pose).record(3)
+    v, t = box_mesh(he)
+    mesh = RigidBody(("trimesh", (v, t)), **pose).record(3)
+    rng = np.random.default_rng(3)
+    cap = 0.03
+    checked = 0
+    for _ in range(400):
+        # a point near the surface: a surface point pushed along a random direction
+        local = rng.uniform(-1, 1, 3) * np.array(he)
+        axis = rng.integers(3)
+        local[axis] = np.sign(local[axis] or 1.0) * he[axis]
+        local += rng.normal(size=3) * 0.01
+        q = np.array(pose["rotation"], np.float64)
+        from slosh_b200.pipeline import quat_to_matrix
+
+        world = quat_to_matrix(q) @ local + np.array(pose["translation"])
+        c = oracle_lib.project_on_boundary(3, cub, world)
+        m = oracle_lib.project_on_trimesh(v, t, mesh, world, cap)
+        dist = np.linalg.norm(c[0] - world)
+        if dist > cap * 0.999:
+            continue
+        assert m is not None
+        assert m[1] == c[1]
+        assert np.abs(m[0] - c[0]).max() < 2e-6
+        checked += 1
+    assert checked > 300
+    far = np.array(pose["translation"]) + np.array([0.3, 0.0, 0.0])
+    assert oracle_lib.project_on_trimesh(v, t, mesh, far, cap) is None
+
+
+def test_heightfield_mesh_sides(oracle_lib):
+    """A heightfield mesh (up = +y): points below the surface are inside,
+    points above outside, and project vertically onto a flat field."""
+    from slosh_b200.pipeline import heightfield_mesh
+
+    v, t = heightfield_mesh(np.zeros((5, 6), np.float32), (1.0, 1.0))
+    rec = RigidBody(("trimesh", (v, t)), translation=(0.5, 0.2, 0.5)).record(3)
+    for y, inside in ((0.19, True), (0.215, False)):
+        r = oracle_lib.project_on_trimesh(v, t, rec, (0.43, y, 0.61), 0.05)
+        assert r is not None and r[1] == inside
+        assert np.allclose(r[0], (0.43, 0.2, 0.61), atol=1e-6)
