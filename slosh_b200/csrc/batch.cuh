@@ -79,6 +79,7 @@ DevScene make_batch_scene(slosh_batch *b, uint32_t parity) {
     s.scene_fill = b->scene_fill;
     s.n_bodies = b->body_top;
     s.use_partial = 1u;
+    s.p2g_coop_below = 0u;  // one mode for every scene: a scene's bits do not depend on its batch
     return s;
 }
 

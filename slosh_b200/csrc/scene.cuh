@@ -74,6 +74,7 @@ struct DevScene {
     float4 *nodes;         // 64 nodes per block: (momentum | velocity, mass)
     float4 *partial;       // TILE nodes per block: the block's own P2G sums over its (block + 2)^D tile
     uint32_t use_partial;  // P2G wrote `partial` (deterministic path); grid update gathers it
+    uint32_t p2g_coop_below;  // P2G shares a block between a CTA's warps below this many blocks
     uint32_t gather_only;  // grid update stops after the gather (P2G node sums, debug)
     float4 *coll;          // node collision cache of this substep: (normal, d0)
     uint32_t *coll_id;     // collider id or NONE

@@ -201,6 +201,9 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.partial = c->partial;
     s.use_partial = (c->p2g_variant == 0) ? 1u : 0u;
     s.gather_only = 0u;
+    // P2G: one warp a block fills the GPU from about 10 blocks an SM; below
+    // that a CTA's four warps share each block
+    s.p2g_coop_below = (uint32_t)c->sm_count * 10u;
     s.coll = c->coll[cur];
     s.coll_id = c->coll_id[cur];
     s.prev_coll = c->coll[prv];

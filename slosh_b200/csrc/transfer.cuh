@@ -157,9 +157,167 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
     const size_t n = s.n;
     const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
     float4 *tiles = stile[wl];
-    float h = s.h, inv_h = 1.0f / s.h;
-    // blocks are taken from a queue (one atomic a block), so warps that get
-    // light blocks take more of them
+    // One pass of block r: 32 (cell, slab) items (`ord` their cells)
+    // summed into this warp's slab tiles.  Returns false when the pass's
+    // cells are empty (and so are the later passes').  With `next`, `ord`
+    // is reloaded with the next pass's cells once this pass's are read.
+    auto run_pass = [&](uint32_t r, uint32_t first, const int (&bv)[D], float h, float inv_h, uint32_t pass,
+                        uint2 &ord, bool next) -> bool {
+        const uint32_t item = 32u * pass + lane;
+        const int slab = (int)(item % 3u);
+        const uint32_t lo = ord.x >> 6, hi = lo + ord.y;
+        const int cell = (int)(ord.x & 63u);
+        if (__shfl_sync(FULL_MASK, ord.y, 0) == 0u) return false;
+        if (next) ord = s.bord[(size_t)r * CELLS + (item + 32u) / 3u];
+        int ca[D];
+        if constexpr (D == 3) {
+            ca[0] = cell & 3;
+            ca[1] = (cell >> 2) & 3;
+            ca[2] = cell >> 4;
+        } else {
+            ca[0] = cell & 7;
+            ca[1] = cell >> 3;
+        }
+        float assoc[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) assoc[k] = (float)(bv[k] * BW + ca[k]);
+        float4 acc[NACC];
+#pragma unroll
+        for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        // The first lane of each cell in this pass (its slab-0 lane, or lane
+        // 0 for a cell begun in the previous pass) copies the cell's
+        // particles into the cell's staging slot; the three slab lanes of a
+        // cell read the same slot.  The lanes step through particle k
+        // together (k up to the pass's largest count, lane 0's), so the warp
+        // can sync around the copies.
+        const uint32_t cnt = hi - lo, kmax = __shfl_sync(FULL_MASK, cnt, 0);
+        const uint32_t cs = item / 3u - (32u * pass) / 3u;
+        const bool loader = slab == 0 || lane == 0;
+        auto stage = [&](uint32_t k, uint32_t i) {
+            if (loader && k < cnt) {
+                const int b = (int)(k % NBUF);
+                cp_async16(&sp_pm[wl][b][cs], &s.pm[i]);
+                cp_async16(&sp_vv[wl][b][cs], &s.vv[i]);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) cp_async16(&sp_cq[wl][b][q][cs], &s.cq[q * n + i]);
+            }
+            cp_async_commit();
+        };
+        auto index = [&](uint32_t k) { return (loader && k < cnt) ? s.perm[first + lo + k] : 0u; };
+#pragma unroll
+        for (uint32_t k = 0; k + 1 < (uint32_t)NBUF; ++k) stage(k, index(k));
+        uint32_t i_next = index(NBUF - 1u);  // loaded one iteration before its copies
+        for (uint32_t k = 0; k < kmax; ++k) {
+            stage(k + NBUF - 1u, i_next);
+            i_next = index(k + NBUF);
+            cp_async_wait<NBUF - 1>();
+            __syncwarp();  // the loaders' copies of particle k have landed
+            if (k < cnt) {
+                const int b = (int)(k % NBUF);
+                float fdt[3] = {0.f, 0.f, 0.f};
+                if (s.force_pending) {
+                    const uint32_t i = s.perm[first + lo + k];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) fdt[d] = s.fdt[d * n + i];
+                }
+                float4 cv[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) cv[q] = sp_cq[wl][b][q][cs];
+                if (!p2g_particle<D>(sp_pm[wl][b][cs], sp_vv[wl][b][cs], cv, fdt, assoc, h, inv_h, slab, acc))
+                    atomicOr(s.err, ERR_KEY_RANGE);
+            }
+            __syncwarp();  // slot k % NBUF is refilled by the next iteration's copies
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+        // node (cell + stencil offset) in the slab's tile, whose slab-axis
+        // coordinate is relative to the slab: 3D z - slab = ca[2], 2D
+        // y - slab = ca[1]
+        float4 *pt = tiles + slab * SSZ;
+#pragma unroll
+        for (int k = 0; k < NACC; ++k) {
+            const int sx = k % 3;
+            int idx;
+            if constexpr (D == 3) idx = (ca[0] + sx) + PY * (ca[1] + k / 3) + PZ * ca[2];
+            else idx = (ca[0] + sx) + PY * ca[1];
+            float4 v = pt[idx];
+            v.x += acc[k].x;
+            v.y += acc[k].y;
+            v.z += acc[k].z;
+            v.w += acc[k].w;
+            pt[idx] = v;
+            __syncwarp();
+        }
+        return true;
+    };
+    // Node t of the block's (block + 2)^D tile: the sum of the slab tiles of
+    // warps [w0, w1) in warp then slab order.
+    auto tile_node = [&](int t, uint32_t w0, uint32_t w1) {
+        int tc[D];
+        tc[0] = t % TW;
+        if constexpr (D == 3) {
+            tc[1] = (t / TW) % TW;
+            tc[2] = t / (TW * TW);
+        } else {
+            tc[1] = t / TW;
+        }
+        const int along = tc[D - 1];  // slab axis: z in 3D, y in 2D
+        float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t w = w0; w < w1; ++w)
+#pragma unroll
+            for (int sl = 0; sl < 3; ++sl) {
+                const int rel = along - sl;  // node plane within slab sl's tile
+                if (rel < 0 || rel >= BW) continue;
+                const int lay = (D == 3) ? tc[0] + PY * tc[1] + PZ * rel : tc[0] + PY * rel;
+                const float4 v = stile[w][sl * SSZ + lay];
+                sum.x += v.x;
+                sum.y += v.y;
+                sum.z += v.z;
+                sum.w += v.w;
+            }
+        return sum;
+    };
+    auto block_setup = [&](uint32_t r, float &h, float &inv_h, int (&bv)[D]) {
+        if constexpr (B) {
+            h = s.scenes[s.bscene[r]].h;
+            inv_h = 1.0f / h;
+        }
+        unpack_key<D>(s.bkey[r], bv);
+        for (uint32_t q = lane; q < 3u * SSZ; q += 32u) tiles[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    if (!B && nb < s.p2g_coop_below) {
+        // Few blocks (a small scene): the CTA's warps share a block, warp w
+        // taking passes w and w + 4, and the block's tile sums the warps'
+        // slab tiles in warp order.
+        __shared__ uint32_t coop_r;
+        for (;;) {
+            __syncthreads();  // the previous block's tile sum has read the slab tiles
+            if (threadIdx.x == 0) coop_r = atomicAdd(&s.ctr->p2g_next, 1u);
+            __syncthreads();
+            const uint32_t r = coop_r;
+            if (r >= nb) break;
+            const uint32_t np = s.bnp[r];
+            if (np == 0) continue;
+            const uint32_t first = s.bfirst[r];
+            if (first + np > s.n) {
+                if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+                continue;
+            }
+            float h = s.h, inv_h = 1.0f / s.h;
+            int bv[D];
+            block_setup(r, h, inv_h, bv);
+            for (uint32_t pass = wl; pass < 6u; pass += P2G_WARPS) {
+                uint2 ord = s.bord[(size_t)r * CELLS + (32u * pass + lane) / 3u];
+                if (!run_pass(r, first, bv, h, inv_h, pass, ord, false)) break;
+            }
+            __syncthreads();
+            for (int t = (int)threadIdx.x; t < TILE; t += 32 * P2G_WARPS)
+                s.partial[(size_t)r * TILE + t] = tile_node(t, 0, P2G_WARPS);
+        }
+        return;
+    }
+    // One warp a block.  Blocks are taken from a queue (one atomic a
+    // block), so warps that get light blocks take more of them.
     auto next_block = [&]() {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(&s.ctr->p2g_next, 1u);
@@ -173,125 +331,14 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
             if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
         }
-        if constexpr (B) {
-            h = s.scenes[s.bscene[r]].h;
-            inv_h = 1.0f / h;
-        }
+        float h = s.h, inv_h = 1.0f / s.h;
         int bv[D];
-        unpack_key<D>(s.bkey[r], bv);
-        for (uint32_t q = lane; q < 3u * SSZ; q += 32u) tiles[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        block_setup(r, h, inv_h, bv);
         uint2 ord = s.bord[(size_t)r * CELLS + lane / 3u];
-        for (uint32_t pass = 0; pass < 6u; ++pass) {
-            const uint32_t item = 32u * pass + lane;
-            const int slab = (int)(item % 3u);
-            const uint32_t lo = ord.x >> 6, hi = lo + ord.y;
-            const int cell = (int)(ord.x & 63u);
-            if (__shfl_sync(FULL_MASK, ord.y, 0) == 0u) break;  // this and later passes hold empty cells
-            if (pass < 5u) ord = s.bord[(size_t)r * CELLS + (item + 32u) / 3u];
-            int ca[D];
-            if constexpr (D == 3) {
-                ca[0] = cell & 3;
-                ca[1] = (cell >> 2) & 3;
-                ca[2] = cell >> 4;
-            } else {
-                ca[0] = cell & 7;
-                ca[1] = cell >> 3;
-            }
-            float assoc[D];
-#pragma unroll
-            for (int k = 0; k < D; ++k) assoc[k] = (float)(bv[k] * BW + ca[k]);
-            float4 acc[NACC];
-#pragma unroll
-            for (int k = 0; k < NACC; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-            // The first lane of each cell in this pass (its slab-0 lane, or
-            // lane 0 for a cell begun in the previous pass) copies the cell's
-            // particles into the cell's staging slot; the three slab lanes
-            // of a cell read the same slot.  The lanes step through particle
-            // k together (k up to the pass's largest count, lane 0's), so the
-            // warp can sync around the copies.
-            const uint32_t cnt = hi - lo, kmax = __shfl_sync(FULL_MASK, cnt, 0);
-            const uint32_t cs = item / 3u - (32u * pass) / 3u;
-            const bool loader = slab == 0 || lane == 0;
-            auto stage = [&](uint32_t k, uint32_t i) {
-                if (loader && k < cnt) {
-                    const int b = (int)(k % NBUF);
-                    cp_async16(&sp_pm[wl][b][cs], &s.pm[i]);
-                    cp_async16(&sp_vv[wl][b][cs], &s.vv[i]);
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) cp_async16(&sp_cq[wl][b][q][cs], &s.cq[q * n + i]);
-                }
-                cp_async_commit();
-            };
-            auto index = [&](uint32_t k) { return (loader && k < cnt) ? s.perm[first + lo + k] : 0u; };
-#pragma unroll
-            for (uint32_t k = 0; k + 1 < (uint32_t)NBUF; ++k) stage(k, index(k));
-            uint32_t i_next = index(NBUF - 1u);  // loaded one iteration before its copies
-            for (uint32_t k = 0; k < kmax; ++k) {
-                stage(k + NBUF - 1u, i_next);
-                i_next = index(k + NBUF);
-                cp_async_wait<NBUF - 1>();
-                __syncwarp();  // the loaders' copies of particle k have landed
-                if (k < cnt) {
-                    const int b = (int)(k % NBUF);
-                    float fdt[3] = {0.f, 0.f, 0.f};
-                    if (s.force_pending) {
-                        const uint32_t i = s.perm[first + lo + k];
-#pragma unroll
-                        for (int d = 0; d < D; ++d) fdt[d] = s.fdt[d * n + i];
-                    }
-                    float4 cv[Q];
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) cv[q] = sp_cq[wl][b][q][cs];
-                    if (!p2g_particle<D>(sp_pm[wl][b][cs], sp_vv[wl][b][cs], cv, fdt, assoc, h, inv_h, slab, acc))
-                        atomicOr(s.err, ERR_KEY_RANGE);
-                }
-                __syncwarp();  // slot k % NBUF is refilled by the next iteration's copies
-            }
-            cp_async_wait<0>();
-            __syncwarp();
-            // node (cell + stencil offset) in the slab's tile, whose slab-axis
-            // coordinate is relative to the slab: 3D z - slab = ca[2], 2D
-            // y - slab = ca[1]
-            float4 *pt = tiles + slab * SSZ;
-#pragma unroll
-            for (int k = 0; k < NACC; ++k) {
-                const int sx = k % 3;
-                int idx;
-                if constexpr (D == 3) idx = (ca[0] + sx) + PY * (ca[1] + k / 3) + PZ * ca[2];
-                else idx = (ca[0] + sx) + PY * ca[1];
-                float4 v = pt[idx];
-                v.x += acc[k].x;
-                v.y += acc[k].y;
-                v.z += acc[k].z;
-                v.w += acc[k].w;
-                pt[idx] = v;
-                __syncwarp();
-            }
-        }
-        for (int t = (int)lane; t < TILE; t += 32) {
-            int tc[D];
-            tc[0] = t % TW;
-            if constexpr (D == 3) {
-                tc[1] = (t / TW) % TW;
-                tc[2] = t / (TW * TW);
-            } else {
-                tc[1] = t / TW;
-            }
-            const int along = tc[D - 1];  // slab axis: z in 3D, y in 2D
-            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int sl = 0; sl < 3; ++sl) {
-                const int rel = along - sl;  // node plane within slab sl's tile
-                if (rel < 0 || rel >= BW) continue;
-                const int lay = (D == 3) ? tc[0] + PY * tc[1] + PZ * rel : tc[0] + PY * rel;
-                const float4 v = tiles[sl * SSZ + lay];
-                sum.x += v.x;
-                sum.y += v.y;
-                sum.z += v.z;
-                sum.w += v.w;
-            }
-            s.partial[(size_t)r * TILE + t] = sum;
-        }
+        for (uint32_t pass = 0; pass < 6u; ++pass)
+            if (!run_pass(r, first, bv, h, inv_h, pass, ord, pass < 5u)) break;  // later passes hold empty cells
+        __syncwarp();
+        for (int t = (int)lane; t < TILE; t += 32) s.partial[(size_t)r * TILE + t] = tile_node(t, wl, wl + 1);
         __syncwarp();
     }
 }

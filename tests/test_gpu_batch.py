@@ -49,6 +49,10 @@ def fields(p):
 
 
 def test_batch_of_one_matches_single_context(cuda_lib):
+    """A scene alone in a batch advances like its own context, to FP32
+    summation order: a context this small has its P2G blocks shared by a
+    CTA's warps (a different, fixed order of the node sums), which a batch
+    never does so that a scene's bits do not depend on its batch."""
     sc = scenes.sand_column_3d(h=1 / 32, substeps=10)
     data = scenes.build_mpm_data(sc)
     MpmPipeline().launch_step(data, 10)
@@ -60,7 +64,7 @@ def test_batch_of_one_matches_single_context(cuda_lib):
     got = b.download_particles(slot)
     b.close()
     for k, v in fields(single).items():
-        close(f"batch of one vs context {k}", got[k], v, 1e-7, 1e-6)
+        close(f"batch of one vs context {k}", got[k], v, 1e-6, 1e-5)
     assert np.array_equal(got["init_radius"], single["init_radius"])
 
 
