@@ -247,7 +247,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
         (st = dalloc(c, &c->bkey, cap)) || (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &b->bscene, cap)) ||
         (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
-        (st = dalloc(c, &c->bord, (size_t)cap * CELLS)) ||
+        (st = dalloc(c, &c->bord, (size_t)cap * CELLS)) || (st = dalloc(c, &c->qorder, cap)) ||
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||
@@ -270,6 +270,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     cudaMemset(c->err, 0, 4);
     cudaMemset(c->small, 0, 16);
     cudaMemset(c->body_imp, 0, (size_t)b->max_bodies * 6 * sizeof(unsigned long long));
+
     cudaMemset(c->mat_hkeys, 0xff, MAT_HASH * 4);
     cudaMemset(b->scene_nblk, 0, b->max_scenes * 4);
     cudaMemset(b->scenes_dev, 0, b->max_scenes * sizeof(SceneRec));

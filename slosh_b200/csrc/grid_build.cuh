@@ -633,7 +633,25 @@ template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
 // (copy_particles_len_to_scan_value + prefix_sum +
 // copy_scan_values_to_first_particles, sort.slang:248-302).  One CTA.
 template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) {
-    cta_scan_vec16<NT>(s.bnp, s.bfirst, s.ctr->n_blocks);
+    const uint32_t nb = s.ctr->n_blocks;
+    cta_scan_vec16<NT>(s.bnp, s.bfirst, nb);
+    // P2G's queue order, heaviest blocks first (buckets of 8 particles), so
+    // that the last blocks its warps take are light and they finish together.
+    __shared__ uint32_t cnt[64];
+    if (threadIdx.x < 64) cnt[threadIdx.x] = 0u;
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < nb; r += NT) atomicAdd(&cnt[min(s.bnp[r] >> 3, 63u)], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int b = 63; b >= 0; --b) {
+            const uint32_t c = cnt[b];
+            cnt[b] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < nb; r += NT) s.qorder[atomicAdd(&cnt[min(s.bnp[r] >> 3, 63u)], 1u)] = r;
 }
 
 // Per particle: claim its slot in the block's cell range (the primary part

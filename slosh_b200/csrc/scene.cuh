@@ -64,6 +64,7 @@ struct DevScene {
     uint32_t *bnp;         // number of primary particles
     uint32_t *bcell;       // 64 per block: first entry of each cell, relative to bfirst
     uint32_t *bcur;        // 64 per block: insertion cursors, relative to bfirst
+    uint32_t *qorder;      // ranks of the blocks, heaviest first: P2G's queue order
     uint2 *bord;           // 64 per block: cells by decreasing particle count (ties: cell index),
                            // each (cell | first << 6, count) with first relative to bfirst
     uint32_t *bnbh;        // (NASSOC - 1) neighbour ranks per block, NONE if inactive

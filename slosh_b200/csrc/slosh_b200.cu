@@ -48,6 +48,7 @@ struct slosh_ctx {
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
              *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr, *bnbh_rev = nullptr;
     uint2 *bord = nullptr;
+    uint32_t *qorder = nullptr;
     // P2G reduction (environment SLOSH_P2G at creation): 0 fixed-order,
     // bit-reproducible (default); 3 "direct": the same cell-owner kernel with
     // shared-memory and global float atomics, kept for A/B comparison.
@@ -191,6 +192,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.bnp = c->bnp;
     s.bcell = c->bcell;
     s.bord = c->bord;
+    s.qorder = c->qorder;
     s.bcur = c->bcur;
     s.bnbh = c->bnbh;
     s.bnbh_rev = c->bnbh_rev;
@@ -509,7 +511,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) || (st = dalloc(c, &c->bkey, cap)) ||
         (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
-        (st = dalloc(c, &c->bord, (size_t)cap * CELLS)) ||
+        (st = dalloc(c, &c->bord, (size_t)cap * CELLS)) || (st = dalloc(c, &c->qorder, cap)) ||
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||

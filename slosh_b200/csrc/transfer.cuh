@@ -292,7 +292,10 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
         __shared__ uint32_t coop_r;
         for (;;) {
             __syncthreads();  // the previous block's tile sum has read the slab tiles
-            if (threadIdx.x == 0) coop_r = atomicAdd(&s.ctr->p2g_next, 1u);
+            if (threadIdx.x == 0) {
+                const uint32_t q = atomicAdd(&s.ctr->p2g_next, 1u);
+                coop_r = q < nb ? s.qorder[q] : nb;
+            }
             __syncthreads();
             const uint32_t r = coop_r;
             if (r >= nb) break;
@@ -319,9 +322,12 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
     // One warp a block.  Blocks are taken from a queue (one atomic a
     // block), so warps that get light blocks take more of them.
     auto next_block = [&]() {
-        uint32_t q = 0;
-        if (lane == 0) q = atomicAdd(&s.ctr->p2g_next, 1u);
-        return __shfl_sync(FULL_MASK, q, 0);
+        uint32_t r = 0;
+        if (lane == 0) {
+            const uint32_t q = atomicAdd(&s.ctr->p2g_next, 1u);
+            r = q < nb ? s.qorder[q] : nb;
+        }
+        return __shfl_sync(FULL_MASK, r, 0);
     };
     for (uint32_t r = next_block(); r < nb; r = next_block()) {
         const uint32_t np = s.bnp[r];
