@@ -452,17 +452,26 @@ __global__ void k_bin_scatter(DevScene s) {
 }
 
 // Canonical rank = number of active keys smaller than this one.  Keys of one
-// top-16-bit bin are compared against each other only.
+// top-16-bit bin are compared against each other only, by RANK_LANES lanes
+// a key, each counting every RANK_LANES-th key of the bin (a bin holds a
+// whole z slab of a compact scene, hundreds of keys).
+constexpr uint32_t RANK_LANES = 8;
 __global__ void k_rank(DevScene s) {
     const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const uint32_t g = threadIdx.x % RANK_LANES;
+    const unsigned gmask = ((1u << RANK_LANES) - 1u) << (lane_id() & ~(RANK_LANES - 1u));
+    const uint32_t stride = gridDim.x * (blockDim.x / RANK_LANES);
+    for (uint32_t t = blockIdx.x * (blockDim.x / RANK_LANES) + threadIdx.x / RANK_LANES; t < total; t += stride) {
         const uint32_t key = s.tmp_key[t];
         const uint32_t b = key >> 16;
-        const uint32_t start = s.hist_start[b], cnt = s.hist[b];
-        uint32_t r = start;
-        for (uint32_t j = start; j < start + cnt; ++j) r += (s.tmp_key[j] < key) ? 1u : 0u;
-        if (r < s.cap) {
+        const uint32_t start = s.hist_start[b], end = start + s.hist[b];
+        uint32_t part = 0;
+#pragma unroll 4
+        for (uint32_t j = start + g; j < end; j += RANK_LANES) part += (s.tmp_key[j] < key) ? 1u : 0u;
+#pragma unroll
+        for (uint32_t off = RANK_LANES / 2; off > 0; off >>= 1) part += __shfl_xor_sync(gmask, part, off);
+        const uint32_t r = start + part;
+        if (g == 0 && r < s.cap) {
             const uint32_t slot = s.tmp_slot[t];
             s.bkey[r] = key;
             s.bslot[r] = slot;

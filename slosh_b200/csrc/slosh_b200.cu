@@ -273,7 +273,7 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
     k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(3);
     PROF_BEGIN(4);
-    k_rank<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    k_rank<<<grid_for(2ull * c->cap * RANK_LANES, 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(4);
     PROF_BEGIN(5);
     k_block_setup<D><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
