@@ -248,6 +248,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
         (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
         (st = dalloc(c, &c->bord, (size_t)cap * CELLS)) || (st = dalloc(c, &c->qorder, cap)) ||
+        (st = dalloc(c, &c->bprev, cap)) ||
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||

@@ -569,7 +569,8 @@ template <int NT, uint32_t PMIN, uint32_t PMAX> __global__ void __launch_bounds_
 // One warp per block: per-cell counts (cleared in the hash-slot array once
 // read) with their in-block exclusive scan, the block total, the cells in
 // decreasing count order for P2G's thread assignment, the +1 and -1
-// neighbour ranks (update_nbh_block_ids, sort.slang:100-117) and, for the
+// neighbour ranks (update_nbh_block_ids, sort.slang:100-117), the block's
+// rank in the previous substep's map (the grid update's collision cache) and, for the
 // atomic P2G variants, zeroed nodes (reset, grid.slang:455-485).
 template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
     constexpr int NN = Geo<D>::NASSOC - 1;
@@ -634,6 +635,9 @@ template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
             const uint32_t rank = (slot == NONE) ? NONE : s.hvals[slot];
             if (fwd) s.bnbh[r * NN + q] = rank;
             else s.bnbh_rev[r * NN + q] = rank;
+        } else if (lane == (uint32_t)(2 * NN)) {
+            const uint32_t slot = map_find_prev<B>(s, s.bkey[r], B ? s.bscene[r] : 0u);
+            s.bprev[r] = (slot == NONE) ? NONE : s.prev_hvals[slot];
         }
     }
 }

@@ -72,6 +72,7 @@ struct DevScene {
     uint32_t *perm;        // primary order: scatter output, canonicalised in place
     unsigned long long *skey;  // beside perm: (cell << 32 | original id), the canonical sort key
     uint32_t *bnbh_rev;    // (NASSOC - 1) ranks of the blocks b - o (the -1 neighbours), NONE if inactive
+    uint32_t *bprev;       // rank of the block in the previous substep's map (its collision cache), NONE if new
     float4 *nodes;         // 64 nodes per block: (momentum | velocity, mass)
     float4 *partial;       // TILE nodes per block: the block's own P2G sums over its (block + 2)^D tile
     uint32_t use_partial;  // P2G wrote `partial` (deterministic path); grid update gathers it

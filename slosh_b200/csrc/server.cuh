@@ -7,9 +7,9 @@
 // 70 % as particle pool (280 bytes a particle: two copies of the 128-byte
 // particle state and of the original-index plane, the sort key, the
 // permutation and the cell slot) and up to 30 % as block
-// capacity (8752 bytes a block: hash slots, per-cell counts, cursors and order,
+// capacity (8756 bytes a block: hash slots, per-cell counts, cursors and order,
 // neighbour ranks, the P2G partial tile, nodes and the collision caches).  A
-// request's footprint is n * 280 + blocks * 8752 with blocks estimated as
+// request's footprint is n * 280 + blocks * 8756 with blocks estimated as
 // 2.5 n / 512 + 64 (8 particles per cell fill 512 per block; the factor
 // covers the +1 neighbour blocks and partly filled blocks).  Admission needs
 // the pool's free particles, the estimated blocks and a free scene slot.
@@ -59,7 +59,7 @@ struct slosh_server {
 namespace {
 
 constexpr uint64_t POOL_BYTES_PER_PARTICLE = 280;
-constexpr uint64_t POOL_BYTES_PER_BLOCK = 8752;
+constexpr uint64_t POOL_BYTES_PER_BLOCK = 8756;
 constexpr uint32_t AUTOTUNE_SUBSTEPS = 12;  // 6 launch shapes x (1 warm-up + 1 timed)
 
 uint32_t request_blocks(uint32_t n) { return (uint32_t)(2.5 * (double)n / 512.0) + 64u; }

@@ -48,7 +48,7 @@ struct slosh_ctx {
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
              *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr, *bnbh_rev = nullptr;
     uint2 *bord = nullptr;
-    uint32_t *qorder = nullptr;
+    uint32_t *qorder = nullptr, *bprev = nullptr;
     // P2G reduction (environment SLOSH_P2G at creation): 0 fixed-order,
     // bit-reproducible (default); 3 "direct": the same cell-owner kernel with
     // shared-memory and global float atomics, kept for A/B comparison.
@@ -196,6 +196,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.bcur = c->bcur;
     s.bnbh = c->bnbh;
     s.bnbh_rev = c->bnbh_rev;
+    s.bprev = c->bprev;
     s.pslot = c->pslot;
     s.perm = c->perm;
     s.skey = c->skey;
@@ -512,6 +513,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
         (st = dalloc(c, &c->bord, (size_t)cap * CELLS)) || (st = dalloc(c, &c->qorder, cap)) ||
+        (st = dalloc(c, &c->bprev, cap)) ||
         (st = dalloc(c, &c->bnbh, (size_t)cap * nnb(D))) || (st = dalloc(c, &c->bnbh_rev, (size_t)cap * nnb(D))) ||
         (st = dalloc(c, &c->partial, (size_t)cap * (D == 3 ? Geo<3>::TILE : Geo<2>::TILE))) ||
         (st = dalloc(c, &c->pslot, N)) || (st = dalloc(c, &c->perm, N)) ||

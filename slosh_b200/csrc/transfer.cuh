@@ -300,7 +300,11 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
             const uint32_t r = coop_r;
             if (r >= nb) break;
             const uint32_t np = s.bnp[r];
-            if (np == 0) continue;
+            if (np == 0) {  // the grid update gathers every neighbour's tile
+                for (int t = (int)threadIdx.x; t < TILE; t += 32 * P2G_WARPS)
+                    s.partial[(size_t)r * TILE + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+                continue;
+            }
             const uint32_t first = s.bfirst[r];
             if (first + np > s.n) {
                 if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
@@ -331,7 +335,10 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
     };
     for (uint32_t r = next_block(); r < nb; r = next_block()) {
         const uint32_t np = s.bnp[r];
-        if (np == 0) continue;
+        if (np == 0) {  // the grid update gathers every neighbour's tile
+            for (int t = (int)lane; t < TILE; t += 32) s.partial[(size_t)r * TILE + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
         const uint32_t first = s.bfirst[r];
         if (first + np > s.n) {  // only after an earlier overflow left stale counts
             if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
@@ -835,8 +842,9 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
                     mul *= TW;
                 }
                 if (!inside) continue;
+                // blocks without particles store a zero tile
                 const uint32_t ra = (q == 0) ? r : s.bnbh_rev[r * NN + q - 1];
-                if (ra == NONE || ra >= nb || s.bnp[ra] == 0u) continue;
+                if (ra >= nb) continue;
                 const float4 v = s.partial[(size_t)ra * Geo<D>::TILE + tix];
                 nv.x += v.x;
                 nv.y += v.y;
@@ -861,8 +869,7 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
         }
         float4 cn;
         uint32_t cid;
-        const uint32_t pslot = map_find_prev<B>(s, key, sc);
-        const uint32_t prank = (pslot == NONE) ? NONE : s.prev_hvals[pslot];
+        const uint32_t prank = s.bprev[r];
         if (prank != NONE && !s.coll_dynamic) {
             cn = s.prev_coll[(size_t)prank * 64u + node];
             cid = s.prev_coll_id[(size_t)prank * 64u + node];
