@@ -242,7 +242,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
         (st = dalloc(c, &c->hvals[1], hcap)) || (st = dalloc(c, &c->slot_counts, (size_t)hcap * CELLS)) ||
         (st = dalloc(c, &c->blist_key, cap)) || (st = dalloc(c, &c->blist_slot, cap)) ||
         (st = dalloc(c, &c->blist2_key, cap)) || (st = dalloc(c, &c->blist2_slot, cap)) ||
-        (st = dalloc(c, &c->hist, HIST_BINS)) || (st = dalloc(c, &c->hist_fill, HIST_BINS)) ||
+        (st = dalloc(c, &c->hist, HIST_BINS)) || (st = dalloc(c, &c->hist_coarse, HIST_COARSE)) ||
         (st = dalloc(c, &c->tmp_key, 2 * (size_t)cap)) || (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) ||
         (st = dalloc(c, &c->bkey, cap)) || (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &b->bscene, cap)) ||
         (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||

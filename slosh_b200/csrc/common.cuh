@@ -14,6 +14,7 @@ constexpr uint32_t MAX_BODIES = 16;       // collide() unrolls 16 shapes (collid
 constexpr uint32_t MAX_MATERIALS = 4096;  // distinct particle models per context
 constexpr uint32_t MAT_HASH = 8192;       // material hash slots (power of two)
 constexpr uint32_t HIST_BINS = 65536;     // top-16-bit bins of the packed block key
+constexpr uint32_t HIST_COARSE = 64;      // sums of 1024 consecutive bins (key >> 26)
 
 // Device error bits (accumulated; read by slosh_sync).
 constexpr uint32_t ERR_HASH_OVERFLOW = 1u << 0;    // block hash map full

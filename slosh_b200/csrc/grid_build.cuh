@@ -143,10 +143,8 @@ template <bool B = false> __global__ void k_clear(DevScene s) {
         for (uint32_t i = tid; i < s.n_scenes; i += stride) s.scene_nblk[i] = 0u;
     if (*s.err != 0u)
         for (size_t i = tid; i < (size_t)s.hcap * CELLS; i += stride) s.slot_counts[i] = 0u;
-    for (uint32_t i = tid; i < HIST_BINS; i += stride) {
-        s.hist[i] = 0u;
-        s.hist_fill[i] = 0u;
-    }
+    for (uint32_t i = tid; i < HIST_BINS; i += stride) s.hist[i] = 0u;
+    if (tid < HIST_COARSE) s.hist_coarse[tid] = 0u;
     if (tid == 0) {
         s.ctr->n_primary = 0u;
         s.ctr->n_extra = 0u;
@@ -231,6 +229,9 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
 
 // Activates the +1 neighbours of every primary block, one thread per
 // (block, neighbour).  Replaces touch_neighbor_blocks (sort.slang:75-92).
+// Single scene: also counts the primary and the new blocks in the coarse
+// histogram (key >> 26), aggregated over the warp (a compact scene has one
+// or two coarse bins, so per-block atomics would all hit one address).
 template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t np = min(s.ctr->n_primary, s.cap);
@@ -239,13 +240,14 @@ template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
         const uint32_t j = t / NN;
         const int sidx = (int)(t % NN) + 1;
         int b[D], o[D];
-        unpack_key<D>(s.blist_key[j], b);
+        const uint32_t pkey = s.blist_key[j];
+        unpack_key<D>(pkey, b);
         assoc_offset<D>(sidx, o);
         for (int k = 0; k < D; ++k) b[k] += o[k];
         const uint32_t key = pack_key<D>(b);
         uint32_t sc = 0;
         if constexpr (B) sc = (uint32_t)(s.hkeys64[s.blist_slot[j]] >> 32);
-        bool inserted = false;
+        bool inserted = false, counted = false;
         const uint32_t slot = map_insert<B>(s, key, sc, inserted);
         if (inserted) {
             const uint32_t jj = atomicAdd(&s.ctr->n_extra, 1u);
@@ -254,9 +256,18 @@ template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
                 s.blist2_slot[jj] = slot;
                 if constexpr (B) atomicAdd(&s.scene_nblk[sc], 1u);
                 else atomicAdd(&s.hist[key >> 16], 1u);
+                counted = true;
             } else {
                 atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             }
+        }
+        if constexpr (!B) {
+            const unsigned act = __activemask();
+            const uint32_t lane = lane_id();
+            const uint32_t cp = sidx == 1 ? pkey >> 26 : NONE, ce = counted ? key >> 26 : NONE;
+            const unsigned pp = __match_any_sync(act, cp), pe = __match_any_sync(act, ce);
+            if (cp != NONE && (int)lane == __ffs(pp) - 1) atomicAdd(&s.hist_coarse[cp], (uint32_t)__popc(pp));
+            if (ce != NONE && (int)lane == __ffs(pe) - 1) atomicAdd(&s.hist_coarse[ce], (uint32_t)__popc(pe));
         }
     }
 }
@@ -372,65 +383,39 @@ template <int NT> __device__ __forceinline__ uint32_t cta_scan_vec16(const uint3
     return carry;
 }
 
-// Exclusive scan of the key histogram (one CTA) and the final block count.
-// Warp w owns HIST_BINS / (NT / 32) consecutive bins, read as rows of 32
-// uint4 (one coalesced 512-byte load per row, BATCH rows in flight).  Pass 1
-// sums each warp's bins and scans the warp totals across the CTA; pass 2
-// re-reads the rows (L2 hits) and writes the prefix, a warp scan per row
-// with a running carry.
+// Exclusive scan of the key histogram and the final block count.  CTA c
+// scans bins [1024 c, 1024 c + 1024), one uint4 a thread, on top of the
+// coarse counts of the bins before them.
 template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) {
-    constexpr uint32_t NW = NT / 32, SEG = HIST_BINS / NW, ROWS = SEG / 128, BATCH = 8;
-    static_assert(SEG % 128 == 0 && ROWS % BATCH == 0, "bins per warp");
+    constexpr uint32_t PER = HIST_BINS / HIST_COARSE, NW = NT / 32;
+    static_assert(PER == 4 * NT && HIST_COARSE <= 64, "one uint4 of bins a thread");
     __shared__ uint32_t wtot[NW];
-    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    const uint4 *in = reinterpret_cast<const uint4 *>(s.hist + (size_t)w * SEG);
-    uint32_t part = 0;
-    for (uint32_t q0 = 0; q0 < ROWS; q0 += BATCH) {
-        uint4 v[BATCH];
-#pragma unroll
-        for (uint32_t q = 0; q < BATCH; ++q) v[q] = in[(q0 + q) * 32 + lane];
-#pragma unroll
-        for (uint32_t q = 0; q < BATCH; ++q) part += v[q].x + v[q].y + v[q].z + v[q].w;
-    }
-    part = __reduce_add_sync(FULL_MASK, part);
-    if (lane == 0) wtot[w] = part;
-    __syncthreads();
+    __shared__ uint32_t base;
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5, c = blockIdx.x;
     if (w == 0) {
-        const uint32_t t = lane < NW ? wtot[lane] : 0u;
-        uint32_t incl = t;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
-            if (lane >= (uint32_t)off) incl += y;
-        }
-        if (lane < NW) wtot[lane] = incl - t;
+        uint32_t v = (lane < c ? s.hist_coarse[lane] : 0u) + (lane + 32u < c ? s.hist_coarse[lane + 32u] : 0u);
+        v = __reduce_add_sync(FULL_MASK, v);
+        if (lane == 0) base = v;
     }
+    const uint4 v = reinterpret_cast<const uint4 *>(s.hist + (size_t)c * PER)[threadIdx.x];
+    const uint32_t sum = v.x + v.y + v.z + v.w;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
+        if (lane >= (uint32_t)off) incl += y;
+    }
+    if (lane == 31) wtot[w] = incl;
     __syncthreads();
-    uint32_t carry = wtot[w];
-    uint4 *out = reinterpret_cast<uint4 *>(s.hist_start + (size_t)w * SEG);
-    for (uint32_t q0 = 0; q0 < ROWS; q0 += BATCH) {
-        uint4 v[BATCH];
-#pragma unroll
-        for (uint32_t q = 0; q < BATCH; ++q) v[q] = in[(q0 + q) * 32 + lane];
-#pragma unroll
-        for (uint32_t q = 0; q < BATCH; ++q) {
-            const uint32_t sum = v[q].x + v[q].y + v[q].z + v[q].w;
-            uint32_t incl = sum;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
-                if (lane >= (uint32_t)off) incl += y;
-            }
-            uint4 o;
-            o.x = carry + incl - sum;
-            o.y = o.x + v[q].x;
-            o.z = o.y + v[q].y;
-            o.w = o.z + v[q].z;
-            out[(q0 + q) * 32 + lane] = o;
-            carry += __shfl_sync(FULL_MASK, incl, 31);
-        }
-    }
-    if (threadIdx.x == 0) {
+    uint32_t pre = base;
+    for (uint32_t q = 0; q < w; ++q) pre += wtot[q];
+    uint4 o;
+    o.x = pre + incl - sum;
+    o.y = o.x + v.x;
+    o.z = o.y + v.y;
+    o.w = o.z + v.z;
+    reinterpret_cast<uint4 *>(s.hist_start + (size_t)c * PER)[threadIdx.x] = o;
+    if (c == 0 && threadIdx.x == 0) {
         const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
         if (total > s.cap) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
         s.ctr->n_blocks = min(total, s.cap);
@@ -445,7 +430,7 @@ __global__ void k_bin_scatter(DevScene s) {
         const uint32_t key = t < n1 ? s.blist_key[t] : s.blist2_key[t - n1];
         const uint32_t slot = t < n1 ? s.blist_slot[t] : s.blist2_slot[t - n1];
         const uint32_t b = key >> 16;
-        const uint32_t pos = s.hist_start[b] + atomicAdd(&s.hist_fill[b], 1u);
+        const uint32_t pos = atomicAdd(&s.hist_start[b], 1u);
         s.tmp_key[pos] = key;
         s.tmp_slot[pos] = slot;
     }
@@ -464,7 +449,7 @@ __global__ void k_rank(DevScene s) {
     for (uint32_t t = blockIdx.x * (blockDim.x / RANK_LANES) + threadIdx.x / RANK_LANES; t < total; t += stride) {
         const uint32_t key = s.tmp_key[t];
         const uint32_t b = key >> 16;
-        const uint32_t start = s.hist_start[b], end = start + s.hist[b];
+        const uint32_t end = s.hist_start[b], start = end - s.hist[b];  // advanced by k_bin_scatter
         uint32_t part = 0;
 #pragma unroll 4
         for (uint32_t j = start + g; j < end; j += RANK_LANES) part += (s.tmp_key[j] < key) ? 1u : 0u;

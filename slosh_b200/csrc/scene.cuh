@@ -54,8 +54,8 @@ struct DevScene {
     uint32_t *blist2_key;  // neighbour-only blocks in append order [cap]
     uint32_t *blist2_slot;
     uint32_t *hist;        // HIST_BINS counts of key >> 16
-    uint32_t *hist_start;
-    uint32_t *hist_fill;
+    uint32_t *hist_start;  // their exclusive scan; k_bin_scatter advances it to the bins' ends
+    uint32_t *hist_coarse; // HIST_COARSE counts of key >> 26
     uint32_t *tmp_key;     // [2 cap] keys grouped by key >> 16
     uint32_t *tmp_slot;
     uint32_t *bkey;        // canonical block order: packed key [cap]

@@ -44,7 +44,7 @@ struct slosh_ctx {
     // grid
     uint32_t *hkeys[2] = {nullptr, nullptr}, *hvals[2] = {nullptr, nullptr};
     uint32_t *slot_counts = nullptr, *blist_key = nullptr, *blist_slot = nullptr, *blist2_key = nullptr,
-             *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_fill = nullptr, *tmp_key = nullptr,
+             *blist2_slot = nullptr, *hist = nullptr, *hist_start = nullptr, *hist_coarse = nullptr, *tmp_key = nullptr,
              *tmp_slot = nullptr, *bkey = nullptr, *bslot = nullptr, *bfirst = nullptr, *bnp = nullptr,
              *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr, *bnbh_rev = nullptr;
     uint2 *bord = nullptr;
@@ -183,7 +183,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.blist2_slot = c->blist2_slot;
     s.hist = c->hist;
     s.hist_start = c->hist_start;
-    s.hist_fill = c->hist_fill;
+    s.hist_coarse = c->hist_coarse;
     s.tmp_key = c->tmp_key;
     s.tmp_slot = c->tmp_slot;
     s.bkey = c->bkey;
@@ -268,7 +268,7 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
     k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(1);
     PROF_BEGIN(2);
-    k_hist_scan<1024><<<1, 1024, 0, st>>>(s);
+    k_hist_scan<256><<<HIST_COARSE, 256, 0, st>>>(s);
     PROF_END(2);
     PROF_BEGIN(3);
     k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
@@ -508,7 +508,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->blist_key, cap)) || (st = dalloc(c, &c->blist_slot, cap)) ||
         (st = dalloc(c, &c->blist2_key, cap)) || (st = dalloc(c, &c->blist2_slot, cap)) ||
         (st = dalloc(c, &c->hist, HIST_BINS)) || (st = dalloc(c, &c->hist_start, HIST_BINS)) ||
-        (st = dalloc(c, &c->hist_fill, HIST_BINS)) || (st = dalloc(c, &c->tmp_key, 2 * (size_t)cap)) ||
+        (st = dalloc(c, &c->hist_coarse, HIST_COARSE)) || (st = dalloc(c, &c->tmp_key, 2 * (size_t)cap)) ||
         (st = dalloc(c, &c->tmp_slot, 2 * (size_t)cap)) || (st = dalloc(c, &c->bkey, cap)) ||
         (st = dalloc(c, &c->bslot, cap)) || (st = dalloc(c, &c->bfirst, cap)) || (st = dalloc(c, &c->bnp, cap)) ||
         (st = dalloc(c, &c->bcur, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bcell, (size_t)cap * CELLS)) ||
@@ -574,7 +574,7 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     }
     CK(cudaMemsetAsync(c->slot_counts, 0, (size_t)c->hcap * CELLS * 4, st));
     CK(cudaMemsetAsync(c->hist, 0, HIST_BINS * 4, st));
-    CK(cudaMemsetAsync(c->hist_fill, 0, HIST_BINS * 4, st));
+    CK(cudaMemsetAsync(c->hist_coarse, 0, HIST_COARSE * 4, st));
     c->parity = 0;
     if (n > 0) {
         DevScene s = make_scene(c, 0, false);

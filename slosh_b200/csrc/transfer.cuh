@@ -972,10 +972,8 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
         if constexpr (B) {
             for (uint32_t q = g0; q < s.n_scenes; q += gs) s.scene_nblk[q] = 0u;
         } else {
-            for (uint32_t q = g0; q < HIST_BINS; q += gs) {
-                s.hist[q] = 0u;
-                s.hist_fill[q] = 0u;
-            }
+            for (uint32_t q = g0; q < HIST_BINS; q += gs) s.hist[q] = 0u;
+            if (g0 < HIST_COARSE) s.hist_coarse[g0] = 0u;
         }
         if (*s.err != 0u)
             for (size_t q = g0; q < (size_t)s.hcap * CELLS; q += gs) s.slot_counts[q] = 0u;
