@@ -660,7 +660,8 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
 // particles handled by one warp land in storage order, which is already the
 // canonical order for particles that stayed in their cell.  Only cells split
 // between two chunks (and cells entered from another cell) need k_canon's
-// fix-up.
+// fix-up.  Like k_touch, a warp remembers the block of its last lane (hash
+// slot -> rank, first entry), so most iterations go straight to the claim.
 template <bool B = false> __global__ void k_scatter(DevScene s) {
     const uint32_t lane = lane_id();
     const uint32_t n = n_particles<B>(s);
@@ -669,21 +670,38 @@ template <bool B = false> __global__ void k_scatter(DevScene s) {
     const uint32_t chunk = (((n + warps - 1) / warps) + 31u) & ~31u;
     const uint32_t begin = wid * chunk;
     const uint32_t end = min(n, begin + chunk);
+    uint32_t c_slot = NONE, c_r = NONE, c_first = 0;
+    uint32_t bin_next = begin + lane < end ? s.pslot[begin + lane] : NONE;
     for (uint32_t base = begin; base < end; base += 32) {
         const uint32_t i = base + lane;
         const bool valid = i < end;
         const unsigned mask = __ballot_sync(FULL_MASK, valid);
         if (!valid) break;
-        const uint32_t bin = s.pslot[i];
+        const uint32_t bin = bin_next;
+        bin_next = i + 32u < end ? s.pslot[i + 32u] : NONE;
         const unsigned peers = __match_any_sync(mask, bin);
         const int leader = __ffs(peers) - 1;
-        uint32_t pos = NONE;
+        const uint32_t sl = bin >> 6;
+        uint32_t pos = NONE, r = NONE, first = 0;
         if ((int)lane == leader && bin != NONE) {
-            const uint32_t r = s.hvals[bin >> 6];
-            if (r != NONE)
-                pos = s.bfirst[r] + atomicAdd(&s.bcur[(size_t)r * CELLS + (bin & 63u)], (uint32_t)__popc(peers));
+            if (sl == c_slot) {
+                r = c_r;
+                first = c_first;
+            } else {
+                r = s.hvals[sl];
+                if (r != NONE) first = s.bfirst[r];
+            }
+            if (r != NONE) pos = first + atomicAdd(&s.bcur[(size_t)r * CELLS + (bin & 63u)], (uint32_t)__popc(peers));
         }
         pos = __shfl_sync(mask, pos, leader);
+        r = __shfl_sync(mask, r, leader);
+        first = __shfl_sync(mask, first, leader);
+        const int top = 31 - __clz(mask);
+        if (__shfl_sync(mask, bin, top) != NONE) {
+            c_slot = __shfl_sync(mask, sl, top);
+            c_r = __shfl_sync(mask, r, top);
+            c_first = __shfl_sync(mask, first, top);
+        }
         if (pos != NONE) {
             const uint32_t at = pos + __popc(peers & lanemask_lt());
             if (at < s.n) {
@@ -703,8 +721,10 @@ template <bool B = false> __global__ void k_scatter(DevScene s) {
 // storage order, so most cells come out sorted; the ones that do not are
 // cells whose particles were scattered by two different warps.  One warp per
 // block compares neighbouring keys (coalesced loads of the block's
-// contiguous entries), and the lanes owning an out-of-order cell
-// insertion-sort it, keys and permutation together.
+// contiguous entries); each out-of-order cell is then sorted by the whole
+// warp: lane l holds entry l, its rank is the number of smaller original ids
+// (shuffles), and entries are stored at their ranks.  Cells of more than 32
+// entries are insertion-sorted by one lane.
 __device__ __forceinline__ void sort_cell_keys(unsigned long long *key, uint32_t *perm, uint32_t m) {
     for (uint32_t j = 1; j < m; ++j) {
         const unsigned long long kj = key[j];
@@ -740,12 +760,32 @@ __global__ void k_canon(DevScene s) {
         const uint32_t lo = __reduce_or_sync(FULL_MASK, (uint32_t)bad);
         const uint32_t hi = __reduce_or_sync(FULL_MASK, (uint32_t)(bad >> 32));
         if ((lo | hi) == 0u) continue;
-        for (uint32_t c = lane; c < CELLS; c += 32) {
-            const uint32_t word = c < 32 ? lo : hi;
-            if (!((word >> (c & 31u)) & 1u)) continue;
+        unsigned long long cells = ((unsigned long long)hi << 32) | lo;
+        while (cells != 0ull) {
+            const uint32_t c = (uint32_t)__ffsll((long long)cells) - 1u;
+            cells &= cells - 1ull;
             const uint32_t b0 = s.bcell[(size_t)r * CELLS + c];
             const uint32_t b1 = (c < CELLS - 1) ? s.bcell[(size_t)r * CELLS + c + 1] : np;
-            if (b1 > b0 + 1) sort_cell_keys(s.skey + first + b0, s.perm + first + b0, b1 - b0);
+            if (b1 <= b0 + 1 || b1 > np) continue;
+            const uint32_t m = b1 - b0;
+            unsigned long long *ck = s.skey + first + b0;
+            uint32_t *cp = s.perm + first + b0;
+            if (m > 32u) {
+                if (lane == 0) sort_cell_keys(ck, cp, m);
+                __syncwarp();
+                continue;
+            }
+            const unsigned long long kl = lane < m ? ck[lane] : ~0ull;
+            const uint32_t pl = lane < m ? cp[lane] : 0u;
+            const uint32_t id = (uint32_t)kl;  // the cell part of the keys is equal
+            uint32_t rank = 0;
+            for (uint32_t j = 0; j < m; ++j) rank += __shfl_sync(FULL_MASK, id, j) < id ? 1u : 0u;
+            __syncwarp();  // every lane has read its entry
+            if (lane < m) {
+                ck[rank] = kl;
+                cp[rank] = pl;
+            }
+            __syncwarp();
         }
     }
 }
