@@ -561,7 +561,10 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     if (n > c->max_n) return fail(c, SLOSH_E_CAPACITY, "%u particles exceed max_particles %u", n, c->max_n);
     CK(cudaSetDevice(c->device));
     cudaStream_t st = pick(c, stream);
-    destroy_graphs(c);
+    // The substep graphs bake the particle count and the scene flags in; an
+    // upload that keeps them keeps the graphs.
+    const uint32_t old_mat = c->n_materials, old_damp = c->has_damping, old_sand = c->has_sand;
+    if (n != c->n) destroy_graphs(c);
     c->n = n;
     CK(cudaMemcpyAsync(c->staging, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(c->mat_hkeys, 0xff, MAT_HASH * 4, st));
@@ -599,6 +602,7 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     c->has_damping = (small[1] & SCENE_DAMPING) ? 1u : 0u;
     c->force_pending = (small[1] & SCENE_FORCE) ? 1u : 0u;
     c->has_sand = (small[1] & SCENE_SAND) ? 1u : 0u;
+    if (c->n_materials != old_mat || c->has_damping != old_damp || c->has_sand != old_sand) destroy_graphs(c);
     return check_device_error(c);
 }
 
