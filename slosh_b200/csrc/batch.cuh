@@ -52,7 +52,7 @@ struct slosh_batch {
     slosh_particle *up = nullptr;
     uint32_t up_cap = 0, up_used = 0, staged_n = 0;
     cudaStream_t up_stream = nullptr;
-    slosh_tuning tune{5, 128, 8, 0};
+    slosh_tuning tune{5, 64, 8, 0};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
     uint32_t graph_flags = 0;       // has_damping | has_sand << 1 the graphs were captured with
@@ -672,8 +672,8 @@ int batch_autotune(slosh_batch *b, uint32_t substeps, void *stream, uint32_t *ra
     }
     CK(cudaSetDevice(c->device));
     cudaStream_t st = pick(c, stream);
-    const slosh_tuning cands[] = {{5, 128, 8, 0}, {4, 128, 4, 0},  {10, 128, 16, 0},
-                                  {5, 64, 16, 0}, {5, 256, 4, 0},  {4, 64, 8, 0}};
+    const slosh_tuning cands[] = {{5, 64, 8, 0},  {5, 128, 8, 0}, {4, 128, 4, 0},
+                                  {10, 128, 16, 0}, {5, 64, 16, 0}, {4, 64, 8, 0}};
     const uint32_t reps = std::max<uint32_t>(substeps, 1u);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));

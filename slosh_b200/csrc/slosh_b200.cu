@@ -321,8 +321,10 @@ void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force,
     enqueue_p2g<D>(c, s, st, p);
     enqueue_grid_update<D>(c, s, st, p);
     PROF_BEGIN(11);
-    // persistent: 4 CTAs of 128 fit an SM; each takes blocks from the queue
-    k_g2p_update<D, 128><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 4), 128, 0, st>>>(s);
+    // persistent: 8 CTAs of 64 fit an SM; each takes blocks from the queue.
+    // Small CTAs wait less at the per-block barriers (tile load, the
+    // slowest thread's last particle) than CTAs of 128 or 256.
+    k_g2p_update<D, 64><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), 64, 0, st>>>(s);
     PROF_END(11);
     PROF_BEGIN(12);
     k_rigid<D><<<1, 32, 0, st>>>(s);
