@@ -9,6 +9,10 @@
 namespace slosh {
 
 constexpr uint32_t NONE = 0xffffffffu;
+// Flag of a block-map value (a block rank): the block holds no particles
+// (a neighbour-only block), so P2G wrote no tile for it.
+constexpr uint32_t RANK_EXTRA = 0x80000000u;
+__host__ __device__ __forceinline__ uint32_t rank_of(uint32_t v) { return v == NONE ? NONE : (v & ~RANK_EXTRA); }
 constexpr unsigned FULL_MASK = 0xffffffffu;
 constexpr uint32_t MAX_BODIES = 16;       // collide() unrolls 16 shapes (collide.slang:362-363)
 constexpr uint32_t MAX_MATERIALS = 4096;  // distinct particle models per context

@@ -432,7 +432,7 @@ __global__ void k_bin_scatter(DevScene s) {
         const uint32_t b = key >> 16;
         const uint32_t pos = atomicAdd(&s.hist_start[b], 1u);
         s.tmp_key[pos] = key;
-        s.tmp_slot[pos] = slot;
+        s.tmp_slot[pos] = slot | (t < n1 ? 0u : RANK_EXTRA);
     }
 }
 
@@ -457,10 +457,10 @@ __global__ void k_rank(DevScene s) {
         for (uint32_t off = RANK_LANES / 2; off > 0; off >>= 1) part += __shfl_xor_sync(gmask, part, off);
         const uint32_t r = start + part;
         if (g == 0 && r < s.cap) {
-            const uint32_t slot = s.tmp_slot[t];
+            const uint32_t ts = s.tmp_slot[t], slot = ts & ~RANK_EXTRA;
             s.bkey[r] = key;
             s.bslot[r] = slot;
-            s.hvals[slot] = r;
+            s.hvals[slot] = r | (ts & RANK_EXTRA);
         }
     }
 }
@@ -491,7 +491,7 @@ __global__ void k_scene_scatter(DevScene s) {
         const uint32_t pos = atomicAdd(&s.scene_fill[sc], 1u);
         if (pos < 2u * s.cap) {
             s.tmp_key[pos] = key;
-            s.tmp_slot[pos] = slot;
+            s.tmp_slot[pos] = slot | (t < n1 ? 0u : RANK_EXTRA);
         }
     }
 }
@@ -541,11 +541,11 @@ template <int NT, uint32_t PMIN, uint32_t PMAX> __global__ void __launch_bounds_
             const uint32_t r = base + q;
             if (r >= s.cap) break;
             const unsigned long long v = sbuf[q];
-            const uint32_t slot = (uint32_t)v;
+            const uint32_t ts = (uint32_t)v, slot = ts & ~RANK_EXTRA;
             s.bkey[r] = (uint32_t)(v >> 32);
             s.bslot[r] = slot;
             s.bscene[r] = sc;
-            s.hvals[slot] = r;
+            s.hvals[slot] = r | (ts & RANK_EXTRA);
         }
         __syncthreads();
     }
@@ -617,12 +617,13 @@ template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
             assoc_offset<D>(q + 1, o);
             for (int k = 0; k < D; ++k) b[k] += fwd ? o[k] : -o[k];
             const uint32_t slot = map_find<B>(s, pack_key<D>(b), B ? s.bscene[r] : 0u);
-            const uint32_t rank = (slot == NONE) ? NONE : s.hvals[slot];
-            if (fwd) s.bnbh[r * NN + q] = rank;
-            else s.bnbh_rev[r * NN + q] = rank;
+            const uint32_t v = (slot == NONE) ? NONE : s.hvals[slot];
+            // the grid update gathers the tiles of the -1 neighbours that hold particles
+            if (fwd) s.bnbh[r * NN + q] = rank_of(v);
+            else s.bnbh_rev[r * NN + q] = (v & RANK_EXTRA) ? NONE : v;
         } else if (lane == (uint32_t)(2 * NN)) {
             const uint32_t slot = map_find_prev<B>(s, s.bkey[r], B ? s.bscene[r] : 0u);
-            s.bprev[r] = (slot == NONE) ? NONE : s.prev_hvals[slot];
+            s.bprev[r] = (slot == NONE) ? NONE : rank_of(s.prev_hvals[slot]);
         }
     }
 }
@@ -688,7 +689,7 @@ template <bool B = false> __global__ void k_scatter(DevScene s) {
                 r = c_r;
                 first = c_first;
             } else {
-                r = s.hvals[sl];
+                r = rank_of(s.hvals[sl]);
                 if (r != NONE) first = s.bfirst[r];
             }
             if (r != NONE) pos = first + atomicAdd(&s.bcur[(size_t)r * CELLS + (bin & 63u)], (uint32_t)__popc(peers));

@@ -302,7 +302,7 @@ __device__ __forceinline__ bool particle_rank_local(const DevScene &s, uint32_t 
     const CellLoc<D> c = locate<D>(x, s.h, s.inv_h, s.h_pow2);
     const uint32_t slot = hash_find(s.hkeys, s.hcap, pack_key<D>(c.block));
     if (slot == NONE) return false;
-    r0 = s.hvals[slot];
+    r0 = rank_of(s.hvals[slot]);
     if (r0 == NONE) return false;
     for (int k = 0; k < D; ++k) a[k] = c.local[k];
     return true;

@@ -300,11 +300,7 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
             const uint32_t r = coop_r;
             if (r >= nb) break;
             const uint32_t np = s.bnp[r];
-            if (np == 0) {  // the grid update gathers every neighbour's tile
-                for (int t = (int)threadIdx.x; t < TILE; t += 32 * P2G_WARPS)
-                    s.partial[(size_t)r * TILE + t] = make_float4(0.f, 0.f, 0.f, 0.f);
-                continue;
-            }
+            if (np == 0) continue;
             const uint32_t first = s.bfirst[r];
             if (first + np > s.n) {
                 if (threadIdx.x == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
@@ -335,10 +331,7 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
     };
     for (uint32_t r = next_block(); r < nb; r = next_block()) {
         const uint32_t np = s.bnp[r];
-        if (np == 0) {  // the grid update gathers every neighbour's tile
-            for (int t = (int)lane; t < TILE; t += 32) s.partial[(size_t)r * TILE + t] = make_float4(0.f, 0.f, 0.f, 0.f);
-            continue;
-        }
+        if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
         if (first + np > s.n) {  // only after an earlier overflow left stale counts
             if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
@@ -842,8 +835,9 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
                     mul *= TW;
                 }
                 if (!inside) continue;
-                // blocks without particles store a zero tile
-                const uint32_t ra = (q == 0) ? r : s.bnbh_rev[r * NN + q - 1];
+                // blocks without particles have no tile (their -1
+                // neighbour ranks are NONE)
+                const uint32_t ra = (q == 0) ? (s.bnp[r] != 0u ? r : NONE) : s.bnbh_rev[r * NN + q - 1];
                 if (ra >= nb) continue;
                 const float4 v = s.partial[(size_t)ra * Geo<D>::TILE + tix];
                 nv.x += v.x;
