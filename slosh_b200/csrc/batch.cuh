@@ -80,6 +80,9 @@ DevScene make_batch_scene(slosh_batch *b, uint32_t parity) {
     s.n_bodies = b->body_top;
     s.use_partial = 1u;
     s.p2g_coop_below = 0u;  // one mode for every scene: a scene's bits do not depend on its batch
+    // Batches of many small scenes have tens of thousands of blocks: one CTA
+    // ordering them costs more than the balance gains, so P2G takes ranks in order.
+    s.p2g_heavy_first = 0u;
     return s;
 }
 

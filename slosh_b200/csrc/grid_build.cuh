@@ -636,6 +636,7 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
     cta_scan_vec16<NT>(s.bnp, s.bfirst, nb);
     // P2G's queue order, heaviest blocks first (buckets of 8 particles), so
     // that the last blocks its warps take are light and they finish together.
+    if (!s.p2g_heavy_first) return;
     __shared__ uint32_t cnt[64];
     if (threadIdx.x < 64) cnt[threadIdx.x] = 0u;
     __syncthreads();

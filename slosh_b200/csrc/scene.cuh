@@ -77,6 +77,7 @@ struct DevScene {
     float4 *partial;       // TILE nodes per block: the block's own P2G sums over its (block + 2)^D tile
     uint32_t use_partial;  // P2G wrote `partial` (deterministic path); grid update gathers it
     uint32_t p2g_coop_below;  // P2G shares a block between a CTA's warps below this many blocks
+    uint32_t p2g_heavy_first; // P2G takes blocks in `qorder` (heaviest first), else in rank order
     uint32_t gather_only;  // grid update stops after the gather (P2G node sums, debug)
     float4 *coll;          // node collision cache of this substep: (normal, d0)
     uint32_t *coll_id;     // collider id or NONE

@@ -207,6 +207,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     // P2G: one warp a block fills the GPU from about 10 blocks an SM; below
     // that a CTA's four warps share each block
     s.p2g_coop_below = (uint32_t)c->sm_count * 10u;
+    s.p2g_heavy_first = 1u;
     s.coll = c->coll[cur];
     s.coll_id = c->coll_id[cur];
     s.prev_coll = c->coll[prv];

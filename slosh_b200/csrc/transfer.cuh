@@ -294,7 +294,7 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
             __syncthreads();  // the previous block's tile sum has read the slab tiles
             if (threadIdx.x == 0) {
                 const uint32_t q = atomicAdd(&s.ctr->p2g_next, 1u);
-                coop_r = q < nb ? s.qorder[q] : nb;
+                coop_r = q < nb ? (s.p2g_heavy_first ? s.qorder[q] : q) : nb;
             }
             __syncthreads();
             const uint32_t r = coop_r;
@@ -325,7 +325,7 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
         uint32_t r = 0;
         if (lane == 0) {
             const uint32_t q = atomicAdd(&s.ctr->p2g_next, 1u);
-            r = q < nb ? s.qorder[q] : nb;
+            r = q < nb ? (s.p2g_heavy_first ? s.qorder[q] : q) : nb;
         }
         return __shfl_sync(FULL_MASK, r, 0);
     };
