@@ -194,7 +194,9 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
         const uint32_t key = pack_key<D>(c.block);
         const uint32_t cell = cell_index<D>(c.local);
         const unsigned long long ckey = live ? (((unsigned long long)sc << 32) | key) : NONE64;
-        const unsigned peers = __match_any_sync(mask, ckey);
+        unsigned peers;
+        if constexpr (B) peers = __match_any_sync(mask, ckey);
+        else peers = __match_any_sync(mask, key);  // one scene: the 32-bit key is the whole key
         const int leader = __ffs(peers) - 1;
         uint32_t slot = NONE;
         if ((int)lane == leader && live) {
@@ -218,7 +220,8 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
         }
         slot = __shfl_sync(mask, slot, leader);
         const int top = 31 - __clz(mask);  // last valid lane: its block is the likeliest next
-        last_key = __shfl_sync(mask, ckey, top);
+        if constexpr (B) last_key = __shfl_sync(mask, ckey, top);
+        else last_key = __shfl_sync(mask, key, top);
         last_slot = __shfl_sync(mask, slot, top);
         const uint32_t bin = (slot == NONE) ? NONE : (slot << 6) | cell;
         const unsigned peers2 = __match_any_sync(mask, bin);
