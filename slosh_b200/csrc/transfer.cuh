@@ -79,21 +79,39 @@ __device__ __forceinline__ bool p2g_particle(const float4 p, const float4 vv, co
     }
     const float fsl = (float)slab;
     if constexpr (D == 3) {
+        // Paired FP32 arithmetic (sm_100 f32x2 FMA): the node value
+        // (b + s h C, m) is carried as the pairs (x, y) and (z, m); the m
+        // lane's offsets are zero, so it stays m exactly.  Offset 0 adds
+        // nothing to a finite value and is skipped.
         const float wz = slab == 0 ? w[2][0] : (slab == 1 ? w[2][1] : w[2][2]);
-        const float mz0 = bm[0] + fsl * hc[2][0], mz1 = bm[1] + fsl * hc[2][1], mz2 = bm[2] + fsl * hc[2][2];
+        const float2 hx01 = make_float2(hc[0][0], hc[0][1]), hx2 = make_float2(hc[0][2], 0.f);
+        const float2 hy01 = make_float2(hc[1][0], hc[1][1]), hy2 = make_float2(hc[1][2], 0.f);
+        const float2 fs2 = make_float2(fsl, fsl);
+        const float2 mz01 = __ffma2_rn(fs2, make_float2(hc[2][0], hc[2][1]), make_float2(bm[0], bm[1]));
+        const float2 mz2 = __ffma2_rn(fs2, make_float2(hc[2][2], 0.f), make_float2(bm[2], m));
 #pragma unroll
         for (int sy = 0; sy < 3; ++sy) {
             const float wyz = w[1][sy] * wz;
-            const float my0 = mz0 + (float)sy * hc[1][0], my1 = mz1 + (float)sy * hc[1][1],
-                        my2 = mz2 + (float)sy * hc[1][2];
+            float2 my01 = mz01, my2 = mz2;
+            if (sy > 0) {
+                const float2 sy2 = make_float2((float)sy, (float)sy);
+                my01 = __ffma2_rn(sy2, hy01, mz01);
+                my2 = __ffma2_rn(sy2, hy2, mz2);
+            }
 #pragma unroll
             for (int sx = 0; sx < 3; ++sx) {
+                float2 t01 = my01, t2 = my2;
+                if (sx > 0) {
+                    const float2 sx2 = make_float2((float)sx, (float)sx);
+                    t01 = __ffma2_rn(sx2, hx01, my01);
+                    t2 = __ffma2_rn(sx2, hx2, my2);
+                }
                 const float wt = w[0][sx] * wyz;
+                const float2 wt2 = make_float2(wt, wt);
                 float4 &a = acc[sx + 3 * sy];
-                a.x += wt * (my0 + (float)sx * hc[0][0]);
-                a.y += wt * (my1 + (float)sx * hc[0][1]);
-                a.z += wt * (my2 + (float)sx * hc[0][2]);
-                a.w += wt * m;
+                const float2 axy = __ffma2_rn(wt2, t01, make_float2(a.x, a.y));
+                const float2 azw = __ffma2_rn(wt2, t2, make_float2(a.z, a.w));
+                a = make_float4(axy.x, axy.y, azw.x, azw.y);
             }
         }
     } else {
