@@ -136,6 +136,12 @@ __device__ __forceinline__ void bspline_weights(float x, float *w) {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// Pairs for sm_100's f32x2 arithmetic (__ffma2_rn and friends): one
+// instruction computes two FP32 lanes, each rounded as its scalar form.
+__device__ __forceinline__ float2 pair(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 lo_pair(const float4 &v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi_pair(const float4 &v) { return make_float2(v.z, v.w); }
+
 // Asynchronous global -> shared copies (cp.async), used to stage the next
 // particle's inputs while the current one is computed.
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {

@@ -1075,68 +1075,82 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
                 //   vel_grad_det = trace(grad v),
                 // with M0 = sum_s w_s v_s and M_r = sum_s w_s s_r v_s,
                 // accumulated axis by axis.
-                float M0[D], Mr[D][D];
+                // Separable gather in paired FP32 arithmetic: the node
+                // velocity (x, y, z, mass) is read as the pairs (x, y) and
+                // (z, mass); the mass lane is carried along unused.  Terms
+                // with offset 0 (s_r = 0) add nothing and are skipped.
+                constexpr int NP = (D == 3) ? 2 : 1;
+                float2 M0p[NP], Mrp[D][NP];
 #pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    M0[c] = 0.f;
+                for (int q = 0; q < NP; ++q) {
+                    M0p[q] = make_float2(0.f, 0.f);
 #pragma unroll
-                    for (int k = 0; k < D; ++k) Mr[k][c] = 0.f;
+                    for (int k = 0; k < D; ++k) Mrp[k][q] = make_float2(0.f, 0.f);
                 }
-                const float wx0 = w[0][0], wx1 = w[0][1], wx2 = w[0][2], wx2b = 2.f * w[0][2];
+                const float2 wx0p = pair(w[0][0]), wx1p = pair(w[0][1]), wx2p = pair(w[0][2]),
+                             wx2bp = pair(2.f * w[0][2]);
+                auto row = [&](const float4 &n0, const float4 &n1, const float4 &n2, int q, float2 &R0, float2 &Rx) {
+                    const float2 v0 = q ? hi_pair(n0) : lo_pair(n0), v1 = q ? hi_pair(n1) : lo_pair(n1),
+                                 v2 = q ? hi_pair(n2) : lo_pair(n2);
+                    R0 = __ffma2_rn(wx2p, v2, __ffma2_rn(wx1p, v1, __fmul2_rn(wx0p, v0)));
+                    Rx = __ffma2_rn(wx2bp, v2, __fmul2_rn(wx1p, v1));
+                };
                 if constexpr (D == 3) {
 #pragma unroll
                     for (int sz = 0; sz < 3; ++sz) {
-                        float S0[3] = {0.f, 0.f, 0.f}, Sx[3] = {0.f, 0.f, 0.f}, Sy[3] = {0.f, 0.f, 0.f};
+                        float2 S0[2], Sx[2], Sy[2];
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) S0[q] = Sx[q] = Sy[q] = make_float2(0.f, 0.f);
 #pragma unroll
                         for (int sy = 0; sy < 3; ++sy) {
                             const int idx = a[0] + TW * ((a[1] + sy) + TW * (a[2] + sz));
-                            const float wy = w[1][sy], wys = (float)sy * w[1][sy];
+                            const float2 wyp = pair(w[1][sy]), wysp = pair((float)sy * w[1][sy]);
                             const float4 n0 = tv[idx], n1 = tv[idx + 1], n2 = tv[idx + 2];
-                            const float a0[3] = {n0.x, n0.y, n0.z}, a1[3] = {n1.x, n1.y, n1.z},
-                                        a2[3] = {n2.x, n2.y, n2.z};
 #pragma unroll
-                            for (int c = 0; c < 3; ++c) {
-                                const float v0 = a0[c], v1 = a1[c], v2 = a2[c];
-                                const float R0 = wx0 * v0 + wx1 * v1 + wx2 * v2;
-                                const float Rx = wx1 * v1 + wx2b * v2;
-                                S0[c] += wy * R0;
-                                Sx[c] += wy * Rx;
-                                Sy[c] += wys * R0;
+                            for (int q = 0; q < 2; ++q) {
+                                float2 R0, Rx;
+                                row(n0, n1, n2, q, R0, Rx);
+                                S0[q] = __ffma2_rn(wyp, R0, S0[q]);
+                                Sx[q] = __ffma2_rn(wyp, Rx, Sx[q]);
+                                if (sy > 0) Sy[q] = __ffma2_rn(wysp, R0, Sy[q]);
                             }
                         }
-                        const float wz = w[2][sz], wzs = (float)sz * w[2][sz];
+                        const float2 wzp = pair(w[2][sz]), wzsp = pair((float)sz * w[2][sz]);
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            M0[c] += wz * S0[c];
-                            Mr[0][c] += wz * Sx[c];
-                            Mr[1][c] += wz * Sy[c];
-                            Mr[2][c] += wzs * S0[c];
+                        for (int q = 0; q < 2; ++q) {
+                            M0p[q] = __ffma2_rn(wzp, S0[q], M0p[q]);
+                            Mrp[0][q] = __ffma2_rn(wzp, Sx[q], Mrp[0][q]);
+                            Mrp[1][q] = __ffma2_rn(wzp, Sy[q], Mrp[1][q]);
+                            if (sz > 0) Mrp[2][q] = __ffma2_rn(wzsp, S0[q], Mrp[2][q]);
                         }
                     }
                 } else {
 #pragma unroll
                     for (int sy = 0; sy < 3; ++sy) {
                         const int idx = a[0] + TW * (a[1] + sy);
-                        const float wy = w[1][sy], wys = (float)sy * w[1][sy];
-                        const float4 n0 = tv[idx], n1 = tv[idx + 1], n2 = tv[idx + 2];
-                        const float a0[2] = {n0.x, n0.y}, a1[2] = {n1.x, n1.y}, a2[2] = {n2.x, n2.y};
-#pragma unroll
-                        for (int c = 0; c < 2; ++c) {
-                            const float v0 = a0[c], v1 = a1[c], v2 = a2[c];
-                            const float R0 = wx0 * v0 + wx1 * v1 + wx2 * v2;
-                            const float Rx = wx1 * v1 + wx2b * v2;
-                            M0[c] += wy * R0;
-                            Mr[0][c] += wy * Rx;
-                            Mr[1][c] += wys * R0;
-                        }
+                        const float2 wyp = pair(w[1][sy]), wysp = pair((float)sy * w[1][sy]);
+                        float2 R0, Rx;
+                        row(tv[idx], tv[idx + 1], tv[idx + 2], 0, R0, Rx);
+                        M0p[0] = __ffma2_rn(wyp, R0, M0p[0]);
+                        Mrp[0][0] = __ffma2_rn(wyp, Rx, Mrp[0][0]);
+                        if (sy > 0) Mrp[1][0] = __ffma2_rn(wysp, R0, Mrp[1][0]);
                     }
                 }
+                // v = M0, grad v[c][r] = inv_d (d0_r M0_c + h M_r,c), pairs over c
+                const float2 hp = pair(h), invdp = pair(inv_d);
 #pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    vel[c] = M0[c];
+                for (int rr = 0; rr < D; ++rr) {
+                    const float2 d0p = pair(d0[rr]);
 #pragma unroll
-                    for (int rr = 0; rr < D; ++rr) grad[c][rr] = inv_d * (d0[rr] * M0[c] + h * Mr[rr][c]);
+                    for (int q = 0; q < NP; ++q) {
+                        const float2 g = __fmul2_rn(invdp, __ffma2_rn(d0p, M0p[q], __fmul2_rn(hp, Mrp[rr][q])));
+                        grad[2 * q][rr] = g.x;
+                        if (2 * q + 1 < D) grad[2 * q + 1][rr] = g.y;
+                    }
                 }
+                vel[0] = M0p[0].x;
+                vel[1] = M0p[0].y;
+                if constexpr (D == 3) vel[2] = M0p[1].x;
                 div = grad[0][0] + grad[1][1];
                 if constexpr (D == 3) div += grad[2][2];
             }
@@ -1172,16 +1186,25 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
                 mat_from<D>(fv, __uint_as_float(fo.w), F);
             }
             if (!fluid) {
+                // F <- F + (dt grad v) F, row by row in column pairs (c, c + 1)
                 float Fn[D][D];
 #pragma unroll
-                for (int rr = 0; rr < D; ++rr)
+                for (int rr = 0; rr < D; ++rr) {
+                    float2 g[D];
 #pragma unroll
-                    for (int c = 0; c < D; ++c) {
-                        float acc = 0.f;
+                    for (int k = 0; k < D; ++k) g[k] = pair(grad[rr][k] * dt);
 #pragma unroll
-                        for (int k = 0; k < D; ++k) acc += F[k][c] * (grad[rr][k] * dt);
-                        Fn[rr][c] = F[rr][c] + acc;
+                    for (int c = 0; c < D; c += 2) {
+                        const bool two = c + 1 < D;
+                        auto col = [&](int k) { return make_float2(F[k][c], two ? F[k][c + 1] : 0.f); };
+                        float2 acc = __fmul2_rn(col(0), g[0]);
+#pragma unroll
+                        for (int k = 1; k < D; ++k) acc = __ffma2_rn(col(k), g[k], acc);
+                        const float2 r = __fadd2_rn(make_float2(F[rr][c], two ? F[rr][c + 1] : 0.f), acc);
+                        Fn[rr][c] = r.x;
+                        if (two) Fn[rr][c + 1] = r.y;
                     }
+                }
 #pragma unroll
                 for (int rr = 0; rr < D; ++rr)
 #pragma unroll
