@@ -325,7 +325,9 @@ void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force,
     // persistent: 8 CTAs of 64 fit an SM; each takes blocks from the queue.
     // Small CTAs wait less at the per-block barriers (tile load, the
     // slowest thread's last particle) than CTAs of 128 or 256.
-    k_g2p_update<D, 64><<<std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8), 64, 0, st>>>(s);
+    const uint32_t g2p_grid = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
+    if (s.h_pow2) k_g2p_update<D, 64, false, true><<<g2p_grid, 64, 0, st>>>(s);
+    else k_g2p_update<D, 64, false, false><<<g2p_grid, 64, 0, st>>>(s);
     PROF_END(11);
     PROF_BEGIN(12);
     k_rigid<D><<<1, 32, 0, st>>>(s);

@@ -957,7 +957,10 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
 // staged into shared memory with cp.async while the current particle is
 // computed; each thread consumes only its own staged slot, so the particle
 // loop has no barrier.
-template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
+// POW2: the cell width is a power of two (known at launch), so x / h is
+// exactly x * (1/h) and no division is compiled in.
+template <int D, int NT, bool B = false, bool POW2 = false>
+__global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float4 tv[TILE];  // node (velocity, mass): one 16-byte load per node
     constexpr int Q = MQ<D>::Q;
@@ -1058,11 +1061,11 @@ template <int D, int NT, bool B = false> __global__ void __launch_bounds__(NT, 5
                 bool in_block = true;
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
-                    const float assoc = rintf(div_h(x[k], h, inv_h, h_pow2)) - 1.0f;
+                    const float assoc = rintf(POW2 ? x[k] * inv_h : div_h(x[k], h, inv_h, h_pow2)) - 1.0f;
                     a[k] = (int)assoc - bv[k] * BW;
                     in_block = in_block && a[k] >= 0 && a[k] < BW;
                     d0[k] = assoc * h - x[k];
-                    bspline_weights(div_h(-d0[k], h, inv_h, h_pow2), w[k]);
+                    bspline_weights(POW2 ? -d0[k] * inv_h : div_h(-d0[k], h, inv_h, h_pow2), w[k]);
                 }
                 if (!in_block) {  // packed-key aliasing: gather nothing
                     atomicOr(s.err, ERR_KEY_RANGE);

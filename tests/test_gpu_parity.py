@@ -157,6 +157,24 @@ def test_substep_parity(cuda_lib, name):
     data.close()
 
 
+@pytest.mark.parametrize("dim", [3, 2])
+def test_substep_parity_cell_width_not_power_of_two(cuda_lib, dim):
+    """A cell width that is not a power of two takes the correctly rounded
+    division x / h (a power of two multiplies by 1/h): grid build bit-exact
+    and substeps within the FP32 tolerance of the oracle."""
+    sc = scenes.sand_column_3d(h=1 / 48, substeps=10) if dim == 3 else scenes.dam_break_2d(h=1 / 96, substeps=10)
+    data, orc = pair(sc)
+    grid_equal(data.grid_debug(), orc.grid())
+    pipe = MpmPipeline()
+    pipe.launch_step(data, 1)
+    orc.step(1)
+    compare_particles(f"h=1/{round(1 / sc.cell_width)} 1 step", data.download_particles(), orc.get_particles(), dim)
+    pipe.launch_step(data, 9)
+    orc.step(9)
+    compare_particles(f"h=1/{round(1 / sc.cell_width)} 10 steps", data.download_particles(), orc.get_particles(), dim, loose=10.0)
+    data.close()
+
+
 @pytest.mark.parametrize("name", ["sand3d_fine", "fluid2d"])
 def test_bit_reproducible(cuda_lib, name, monkeypatch):
     """The default P2G reduces in a fixed order (no float atomics), so two
