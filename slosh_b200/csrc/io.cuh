@@ -13,12 +13,14 @@ struct IoBuffers {
     uint32_t *mat_hkeys;       // MAT_HASH material-key hashes
     uint32_t *mat_dense;       // MAT_HASH dense material ids
     uint32_t *n_mat;           // device counter
-    uint32_t *scene_flags;     // bit0 damping, bit1 force, bit2 sand
+    uint32_t *scene_flags;     // bit0 damping, bit1 force, bit2 sand, bits 8-15 model tags
     float *r0;
     float *phase;
 };
 
 constexpr uint32_t SCENE_DAMPING = 1u, SCENE_FORCE = 2u, SCENE_SAND = 4u;
+// bits SCENE_MODEL_SHIFT + tag: the model tags present (tags above 6 share bit 7)
+constexpr uint32_t SCENE_MODEL_SHIFT = 8;
 
 // Words of the material key: tag + 12 payload words, with the per-particle
 // plastic state (payload words 0..2 of the sand models) zeroed.
@@ -146,6 +148,7 @@ __global__ void k_ingest(DevScene s, IoBuffers io, uint32_t base, uint32_t count
         s.ps[i] = sand ? make_float4(p.model.data[0], p.model.data[1], p.model.data[2], p.damping)
                        : make_float4(0.f, 0.f, 0.f, p.damping);
         if (sand) sflags |= SCENE_SAND;
+        sflags |= 1u << (SCENE_MODEL_SHIFT + min(p.model.tag, 7u));
     }
     sflags = __reduce_or_sync(FULL_MASK, sflags);
     if (lane_id() == 0 && sflags) atomicOr(io.scene_flags, sflags);

@@ -196,10 +196,12 @@ __device__ __forceinline__ void drucker_prager(float *st, const float *p, SvdD<D
 
 // DefaultParticleModel::update (shaders/slosh/models/default.slang:51-92)
 // plus the Tait fluid.  `st` is the particle's plastic state (sand only).
+// `tag` is the material's model tag (a constant when the kernel is
+// instantiated for a scene of one model, which leaves the other models out).
 template <int D>
-__device__ __forceinline__ void model_update(const Material &mat, float (&F)[D][D], float *st, float (&tau)[D][D],
-                                             unsigned *fp64) {
-    switch (mat.tag) {
+__device__ __forceinline__ void model_update(const Material &mat, uint32_t tag, float (&F)[D][D], float *st,
+                                             float (&tau)[D][D], unsigned *fp64) {
+    switch (tag) {
         case SLOSH_MODEL_ELASTIC_LINEAR: {
             SvdD<D> sv;
             sv.compute(F, fp64);

@@ -40,6 +40,7 @@ struct slosh_ctx {
     Material *materials = nullptr;
     uint32_t *mat_hkeys = nullptr, *mat_dense = nullptr;
     uint32_t has_damping = 0, force_pending = 0, has_sand = 0, n_materials = 0;
+    uint32_t model_mask = 0;  // model tags present among the particles (bit = tag)
 
     // grid
     uint32_t *hkeys[2] = {nullptr, nullptr}, *hvals[2] = {nullptr, nullptr};
@@ -325,9 +326,17 @@ void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force,
     // persistent: 8 CTAs of 64 fit an SM; each takes blocks from the queue.
     // Small CTAs wait less at the per-block barriers (tile load, the
     // slowest thread's last particle) than CTAs of 128 or 256.
+    // Instantiated for a power-of-two cell width and, with it, for scenes
+    // of a single model among the linear elastic, sand and fluid ones.
     const uint32_t g2p_grid = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
-    if (s.h_pow2) k_g2p_update<D, 64, false, true><<<g2p_grid, 64, 0, st>>>(s);
-    else k_g2p_update<D, 64, false, false><<<g2p_grid, 64, 0, st>>>(s);
+    if (!s.h_pow2) k_g2p_update<D, 64, false, false><<<g2p_grid, 64, 0, st>>>(s);
+    else if (c->model_mask == 1u << SLOSH_MODEL_SAND_LINEAR)
+        k_g2p_update<D, 64, false, true, SLOSH_MODEL_SAND_LINEAR><<<g2p_grid, 64, 0, st>>>(s);
+    else if (c->model_mask == 1u << SLOSH_MODEL_ELASTIC_LINEAR)
+        k_g2p_update<D, 64, false, true, SLOSH_MODEL_ELASTIC_LINEAR><<<g2p_grid, 64, 0, st>>>(s);
+    else if (c->model_mask == 1u << SLOSH_MODEL_FLUID_TAIT)
+        k_g2p_update<D, 64, false, true, SLOSH_MODEL_FLUID_TAIT><<<g2p_grid, 64, 0, st>>>(s);
+    else k_g2p_update<D, 64, false, true><<<g2p_grid, 64, 0, st>>>(s);
     PROF_END(11);
     PROF_BEGIN(12);
     k_rigid<D><<<1, 32, 0, st>>>(s);
@@ -568,7 +577,8 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     cudaStream_t st = pick(c, stream);
     // The substep graphs bake the particle count and the scene flags in; an
     // upload that keeps them keeps the graphs.
-    const uint32_t old_mat = c->n_materials, old_damp = c->has_damping, old_sand = c->has_sand;
+    const uint32_t old_mat = c->n_materials, old_damp = c->has_damping, old_sand = c->has_sand,
+                   old_models = c->model_mask;
     if (n != c->n) destroy_graphs(c);
     c->n = n;
     CK(cudaMemcpyAsync(c->staging, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice, st));
@@ -607,7 +617,10 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     c->has_damping = (small[1] & SCENE_DAMPING) ? 1u : 0u;
     c->force_pending = (small[1] & SCENE_FORCE) ? 1u : 0u;
     c->has_sand = (small[1] & SCENE_SAND) ? 1u : 0u;
-    if (c->n_materials != old_mat || c->has_damping != old_damp || c->has_sand != old_sand) destroy_graphs(c);
+    c->model_mask = (small[1] >> SCENE_MODEL_SHIFT) & 0xffu;
+    if (c->n_materials != old_mat || c->has_damping != old_damp || c->has_sand != old_sand ||
+        c->model_mask != old_models)
+        destroy_graphs(c);
     return check_device_error(c);
 }
 
@@ -650,6 +663,7 @@ int slosh_append_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     c->n_materials = small[0];
     c->has_damping = (small[1] & SCENE_DAMPING) ? 1u : 0u;
     c->has_sand = (small[1] & SCENE_SAND) ? 1u : 0u;
+    c->model_mask = (small[1] >> SCENE_MODEL_SHIFT) & 0xffu;
     c->force_pending = (c->force_pending || forces) ? 1u : 0u;
     return check_device_error(c);
 }

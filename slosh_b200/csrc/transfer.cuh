@@ -958,8 +958,10 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
 // computed; each thread consumes only its own staged slot, so the particle
 // loop has no barrier.
 // POW2: the cell width is a power of two (known at launch), so x / h is
-// exactly x * (1/h) and no division is compiled in.
-template <int D, int NT, bool B = false, bool POW2 = false>
+// exactly x * (1/h) and no division is compiled in.  MODEL >= 0: every
+// particle of the scene uses that model tag (known at upload), so only its
+// constitutive code is compiled in; MODEL < 0 reads each particle's tag.
+template <int D, int NT, bool B = false, bool POW2 = false, int MODEL = -1>
 __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     __shared__ float4 tv[TILE];  // node (velocity, mass): one 16-byte load per node
@@ -1159,8 +1161,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
             }
             // ---- particle update ----
             const Material &mat = s.materials[fl & FLAG_MAT_MASK];
-            const bool fluid = mat.tag == SLOSH_MODEL_FLUID_TAIT;
-            const bool sand = mat.tag == SLOSH_MODEL_SAND_LINEAR || mat.tag == SLOSH_MODEL_SAND_NEO_HOOKEAN;
+            const uint32_t tag = MODEL >= 0 ? (uint32_t)MODEL : mat.tag;
+            const bool fluid = tag == SLOSH_MODEL_FLUID_TAIT;
+            const bool sand = tag == SLOSH_MODEL_SAND_LINEAR || tag == SLOSH_MODEL_SAND_NEO_HOOKEAN;
             float len2 = 0.f;
 #pragma unroll
             for (int k = 0; k < D; ++k) len2 += vel[k] * vel[k];
@@ -1232,7 +1235,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
                 st[2] = ps.z;
             }
             float tau[D][D];
-            model_update<D>(mat, F, st, tau, &s.ctr->n_svd_fp64);
+            model_update<D>(mat, tag, F, st, tau, &s.ctr->n_svd_fp64);
             const float v0 = __uint_as_float(fo.z);
             const float coef = v0 * inv_d * dt;
             bool finite = true;

@@ -175,6 +175,40 @@ def test_substep_parity_cell_width_not_power_of_two(cuda_lib, dim):
     data.close()
 
 
+def test_substep_parity_mixed_models(cuda_lib):
+    """A scene mixing every model (both sands, fixed-corotated, neo-Hookean,
+    Tait fluid) runs the kernel that reads each particle's model tag; scenes of
+    one model run kernels compiled for that model alone (the other parity
+    tests)."""
+    h = 1 / 32
+    rng = np.random.default_rng(17)
+    models = [
+        ParticleModel.sand(3.5e5, 0.3, friction_angle_deg=30.0),
+        ParticleModel.elastic(1e5, 0.3),
+        ParticleModel.elastic_neo_hookean(1e5, 0.3),
+        ParticleModel.sand_neo_hookean(3.5e5, 0.3, friction_angle_deg=30.0),
+        ParticleModel.fluid_tait(1000.0, 1e4, 7.0),
+    ]
+    parts = []
+    for k, model in enumerate(models):
+        lo = np.array([0.1 + 0.16 * k, 0.1, 0.4])
+        pts = lo + rng.uniform(0.0, 0.12, size=(400, 3))
+        parts.append(make_particles(pts, h / 4, 1000.0, model, dim=3))
+    parts = np.concatenate(parts)
+    parts["velocity"][:, :3] = rng.normal(scale=0.3, size=(len(parts), 3)).astype(np.float32)
+    floor = RigidBody(("cuboid", (2.0, 4 * h, 2.0)), translation=(0.5, 0.05 - 4 * h, 0.5))
+    sc = scenes.Scene("mixed_models", 3, h, SimulationParams((0.0, -9.81, 0.0), 5e-5), parts, [floor], 10, 4096)
+    data, orc = pair(sc)
+    pipe = MpmPipeline()
+    pipe.launch_step(data, 1)
+    orc.step(1)
+    compare_particles("mixed models 1 step", data.download_particles(), orc.get_particles(), 3)
+    pipe.launch_step(data, 9)
+    orc.step(9)
+    compare_particles("mixed models 10 steps", data.download_particles(), orc.get_particles(), 3, loose=10.0)
+    data.close()
+
+
 @pytest.mark.parametrize("name", ["sand3d_fine", "fluid2d"])
 def test_bit_reproducible(cuda_lib, name, monkeypatch):
     """The default P2G reduces in a fixed order (no float atomics), so two
