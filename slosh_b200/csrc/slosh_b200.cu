@@ -299,7 +299,8 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
         k_p2g_atomic<D><<<g, P2G_ATOMIC_THREADS, 0, st>>>(s);
     } else {
         const uint32_t g = std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, (uint32_t)c->sm_count * 5);
-        k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
+        if (s.force_pending) k_p2g<D, false, true><<<g, 32 * P2G_WARPS, 0, st>>>(s);
+        else k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
     }
     PROF_END(9);
 }

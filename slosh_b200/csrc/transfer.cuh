@@ -157,7 +157,10 @@ template <> struct SlabTile<2> {
     static constexpr int PY = 10, PZ = 0, SIZE = 80;  // x 10, y 8
 };
 
-template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
+// FORCE: the substep adds the particles' pending force impulses (the first
+// substep after they were set); the other substeps compile without them.
+template <int D, bool B = false, bool FORCE = false>
+__global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
     constexpr int PY = SlabTile<D>::PY, PZ = SlabTile<D>::PZ, SSZ = SlabTile<D>::SIZE;
@@ -233,7 +236,7 @@ template <int D, bool B = false> __global__ void __launch_bounds__(32 * P2G_WARP
             if (k < cnt) {
                 const int b = (int)(k % NBUF);
                 float fdt[3] = {0.f, 0.f, 0.f};
-                if (s.force_pending) {
+                if constexpr (FORCE) {
                     const uint32_t i = s.perm[first + lo + k];
 #pragma unroll
                     for (int d = 0; d < D; ++d) fdt[d] = s.fdt[d * n + i];
