@@ -65,8 +65,10 @@ def parse():
     ap.add_argument(
         "--ncu-case",
         action="store_true",
-        help="profiling case for ncu: build the scene at --h, run --steps substeps, print stats, exit",
+        help="profiling case for ncu: build the scene at --h (column radius --radius), run --steps substeps, "
+        "print stats, exit",
     )
+    ap.add_argument("--radius", type=float, default=0.15, help="ncu case: radius of the sand column")
     return ap.parse_args()
 
 
@@ -74,7 +76,7 @@ def main_ncu_case(args):
     from slosh_b200 import scenes
     from slosh_b200.pipeline import MpmPipeline
 
-    sc = bench_scene(args.h)
+    sc = scenes.sand_column_3d(h=args.h, substeps=500, radius=args.radius)
     data = scenes.build_mpm_data(sc)
     MpmPipeline().launch_step(data, args.steps)
     data.sync()

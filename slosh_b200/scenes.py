@@ -142,15 +142,17 @@ def elastic_drop_3d(h: float = 1.0 / 128.0, seed: int = 2, substeps: int = 2000)
     )
 
 
-def sand_column_3d(h: float = 1.0 / 256.0, seed: int = 3, substeps: int = 500, cube_coupling: str = "one_way") -> Scene:
+def sand_column_3d(
+    h: float = 1.0 / 256.0, seed: int = 3, substeps: int = 500, cube_coupling: str = "one_way", radius: float = 0.15
+) -> Scene:
     """Drucker-Prager sand (friction angle 30 deg, E = 3.5e5, nu = 0.3,
-    density 2200): a cylinder of radius 0.15 and height 0.5 standing on a
+    density 2200): a cylinder of radius 0.15 (``radius``) and height 0.5 standing on a
     Separate(1.0) floor at y = 0.05, axis through (0.5, ., 0.5), 8 jittered
     particles per cell, plus a 0.1^3 rigid cuboid (density 500) resting 2h
     above the column, coupled as a collider (one-way; ``cube_coupling``
     "two_way" makes it a dynamic body the sand pushes).  dt = 2e-5."""
     rng = np.random.default_rng(seed)
-    r, height, base = 0.15, 0.5, 0.05
+    r, height, base = radius, 0.5, 0.05
     sp = h / 2
     pts = _lattice((0.5 - r, base, 0.5 - r), (0.5 + r, base + height, 0.5 + r), sp)
     inside = (pts[:, 0] - 0.5) ** 2 + (pts[:, 2] - 0.5) ** 2 <= r * r
