@@ -112,15 +112,19 @@ __device__ __forceinline__ float div_h(float x, float h, float inv_h, uint32_t h
     return h_pow2 ? x * inv_h : __fdiv_rn(x, h);
 }
 
+// Base cell round(x / h) - 1, its block floor(cell / BW) and its place in
+// the block.  One round-to-nearest-even conversion, then integer shifts:
+// the same values as rintf / floorf in float for every |x / h| < 2^24.
 template <int D>
 __device__ __forceinline__ CellLoc<D> locate(const float *x, float h, float inv_h, uint32_t h_pow2) {
+    constexpr int SHIFT = Geo<D>::BW == 4 ? 2 : 3;
+    static_assert(Geo<D>::BW == (1 << SHIFT), "block width is 4 or 8");
     CellLoc<D> c;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        float assoc = rintf(div_h(x[k], h, inv_h, h_pow2)) - 1.0f;
-        float ab = floorf(assoc * (1.0f / Geo<D>::BW));
-        c.block[k] = (int)ab;
-        c.local[k] = (int)(assoc - ab * (float)Geo<D>::BW);
+        const int cell = __float2int_rn(div_h(x[k], h, inv_h, h_pow2)) - 1;
+        c.block[k] = cell >> SHIFT;  // arithmetic shift: floor division
+        c.local[k] = cell & (Geo<D>::BW - 1);
     }
     return c;
 }
