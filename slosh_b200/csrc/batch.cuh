@@ -55,7 +55,8 @@ struct slosh_batch {
     slosh_tuning tune{5, 64, 8, 0};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
-    uint32_t graph_flags = 0;       // has_damping | has_sand << 1 the graphs were captured with
+    uint32_t graph_flags = 0;       // has_damping | has_sand << 1 | all_pow2 << 2 the graphs were captured with
+    uint32_t all_pow2 = 1;          // every scene admitted so far has a power-of-two cell width (sticky)
 };
 
 namespace {
@@ -86,9 +87,12 @@ DevScene make_batch_scene(slosh_batch *b, uint32_t parity) {
     return s;
 }
 
+// While every admitted scene has a power-of-two cell width, G2P compiles
+// x / h as the exact x * (1/h) of each scene.
 template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s, cudaStream_t st) {
     const uint32_t g = std::min<uint32_t>(b->c.cap, (uint32_t)b->c.sm_count * b->tune.g2p_ctas_per_sm);
-    k_g2p_update<D, NT, true><<<g, NT, 0, st>>>(s);
+    if (b->all_pow2) k_g2p_update<D, NT, true, true><<<g, NT, 0, st>>>(s);
+    else k_g2p_update<D, NT, true, false><<<g, NT, 0, st>>>(s);
 }
 
 // One batched substep: 14 kernels over all scenes.
@@ -145,7 +149,7 @@ int build_batch_graphs(slosh_batch *b) {
         if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
     }
     b->graphs_valid = true;
-    b->graph_flags = c->has_damping | (c->has_sand << 1);
+    b->graph_flags = c->has_damping | (c->has_sand << 1) | (b->all_pow2 << 2);
     return SLOSH_OK;
 }
 
@@ -426,6 +430,7 @@ int batch_activate(slosh_batch *b, cudaStream_t st) {
         for (int k = 0; k < 3; ++k) rec.gravity[k] = sg.desc.params.gravity[k];
         int ex = 0;
         rec.h_pow2 = (std::frexp(sg.desc.cell_width, &ex) == 0.5f) ? 1u : 0u;
+        b->all_pow2 &= rec.h_pow2;
         rec.body_first = b->body_top;
         rec.n_bodies = (uint32_t)sg.bodies.size();
         rec.live = 1u;
@@ -445,7 +450,8 @@ int batch_activate(slosh_batch *b, cudaStream_t st) {
     c->has_damping |= (small[1] & SCENE_DAMPING) ? 1u : 0u;
     c->has_sand |= (small[1] & SCENE_SAND) ? 1u : 0u;
     b->n_storage = new_n;
-    if (b->graphs_valid && (b->graph_flags != (c->has_damping | (c->has_sand << 1)) || new_bodies))
+    if (b->graphs_valid &&
+        (b->graph_flags != (c->has_damping | (c->has_sand << 1) | (b->all_pow2 << 2)) || new_bodies))
         destroy_batch_graphs(b);  // captured scene flags or body count changed
     b->staged.clear();
     b->up_used = 0;

@@ -216,3 +216,31 @@ def test_two_way_scene_in_batch_matches_context(cuda_lib):
         close(f"batched ball {k}", body[k][:3], single_body[k][:3], 1e-7, 1e-5)
     for k, v in fields(single).items():
         close(f"batched two-way scene {k}", got[k], v, 1e-7, 1e-6)
+
+
+def test_cell_width_not_power_of_two_joins_batch(cuda_lib):
+    """A scene whose cell width is not a power of two may join a batch of
+    power-of-two scenes (the batch then stops using the multiply-only
+    G2P): the earlier scene keeps its bits, and the new scene advances as in
+    its own batch."""
+    target = scenes.random_scene_3d(8000, "sand", 1 / 64, seed=21)
+    odd = scenes.random_scene_3d(6000, "elastic", 1 / 48, seed=22)
+    alone = new_batch()
+    s0 = alone.add(target)
+    alone.step(12)
+    ref = alone.download_particles(s0)
+    alone.close()
+    odd_alone = new_batch()
+    s1 = odd_alone.add(odd)
+    odd_alone.step(6)
+    ref_odd = odd_alone.download_particles(s1)
+    odd_alone.close()
+    mix = new_batch()
+    st = mix.add(target)
+    mix.step(6)
+    so = mix.add(odd)
+    mix.step(6)
+    got, got_odd = mix.download_particles(st), mix.download_particles(so)
+    mix.close()
+    assert got.tobytes() == ref.tobytes()
+    assert got_odd.tobytes() == ref_odd.tobytes()
