@@ -264,7 +264,7 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
     const uint32_t sm = (uint32_t)c->sm_count;
     if (standalone) k_clear<<<sm * 4, 256, 0, st>>>(s);
     PROF_BEGIN(0);
-    k_touch<D><<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
+    k_touch<D><<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // one wave of warps, a chunk each
     PROF_END(0);
     PROF_BEGIN(1);
     k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
@@ -285,7 +285,7 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
     k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     PROF_END(6);
     PROF_BEGIN(7);
-    k_scatter<<<grid_for(c->n, 256, sm * 16), 256, 0, st>>>(s);
+    k_scatter<<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // longer chunks: fewer cells split for k_canon
     PROF_END(7);
     PROF_BEGIN(8);
     k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
