@@ -507,9 +507,20 @@ def main_batched(args):
     st = b.stats()
 
     # end to end through the public API: every scene uploaded from host
-    # records, K substeps, every scene's positions read back.
-    host = [np.ascontiguousarray(sc.particles) for sc in scs]
-    outs = [np.empty((sc.n, 4), np.float32) for sc in scs]
+    # records in pinned memory, K substeps, every scene's positions read back
+    # into pinned memory.
+    from slosh_b200._lib import PARTICLE_DTYPE
+
+    rec_buf = torch.empty(total * PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+    out_buf = torch.empty(total * 16, dtype=torch.uint8, pin_memory=True)
+    recs = rec_buf.numpy().view(PARTICLE_DTYPE)
+    pos = out_buf.numpy().view(np.float32).reshape(total, 4)
+    host, outs, at = [], [], 0
+    for sc in scs:
+        recs[at : at + sc.n] = sc.particles
+        host.append(recs[at : at + sc.n])
+        outs.append(pos[at : at + sc.n])
+        at += sc.n
     for sl in slots:
         b.remove_scene(sl)
     b.step(1, sptr)

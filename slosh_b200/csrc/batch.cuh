@@ -309,8 +309,48 @@ void slosh_batch_destroy(slosh_batch *b) {
 namespace {
 
 // Checks a scene before anything is claimed; returns its model-tag mask.
+// One pass over a scene's host records: the model tags present, whether any
+// record carries a force impulse, and the host-kept fields (initial radius,
+// phase).  Large scenes are split over a few host threads (the pass reads
+// every 192-byte record, gigabytes for a large batch).
+struct RecordScan {
+    uint32_t tags = 0;
+    bool force = false;
+    std::vector<float> r0, phase;
+};
+void scan_records(const slosh_particle *particles, uint32_t n, RecordScan &out) {
+    out.r0.resize(n);
+    out.phase.resize(n);
+    const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t nt = n >= (1u << 18) ? std::min(hw, 8u) : 1u;
+    std::vector<uint32_t> tags(nt, 0u);
+    std::vector<uint8_t> force(nt, 0u);
+    auto part = [&](uint32_t t) {
+        const uint32_t lo = (uint32_t)((uint64_t)n * t / nt), hi = (uint32_t)((uint64_t)n * (t + 1) / nt);
+        uint32_t m = 0;
+        bool f = false;
+        for (uint32_t i = lo; i < hi; ++i) {
+            const slosh_particle &p = particles[i];
+            f = f || p.force_dt[0] != 0.f || p.force_dt[1] != 0.f || p.force_dt[2] != 0.f;
+            if (p.model.tag < 32) m |= 1u << p.model.tag;
+            out.r0[i] = p.init_radius;
+            out.phase[i] = p.phase;
+        }
+        tags[t] = m;
+        force[t] = f ? 1u : 0u;
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nt; ++t) pool.emplace_back(part, t);
+    part(0);
+    for (auto &th : pool) th.join();
+    for (uint32_t t = 0; t < nt; ++t) {
+        out.tags |= tags[t];
+        out.force = out.force || force[t] != 0u;
+    }
+}
+
 int batch_validate(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles, uint32_t n,
-                   const slosh_body *bodies, uint32_t n_bodies, uint32_t *tags) {
+                   const slosh_body *bodies, uint32_t n_bodies, RecordScan &scan) {
     slosh_ctx *c = &b->c;
     if (n == 0) return fail(c, SLOSH_E_INVALID, "a scene needs particles");
     if (!(desc->cell_width > 0.f) || !(desc->params.dt > 0.f))
@@ -324,14 +364,8 @@ int batch_validate(slosh_batch *b, const slosh_scene_desc *desc, const slosh_par
         if (d.coupling > SLOSH_COUPLING_TWO_WAY)
             return fail(c, SLOSH_E_INVALID, "body %u: unknown coupling %u", k, d.coupling);
     }
-    uint32_t m = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        const slosh_particle &p = particles[i];
-        if (p.force_dt[0] != 0.f || p.force_dt[1] != 0.f || p.force_dt[2] != 0.f)
-            return fail(c, SLOSH_E_INVALID, "external forces (force_dt) are not supported in batches");
-        if (p.model.tag < 32) m |= 1u << p.model.tag;
-    }
-    *tags = m;
+    scan_records(particles, n, scan);
+    if (scan.force) return fail(c, SLOSH_E_INVALID, "external forces (force_dt) are not supported in batches");
     return SLOSH_OK;
 }
 
@@ -341,7 +375,8 @@ int batch_validate(slosh_batch *b, const slosh_scene_desc *desc, const slosh_par
 // SLOSH_E_CAPACITY when the pool, the slots, the body table or the upload
 // buffer cannot take the scene now.
 int batch_stage(slosh_batch *b, const slosh_scene_desc *desc, const slosh_particle *particles, uint32_t n,
-                const slosh_body *bodies, uint32_t n_bodies, uint32_t tags, uint32_t *slot_out) {
+                const slosh_body *bodies, uint32_t n_bodies, RecordScan &scan, uint32_t *slot_out) {
+    const uint32_t tags = scan.tags;
     slosh_ctx *c = &b->c;
     if ((uint64_t)b->n_storage + b->staged_n + n > c->max_n)
         return fail(c, SLOSH_E_CAPACITY, "%u + %u particles exceed the pool of %u", b->n_storage + b->staged_n, n,
@@ -379,12 +414,8 @@ int batch_stage(slosh_batch *b, const slosh_scene_desc *desc, const slosh_partic
     sl.n = n;
     sl.n_bodies = n_bodies;
     sl.tags = tags;
-    sl.r0.resize(n);
-    sl.phase.resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        sl.r0[i] = particles[i].init_radius;
-        sl.phase[i] = particles[i].phase;
-    }
+    sl.r0 = std::move(scan.r0);
+    sl.phase = std::move(scan.phase);
     b->up_used += n;
     b->staged_n += n;
     b->staged.push_back(std::move(sg));
@@ -483,8 +514,8 @@ int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const sl
                           const slosh_body *bodies, uint32_t n_bodies, uint32_t *slot_out, void *stream) {
     if (!b || !desc || (!particles && n) || (!bodies && n_bodies) || !slot_out) return SLOSH_E_INVALID;
     slosh_ctx *c = &b->c;
-    uint32_t tags = 0;
-    int r = batch_validate(b, desc, particles, n, bodies, n_bodies, &tags);
+    RecordScan scan;
+    int r = batch_validate(b, desc, particles, n, bodies, n_bodies, scan);
     if (r) return r;
     CK(cudaSetDevice(c->device));
     CK(cudaDeviceSynchronize());  // no substep may run while the pool and tables change
@@ -502,7 +533,7 @@ int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const sl
         if (r) return r;
         b->staging_cap = n;
     }
-    r = batch_stage(b, desc, particles, n, bodies, n_bodies, tags, slot_out);
+    r = batch_stage(b, desc, particles, n, bodies, n_bodies, scan, slot_out);
     if (r) return r;
     return batch_activate(b, pick(c, stream));
 }

@@ -97,10 +97,11 @@ void stage_pending(slosh_server *s, std::unique_lock<std::mutex> &lk) {
         slosh_server::Req r = q;
         s->queue.pop_front();
         lk.unlock();
-        uint32_t tags = 0, slot = 0;
-        int st = batch_validate(b, &r.r.desc, r.r.particles, r.r.n, r.r.bodies, r.r.n_bodies, &tags);
+        uint32_t slot = 0;
+        RecordScan scan;
+        int st = batch_validate(b, &r.r.desc, r.r.particles, r.r.n, r.r.bodies, r.r.n_bodies, scan);
         if (st == SLOSH_OK)
-            st = batch_stage(b, &r.r.desc, r.r.particles, r.r.n, r.r.bodies, r.r.n_bodies, tags, &slot);
+            st = batch_stage(b, &r.r.desc, r.r.particles, r.r.n, r.r.bodies, r.r.n_bodies, scan, &slot);
         lk.lock();
         s->admitted += 1;
         s->in_flight_bytes += r.bytes;
