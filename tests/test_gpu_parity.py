@@ -488,6 +488,33 @@ def test_append_and_shift_remove(cuda_lib):
     data.close()
 
 
+def test_append_other_model(cuda_lib):
+    """Appending particles of another model to a single-model scene moves
+    the substep from the kernel compiled for that model to the one that
+    reads each particle's tag; stepping matches the oracle."""
+    sc = small_scenes()["elastic3d"]
+    h = sc.cell_width
+    rng = np.random.default_rng(23)
+    sand = make_particles(
+        np.array([0.5, 0.2, 0.5]) + rng.uniform(-0.06, 0.06, size=(600, 3)),
+        h / 4,
+        2200.0,
+        ParticleModel.sand(3.5e5, 0.3, friction_angle_deg=30.0),
+        dim=3,
+    )
+    data = scenes.build_mpm_data(sc, max_particles=len(sc.particles) + len(sand))
+    orc = O.from_scene(sc, threads=8)
+    pipe = MpmPipeline()
+    pipe.launch_step(data, 2)
+    orc.step(2)
+    data.append(sand)
+    orc.set_particles(np.concatenate([orc.get_particles(), sand]))
+    pipe.launch_step(data, 3)
+    orc.step(3)
+    compare_particles("elastic + appended sand", data.download_particles(), orc.get_particles(), 3, loose=5.0)
+    data.close()
+
+
 @pytest.mark.parametrize("dim", [3, 2])
 def test_two_way_coupling_parity(cuda_lib, dim):
     """Two-way coupling against the oracle's restatement: particles and the
