@@ -322,7 +322,7 @@ void scan_records(const slosh_particle *particles, uint32_t n, RecordScan &out) 
     out.r0.resize(n);
     out.phase.resize(n);
     const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const uint32_t nt = n >= (1u << 18) ? std::min(hw, 8u) : 1u;
+    const uint32_t nt = std::max(1u, std::min(std::min(hw, 8u), n >> 15));  // a thread per 32k records
     std::vector<uint32_t> tags(nt, 0u);
     std::vector<uint8_t> force(nt, 0u);
     auto part = [&](uint32_t t) {
