@@ -1170,10 +1170,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
             float len2 = 0.f;
 #pragma unroll
             for (int k = 0; k < D; ++k) len2 += vel[k] * vel[k];
-            const float len = sqrtf(len2);
-            if (len > vmax)
+            // |v| > h / dt, tested on the squares first (sqrt is monotone; the
+            // square root is taken only for a particle that is clamped)
+            if (len2 > vmax * vmax * (1.0f - 4e-7f)) {
+                const float len = sqrtf(len2);
+                if (len > vmax)
 #pragma unroll
-                for (int k = 0; k < D; ++k) vel[k] = vel[k] / len * h / dt;
+                    for (int k = 0; k < D; ++k) vel[k] = vel[k] / len * h / dt;
+            }
             const float4 ps = (s.has_sand | s.has_damping) ? st_ps[buf][tid] : make_float4(0.f, 0.f, 0.f, 0.f);
             if (s.has_damping) {
                 const float dmp = 1.0f + ps.w * dt;
