@@ -327,9 +327,12 @@ int slosh_prefix_sum(slosh_ctx *ctx, const uint32_t *in, uint32_t *out,
  *    SLOSH_E_CAPACITY without launching anything.
  *  - Scratch: a 64 KiB file-scope __device__ array that every GPU loading
  *    the library holds until exit.  It allocates nothing: no cudaMalloc,
- *    cudaFree or allocating library call.  The first call on a device looks
- *    up the array's device address (cudaGetSymbolAddress) with that device
- *    current; make that first call before any stream capture.
+ *    cudaFree or allocating library call.  Every call looks up the array's
+ *    device address (cudaGetSymbolAddress) in the current context, so a
+ *    device reset or a context switch between calls is safe; make the first
+ *    call on a device before any stream capture.
+ *  - Returns SLOSH_E_CUDA without launching while an earlier CUDA error is
+ *    pending on the calling thread, and leaves that error for its owner.
  *  - Every call shares the scratch array: calls that overlap on the GPU
  *    (other streams, other host threads) race and must be serialised by the
  *    caller.  Nothing in the scratch needs to start at zero.

@@ -15,7 +15,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 
 #include "../../include/slosh_b200.h"
 
@@ -32,22 +31,15 @@ constexpr uint64_t NA_MAX_N = (uint64_t)NA_TILE * NA_MAX_TILES;  // 67,108,864
 // on the GPU race on it.
 __device__ __align__(256) uint32_t g_scan_scratch[NA_MAX_TILES];
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_mutex;
-uint32_t *g_scratch_ptr[MAX_DEVICES] = {};
-
-// Device address of g_scan_scratch on the current device, looked up once per
-// device (the host-side symbol is only a stand-in for the device array).
-int scratch_for_current_device(uint32_t **out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return SLOSH_E_CUDA;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_scan_scratch) != cudaSuccess || !p) return SLOSH_E_CUDA;
-        g_scratch_ptr[dev] = (uint32_t *)p;
-    }
-    *out = g_scratch_ptr[dev];
+// Device address of g_scan_scratch in the current context.  The host-side
+// symbol is only a stand-in for the device array, so the address is looked
+// up on every call: the lookup allocates nothing, and a cached address would
+// go stale when the caller resets the device or switches contexts (the
+// module is then loaded again, possibly at another address).
+int scratch_for_current_context(uint32_t **out) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_scan_scratch) != cudaSuccess || !p) return SLOSH_E_CUDA;
+    *out = (uint32_t *)p;
     return SLOSH_OK;
 }
 
@@ -132,13 +124,17 @@ extern "C" int slosh_prefix_sum_noalloc(const uint32_t *d_in, uint32_t *d_out, u
     if (n == 0) return SLOSH_OK;
     if (!d_in || !d_out || d_in == d_out) return SLOSH_E_INVALID;
     if ((uint64_t)n > NA_MAX_N) return SLOSH_E_CAPACITY;
+    // A CUDA error left pending by the caller's earlier work is not ours to
+    // consume: return without launching and leave it for its owner.
+    if (cudaPeekAtLastError() != cudaSuccess) return SLOSH_E_CUDA;
     uint32_t *scratch = nullptr;
-    const int st = scratch_for_current_device(&scratch);
+    const int st = scratch_for_current_context(&scratch);
     if (st != SLOSH_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t ntiles = (uint32_t)(((uint64_t)n + NA_TILE - 1) / NA_TILE);
     k_na_tile_sums<<<ntiles, NA_THREADS, 0, s>>>(d_in, n, scratch);
     k_na_scan_tile_sums<<<1, NA_THREADS, 0, s>>>(scratch, ntiles);
     k_na_tile_scan<<<ntiles, NA_THREADS, 0, s>>>(d_in, d_out, n, scratch);
+    // nothing was pending before the launches, so an error now is theirs
     return cudaGetLastError() == cudaSuccess ? SLOSH_OK : SLOSH_E_CUDA;
 }

@@ -1171,8 +1171,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
 #pragma unroll
             for (int k = 0; k < D; ++k) len2 += vel[k] * vel[k];
             // |v| > h / dt, tested on the squares first (sqrt is monotone; the
-            // square root is taken only for a particle that is clamped)
-            if (len2 > vmax * vmax * (1.0f - 4e-7f)) {
+            // square root is taken only for a particle near the clamp).  When
+            // (h / dt)^2 overflows, every particle takes the exact test.
+            const float vclamp2 = vmax * vmax * (1.0f - 4e-7f);
+            if (len2 > vclamp2 || isinf(vclamp2)) {
                 const float len = sqrtf(len2);
                 if (len > vmax)
 #pragma unroll

@@ -1,0 +1,194 @@
+"""GPU parity at the benchmark configurations' own sizes, through the C ABI.
+
+The same seeded scenes the benchmark runs, at full particle count, against
+the oracle (FP32, canonical order) and the FP64 oracle:
+
+  - 3D sand column, dx = 1/256, 4,741,888 particles: the grid build
+    (keys, offsets, per-bucket counts, slosh's full sorted layout and the hot
+    path's primary permutation) bit-exact on the initial state and after 20
+    GPU substeps; particle state after 1 and 10 substeps; P2G mass and
+    momentum sums and the totals after 10 substeps against FP64.
+  - 2D dam break, dx = 1/256, 62,628 particles: all 1000 substeps.
+  - 3D elastic drop, dx = 1/128, 524,288 particles: the first 200 of its
+    2000 substeps.
+
+Tolerances are stated per checkpoint as max |gpu - oracle| <= atol + rtol *
+max |oracle| over the compared field.  Over hundreds of substeps the FP32
+differences of the two implementations (summation order, FMA contraction,
+the two SVDs) are amplified by the dynamics (plastic flow in the sand,
+pressure waves in the fluid), so the bounds grow with the substep count.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from slosh_b200 import scenes
+from slosh_b200.pipeline import MpmPipeline
+from test_gpu_parity import grid_equal
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 8
+
+
+def _err(got, exp):
+    d = np.asarray(got, np.float64) - np.asarray(exp, np.float64)
+    return float(np.abs(d).max()), float(np.sqrt((d * d).mean())), float(np.abs(np.asarray(exp, np.float64)).max())
+
+
+def check_state(tag, g, o, dim, bounds):
+    """bounds: field -> (atol, rtol); prints max / rms / scale of each field."""
+    assert np.array_equal(g["enabled"], o["enabled"]), f"{tag}: enabled flags differ"
+    assert np.array_equal(g["mass"], o["mass"]), f"{tag}: mass differs"
+    idx = [c * 3 + r for c in range(dim) for r in range(dim)]
+    fields = {
+        "position": (g["position"][:, :dim], o["position"][:, :dim]),
+        "velocity": (g["velocity"][:, :dim], o["velocity"][:, :dim]),
+        "def_grad": (g["def_grad"][:, idx], o["def_grad"][:, idx]),
+        "affine": (g["affine"][:, idx], o["affine"][:, idx]),
+    }
+    failed = []
+    for name, (a, b) in fields.items():
+        mx, rms, scale = _err(a, b)
+        atol, rtol = bounds[name]
+        bound = atol + rtol * scale
+        print(f"{tag} {name}: max {mx:.3e} rms {rms:.3e} scale {scale:.3e} bound {bound:.3e}")
+        if not mx <= bound:
+            failed.append(f"{name} {mx:.3e} > {bound:.3e}")
+    assert not failed, f"{tag}: " + "; ".join(failed)
+
+
+def check_totals_fp64(tag, g, o64, dim, rtol_p):
+    """Total mass (exact) and momentum of the GPU's FP32 state against the
+    FP64 oracle's after the same substeps."""
+    m = g["mass"].astype(np.float64)
+    p = (g["velocity"][:, :dim].astype(np.float64) * m[:, None]).sum(0)
+    o = o64.get_particles()
+    m64 = o["mass"].astype(np.float64)
+    p64 = (o["velocity"][:, :dim].astype(np.float64) * m64[:, None]).sum(0)
+    rel_m = abs(m.sum() - m64.sum()) / m64.sum()
+    rel_p = np.abs(p - p64).max() / max(np.abs(p64).max(), 1e-30)
+    print(f"{tag} vs FP64: mass rel {rel_m:.2e}, momentum rel {rel_p:.2e} (|p| = {np.abs(p64).max():.3e})")
+    assert rel_m == 0.0
+    assert rel_p <= rtol_p
+
+
+def p2g_totals_fp64(data, sc):
+    """P2G node sums of the GPU against the FP64 oracle (mass exact to 1e-6,
+    momentum to 1e-5) on the uploaded state."""
+    o64 = O.from_scene(sc, double=True, threads=THREADS)
+    nodes = data.debug_nodes(1).astype(np.float64)
+    ref = o64.node_totals(1)
+    o64.close()
+    d = sc.dim
+    rel_m = abs(nodes[:, 3].sum() - ref[3]) / ref[3]
+    rel_p = np.abs(nodes[:, :d].sum(0) - ref[:d]).max() / max(np.abs(ref[:d]).max(), 1e-30)
+    print(f"{sc.name} P2G vs FP64: mass rel {rel_m:.2e}, momentum rel {rel_p:.2e}")
+    assert rel_m < 1e-6
+    assert rel_p < 1e-5 or np.abs(ref[:d]).max() < 1e-12
+
+
+@pytest.fixture(scope="module")
+def sand_full():
+    sc = scenes.sand_column_3d()
+    assert sc.n == 4_741_888
+    return sc
+
+
+def test_config3_grid_build_full_size(cuda_lib, sand_full):
+    sc = sand_full
+    data = scenes.build_mpm_data(sc)
+    orc = O.from_scene(sc, threads=THREADS)
+    grid_equal(data.grid_debug(), orc.grid())
+    MpmPipeline().launch_step(data, 20)
+    orc.set_particles(data.download_particles())
+    grid_equal(data.grid_debug(), orc.grid())
+    orc.close()
+    data.close()
+
+
+SAND_BOUNDS = {
+    1: {"position": (2e-6, 0), "velocity": (1e-6, 1e-4), "def_grad": (2e-6, 2e-6), "affine": (1e-6, 2e-3)},
+    10: {"position": (2e-5, 0), "velocity": (1e-5, 1e-3), "def_grad": (2e-5, 2e-5), "affine": (1e-5, 2e-2)},
+}
+
+
+def test_config3_substeps_full_size(cuda_lib, sand_full):
+    sc = sand_full
+    data = scenes.build_mpm_data(sc)
+    p2g_totals_fp64(data, sc)
+    orc = O.from_scene(sc, threads=THREADS)
+    pipe = MpmPipeline()
+    done = 0
+    for n in (1, 10):
+        pipe.launch_step(data, n - done)
+        orc.step(n - done)
+        done = n
+        check_state(f"sand 4.74M after {n}", data.download_particles(), orc.get_particles(), 3, SAND_BOUNDS[n])
+    orc.close()
+    o64 = O.from_scene(sc, double=True, threads=THREADS)
+    o64.step(10)
+    check_totals_fp64("sand 4.74M after 10", data.download_particles(), o64, 3, 1e-4)
+    o64.close()
+    data.close()
+
+
+DAM_BOUNDS = {
+    1: {"position": (2e-6, 0), "velocity": (1e-6, 1e-4), "def_grad": (2e-6, 2e-6), "affine": (1e-6, 2e-3)},
+    10: {"position": (2e-5, 0), "velocity": (1e-5, 1e-3), "def_grad": (2e-5, 2e-5), "affine": (1e-5, 2e-2)},
+    100: {"position": (1e-4, 0), "velocity": (1e-4, 1e-2), "def_grad": (1e-4, 1e-4), "affine": (1e-4, 1e-1)},
+    1000: {"position": (1e-3, 0), "velocity": (1e-3, 1e-1), "def_grad": (1e-3, 1e-3), "affine": (1e-3, 1.0)},
+}
+
+
+def test_config1_dam_break_all_1000_substeps(cuda_lib):
+    sc = scenes.dam_break_2d()
+    assert sc.n == 62_628
+    data = scenes.build_mpm_data(sc)
+    p2g_totals_fp64(data, sc)
+    orc = O.from_scene(sc, threads=THREADS)
+    grid_equal(data.grid_debug(), orc.grid())
+    pipe = MpmPipeline()
+    done = 0
+    for n in (1, 10, 100, 1000):
+        pipe.launch_step(data, n - done)
+        orc.step(n - done)
+        done = n
+        check_state(f"dam break after {n}", data.download_particles(), orc.get_particles(), 2, DAM_BOUNDS[n])
+    orc.close()
+    o64 = O.from_scene(sc, double=True, threads=THREADS)
+    o64.step(1000)
+    check_totals_fp64("dam break after 1000", data.download_particles(), o64, 2, 1e-3)
+    o64.close()
+    data.close()
+
+
+DROP_BOUNDS = {
+    1: {"position": (2e-6, 0), "velocity": (1e-6, 1e-4), "def_grad": (2e-6, 2e-6), "affine": (1e-6, 2e-3)},
+    10: {"position": (2e-5, 0), "velocity": (1e-5, 1e-3), "def_grad": (2e-5, 2e-5), "affine": (1e-5, 2e-2)},
+    200: {"position": (2e-4, 0), "velocity": (1e-4, 1e-2), "def_grad": (2e-4, 2e-4), "affine": (1e-4, 1e-1)},
+}
+
+
+def test_config2_elastic_drop_first_200_substeps(cuda_lib):
+    sc = scenes.elastic_drop_3d()
+    assert sc.n == 524_288
+    data = scenes.build_mpm_data(sc)
+    p2g_totals_fp64(data, sc)
+    orc = O.from_scene(sc, threads=THREADS)
+    grid_equal(data.grid_debug(), orc.grid())
+    pipe = MpmPipeline()
+    done = 0
+    for n in (1, 10, 200):
+        pipe.launch_step(data, n - done)
+        orc.step(n - done)
+        done = n
+        check_state(f"elastic drop after {n}", data.download_particles(), orc.get_particles(), 3, DROP_BOUNDS[n])
+    orc.close()
+    o64 = O.from_scene(sc, double=True, threads=THREADS)
+    o64.step(200)
+    check_totals_fp64("elastic drop after 200", data.download_particles(), o64, 3, 1e-4)
+    o64.close()
+    data.close()

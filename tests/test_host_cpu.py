@@ -135,3 +135,52 @@ def test_scene_determinism():
     a = scenes.sand_column_3d(h=1 / 32).particles
     b = scenes.sand_column_3d(h=1 / 32).particles
     assert np.array_equal(a, b)
+
+
+def _c_structs(src):
+    """typedef struct name { fields } name; -> {name: [(field, type, count)]}."""
+    out = {}
+    for name, body in re.findall(r"typedef struct (\w+) \{(.*?)\} \1;", src, re.S):
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            ty, rest = decl.split(None, 1) if not decl.startswith("const ") else ("const " + decl.split()[1], decl.split(None, 2)[2])
+            for item in rest.split(","):
+                m = re.fullmatch(r"\s*\*?\s*(\w+)\s*(?:\[(\d+)\])?\s*", item)
+                assert m, (name, decl)
+                fields.append((m.group(1), ty, int(m.group(2) or 1)))
+        out[name] = fields
+    return out
+
+
+def _rust_structs(md):
+    """#[repr(C)] structs of INTEGRATION.md's Rust binding block."""
+    block = md.split("## Rust binding", 1)[1].split("```rust", 1)[1].split("```", 1)[0]
+    block = re.sub(r"//[^\n]*", "", block)
+    out = {}
+    for name, body in re.findall(r"#\[repr\(C\)\][^{]*?pub struct (\w+)\s*\{(.*?)\}", block, re.S):
+        fields = []
+        for m in re.finditer(r"(?:pub\s+)?(\w+)\s*:\s*(\[\s*\w+\s*;\s*\d+\s*\]|\w+)", body):
+            ty = m.group(2).replace(" ", "")
+            arr = re.fullmatch(r"\[(\w+);(\d+)\]", ty)
+            fields.append((m.group(1), arr.group(1), int(arr.group(2))) if arr else (m.group(1), ty, 1))
+        out[name] = fields
+    return out
+
+
+def test_integration_rust_records_match_header():
+    """The #[repr(C)] records of the documented Rust binding have the
+    header's fields, types and order, so a maintainer who copies them gets
+    the library's exact layouts."""
+    c = _c_structs(open(HEADER).read())
+    rust = _rust_structs(open(os.path.join(ROOT, "INTEGRATION.md")).read())
+    c_to_rust = {"float": "f32", "uint32_t": "u32", "int32_t": "i32", "slosh_model": "SloshModel"}
+    pairs = {"SloshModel": "slosh_model", "SloshParticle": "slosh_particle", "SloshBody": "slosh_body",
+             "SloshConfig": "slosh_config", "SloshParams": "slosh_params"}
+    assert set(pairs) <= set(rust), sorted(rust)
+    for rname, cname in pairs.items():
+        want = [(f, c_to_rust[t], k) for f, t, k in c[cname]]
+        assert rust[rname] == want, (rname, rust[rname], want)

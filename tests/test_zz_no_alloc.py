@@ -69,6 +69,34 @@ def test_noalloc_prefix_sum_matches_context_scan(cuda_lib):
         lib.slosh_ctx_destroy(ctx)
 
 
+def _numpy_scan(v):
+    """Exclusive scan in u32 arithmetic (wraps at 2^32 like the device sums)."""
+    out = np.zeros_like(v)
+    np.cumsum(v[:-1], dtype=np.uint32, out=out[1:])
+    return out
+
+
+def test_noalloc_prefix_sum_large_and_wrapping(cuda_lib):
+    """Inputs beyond the context scan's size: more than 256 tiles (several
+    rounds of the tile-sum carry), the maximum size, and totals that wrap
+    past 2^32, each scanned twice in a row."""
+    import torch
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(22)
+    cases = [
+        rng.integers(0, 1000, size=1_050_000, dtype=np.uint32),  # 257 tiles
+        rng.integers(0, 1000, size=5_000_003, dtype=np.uint32),  # 1221 tiles, ragged end
+        rng.integers(0, 4, size=67_108_864, dtype=np.uint32),  # the maximum n
+        rng.integers(1 << 30, 1 << 31, size=300_001, dtype=np.uint32),  # total wraps 2^32 many times
+    ]
+    for v in cases:
+        ref = _numpy_scan(v)
+        assert np.array_equal(_noalloc_scan(cuda_lib, torch, v), ref), len(v)
+        assert np.array_equal(_noalloc_scan(cuda_lib, torch, v), ref), len(v)
+        torch.cuda.empty_cache()
+
+
 def test_noalloc_prefix_sum_rejects_oversize(cuda_lib):
     import torch
 
