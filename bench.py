@@ -318,6 +318,7 @@ def main_ours(args):
         torch.cuda.synchronize(dev)
 
     clocks = ClockSampler(local)
+    st0 = data.stats()
     barrier()
     clocks.start()
     time.sleep(0.3)
@@ -331,7 +332,22 @@ def main_ours(args):
     data.sync(sptr)
     ms = max_over_ranks(ev0.elapsed_time(ev1), pg, dev)
     value = aggregate_rate(world, n * args.steps, ms)
-    launches = data.kernels_per_substep * args.steps
+    st1 = data.stats()
+    reused = st1["n_grid_reuses"] - st0["n_grid_reuses"]
+    rebuilt = st1["n_grid_rebuilds"] - st0["n_grid_rebuilds"]
+    # kernels launched in the timed region: with conditional graphs a
+    # substep that keeps its grid launches 7, a full build 14
+    if st1["conditional_graphs"]:
+        launches = 14 * rebuilt + 7 * reused
+    else:
+        launches = data.kernels_per_substep * args.steps
+    grid_reuse = {"reused_substeps": reused, "rebuilt_substeps": rebuilt,
+                  "conditional_graphs": bool(st1["conditional_graphs"])}
+    svd_fp64 = st1["n_svd_fp64"] - st0["n_svd_fp64"]
+
+    # per-kernel device time right after the timed region (direct launches
+    # with events around each kernel; same scene state)
+    prof = data.profile_substeps(args.profile_steps, sptr)
 
     # median of 5 timed regions of max(K, 100) substeps each (same stream,
     # same graphs), beside the single K-substep region above
@@ -355,8 +371,6 @@ def main_ours(args):
         "ms_per_step_all": [r / rep_k for r in reps],
     }
 
-    # per-kernel device time (direct launches with events around each kernel)
-    prof = data.profile_substeps(args.profile_steps, sptr)
     per_substep = {k: v / args.profile_steps for k, v in prof.items()}
     dom = max(per_substep, key=per_substep.get)
     peak, peak_kind = measured_peaks()
@@ -454,6 +468,8 @@ def main_ours(args):
             "kernel_ms_per_substep": per_substep,
             "active_blocks": nb,
             "repeat_median": repeat,
+            "grid_reuse": grid_reuse,
+            "svd_fp64_fallbacks_timed": svd_fp64,
         }
     data.close()
     if rank == 0:

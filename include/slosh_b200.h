@@ -238,14 +238,25 @@ int slosh_add_trimesh(slosh_ctx *ctx, const float *vertices, uint32_t n_vertices
 /* Enqueues `n_substeps` substeps on `stream` without any host round trip.
  * Replaces MpmPipeline::launch_step (src/pipeline.rs:562-770) called
  * n_substeps times into one encoder.  Asynchronous: errors raised on the
- * device are reported by slosh_sync. */
+ * device are reported by slosh_sync.
+ * Grid reuse: slosh rebuilds the sparse grid every substep
+ * (src/grid/grid.rs:78-238).  Here a substep keeps the previous substep's
+ * blocks, ranks and hash map when no particle left the set of blocks that
+ * hold particles, and only re-counts the cells particles entered or left;
+ * the decision is taken on the device.  The layout is the one a full build
+ * gives, bit for bit.  The environment variable SLOSH_GRID_REUSE=0 at
+ * context creation makes every substep run the full build. */
 int slosh_step(slosh_ctx *ctx, uint32_t n_substeps, void *stream);
 
 /* Waits for the context's work and returns the device error status
  * (SLOSH_E_OVERFLOW when the block hash map or block list overflowed). */
 int slosh_sync(slosh_ctx *ctx, void *stream);
 
-/* Number of device kernels one substep launches (for launch accounting). */
+/* Number of device kernels a substep launches that runs the full grid
+ * build (for launch accounting).  With grid reuse and conditional graphs a
+ * substep that keeps the previous grid launches 7: the reuse decision, the
+ * block scan, the permutation update, P2G, the grid update, G2P and the
+ * rigid update (slosh_get_stats counts both kinds of substep). */
 uint32_t slosh_kernels_per_substep(const slosh_ctx *ctx);
 
 /* Runs `n_substeps` substeps with direct launches (not the CUDA graph) and a
@@ -267,7 +278,10 @@ typedef struct slosh_stats {
     uint32_t n_primary_blocks; /* blocks holding at least one particle */
     uint32_t n_materials;      /* distinct particle models */
     uint32_t n_svd_fp64;       /* SVDs recomputed in FP64 since upload */
-    uint32_t pad[3];
+    uint32_t n_grid_rebuilds;  /* substeps that ran the full grid build   */
+    uint32_t n_grid_reuses;    /* substeps that kept the previous grid    */
+    uint32_t conditional_graphs; /* 1: the substep graphs launch only the
+                                    selected grid-build branch            */
 } slosh_stats;
 
 int slosh_get_stats(slosh_ctx *ctx, slosh_stats *out);

@@ -28,6 +28,7 @@ constexpr uint32_t ERR_MATERIAL_HASH = 1u << 3;    // two materials share a 32-b
 constexpr uint32_t ERR_KEY_RANGE = 1u << 4;        // a block coordinate outside the packed-key range
 constexpr uint32_t ERR_BLOCK_PARTICLES = 1u << 6;  // a block holds 2^26 particles or more
 constexpr uint32_t ERR_SCENE_BLOCKS = 1u << 5;     // a batch scene has more blocks than the per-scene sort holds
+constexpr uint32_t ERR_GRID_REUSE = 1u << 7;       // a kept grid's cell counts and its gathered cells disagree
 
 // Sparse grid geometry per dimension (shaders/slosh/grid/grid.slang:224-257).
 template <int D> struct Geo;
@@ -303,8 +304,13 @@ struct Counters {
     uint32_t n_svd_fp64;     // particles whose SVD fell back to FP64 (cumulative)
     uint32_t last_n_blocks;  // n_blocks of the last completed substep
     uint32_t last_n_primary; // n_primary of the last completed substep
-    uint32_t p2g_next;       // next block for a P2G warp (reset by k_block_setup)
-    uint32_t g2p_next;       // next block for a G2P CTA (reset by k_block_setup)
+    uint32_t p2g_next;       // next block for a P2G warp (reset by k_block_setup or k_reuse_perm)
+    uint32_t g2p_next;       // next block for a G2P CTA (reset by k_block_setup or k_reuse_perm)
+    uint32_t rebuild[2];     // grid reuse: the substep of this parity runs the full grid build
+                             // (set by the host, by G2P for the next substep, by k_grid_reuse)
+    uint32_t reuse_done;     // CTAs of k_grid_reuse that finished (the last one decides)
+    uint32_t n_rebuilds;     // substeps that ran the full grid build (cumulative)
+    uint32_t n_reuses;       // substeps that kept the previous grid (cumulative)
     uint32_t pad[3];
 };
 

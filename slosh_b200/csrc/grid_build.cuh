@@ -159,6 +159,7 @@ template <bool B = false> __global__ void k_clear(DevScene s) {
 // cell width from the scene table, and particles of a dropped scene get no
 // block (they leave storage at this substep).
 template <int D, bool B = false> __global__ void k_touch(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     // Each warp takes a contiguous chunk of storage.  Storage is in the
     // previous substep's canonical order (block by block), so successive
     // iterations of a warp mostly hit the block of the last one: the warp
@@ -236,6 +237,7 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
 // histogram (key >> 26), aggregated over the warp (a compact scene has one
 // or two coarse bins, so per-block atomics would all hit one address).
 template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t np = min(s.ctr->n_primary, s.cap);
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -390,6 +392,7 @@ template <int NT> __device__ __forceinline__ uint32_t cta_scan_vec16(const uint3
 // scans bins [1024 c, 1024 c + 1024), one uint4 a thread, on top of the
 // coarse counts of the bins before them.
 template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     constexpr uint32_t PER = HIST_BINS / HIST_COARSE, NW = NT / 32;
     static_assert(PER == 4 * NT && HIST_COARSE <= 64, "one uint4 of bins a thread");
     __shared__ uint32_t wtot[NW];
@@ -427,6 +430,7 @@ template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) 
 
 // Groups the appended block keys by their top 16 bits.
 __global__ void k_bin_scatter(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t n1 = min(s.ctr->n_primary, s.cap), n2 = min(s.ctr->n_extra, s.cap);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n1 + n2; t += stride) {
@@ -445,6 +449,7 @@ __global__ void k_bin_scatter(DevScene s) {
 // whole z slab of a compact scene, hundreds of keys).
 constexpr uint32_t RANK_LANES = 8;
 __global__ void k_rank(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
     const uint32_t g = threadIdx.x % RANK_LANES;
     const unsigned gmask = ((1u << RANK_LANES) - 1u) << (lane_id() & ~(RANK_LANES - 1u));
@@ -561,6 +566,7 @@ template <int NT, uint32_t PMIN, uint32_t PMAX> __global__ void __launch_bounds_
 // rank in the previous substep's map (the grid update's collision cache) and, for the
 // atomic P2G variants, zeroed nodes (reset, grid.slang:455-485).
 template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t lane = lane_id();
@@ -639,7 +645,10 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
     cta_scan_vec16<NT>(s.bnp, s.bfirst, nb);
     // P2G's queue order, heaviest blocks first (buckets of 8 particles), so
     // that the last blocks its warps take are light and they finish together.
-    if (!s.p2g_heavy_first) return;
+    // A substep that keeps its grid keeps the order too: the same blocks, and
+    // block counts that changed by a few particles at most (the order only
+    // balances P2G's load; results do not depend on it).
+    if (!s.p2g_heavy_first || build_skipped(s)) return;
     __shared__ uint32_t cnt[64];
     if (threadIdx.x < 64) cnt[threadIdx.x] = 0u;
     __syncthreads();
@@ -668,6 +677,7 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
 // fix-up.  Like k_touch, a warp remembers the block of its last lane (hash
 // slot -> rank, first entry), so most iterations go straight to the claim.
 template <bool B = false> __global__ void k_scatter(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t lane = lane_id();
     const uint32_t n = n_particles<B>(s);
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
@@ -746,6 +756,7 @@ __device__ __forceinline__ void sort_cell_keys(unsigned long long *key, uint32_t
 }
 
 __global__ void k_canon(DevScene s) {
+    if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t lane = lane_id();
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);

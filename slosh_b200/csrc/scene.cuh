@@ -95,6 +95,20 @@ struct DevScene {
     Counters *ctr;
     uint32_t *err;
 
+    // ---- grid reuse between substeps (single-scene context) -----------------
+    // bfirst, bnp and bcell are double-buffered by substep parity: the prev_*
+    // arrays hold the previous substep's, whose canonical order storage is in.
+    uint32_t reuse;            // keep the previous grid when no particle changed it (else: full build)
+    uint32_t par;              // parity of this substep (its rebuild flag)
+    const uint32_t *prev_bfirst;
+    const uint32_t *prev_bnp;
+    const uint32_t *prev_bcell;
+    int *cell_delta;           // 64 per block: particles gained - lost per cell, written by G2P
+    unsigned long long *touch; // per block: cells a particle entered or left in G2P
+    unsigned long long *cur_touch;  // per block: the touched cells this substep's reuse applies
+    cudaGraphConditionalHandle cond;  // inside the substep graph: full build (1) or reuse (0)
+    uint32_t use_cond;
+
     // ---- multi-scene batch (unused by the single-scene context) -------------
     // `n` is then the plane stride (pool capacity) and the particle count in
     // storage is *n_dev; blocks are hashed by (scene << 32 | key) in 64-bit
@@ -110,5 +124,11 @@ struct DevScene {
     uint32_t *scene_bbase;           // first block rank of each scene
     uint32_t *scene_fill;            // scatter cursors
 };
+
+// This substep keeps the previous grid: the full build's kernels return at
+// once (they also run under the conditional graph node that skips them).
+__device__ __forceinline__ bool build_skipped(const DevScene &s) {
+    return s.reuse != 0u && s.ctr->rebuild[s.par] == 0u;
+}
 
 }  // namespace slosh

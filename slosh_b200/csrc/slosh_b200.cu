@@ -15,6 +15,7 @@
 
 #include "common.cuh"
 #include "grid_build.cuh"
+#include "grid_reuse.cuh"
 #include "io.cuh"
 #include "transfer.cuh"
 #include "timestep.cuh"
@@ -51,6 +52,14 @@ struct slosh_ctx {
              *bcell = nullptr, *bcur = nullptr, *bnbh = nullptr, *bnbh_rev = nullptr;
     uint2 *bord = nullptr;
     uint32_t *qorder = nullptr, *bprev = nullptr;
+    // grid reuse (single-scene contexts): the second parity's block arrays
+    // and G2P's per-cell bookkeeping; reuse = 0 in batches and when the
+    // environment sets SLOSH_GRID_REUSE=0
+    uint32_t *bfirst2 = nullptr, *bnp2 = nullptr, *bcell2 = nullptr;
+    int *cell_delta = nullptr;
+    unsigned long long *touch = nullptr, *cur_touch = nullptr;
+    uint32_t reuse = 0;
+    bool cond_graphs = false;  // the substep graphs pick the build through a conditional node
     // P2G reduction (environment SLOSH_P2G at creation): 0 fixed-order,
     // bit-reproducible (default); 3 "direct": the same cell-owner kernel with
     // shared-memory and global float atomics, kept for A/B comparison.
@@ -190,9 +199,26 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.tmp_slot = c->tmp_slot;
     s.bkey = c->bkey;
     s.bslot = c->bslot;
-    s.bfirst = c->bfirst;
-    s.bnp = c->bnp;
-    s.bcell = c->bcell;
+    {
+        // block arrays of this parity and of the previous substep
+        const uint32_t pc = parity & 1u;
+        uint32_t *bf[2] = {c->bfirst, c->bfirst2 ? c->bfirst2 : c->bfirst};
+        uint32_t *bn[2] = {c->bnp, c->bnp2 ? c->bnp2 : c->bnp};
+        uint32_t *bc[2] = {c->bcell, c->bcell2 ? c->bcell2 : c->bcell};
+        s.bfirst = bf[pc];
+        s.bnp = bn[pc];
+        s.bcell = bc[pc];
+        s.prev_bfirst = bf[pc ^ 1u];
+        s.prev_bnp = bn[pc ^ 1u];
+        s.prev_bcell = bc[pc ^ 1u];
+        s.reuse = c->reuse;
+        s.par = pc;
+        s.cell_delta = c->cell_delta;
+        s.touch = c->touch;
+        s.cur_touch = c->cur_touch;
+        s.cond = 0;
+        s.use_cond = 0u;
+    }
     s.bord = c->bord;
     s.qorder = c->qorder;
     s.bcur = c->bcur;
@@ -234,10 +260,15 @@ uint32_t grid_for(uint64_t work, uint32_t threads, uint32_t max_ctas) {
 }
 
 // Kernels of one substep, in launch order (profiling names).
-constexpr int N_KERNELS = 13;
+constexpr int N_KERNELS = 15;
 const char *const KERNEL_NAMES[N_KERNELS] = {
-    "k_touch",      "k_neighbors", "k_hist_scan", "k_bin_scatter", "k_rank",        "k_block_setup", "k_block_scan",
-    "k_scatter",    "k_canon",     "k_p2g",       "k_grid_update", "k_g2p_update",  "k_rigid"};
+    "k_grid_reuse", "k_touch",   "k_neighbors", "k_hist_scan", "k_bin_scatter", "k_rank",        "k_block_setup",
+    "k_block_scan", "k_reuse_perm", "k_scatter", "k_canon",     "k_p2g",         "k_grid_update", "k_g2p_update",
+    "k_rigid"};
+// Kernels a substep launches through the conditional graph: the decision,
+// the transfer kernels and the rigid update, plus the full build (9) or the
+// reuse (block scan and permutation).
+constexpr uint32_t KERNELS_FULL_BUILD = 14, KERNELS_REUSE = 7;
 
 // Optional per-kernel CUDA-event timing of the substep launches.
 struct Prof {
@@ -260,41 +291,74 @@ struct Prof {
 // entry points).  Within a substep sequence the hash map, key histogram and
 // counters were cleared by the previous substep's last kernels (or by the
 // upload); a standalone build (debug entry points) clears them first.
-template <int D>
-void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr, bool standalone = false) {
+// front: activation and ranking of the blocks and their cell counts.
+template <int D> void enqueue_build_front(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     const uint32_t sm = (uint32_t)c->sm_count;
-    if (standalone) k_clear<<<sm * 4, 256, 0, st>>>(s);
-    PROF_BEGIN(0);
-    k_touch<D><<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // one wave of warps, a chunk each
-    PROF_END(0);
     PROF_BEGIN(1);
-    k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
+    k_touch<D><<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // one wave of warps, a chunk each
     PROF_END(1);
     PROF_BEGIN(2);
-    k_hist_scan<256><<<HIST_COARSE, 256, 0, st>>>(s);
+    k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(2);
     PROF_BEGIN(3);
-    k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    k_hist_scan<256><<<HIST_COARSE, 256, 0, st>>>(s);
     PROF_END(3);
     PROF_BEGIN(4);
-    k_rank<<<grid_for(2ull * c->cap * RANK_LANES, 256, sm * 8), 256, 0, st>>>(s);
+    k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(4);
     PROF_BEGIN(5);
-    k_block_setup<D><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    k_rank<<<grid_for(2ull * c->cap * RANK_LANES, 256, sm * 8), 256, 0, st>>>(s);
     PROF_END(5);
     PROF_BEGIN(6);
-    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
+    k_block_setup<D><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
     PROF_END(6);
+}
+
+void enqueue_block_scan(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(7);
-    k_scatter<<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // longer chunks: fewer cells split for k_canon
+    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     PROF_END(7);
+}
+
+// The kept grid's permutation (returns at once when the full build runs).
+template <int D> void enqueue_reuse_perm(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(8);
-    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    k_reuse_perm<D><<<grid_for((uint64_t)c->cap * 32, 256, (uint32_t)c->sm_count * 8), 256, 0, st>>>(s);
     PROF_END(8);
 }
 
-template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
+// back: the permutation of the full build.
+void enqueue_build_back(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
+    const uint32_t sm = (uint32_t)c->sm_count;
     PROF_BEGIN(9);
+    k_scatter<<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // longer chunks: fewer cells split for k_canon
+    PROF_END(9);
+    PROF_BEGIN(10);
+    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    PROF_END(10);
+}
+
+// The decision between keeping the previous grid and a full build.
+template <int D> void enqueue_reuse_decision(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
+    PROF_BEGIN(0);
+    k_grid_reuse<D><<<grid_for((uint64_t)c->cap * 32, 256, (uint32_t)c->sm_count * 8), 256, 0, st>>>(s);
+    PROF_END(0);
+}
+
+// A whole grid build as one launch sequence.  With grid reuse on, the full
+// build's kernels and the reuse permutation each return at once unless the
+// substep's decision selects them; standalone builds run with reuse off.
+template <int D>
+void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr, bool standalone = false) {
+    if (standalone) k_clear<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
+    enqueue_build_front<D>(c, s, st, p);
+    enqueue_block_scan(c, s, st, p);
+    if (s.reuse) enqueue_reuse_perm<D>(c, s, st, p);
+    enqueue_build_back(c, s, st, p);
+}
+
+template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
+    PROF_BEGIN(11);
     if (c->p2g_variant == 3) {
         const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
         k_p2g_atomic<D><<<g, P2G_ATOMIC_THREADS, 0, st>>>(s);
@@ -303,13 +367,13 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
         if (s.force_pending) k_p2g<D, false, true><<<g, 32 * P2G_WARPS, 0, st>>>(s);
         else k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
     }
-    PROF_END(9);
+    PROF_END(11);
 }
 
 template <int D> void enqueue_grid_update(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
-    PROF_BEGIN(10);
+    PROF_BEGIN(12);
     k_grid_update<D><<<grid_for((uint64_t)c->cap * 64, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s);
-    PROF_END(10);
+    PROF_END(12);
 }
 
 // Restores the cleared state a debug build consumed, so that the next real
@@ -318,13 +382,11 @@ void enqueue_clear(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
     k_clear<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
 }
 
-template <int D>
-void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force, Prof *p = nullptr) {
-    const DevScene s = make_scene(c, parity, force);
-    enqueue_grid_build<D>(c, s, st, p);
+// P2G, grid update, fused G2P/update and the rigid update.
+template <int D> void enqueue_transfer(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     enqueue_p2g<D>(c, s, st, p);
     enqueue_grid_update<D>(c, s, st, p);
-    PROF_BEGIN(11);
+    PROF_BEGIN(13);
     // persistent: 8 CTAs of 64 fit an SM; each takes blocks from the queue.
     // Small CTAs wait less at the per-block barriers (tile load, the
     // slowest thread's last particle) than CTAs of 128 or 256.
@@ -339,10 +401,18 @@ void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force,
     else if (c->model_mask == 1u << SLOSH_MODEL_FLUID_TAIT)
         k_g2p_update<D, 64, false, true, SLOSH_MODEL_FLUID_TAIT><<<g2p_grid, 64, 0, st>>>(s);
     else k_g2p_update<D, 64, false, true><<<g2p_grid, 64, 0, st>>>(s);
-    PROF_END(11);
-    PROF_BEGIN(12);
+    PROF_END(13);
+    PROF_BEGIN(14);
     k_rigid<D><<<1, 32, 0, st>>>(s);
-    PROF_END(12);
+    PROF_END(14);
+}
+
+template <int D>
+void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force, Prof *p = nullptr) {
+    const DevScene s = make_scene(c, parity, force);
+    if (s.reuse) enqueue_reuse_decision<D>(c, s, st, p);
+    enqueue_grid_build<D>(c, s, st, p);
+    enqueue_transfer<D>(c, s, st, p);
 }
 
 void enqueue_substep_any(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force, Prof *p = nullptr) {
@@ -359,8 +429,91 @@ void destroy_graphs(slosh_ctx *c) {
     c->graphs_valid = false;
 }
 
+// Substep graph with the grid build under a conditional node: the reuse
+// decision, then IF (full build) ELSE (reuse permutation), then the transfer
+// kernels.  Only the selected branch's kernels launch.
+template <int D> cudaError_t capture_conditional(slosh_ctx *c, uint32_t par, cudaGraph_t *out) {
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    cudaStream_t st = c->stream;
+    *out = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    auto bail = [&](cudaError_t err) {
+        cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
+            cudaGraph_t left = nullptr;  // the graph being captured into: destroyed below (or owned by g)
+            cudaStreamEndCapture(st, &left);
+        }
+        cudaGraphDestroy(g);
+        return err;
+    };
+    cudaGraphConditionalHandle handle = 0;
+    if ((e = cudaGraphConditionalHandleCreate(&handle, g, 1u, cudaGraphCondAssignDefault)) != cudaSuccess) return bail(e);
+    DevScene s = make_scene(c, par, false);
+    s.cond = handle;
+    s.use_cond = 1u;
+    // the decision
+    if ((e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode)) != cudaSuccess) return bail(e);
+    enqueue_reuse_decision<D>(c, s, st, nullptr);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd);
+    cudaGraphNode_t decision = (e == cudaSuccess && nd == 1) ? deps[0] : nullptr;
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &captured);
+    if (e != cudaSuccess) return bail(e);
+    if (e2 != cudaSuccess) return bail(e2);
+    if (!decision) return bail(cudaErrorInvalidValue);
+    // IF rebuild: the full build; ELSE: the reuse
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 2;
+    cudaGraphNode_t cnode = nullptr;
+    if ((e = cudaGraphAddNode(&cnode, g, &decision, 1, &cp)) != cudaSuccess) return bail(e);
+    cudaGraph_t full = cp.conditional.phGraph_out[0], reuse = cp.conditional.phGraph_out[1];
+    if ((e = cudaStreamBeginCaptureToGraph(st, full, nullptr, nullptr, 0, mode)) != cudaSuccess) return bail(e);
+    enqueue_build_front<D>(c, s, st, nullptr);
+    enqueue_block_scan(c, s, st, nullptr);
+    enqueue_build_back(c, s, st, nullptr);
+    if ((e = cudaStreamEndCapture(st, &full)) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamBeginCaptureToGraph(st, reuse, nullptr, nullptr, 0, mode)) != cudaSuccess) return bail(e);
+    enqueue_block_scan(c, s, st, nullptr);
+    enqueue_reuse_perm<D>(c, s, st, nullptr);
+    if ((e = cudaStreamEndCapture(st, &reuse)) != cudaSuccess) return bail(e);
+    // the transfer kernels after either branch
+    if ((e = cudaStreamBeginCaptureToGraph(st, g, &cnode, nullptr, 1, mode)) != cudaSuccess) return bail(e);
+    enqueue_transfer<D>(c, s, st, nullptr);
+    if ((e = cudaStreamEndCapture(st, &captured)) != cudaSuccess) return bail(e);
+    *out = g;
+    return cudaSuccess;
+}
+
 int build_graphs(slosh_ctx *c) {
     destroy_graphs(c);
+    c->cond_graphs = false;
+    if (c->reuse) {
+        // the grid build under a conditional node; on any failure the plain
+        // sequence below (every kernel, the unused ones returning at once)
+        cudaGraph_t g[2] = {nullptr, nullptr};
+        bool ok = true;
+        for (uint32_t par = 0; par < 2 && ok; ++par) {
+            const cudaError_t e = c->dim == 3 ? capture_conditional<3>(c, par, &g[par]) : capture_conditional<2>(c, par, &g[par]);
+            ok = e == cudaSuccess && cudaGraphInstantiate(&c->graph[par], g[par], 0) == cudaSuccess;
+        }
+        for (auto &x : g)
+            if (x) cudaGraphDestroy(x);
+        if (ok) {
+            c->cond_graphs = true;
+            c->graphs_valid = true;
+            return SLOSH_OK;
+        }
+        destroy_graphs(c);
+        cudaGetLastError();  // the failed capture is not the caller's error
+    }
     for (uint32_t par = 0; par < 2; ++par) {
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         enqueue_substep_any(c, c->stream, par, false);
@@ -371,6 +524,18 @@ int build_graphs(slosh_ctx *c) {
         if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
     }
     c->graphs_valid = true;
+    return SLOSH_OK;
+}
+
+// Makes the next substep run the full grid build: after an upload, an
+// append or removal, or a standalone build (debug entry points), the
+// previous substep's grid no longer describes storage.  G2P's pending
+// per-cell bookkeeping is dropped with it.
+int force_grid_rebuild(slosh_ctx *c, cudaStream_t st) {
+    if (!c->reuse) return SLOSH_OK;
+    CK(cudaMemsetAsync(c->cell_delta, 0, (size_t)c->cap * CELLS * sizeof(int), st));
+    CK(cudaMemsetAsync(c->touch, 0, (size_t)c->cap * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(c->ctr->rebuild, 1, sizeof(c->ctr->rebuild), st));  // nonzero: rebuild
     return SLOSH_OK;
 }
 
@@ -539,7 +704,9 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->coll_id[1], (size_t)cap * 64)) || (st = dalloc(c, &c->bodies, MAX_BODIES)) ||
         (st = dalloc(c, &c->body_imp, (size_t)MAX_BODIES * 6)) ||
         (st = dalloc(c, &c->ctr, 1)) || (st = dalloc(c, &c->err, 1)) || (st = dalloc(c, &c->small, 4)) ||
-        (st = dalloc(c, &c->staging, N)))
+        (st = dalloc(c, &c->staging, N)) || (st = dalloc(c, &c->bfirst2, cap)) || (st = dalloc(c, &c->bnp2, cap)) ||
+        (st = dalloc(c, &c->bcell2, (size_t)cap * CELLS)) || (st = dalloc(c, &c->cell_delta, (size_t)cap * CELLS)) ||
+        (st = dalloc(c, &c->touch, cap)) || (st = dalloc(c, &c->cur_touch, cap)))
         return fail_create(st);
     cudaMemset(c->hkeys[0], 0xff, hcap * 4);
     cudaMemset(c->hkeys[1], 0xff, hcap * 4);
@@ -552,6 +719,13 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     if (const char *variant = std::getenv("SLOSH_P2G")) {
         if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;
     }
+    c->reuse = 1u;
+    if (const char *r = std::getenv("SLOSH_GRID_REUSE")) c->reuse = std::strcmp(r, "0") == 0 ? 0u : 1u;
+    cudaMemset(c->bcell, 0, (size_t)cap * CELLS * 4);
+    cudaMemset(c->bcell2, 0, (size_t)cap * CELLS * 4);
+    cudaMemset(c->bnp, 0, (size_t)cap * 4);
+    cudaMemset(c->bnp2, 0, (size_t)cap * 4);
+    if (force_grid_rebuild(c, nullptr) != SLOSH_OK) return fail_create(SLOSH_E_CUDA);
     if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     c->params.gravity[1] = -9.81f;
     c->params.dt = 1.0f / 60.0f;
@@ -588,6 +762,7 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     CK(cudaMemsetAsync(c->small, 0, 16, st));
     CK(cudaMemsetAsync(c->err, 0, 4, st));
     CK(cudaMemsetAsync(c->ctr, 0, sizeof(Counters), st));
+    if (int r = force_grid_rebuild(c, st)) return r;
     for (int k = 0; k < 2; ++k) {
         CK(cudaMemsetAsync(c->hkeys[k], 0xff, c->hcap * 4, st));
         CK(cudaMemsetAsync(c->hvals[k], 0xff, c->hcap * 4, st));
@@ -654,6 +829,7 @@ int slosh_append_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     io.r0 = c->r0;
     io.phase = c->phase;
     const uint32_t g = grid_for(n, 256, (uint32_t)c->sm_count * 16);
+    if (int r = force_grid_rebuild(c, st)) return r;
     k_mat_insert<<<g, 256, 0, st>>>(s, io, n);
     if (c->dim == 3) k_ingest<3><<<g, 256, 0, st>>>(s, io, base, n, 0u, base);
     else k_ingest<2><<<g, 256, 0, st>>>(s, io, base, n, 0u, base);
@@ -687,6 +863,7 @@ int slosh_remove_particles(slosh_ctx *c, uint32_t start, uint32_t count, uint32_
     // the record staging area (192 bytes a particle) holds the (3 + D)-plane temporary
     float *tmp = reinterpret_cast<float *>(c->staging);
     const uint32_t g = grid_for(c->n, 256, (uint32_t)c->sm_count * 16);
+    if (int r = force_grid_rebuild(c, st)) return r;
     if (c->dim == 3) k_remove<3><<<g, 256, 0, st>>>(s, io, start, end, tmp);
     else k_remove<2><<<g, 256, 0, st>>>(s, io, start, end, tmp);
     CK(cudaGetLastError());
@@ -850,7 +1027,8 @@ int slosh_sync(slosh_ctx *c, void *stream) {
 
 uint32_t slosh_kernels_per_substep(const slosh_ctx *c) {
     if (!c) return 0;
-    return (uint32_t)N_KERNELS;
+    if (!c->reuse) return (uint32_t)N_KERNELS - 2u;
+    return c->cond_graphs ? KERNELS_FULL_BUILD : (uint32_t)N_KERNELS;
 }
 
 int slosh_profile_substeps(slosh_ctx *c, uint32_t n_substeps, void *stream, float *kernel_ms, uint32_t cap,
@@ -906,6 +1084,9 @@ int slosh_get_stats(slosh_ctx *c, slosh_stats *out) {
     out->n_primary_blocks = ctr.last_n_primary;
     out->n_materials = c->n_materials;
     out->n_svd_fp64 = ctr.n_svd_fp64;
+    out->n_grid_rebuilds = ctr.n_rebuilds;
+    out->n_grid_reuses = ctr.n_reuses;
+    out->conditional_graphs = c->cond_graphs ? 1u : 0u;
     return SLOSH_OK;
 }
 
@@ -920,7 +1101,9 @@ int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, u
     if (c->n == 0) return fail(c, SLOSH_E_STATE, "no particles uploaded");
     CK(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
-    const DevScene s = make_scene(c, c->parity, false);
+    DevScene s = make_scene(c, c->parity, false);
+    s.reuse = 0u;  // a full standalone build; the next substep rebuilds too
+    if (int r = force_grid_rebuild(c, st)) return r;
     if (c->dim == 3) enqueue_grid_build<3>(c, s, st, nullptr, true);
     else enqueue_grid_build<2>(c, s, st, nullptr, true);
     CK(cudaGetLastError());
@@ -986,7 +1169,7 @@ int slosh_grid_debug(slosh_ctx *c, slosh_grid_dump *dump, uint32_t cap_blocks, u
     copy(dump->num_particles_with_extras, d.npe, nbc);
     copy(dump->bucket_counts, d.counts, (size_t)nbc * NB);
     copy(dump->sorted_ids, d.sorted2, std::min(total, cap_sorted));
-    copy(dump->primary_first, c->bfirst, nbc);
+    copy(dump->primary_first, s.bfirst, nbc);
     copy(dump->primary_perm, perm_oid, c->n);
     copy(dump->neighbors, c->bnbh, (size_t)nbc * NN);
     cudaFree(blob);
@@ -1002,7 +1185,9 @@ int slosh_debug_nodes(slosh_ctx *c, int stage, float *nodes, uint32_t cap_blocks
     if (c->n == 0) return fail(c, SLOSH_E_STATE, "no particles uploaded");
     CK(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
-    const DevScene s = make_scene(c, c->parity, c->force_pending != 0);
+    DevScene s = make_scene(c, c->parity, c->force_pending != 0);
+    s.reuse = 0u;  // a full standalone build; the next substep rebuilds too
+    if (int r = force_grid_rebuild(c, st)) return r;
     DevScene gather = s;  // stage 1 of the deterministic P2G: node sums only
     gather.gather_only = 1u;
     if (c->dim == 3) {

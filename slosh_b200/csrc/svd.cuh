@@ -15,10 +15,19 @@
 // when singular values coincide or vanish.
 //
 // Precision policy: the FP32 result is recomputed in FP64 when it is not
-// trustworthy: F nearly singular or inverted (s2 <= 1e-3 s0), or R keeps
-// off-diagonal mass above 1e-5 s0, which is how nearly repeated singular
-// values show up (the eigenvectors of F^T F inside a near-degenerate
-// subspace are poorly determined in FP32).
+// trustworthy:
+//  - F nearly singular or inverted (s2 <= 1e-3 s0);
+//  - R keeps off-diagonal mass above 1e-5 s0, which is how nearly repeated
+//    singular values show up (the eigenvectors of F^T F inside a
+//    near-degenerate subspace are poorly determined in FP32);
+//  - all singular values within 1e-5 s0 of each other while F is not near
+//    a rotation (|s0 - 1| > 1e-5).  Drucker-Prager tests the deviatoric
+//    log strain for exact zero (drucker_prager.slang:165-200), a
+//    discontinuity at isotropic stretch: FP32 singular values that come out
+//    equal where FP64 resolves a difference of a few ulps would project a
+//    compressed particle to the yield surface's tip (a jump of |s - 1| in
+//    F).  Near a rotation that jump is below FP32 resolution, so the common
+//    F ~ I case stays in FP32.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -201,7 +210,8 @@ template <typename T> __device__ void svd3_impl(const T (&F)[3][3], Svd3<T> &out
 __device__ __forceinline__ void svd3(const float (&F)[3][3], Svd3<float> &out, unsigned *fp64_count) {
     svd3_impl<float>(F, out);
     const float s0 = fabsf(out.s[0]);
-    const bool degenerate = !(out.s[2] > 1e-3f * s0) || !(out.offdiag <= 1e-5f * s0);
+    const bool isotropic = out.s[0] - out.s[2] <= 1e-5f * s0 && fabsf(s0 - 1.0f) > 1e-5f;
+    const bool degenerate = !(out.s[2] > 1e-3f * s0) || !(out.offdiag <= 1e-5f * s0) || isotropic;
     if (degenerate && s0 > 0.0f) {
         double Fd[3][3];
 #pragma unroll
@@ -260,7 +270,8 @@ template <typename T> __device__ void svd2_impl(const T (&F)[2][2], Svd2<T> &out
 
 __device__ __forceinline__ void svd2(const float (&F)[2][2], Svd2<float> &out, unsigned *fp64_count) {
     svd2_impl<float>(F, out);
-    if (!(out.s[1] > 1e-3f * out.s[0]) && out.s[0] > 0.0f) {
+    const bool isotropic = out.s[0] - out.s[1] <= 1e-5f * out.s[0] && fabsf(out.s[0] - 1.0f) > 1e-5f;
+    if ((!(out.s[1] > 1e-3f * out.s[0]) || isotropic) && out.s[0] > 0.0f) {
         double Fd[2][2] = {{(double)F[0][0], (double)F[0][1]}, {(double)F[1][0], (double)F[1][1]}};
         Svd2<double> d;
         svd2_impl<double>(Fd, d);

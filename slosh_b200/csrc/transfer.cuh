@@ -950,6 +950,60 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
     }
 }
 
+// Grid-reuse bookkeeping of one particle that G2P has just moved from xo to
+// xn (storage position in block r of this substep's grid): when its base
+// cell changed, the per-cell count deltas and touched-cell bits of the old
+// and new blocks, which the next substep's k_grid_reuse applies; when the
+// change is one the kept grid cannot hold (a move of more than one cell, or
+// into a block without particles or outside the grid), the next substep's
+// full build.  The cells are the ones k_touch would compute from the stored
+// positions.
+template <int D, bool POW2>
+__device__ __forceinline__ void note_cell_change(const DevScene &s, uint32_t r, const float4 &xo4, const float4 &xn4,
+                                                 float h, float inv_h, uint32_t h_pow2) {
+    const float xo[3] = {xo4.x, xo4.y, xo4.z}, xn[3] = {xn4.x, xn4.y, xn4.z};
+    // round(x / h) per axis, as locate() computes it (the base cell is one less)
+    int co[D], cn[D];
+    bool moved = false;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        co[k] = __float2int_rn(POW2 ? xo[k] * inv_h : div_h(xo[k], h, inv_h, h_pow2));
+        cn[k] = __float2int_rn(POW2 ? xn[k] * inv_h : div_h(xn[k], h, inv_h, h_pow2));
+        moved = moved || co[k] != cn[k];
+    }
+    if (!moved) return;
+    constexpr int SHIFT = Geo<D>::BW == 4 ? 2 : 3, BW = Geo<D>::BW;
+    int bo[D], bn[D], lo[D], ln[D];
+    bool far = false, same_block = true;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int dc = cn[k] - co[k];
+        far = far || dc > 1 || dc < -1;
+        bo[k] = (co[k] - 1) >> SHIFT;
+        bn[k] = (cn[k] - 1) >> SHIFT;
+        lo[k] = (co[k] - 1) & (BW - 1);
+        ln[k] = (cn[k] - 1) & (BW - 1);
+        same_block = same_block && bo[k] == bn[k];
+    }
+    uint32_t r2 = r;
+    bool ok = !far;
+    if (ok && !same_block) {
+        const uint32_t slot = hash_find(s.hkeys, s.hcap, pack_key<D>(bn));
+        const uint32_t v = slot == NONE ? NONE : s.hvals[slot];
+        ok = v != NONE && (v & RANK_EXTRA) == 0u;
+        r2 = v;
+    }
+    if (!ok) {
+        s.ctr->rebuild[s.par ^ 1u] = 1u;
+        return;
+    }
+    const uint32_t c_old = cell_index<D>(lo), c_new = cell_index<D>(ln);
+    atomicAdd(&s.cell_delta[(size_t)r * CELLS + c_old], -1);
+    atomicAdd(&s.cell_delta[(size_t)r2 * CELLS + c_new], 1);
+    atomicOr(&s.touch[r], 1ull << c_old);
+    atomicOr(&s.touch[r2], 1ull << c_new);
+}
+
 // G2P fused with the particle update.  One CTA per active block with
 // primaries: the block's (block + 2)^D tile of node velocities is staged in
 // shared memory, then each thread gathers v, grad v and div v for its
@@ -1280,6 +1334,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
             float4 cv[Q], fv[Q];
             const float c22 = mat_split<D>(Cn, cv), f22 = mat_split<D>(F, fv);
             s.out_pm[o] = np4;
+            if constexpr (!B) {
+                if (s.reuse && (st_fo[buf][tid].x & FLAG_ENABLED)) note_cell_change<D, POW2>(s, r, st_pm[buf][tid], np4, h, inv_h, h_pow2);
+            }
             s.out_vv[o] = make_float4(vel[0], vel[1], D == 3 ? vel[D - 1] : 0.f, c22);
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
@@ -1309,7 +1366,8 @@ template <int D, bool B = false> __global__ void k_rigid(DevScene s) {
     if (id == 0 && s.clear_tail) {
         const uint32_t nb = s.ctr->n_blocks;
         s.ctr->last_n_blocks = nb;
-        s.ctr->last_n_primary = min(s.ctr->n_primary, s.cap);
+        if (!build_skipped(s)) s.ctr->last_n_primary = min(s.ctr->n_primary, s.cap);
+        if (s.reuse) s.ctr->rebuild[s.par] = 0u;  // read by this substep only; G2P set the next one's
         s.ctr->n_primary = 0u;
         s.ctr->n_extra = 0u;
         s.ctr->n_blocks = 0u;

@@ -510,7 +510,8 @@ class MpmData:
     def stats(self) -> dict:
         raw = np.zeros(8, np.uint32)
         _check(self._lib, self._ctx, self._lib.slosh_get_stats(self._ctx, ptr(raw)))
-        keys = ("n_particles", "n_blocks", "n_primary_blocks", "n_materials", "n_svd_fp64")
+        keys = ("n_particles", "n_blocks", "n_primary_blocks", "n_materials", "n_svd_fp64", "n_grid_rebuilds",
+                "n_grid_reuses", "conditional_graphs")
         return {k: int(raw[i]) for i, k in enumerate(keys)}
 
     def profile_substeps(self, n_substeps: int, stream=None) -> dict:

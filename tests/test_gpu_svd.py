@@ -1,8 +1,11 @@
 """The GPU SVD and its FP64 fallback, through the constitutive models.
 
 The models' 3x3 SVD runs in FP32 and is recomputed in FP64 when F is nearly
-singular or inverted (s2 <= 1e-3 s0) or when the FP32 QR step leaves
-off-diagonal mass above 1e-5 s0 (nearly repeated singular values).  Here
+singular or inverted (s2 <= 1e-3 s0), when the FP32 QR step leaves
+off-diagonal mass above 1e-5 s0 (nearly repeated singular values), or when
+all three singular values lie within 1e-5 s0 of each other away from a
+rotation (nearly isotropic stretch, where Drucker-Prager's exact
+zero-deviator test is discontinuous).  Here
 particles at rest (v = 0, C = 0, no gravity, no collider) carry chosen
 deformation gradients: the grid then holds zero velocity, the substep leaves
 F unchanged up to the model, and the model's output is read back exactly:
@@ -41,7 +44,10 @@ def _rotation(rng):
 def _families(rng, per):
     """F = U diag(sigma) V^T for each family (FP32 entries)."""
     sig = {
-        "repeated": [(1.0, 1.0 + 1e-7, 1.0 - 1e-7), (1.1, 1.1 * (1.0 + 3e-7), 0.97), (0.95, 0.95, 0.95 * (1 + 2e-7))],
+        "repeated": [(1.0, 1.0 + 1e-7, 1.0 - 1e-7), (1.1, 1.1 * (1.0 + 3e-7), 0.97)],
+        # all three nearly equal, away from a rotation: Drucker-Prager's exact
+        # zero-deviator test is discontinuous there
+        "isotropic": [(0.95, 0.95, 0.95 * (1 + 2e-7)), (1.08, 1.08 * (1 - 1e-7), 1.08), (0.9, 0.9 * (1 + 3e-7), 0.9 * (1 - 2e-7))],
         "near_singular": [(1.0, 0.6, 1e-5), (1.2, 2e-4, 1e-5), (0.9, 0.9, 5e-4)],
         "rotated_diagonal": [(1.05, 0.98, 0.93), (1.01, 1.0, 0.99), (0.97, 0.96, 0.9)],
         "inverted": [(1.0, 0.9, -0.8), (1.0, 1.0, -1e-4)],
@@ -122,6 +128,6 @@ def test_svd_fp64_fallback_against_fp64_oracle(cuda_lib, model):
             es = np.abs(got["model"][sel, :3].astype(np.float64) - st64[sel]).max(axis=0)
             print(f"{name}: plastic state err {es}")
             assert (es <= 1e-5 * np.maximum(1.0, np.abs(st64[sel]).max(axis=0))).all(), name
-    must = int(((fam_of == "near_singular") | (fam_of == "inverted")).sum())
+    must = int(((fam_of == "near_singular") | (fam_of == "inverted") | (fam_of == "isotropic")).sum())
     print(f"FP64 SVD fallbacks: {n64} (at least {must} expected)")
     assert n64 >= must
