@@ -248,6 +248,77 @@ int slosh_add_trimesh(slosh_ctx *ctx, const float *vertices, uint32_t n_vertices
  * context creation makes every substep run the full build. */
 int slosh_step(slosh_ctx *ctx, uint32_t n_substeps, void *stream);
 
+/* ---- stage hooks ------------------------------------------------------------
+ * slosh's MpmPipelineHooks (src/pipeline.rs:146-238): callbacks at fixed
+ * points of launch_step (src/pipeline.rs:562-770).  A hook runs on the host
+ * thread inside slosh_step, once per substep, at the point the substep's
+ * kernels have been enqueued up to; it may enqueue its own device work on
+ * `stream` (a cudaStream_t), which then runs in order with the substep.  It
+ * returns 0, or a negative status that stops slosh_step with that status;
+ * the run hooks may return 1 instead, meaning "I replaced this stage", as
+ * slosh's run_p2g / run_g2p return Ok(true).  While any hook is set, the
+ * substeps are launched kernel by kernel instead of as CUDA graphs.
+ *  AFTER_PARTICLE_SORT  after the grid build (the sort of particles by block)
+ *  RUN_P2G              replaces P2G: the hook writes the P2G result of every
+ *                       node of the active blocks, (momentum, mass) in the
+ *                       view's `nodes`; the grid update then reads them
+ *  AFTER_P2G            after P2G; the view's `nodes` hold (momentum, mass)
+ *  AFTER_GRID_UPDATE    after the grid update; `nodes` hold (velocity, mass)
+ *  RUN_G2P              replaces the G2P gather fused with the particle
+ *                       update (slosh's g2p and particles_update passes): the
+ *                       hook writes every particle's next state into the
+ *                       view's out_* planes at its canonical position
+ *  AFTER_G2P            after the fused G2P / particle update
+ *  AFTER_PARTICLES_UPDATE  after AFTER_G2P, before the rigid-body update
+ * The G2P gather and the particle update are one kernel here, so AFTER_G2P
+ * and AFTER_PARTICLES_UPDATE both follow it. */
+#define SLOSH_HOOK_AFTER_PARTICLE_SORT 0u
+#define SLOSH_HOOK_RUN_P2G 1u
+#define SLOSH_HOOK_AFTER_P2G 2u
+#define SLOSH_HOOK_AFTER_GRID_UPDATE 3u
+#define SLOSH_HOOK_RUN_G2P 4u
+#define SLOSH_HOOK_AFTER_G2P 5u
+#define SLOSH_HOOK_AFTER_PARTICLES_UPDATE 6u
+#define SLOSH_HOOK_COUNT 7u
+
+typedef int (*slosh_hook_fn)(slosh_ctx *ctx, uint32_t point, void *stream, void *user);
+
+/* Sets (fn != NULL) or clears the hook of `point`.  `user` is passed back
+ * to the hook (slosh's hooks_state). */
+int slosh_set_hook(slosh_ctx *ctx, uint32_t point, slosh_hook_fn fn, void *user);
+
+/* Enqueues on `stream` the built-in stage that run hook `point` replaces
+ * (SLOSH_HOOK_RUN_P2G: P2G with its node sums written to the view's
+ * `nodes`; SLOSH_HOOK_RUN_G2P: the fused G2P / particle update), so a
+ * replacing hook can wrap the built-in stage with work of its own.  Only
+ * valid inside that hook; the results are those of the built-in substep,
+ * bit for bit. */
+int slosh_enqueue_builtin(slosh_ctx *ctx, uint32_t point, void *stream);
+
+/* Device buffers of the substep a hook runs in (valid inside a hook).
+ * Particle storage is in the canonical order of this substep's grid: block
+ * b's particles are perm[block_first[b] .. + block_count[b]), storage
+ * indices of the input planes.  Planes (capacity entries each): x_mass
+ * float4 (x, y, z, mass); vel float4 (vx, vy, vz, C22); affine and def_grad
+ * two float4 planes each, row-major matrix elements 0-7 (2D: one plane,
+ * elements 0-3); flags uint4 (flags, original index, V0 bits, F22 bits);
+ * plastic float4 (plastic det, hardening q, log_vol_gain, damping).
+ * The out_* planes are the next substep's storage, written by the fused
+ * G2P / particle update at the canonical index.  nodes: 64 float4 a block,
+ * node id = block * 64 + local index (grid.slang:409-417). */
+typedef struct slosh_device_view {
+    uint32_t dim, n_particles, capacity, grid_capacity;
+    float cell_width, dt;
+    uint32_t pad[2];
+    const uint32_t *n_blocks;  /* device word: active blocks of the substep */
+    const uint32_t *block_keys, *block_first, *block_count, *perm;
+    void *x_mass, *vel, *affine, *def_grad, *flags, *plastic;
+    void *out_x_mass, *out_vel, *out_affine, *out_def_grad, *out_flags, *out_plastic;
+    void *nodes;
+} slosh_device_view;
+
+int slosh_device_view_get(slosh_ctx *ctx, slosh_device_view *out);
+
 /* Waits for the context's work and returns the device error status
  * (SLOSH_E_OVERFLOW when the block hash map or block list overflowed). */
 int slosh_sync(slosh_ctx *ctx, void *stream);

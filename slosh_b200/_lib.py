@@ -228,6 +228,56 @@ class SloshServerStats(ctypes.Structure):
     ]
 
 
+# Stage hooks (slosh's MpmPipelineHooks points).
+HOOK_AFTER_PARTICLE_SORT = 0
+HOOK_RUN_P2G = 1
+HOOK_AFTER_P2G = 2
+HOOK_AFTER_GRID_UPDATE = 3
+HOOK_RUN_G2P = 4
+HOOK_AFTER_G2P = 5
+HOOK_AFTER_PARTICLES_UPDATE = 6
+HOOK_NAMES = (
+    "after_particle_sort",
+    "run_p2g",
+    "after_p2g",
+    "after_grid_update",
+    "run_g2p",
+    "after_g2p",
+    "after_particles_update",
+)
+HOOK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p)
+
+
+class SloshDeviceView(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_uint32),
+        ("n_particles", ctypes.c_uint32),
+        ("capacity", ctypes.c_uint32),
+        ("grid_capacity", ctypes.c_uint32),
+        ("cell_width", ctypes.c_float),
+        ("dt", ctypes.c_float),
+        ("pad", ctypes.c_uint32 * 2),
+        ("n_blocks", ctypes.c_void_p),
+        ("block_keys", ctypes.c_void_p),
+        ("block_first", ctypes.c_void_p),
+        ("block_count", ctypes.c_void_p),
+        ("perm", ctypes.c_void_p),
+        ("x_mass", ctypes.c_void_p),
+        ("vel", ctypes.c_void_p),
+        ("affine", ctypes.c_void_p),
+        ("def_grad", ctypes.c_void_p),
+        ("flags", ctypes.c_void_p),
+        ("plastic", ctypes.c_void_p),
+        ("out_x_mass", ctypes.c_void_p),
+        ("out_vel", ctypes.c_void_p),
+        ("out_affine", ctypes.c_void_p),
+        ("out_def_grad", ctypes.c_void_p),
+        ("out_flags", ctypes.c_void_p),
+        ("out_plastic", ctypes.c_void_p),
+        ("nodes", ctypes.c_void_p),
+    ]
+
+
 # Every symbol include/slosh_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
@@ -245,6 +295,9 @@ SIGNATURES = {
     "slosh_add_trimesh": (ctypes.c_int, [_P, _P, _U32, _P, _U32, _P]),
     "slosh_step": (ctypes.c_int, [_P, _U32, _P]),
     "slosh_sync": (ctypes.c_int, [_P, _P]),
+    "slosh_set_hook": (ctypes.c_int, [_P, _U32, HOOK_FN, _P]),
+    "slosh_enqueue_builtin": (ctypes.c_int, [_P, _U32, _P]),
+    "slosh_device_view_get": (ctypes.c_int, [_P, ctypes.POINTER(SloshDeviceView)]),
     "slosh_kernels_per_substep": (_U32, [_P]),
     "slosh_profile_substeps": (ctypes.c_int, [_P, _U32, _P, _P, _U32, ctypes.POINTER(_U32)]),
     "slosh_kernel_name": (ctypes.c_int, [_U32, ctypes.c_char_p, ctypes.c_size_t]),

@@ -60,6 +60,14 @@ struct slosh_ctx {
     unsigned long long *touch = nullptr, *cur_touch = nullptr;
     uint32_t reuse = 0;
     bool cond_graphs = false;  // the substep graphs pick the build through a conditional node
+    // stage hooks (slosh's MpmPipelineHooks); while one is set, substeps are
+    // launched kernel by kernel with the hooks called between the stages
+    slosh_hook_fn hooks[SLOSH_HOOK_COUNT] = {};
+    void *hook_user[SLOSH_HOOK_COUNT] = {};
+    uint32_t n_hooks = 0;
+    bool in_hook = false;
+    uint32_t hook_point = 0;
+    DevScene hook_scene{};  // the substep a hook runs in
     // P2G reduction (environment SLOSH_P2G at creation): 0 fixed-order,
     // bit-reproducible (default); 3 "direct": the same cell-owner kernel with
     // shared-memory and global float atomics, kept for A/B comparison.
@@ -383,9 +391,7 @@ void enqueue_clear(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
 }
 
 // P2G, grid update, fused G2P/update and the rigid update.
-template <int D> void enqueue_transfer(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
-    enqueue_p2g<D>(c, s, st, p);
-    enqueue_grid_update<D>(c, s, st, p);
+template <int D> void enqueue_g2p(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(13);
     // persistent: 8 CTAs of 64 fit an SM; each takes blocks from the queue.
     // Small CTAs wait less at the per-block barriers (tile load, the
@@ -402,6 +408,12 @@ template <int D> void enqueue_transfer(slosh_ctx *c, const DevScene &s, cudaStre
         k_g2p_update<D, 64, false, true, SLOSH_MODEL_FLUID_TAIT><<<g2p_grid, 64, 0, st>>>(s);
     else k_g2p_update<D, 64, false, true><<<g2p_grid, 64, 0, st>>>(s);
     PROF_END(13);
+}
+
+template <int D> void enqueue_transfer(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
+    enqueue_p2g<D>(c, s, st, p);
+    enqueue_grid_update<D>(c, s, st, p);
+    enqueue_g2p<D>(c, s, st, p);
     PROF_BEGIN(14);
     k_rigid<D><<<1, 32, 0, st>>>(s);
     PROF_END(14);
@@ -418,6 +430,79 @@ void enqueue_substep(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force,
 void enqueue_substep_any(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force, Prof *p = nullptr) {
     if (c->dim == 3) enqueue_substep<3>(c, st, parity, force, p);
     else enqueue_substep<2>(c, st, parity, force, p);
+}
+
+// Makes the next substep run the full grid build: after an upload, an
+// append or removal, or a standalone build (debug entry points), the
+// previous substep's grid no longer describes storage.  G2P's pending
+// per-cell bookkeeping is dropped with it.
+int force_grid_rebuild(slosh_ctx *c, cudaStream_t st) {
+    if (!c->reuse) return SLOSH_OK;
+    CK(cudaMemsetAsync(c->cell_delta, 0, (size_t)c->cap * CELLS * sizeof(int), st));
+    CK(cudaMemsetAsync(c->touch, 0, (size_t)c->cap * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(c->ctr->rebuild, 1, sizeof(c->ctr->rebuild), st));  // nonzero: rebuild
+    return SLOSH_OK;
+}
+
+// One substep with the stage hooks called between its kernels, in the
+// order of slosh's launch_step (src/pipeline.rs:562-770).
+int call_hook(slosh_ctx *c, const DevScene &s, uint32_t pt, cudaStream_t st) {
+    if (!c->hooks[pt]) return 0;
+    c->in_hook = true;
+    c->hook_point = pt;
+    c->hook_scene = s;
+    const int r = c->hooks[pt](c, pt, (void *)st, c->hook_user[pt]);
+    c->in_hook = false;
+    return r;
+}
+
+template <int D> int enqueue_substep_hooked(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool force) {
+    const DevScene s = make_scene(c, parity, force);
+    // A hook that fails drops the substep: storage (the input planes) is
+    // untouched, and the grid state is reset so that the substep can run
+    // again from a full build.
+    auto drop = [&](int code) {
+        k_clear<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
+        force_grid_rebuild(c, st);
+        return code;
+    };
+    if (s.reuse) enqueue_reuse_decision<D>(c, s, st, nullptr);
+    enqueue_grid_build<D>(c, s, st);
+    int r = call_hook(c, s, SLOSH_HOOK_AFTER_PARTICLE_SORT, st);
+    if (r < 0) return drop(r);
+    // P2G; the grid update reads node sums from `nodes` when a hook wrote or
+    // may change them (the sums land there bit for bit as the update's own
+    // gather computes them)
+    r = call_hook(c, s, SLOSH_HOOK_RUN_P2G, st);
+    if (r < 0) return drop(r);
+    const bool p2g_replaced = r == 1;
+    DevScene from_nodes = s;
+    from_nodes.use_partial = 0u;
+    if (!p2g_replaced) {
+        enqueue_p2g<D>(c, s, st);
+        if (c->hooks[SLOSH_HOOK_AFTER_P2G]) {
+            DevScene gather = s;
+            gather.gather_only = 1u;
+            enqueue_grid_update<D>(c, gather, st);
+        }
+    }
+    if ((r = call_hook(c, s, SLOSH_HOOK_AFTER_P2G, st)) < 0) return drop(r);
+    const bool via_nodes = p2g_replaced || c->hooks[SLOSH_HOOK_AFTER_P2G] != nullptr;
+    enqueue_grid_update<D>(c, via_nodes ? from_nodes : s, st);
+    if ((r = call_hook(c, s, SLOSH_HOOK_AFTER_GRID_UPDATE, st)) < 0) return drop(r);
+    r = call_hook(c, s, SLOSH_HOOK_RUN_G2P, st);
+    if (r < 0) return drop(r);
+    if (r == 1) {
+        // a replaced update records no cell changes: the next substep rebuilds
+        k_after_replaced_g2p<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
+        if (c->reuse && cudaMemsetAsync(&c->ctr->rebuild[s.par ^ 1u], 1, 4, st) != cudaSuccess) return SLOSH_E_CUDA;
+    } else {
+        enqueue_g2p<D>(c, s, st, nullptr);
+    }
+    if ((r = call_hook(c, s, SLOSH_HOOK_AFTER_G2P, st)) < 0) return drop(r);
+    if ((r = call_hook(c, s, SLOSH_HOOK_AFTER_PARTICLES_UPDATE, st)) < 0) return drop(r);
+    k_rigid<D><<<1, 32, 0, st>>>(s);
+    return cudaGetLastError() == cudaSuccess ? SLOSH_OK : SLOSH_E_CUDA;
 }
 
 void destroy_graphs(slosh_ctx *c) {
@@ -524,18 +609,6 @@ int build_graphs(slosh_ctx *c) {
         if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
     }
     c->graphs_valid = true;
-    return SLOSH_OK;
-}
-
-// Makes the next substep run the full grid build: after an upload, an
-// append or removal, or a standalone build (debug entry points), the
-// previous substep's grid no longer describes storage.  G2P's pending
-// per-cell bookkeeping is dropped with it.
-int force_grid_rebuild(slosh_ctx *c, cudaStream_t st) {
-    if (!c->reuse) return SLOSH_OK;
-    CK(cudaMemsetAsync(c->cell_delta, 0, (size_t)c->cap * CELLS * sizeof(int), st));
-    CK(cudaMemsetAsync(c->touch, 0, (size_t)c->cap * sizeof(unsigned long long), st));
-    CK(cudaMemsetAsync(c->ctr->rebuild, 1, sizeof(c->ctr->rebuild), st));  // nonzero: rebuild
     return SLOSH_OK;
 }
 
@@ -999,7 +1072,12 @@ int slosh_step(slosh_ctx *c, uint32_t n_substeps, void *stream) {
     CK(cudaSetDevice(c->device));
     cudaStream_t st = pick(c, stream);
     for (uint32_t k = 0; k < n_substeps; ++k) {
-        if (c->force_pending) {
+        if (c->n_hooks) {
+            const int r = c->dim == 3 ? enqueue_substep_hooked<3>(c, st, c->parity, c->force_pending != 0)
+                                      : enqueue_substep_hooked<2>(c, st, c->parity, c->force_pending != 0);
+            if (r < 0) return r == SLOSH_E_CUDA ? fail(c, r, "substep with stage hooks: CUDA error") : r;
+            c->force_pending = 0;
+        } else if (c->force_pending) {
             enqueue_substep_any(c, st, c->parity, true);
             CK(cudaGetLastError());
             c->force_pending = 0;
@@ -1014,6 +1092,72 @@ int slosh_step(slosh_ctx *c, uint32_t n_substeps, void *stream) {
         }
         c->parity ^= 1u;
     }
+    return SLOSH_OK;
+}
+
+int slosh_set_hook(slosh_ctx *c, uint32_t point, slosh_hook_fn fn, void *user) {
+    if (!c || point >= SLOSH_HOOK_COUNT) return SLOSH_E_INVALID;
+    if (c->in_hook) return fail(c, SLOSH_E_STATE, "hooks cannot be changed from inside a hook");
+    c->hooks[point] = fn;
+    c->hook_user[point] = fn ? user : nullptr;
+    c->n_hooks = 0;
+    for (uint32_t k = 0; k < SLOSH_HOOK_COUNT; ++k) c->n_hooks += c->hooks[k] ? 1u : 0u;
+    return SLOSH_OK;
+}
+
+int slosh_enqueue_builtin(slosh_ctx *c, uint32_t point, void *stream) {
+    if (!c) return SLOSH_E_INVALID;
+    if (!c->in_hook || c->hook_point != point || (point != SLOSH_HOOK_RUN_P2G && point != SLOSH_HOOK_RUN_G2P))
+        return fail(c, SLOSH_E_STATE, "the built-in stage of hook %u can only be enqueued from inside that run hook", point);
+    cudaStream_t st = pick(c, stream);
+    const DevScene &s = c->hook_scene;
+    if (point == SLOSH_HOOK_RUN_P2G) {
+        DevScene gather = s;  // P2G, then its node sums written to `nodes`
+        gather.gather_only = 1u;
+        if (c->dim == 3) {
+            enqueue_p2g<3>(c, s, st);
+            enqueue_grid_update<3>(c, gather, st);
+        } else {
+            enqueue_p2g<2>(c, s, st);
+            enqueue_grid_update<2>(c, gather, st);
+        }
+    } else {
+        if (c->dim == 3) enqueue_g2p<3>(c, s, st, nullptr);
+        else enqueue_g2p<2>(c, s, st, nullptr);
+    }
+    CK(cudaGetLastError());
+    return SLOSH_OK;
+}
+
+int slosh_device_view_get(slosh_ctx *c, slosh_device_view *out) {
+    if (!c || !out) return SLOSH_E_INVALID;
+    if (!c->in_hook) return fail(c, SLOSH_E_STATE, "the device view is only valid inside a stage hook");
+    const DevScene &s = c->hook_scene;
+    std::memset(out, 0, sizeof(*out));
+    out->dim = (uint32_t)c->dim;
+    out->n_particles = c->n;
+    out->capacity = c->max_n;
+    out->grid_capacity = c->cap;
+    out->cell_width = c->h;
+    out->dt = c->params.dt;
+    out->n_blocks = &c->ctr->n_blocks;
+    out->block_keys = s.bkey;
+    out->block_first = s.bfirst;
+    out->block_count = s.bnp;
+    out->perm = s.perm;
+    out->x_mass = s.pm;
+    out->vel = s.vv;
+    out->affine = s.cq;
+    out->def_grad = s.fq;
+    out->flags = s.fo;
+    out->plastic = s.ps;
+    out->out_x_mass = s.out_pm;
+    out->out_vel = s.out_vv;
+    out->out_affine = s.out_cq;
+    out->out_def_grad = s.out_fq;
+    out->out_flags = s.out_fo;
+    out->out_plastic = s.out_ps;
+    out->nodes = s.nodes;
     return SLOSH_OK;
 }
 

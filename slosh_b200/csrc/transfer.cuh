@@ -950,6 +950,35 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
     }
 }
 
+// Clears the next substep's hash map and the key histogram / per-scene
+// block counts (their readers in this substep have all run), thread g0 of
+// gs.  Done by the fused G2P / particle update, or by k_clear_next when a
+// stage hook replaced it.
+template <bool B> __device__ __forceinline__ void clear_next_map(const DevScene &s, uint32_t g0, uint32_t gs) {
+    for (uint32_t q = g0; q < s.hcap; q += gs) {
+        if constexpr (B) s.clr_hkeys64[q] = NONE64;
+        else s.clr_hkeys[q] = NONE;
+        s.clr_hvals[q] = NONE;
+    }
+    if constexpr (B) {
+        for (uint32_t q = g0; q < s.n_scenes; q += gs) s.scene_nblk[q] = 0u;
+    } else {
+        for (uint32_t q = g0; q < HIST_BINS; q += gs) s.hist[q] = 0u;
+        if (g0 < HIST_COARSE) s.hist_coarse[g0] = 0u;
+    }
+    if (*s.err != 0u)
+        for (size_t q = g0; q < (size_t)s.hcap * CELLS; q += gs) s.slot_counts[q] = 0u;
+}
+
+// After a stage hook replaced the fused G2P / particle update: the next
+// map cleared as G2P would, and the original-index plane of the next
+// storage taken from its flags plane.
+__global__ void k_after_replaced_g2p(DevScene s) {
+    const uint32_t g0 = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    clear_next_map<false>(s, g0, gs);
+    for (uint32_t i = g0; i < s.count; i += gs) s.out_oid[i] = s.out_fo[i].y;
+}
+
 // Grid-reuse bookkeeping of one particle that G2P has just moved from xo to
 // xn (storage position in block r of this substep's grid): when its base
 // cell changed, the per-cell count deltas and touched-cell bits of the old
@@ -1034,24 +1063,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
     float vmax = h / dt;
     const size_t n = s.n;
     const uint32_t tid = threadIdx.x;
-    if (s.clear_tail) {
-        // Clear the next substep's hash map and the key histogram / per-scene
-        // block counts (their readers in this substep have all run).
-        const uint32_t g0 = blockIdx.x * NT + tid, gs = gridDim.x * NT;
-        for (uint32_t q = g0; q < s.hcap; q += gs) {
-            if constexpr (B) s.clr_hkeys64[q] = NONE64;
-            else s.clr_hkeys[q] = NONE;
-            s.clr_hvals[q] = NONE;
-        }
-        if constexpr (B) {
-            for (uint32_t q = g0; q < s.n_scenes; q += gs) s.scene_nblk[q] = 0u;
-        } else {
-            for (uint32_t q = g0; q < HIST_BINS; q += gs) s.hist[q] = 0u;
-            if (g0 < HIST_COARSE) s.hist_coarse[g0] = 0u;
-        }
-        if (*s.err != 0u)
-            for (size_t q = g0; q < (size_t)s.hcap * CELLS; q += gs) s.slot_counts[q] = 0u;
-    }
+    if (s.clear_tail) clear_next_map<B>(s, blockIdx.x * NT + tid, gridDim.x * NT);
     // Issues the copies of sorted entry e (storage index i) of the block into
     // buffer b (an empty group when e is past the block's particles).  The
     // storage index is loaded one iteration before the copies that need it.

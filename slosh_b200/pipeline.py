@@ -562,6 +562,17 @@ class MpmData:
         _check(self._lib, self._ctx, self._lib.slosh_debug_nodes(self._ctx, stage, ptr(out), nb.value, ctypes.byref(nb)))
         return out
 
+    def device_view(self) -> "_lib.SloshDeviceView":
+        """The device buffers of the substep a stage hook runs in (only
+        inside a hook)."""
+        v = _lib.SloshDeviceView()
+        _check(self._lib, self._ctx, self._lib.slosh_device_view_get(self._ctx, ctypes.byref(v)))
+        return v
+
+    def enqueue_builtin(self, point: int, stream) -> None:
+        """The built-in stage a run hook replaces (only inside that hook)."""
+        _check(self._lib, self._ctx, self._lib.slosh_enqueue_builtin(self._ctx, int(point), stream))
+
     def prefix_sum(self, values: np.ndarray) -> np.ndarray:
         v = np.ascontiguousarray(values, dtype=np.uint32)
         out = np.zeros_like(v)
@@ -580,18 +591,80 @@ class MpmData:
             pass
 
 
+class MpmPipelineHooks:
+    """``MpmPipelineHooks`` (src/pipeline.rs:146-238): override the stages
+    to hook.  Each method gets the scene, the CUDA stream of the substep (an
+    int handle; work enqueued on it runs in order with the substep) and the
+    caller's state object.  ``run_p2g`` / ``run_g2p`` return True when they
+    replaced the built-in stage (``data.enqueue_builtin`` runs it from inside
+    the hook); the ``after_*`` methods return None.  ``data.device_view()``
+    gives the substep's device buffers inside a hook."""
+
+    def after_particle_sort(self, data, stream, state):
+        return None
+
+    def run_p2g(self, data, stream, state) -> bool:
+        return False
+
+    def after_p2g(self, data, stream, state):
+        return None
+
+    def after_grid_update(self, data, stream, state):
+        return None
+
+    def run_g2p(self, data, stream, state) -> bool:
+        return False
+
+    def after_g2p(self, data, stream, state):
+        return None
+
+    def after_particles_update(self, data, stream, state):
+        return None
+
+
 class MpmPipeline:
     """``MpmPipeline::launch_step``: enqueues substeps on the GPU.
 
-    The whole substep is one CUDA graph; no host round trip happens inside
-    ``launch_step``.  Device-side errors (block capacity overflow) surface
-    at the next ``MpmData.sync()`` or download."""
+    Without hooks the whole substep is one CUDA graph; no host round trip
+    happens inside ``launch_step``.  Device-side errors (block capacity
+    overflow) surface at the next ``MpmData.sync()`` or download.  With
+    hooks (an ``MpmPipelineHooks`` whose methods are overridden), the
+    substep's kernels are launched one by one and each overridden method is
+    called at its point of every substep."""
 
     def __init__(self):
         self._lib = _lib.load()
 
-    def launch_step(self, data: MpmData, n_substeps: int = 1, stream=None):
-        _check(self._lib, data._ctx, self._lib.slosh_step(data._ctx, int(n_substeps), stream))
+    def launch_step(self, data: MpmData, n_substeps: int = 1, stream=None, hooks=None, hooks_state=None):
+        if hooks is None:
+            _check(self._lib, data._ctx, self._lib.slosh_step(data._ctx, int(n_substeps), stream))
+            return
+        callbacks, errors = [], []
+        base = MpmPipelineHooks
+        for point, name in enumerate(_lib.HOOK_NAMES):
+            method = getattr(type(hooks), name, None)
+            if method is None or method is getattr(base, name):
+                continue
+
+            def call(ctx, pt, st, user, _name=name):
+                try:
+                    r = getattr(hooks, _name)(data, st or 0, hooks_state)
+                    return 1 if r is True else 0
+                except Exception as e:  # reported after slosh_step returns
+                    errors.append(e)
+                    return _lib.SLOSH_E_STATE
+
+            cb = _lib.HOOK_FN(call)
+            callbacks.append(cb)
+            _check(self._lib, data._ctx, self._lib.slosh_set_hook(data._ctx, point, cb, None))
+        try:
+            code = self._lib.slosh_step(data._ctx, int(n_substeps), stream)
+        finally:
+            for point in range(len(_lib.HOOK_NAMES)):
+                self._lib.slosh_set_hook(data._ctx, point, _lib.HOOK_FN(), None)
+        if errors:
+            raise errors[0]
+        _check(self._lib, data._ctx, code)
 
     def compute_timestep_bound(self, data: MpmData, stream=None) -> float:
         """``pipeline.timestep_bounds.compute_bounds`` (src/solver/timestep_bound.rs:58-81)."""
