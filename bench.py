@@ -82,7 +82,12 @@ def main_ncu_case(args):
     from slosh_b200 import scenes
     from slosh_b200.pipeline import MpmPipeline
 
-    sc = scenes.sand_column_3d(h=args.h, substeps=500, radius=args.radius)
+    if args.workload == "dam_break_2d":
+        sc = scenes.dam_break_2d()
+    elif args.workload == "elastic_drop_3d":
+        sc = scenes.elastic_drop_3d()
+    else:
+        sc = scenes.sand_column_3d(h=args.h, substeps=500, radius=args.radius)
     data = scenes.build_mpm_data(sc)
     MpmPipeline().launch_step(data, args.steps)
     data.sync()
@@ -125,16 +130,19 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str):
+def ncu_traffic(kernel: str, workload: str | None = None):
     """Per-launch DRAM bytes of `kernel` from the committed ncu summary
-    (profiles/ncu_traffic.txt lines: `<kernel> <bytes_per_launch> ...`)."""
+    (profiles/ncu_traffic.txt lines: `<kernel> <bytes_per_launch> ...` for
+    the sand column, `<workload>:<kernel> <bytes_per_launch> ...` for the
+    other workloads)."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(p):
         return None
+    name = f"{workload}:{kernel}" if workload else kernel
     with open(p) as f:
         for line in f:
             parts = line.split()
-            if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+            if len(parts) >= 2 and parts[0] == name and not line.startswith("#"):
                 try:
                     return float(parts[1])
                 except ValueError:
@@ -199,6 +207,20 @@ class ClockSampler:
             "reasons": sorted(reasons),
             "samples": len(sm),
         }
+
+
+def timed_launches(data, st0: dict, st1: dict, steps: int):
+    """Kernels launched by `steps` substeps between two stats snapshots, and
+    how many of them kept their grid: with conditional graphs a substep that
+    keeps its grid launches 6 kernels, one that rebuilds it 14."""
+    reused = st1["n_grid_reuses"] - st0["n_grid_reuses"]
+    rebuilt = st1["n_grid_rebuilds"] - st0["n_grid_rebuilds"]
+    if st1["conditional_graphs"]:
+        launches = 14 * rebuilt + 6 * reused
+    else:
+        launches = data.kernels_per_substep * steps
+    return launches, {"reused_substeps": reused, "rebuilt_substeps": rebuilt,
+                      "conditional_graphs": bool(st1["conditional_graphs"])}
 
 
 def bench_scene(h: float):
@@ -333,16 +355,7 @@ def main_ours(args):
     ms = max_over_ranks(ev0.elapsed_time(ev1), pg, dev)
     value = aggregate_rate(world, n * args.steps, ms)
     st1 = data.stats()
-    reused = st1["n_grid_reuses"] - st0["n_grid_reuses"]
-    rebuilt = st1["n_grid_rebuilds"] - st0["n_grid_rebuilds"]
-    # kernels launched in the timed region: with conditional graphs a
-    # substep that keeps its grid launches 7, a full build 14
-    if st1["conditional_graphs"]:
-        launches = 14 * rebuilt + 7 * reused
-    else:
-        launches = data.kernels_per_substep * args.steps
-    grid_reuse = {"reused_substeps": reused, "rebuilt_substeps": rebuilt,
-                  "conditional_graphs": bool(st1["conditional_graphs"])}
+    launches, grid_reuse = timed_launches(data, st0, st1, args.steps)
     svd_fp64 = st1["n_svd_fp64"] - st0["n_svd_fp64"]
 
     # per-kernel device time right after the timed region (direct launches
@@ -353,6 +366,7 @@ def main_ours(args):
     # same graphs), beside the single K-substep region above
     rep_k = max(args.steps, 100)
     reps = []
+    st_r0 = data.stats()
     for _ in range(5):
         r0 = torch.cuda.Event(enable_timing=True)
         r1 = torch.cuda.Event(enable_timing=True)
@@ -370,6 +384,7 @@ def main_ours(args):
         "ms_per_step": rep_ms / rep_k,
         "ms_per_step_all": [r / rep_k for r in reps],
     }
+    _, repeat["grid_reuse"] = timed_launches(data, st_r0, data.stats(), rep_k * len(reps))
 
     per_substep = {k: v / args.profile_steps for k, v in prof.items()}
     dom = max(per_substep, key=per_substep.get)
@@ -476,6 +491,8 @@ def main_ours(args):
         if world == 1 and not args.no_extras:
             # the batched and served configurations, measured in the same run
             drop = ("n_gpus", "higher_is_better", "scaling", "vs_baseline", "dtype", "data")
+            for wl, k in (("dam_break_2d", 1000), ("elastic_drop_3d", 2000)):  # their whole runs
+                line[wl] = {key: v for key, v in plain_line(args, wl, k, args.warmup, 5.0).items() if key not in drop}
             line["batched"] = {k: v for k, v in batched_line(args, args.batched_substeps, args.warmup).items() if k not in drop}
             line["served"] = {k: v for k, v in served_line(args).items() if k not in drop}
         print(json.dumps(line))
@@ -810,7 +827,7 @@ def plain_alg_bytes(dim: int, sand: bool, n: int, n_nodes: int) -> dict:
     }
 
 
-def main_plain(args):
+def plain_line(args, workload: str, steps: int, warmup: int, cpu_seconds: float) -> dict:
     """The other plain single-scene configurations: the 2D dam break
     (62.6 k particles, Tait fluid) and the 3D elastic drop (524 k particles,
     two fixed-corotated cubes), timed like the sand column."""
@@ -825,7 +842,7 @@ def main_plain(args):
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if args.workload == "dam_break_2d":
+    if workload == "dam_break_2d":
         sc = scenes.dam_break_2d()
         desc = "dam_break_2d: Tait fluid column 0.4x0.6 at 2x2 ppc, dx=1/256, stick walls, dt=1e-4"
         b_alg, sand = 129.0, False
@@ -838,22 +855,24 @@ def main_plain(args):
     stream = torch.cuda.Stream(device=dev)
     sptr = ctypes.c_void_p(stream.cuda_stream)
     pipe = MpmPipeline()
-    pipe.launch_step(data, max(args.warmup, 3), sptr)
+    pipe.launch_step(data, max(warmup, 3), sptr)
     data.sync(sptr)
     clocks = ClockSampler(local)
+    st0 = data.stats()
     torch.cuda.synchronize(dev)
     clocks.start()
     time.sleep(0.3)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    pipe.launch_step(data, args.steps, sptr)
+    pipe.launch_step(data, steps, sptr)
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     ck = clocks.stop()
     data.sync(sptr)
     ms = ev0.elapsed_time(ev1)
-    value = n * args.steps / (ms / 1e3)
+    value = n * steps / (ms / 1e3)
+    launches, grid_reuse = timed_launches(data, st0, data.stats(), steps)
     prof = data.profile_substeps(args.profile_steps, sptr)
     per_substep = {k: v / args.profile_steps for k, v in prof.items()}
     dom = max(per_substep, key=per_substep.get)
@@ -864,8 +883,8 @@ def main_plain(args):
     if ab is not None:
         achieved = ab / (per_substep[dom] / 1e3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None}
-    launches = data.kernels_per_substep * args.steps
+                "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes_per_launch": ab,
+                "launch_ms": per_substep[dom], "traffic": ncu_traffic(dom, workload)}
     # e2e: upload + K substeps + positions through the public API
     buf = torch.empty(n * PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
     host = buf.numpy().view(PARTICLE_DTYPE)
@@ -876,18 +895,18 @@ def main_plain(args):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     data.upload(host, sptr)
-    pipe.launch_step(data, args.steps, sptr)
+    pipe.launch_step(data, steps, sptr)
     data.positions(out, sptr)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e = n * args.steps / (e0.elapsed_time(e1) / 1e3)
+    e2e = n * steps / (e0.elapsed_time(e1) / 1e3)
     data.close()
     cpu = None
-    if not args.no_cpu_baseline:
+    if cpu_seconds > 0:
         orc = O.from_scene(sc, threads=os.cpu_count() or 1)
         orc.step(1)
         done, t0 = 0, time.perf_counter()
-        while done < 2 or (time.perf_counter() - t0 < args.cpu_seconds and done < sc.substeps):
+        while done < 2 or (time.perf_counter() - t0 < cpu_seconds and done < sc.substeps):
             orc.step(1)
             done += 1
         el = time.perf_counter() - t0
@@ -895,13 +914,13 @@ def main_plain(args):
         cpu = {"value": n * done / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                "sample": f"full scene, {done} substeps after 1 warm-up"}
     line = {
-        "metric": f"particle-substeps/s ({args.workload})",
+        "metric": f"particle-substeps/s ({workload})",
         "value": value,
         "unit": UNIT,
         "n_gpus": 1,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": ms / args.steps,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": ms / steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -914,10 +933,16 @@ def main_plain(args):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * 192, "d2h_bytes_per_step": n * 16},
         "gpu_launches": launches,
+        "grid_reuse": grid_reuse,
         "clocks": ck,
         "kernel_ms_per_substep": per_substep,
     }
-    print(json.dumps(line))
+    return line
+
+
+def main_plain(args):
+    print(json.dumps(plain_line(args, args.workload, args.steps, args.warmup,
+                                0.0 if args.no_cpu_baseline else args.cpu_seconds)))
     return 0
 
 

@@ -325,9 +325,9 @@ int slosh_sync(slosh_ctx *ctx, void *stream);
 
 /* Number of device kernels a substep launches that runs the full grid
  * build (for launch accounting).  With grid reuse and conditional graphs a
- * substep that keeps the previous grid launches 7: the reuse decision, the
- * block scan, the permutation update, P2G, the grid update, G2P and the
- * rigid update (slosh_get_stats counts both kinds of substep). */
+ * substep that keeps the previous grid launches 6: the reuse decision, the
+ * permutation update, P2G, the grid update, G2P and the rigid update
+ * (slosh_get_stats counts both kinds of substep). */
 uint32_t slosh_kernels_per_substep(const slosh_ctx *ctx);
 
 /* Runs `n_substeps` substeps with direct launches (not the CUDA graph) and a
@@ -467,12 +467,14 @@ typedef struct slosh_scene_desc {
     slosh_params params;     /* gravity, dt (SimulationParams)             */
 } slosh_scene_desc;
 
-/* Launch shape of the batched substep (no effect on results). */
+/* Launch shape and tile parameters of the batched substep (no effect on
+ * results). */
 typedef struct slosh_tuning {
     uint32_t p2g_ctas_per_sm;  /* P2G grid = SMs x this CTAs of 4 warps (5 fit an SM) */
-    uint32_t g2p_threads;      /* G2P CTA size: 64, 128 or 256              */
+    uint32_t g2p_threads;      /* G2P CTA size (particles a CTA holds): 64, 128 or 256 */
     uint32_t g2p_ctas_per_sm;  /* G2P grid = SMs x this                     */
-    uint32_t pad;
+    uint32_t p2g_stages;       /* particles of a cell P2G stages ahead
+                                  through cp.async: 2, 3 or 4 (0: 3)        */
 } slosh_tuning;
 
 typedef struct slosh_batch_stats {
@@ -515,11 +517,12 @@ int slosh_batch_timestep_bound(slosh_batch *b, uint32_t slot, float *dt_out, voi
 int slosh_batch_sync(slosh_batch *b, void *stream);
 int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out);
 
-/* Launch-shape autotuner: times each candidate shape on `substeps` real
- * substeps of the current scenes (the simulation advances; every shape
- * gives identical results), keeps the fastest, and caches it per
- * (dim, material mix, particle-count bucket) for later batches in the
- * process.  A cached entry is reused without timing. */
+/* Autotuner: times six launch shapes (P2G CTAs per SM; G2P CTA size and
+ * CTAs per SM), then P2G's staging depth 2 and 4 with the best shape, each
+ * on `substeps` real substeps of the current scenes (the simulation
+ * advances; every candidate gives identical results), keeps the fastest,
+ * and caches it per (dim, material mix, particle-count bucket) for later
+ * batches in the process.  A cached entry is reused without timing. */
 int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream);
 int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t);
 int slosh_batch_last_error(const slosh_batch *b, char *buf, size_t len);

@@ -154,7 +154,7 @@ class SloshTuning(ctypes.Structure):
         ("p2g_ctas_per_sm", ctypes.c_uint32),
         ("g2p_threads", ctypes.c_uint32),
         ("g2p_ctas_per_sm", ctypes.c_uint32),
-        ("pad", ctypes.c_uint32),
+        ("p2g_stages", ctypes.c_uint32),
     ]
 
 

@@ -142,6 +142,7 @@ class MpmBatch:
                 "p2g_ctas_per_sm": st.tuning.p2g_ctas_per_sm,
                 "g2p_threads": st.tuning.g2p_threads,
                 "g2p_ctas_per_sm": st.tuning.g2p_ctas_per_sm,
+                "p2g_stages": st.tuning.p2g_stages,
             },
         }
 
@@ -150,8 +151,8 @@ class MpmBatch:
         _check(self._lib, self._b, self._lib.slosh_batch_autotune(self._b, int(substeps), stream))
         return self.stats()["tuning"]
 
-    def set_tuning(self, p2g_ctas_per_sm: int, g2p_threads: int, g2p_ctas_per_sm: int):
-        t = SloshTuning(p2g_ctas_per_sm, g2p_threads, g2p_ctas_per_sm, 0)
+    def set_tuning(self, p2g_ctas_per_sm: int, g2p_threads: int, g2p_ctas_per_sm: int, p2g_stages: int = 3):
+        t = SloshTuning(p2g_ctas_per_sm, g2p_threads, g2p_ctas_per_sm, p2g_stages)
         _check(self._lib, self._b, self._lib.slosh_batch_set_tuning(self._b, ctypes.byref(t)))
 
     def close(self):

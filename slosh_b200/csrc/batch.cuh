@@ -52,7 +52,7 @@ struct slosh_batch {
     slosh_particle *up = nullptr;
     uint32_t up_cap = 0, up_used = 0, staged_n = 0;
     cudaStream_t up_stream = nullptr;
-    slosh_tuning tune{5, 64, 8, 0};
+    slosh_tuning tune{5, 64, 8, 3};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
     uint32_t graph_flags = 0;       // has_damping | has_sand << 1 | all_pow2 << 2 the graphs were captured with
@@ -113,8 +113,10 @@ template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uin
     k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     k_scatter<true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
     k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
-    k_p2g<D, true><<<std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, sm * b->tune.p2g_ctas_per_sm),
-                     32 * P2G_WARPS, 0, st>>>(s);
+    const uint32_t p2g_grid = std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, sm * b->tune.p2g_ctas_per_sm);
+    if (b->tune.p2g_stages == 2) k_p2g<D, true, false, 2><<<p2g_grid, 32 * P2G_WARPS, 0, st>>>(s);
+    else if (b->tune.p2g_stages == 4) k_p2g<D, true, false, 4><<<p2g_grid, 32 * P2G_WARPS, 0, st>>>(s);
+    else k_p2g<D, true><<<p2g_grid, 32 * P2G_WARPS, 0, st>>>(s);
     k_grid_update<D, true><<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
     if (b->tune.g2p_threads == 64) launch_batch_g2p<D, 64>(b, s, st);
     else if (b->tune.g2p_threads == 256) launch_batch_g2p<D, 256>(b, s, st);
@@ -686,10 +688,11 @@ int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out) {
 int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t) {
     if (!b || !t) return SLOSH_E_INVALID;
     if ((t->g2p_threads != 64 && t->g2p_threads != 128 && t->g2p_threads != 256) || t->p2g_ctas_per_sm == 0 ||
-        t->p2g_ctas_per_sm > 64 || t->g2p_ctas_per_sm == 0 || t->g2p_ctas_per_sm > 64)
+        t->p2g_ctas_per_sm > 64 || t->g2p_ctas_per_sm == 0 || t->g2p_ctas_per_sm > 64 || t->p2g_stages == 1 ||
+        t->p2g_stages > 4)
         return fail(&b->c, SLOSH_E_INVALID, "invalid tuning");
     b->tune = *t;
-    b->tune.pad = 0;
+    if (b->tune.p2g_stages == 0) b->tune.p2g_stages = 3;
     destroy_batch_graphs(b);
     return SLOSH_OK;
 }
@@ -712,15 +715,24 @@ int batch_autotune(slosh_batch *b, uint32_t substeps, void *stream, uint32_t *ra
     }
     CK(cudaSetDevice(c->device));
     cudaStream_t st = pick(c, stream);
-    const slosh_tuning cands[] = {{5, 64, 8, 0},  {5, 128, 8, 0}, {4, 128, 4, 0},
-                                  {10, 128, 16, 0}, {5, 64, 16, 0}, {4, 64, 8, 0}};
+    // launch shapes first, then P2G's staging depth with the best shape
+    constexpr int N_SHAPES = 6;
+    slosh_tuning cands[N_SHAPES + 2] = {{5, 64, 8, 3},  {5, 128, 8, 3}, {4, 128, 4, 3},
+                                        {10, 128, 16, 3}, {5, 64, 16, 3}, {4, 64, 8, 3}};
     const uint32_t reps = std::max<uint32_t>(substeps, 1u);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
     slosh_tuning pick_t = b->tune;
-    for (const slosh_tuning &t : cands) {
+    for (int ci = 0; ci < N_SHAPES + 2; ++ci) {
+        if (ci == N_SHAPES) {
+            cands[ci] = pick_t;
+            cands[ci].p2g_stages = 2;
+            cands[ci + 1] = pick_t;
+            cands[ci + 1].p2g_stages = 4;
+        }
+        const slosh_tuning &t = cands[ci];
         b->tune = t;
         enqueue_batch_substep_any(b, st, c->parity);  // warm-up of this shape
         c->parity ^= 1u;

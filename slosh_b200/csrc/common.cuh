@@ -311,7 +311,8 @@ struct Counters {
     uint32_t reuse_done;     // CTAs of k_grid_reuse that finished (the last one decides)
     uint32_t n_rebuilds;     // substeps that ran the full grid build (cumulative)
     uint32_t n_reuses;       // substeps that kept the previous grid (cumulative)
-    uint32_t pad[3];
+    uint32_t reuse_per_cta;  // blocks each CTA of k_grid_reuse counted (a contiguous range)
+    uint32_t pad[2];
 };
 
 }  // namespace slosh

@@ -641,6 +641,7 @@ template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
 // (copy_particles_len_to_scan_value + prefix_sum +
 // copy_scan_values_to_first_particles, sort.slang:248-302).  One CTA.
 template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) {
+    if (build_skipped(s)) return;  // a kept grid's offsets come from k_grid_reuse / k_reuse_perm
     const uint32_t nb = s.ctr->n_blocks;
     cta_scan_vec16<NT>(s.bnp, s.bfirst, nb);
     // P2G's queue order, heaviest blocks first (buckets of 8 particles), so
@@ -648,7 +649,7 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
     // A substep that keeps its grid keeps the order too: the same blocks, and
     // block counts that changed by a few particles at most (the order only
     // balances P2G's load; results do not depend on it).
-    if (!s.p2g_heavy_first || build_skipped(s)) return;
+    if (!s.p2g_heavy_first) return;
     __shared__ uint32_t cnt[64];
     if (threadIdx.x < 64) cnt[threadIdx.x] = 0u;
     __syncthreads();

@@ -18,7 +18,8 @@
 //   k_grid_reuse:  per block, the new per-cell counts (old + delta), their
 //                  scan, the cells by decreasing count (touched blocks only),
 //                  the identity previous rank; decides reuse or rebuild;
-//   k_block_scan:  the block offsets, as after a full build;
+//                  the block offsets are scanned by CTA ranges here and
+//                  completed in k_reuse_perm;
 //   k_reuse_perm:  the permutation.  A cell no particle entered or left is a
 //                  shifted range of storage; a touched cell is gathered from
 //                  its own old range and the touched cells around it, and
@@ -44,20 +45,32 @@ template <int D> __device__ __forceinline__ void cell_coords(uint32_t c, int *l)
     }
 }
 
-// Warp per block of the previous substep: new per-cell counts from G2P's
-// deltas (clearing them), their in-block scan, the block total, the cells by
-// decreasing count for P2G (touched blocks; the others keep theirs, which
-// are relative to the block's first entry), the block's previous rank (the
-// collision cache: itself).  Sets the rebuild flag when a block lost its
-// last particle.  The last CTA to finish reads the decision and, inside the
-// substep graph, sets the conditional node that picks the full build or
-// the reuse.
+// CTAs of k_grid_reuse (at most): each counts a contiguous range of blocks.
+constexpr uint32_t REUSE_MAX_CTAS = 4096;
+
+// Warp per block of the previous substep, each CTA a contiguous range of
+// blocks: new per-cell counts from G2P's deltas (clearing them), their
+// in-block scan, the block total, the cells by decreasing count for P2G
+// (touched blocks; the others keep theirs, which are relative to the
+// block's first entry), the block's previous rank (the collision cache:
+// itself).  Sets the rebuild flag when a block lost its last particle.
+// The block offsets come out in two parts: each CTA scans its blocks'
+// totals into offsets relative to its range (left in bfirst) and the last
+// CTA to finish scans the CTAs' totals; k_reuse_perm adds the two.  That
+// last CTA also reads the decision and, inside the substep graph, sets the
+// conditional node that picks the full build or the reuse.
 template <int D> __global__ void k_grid_reuse(DevScene s) {
+    __shared__ uint32_t cta_total;
+    __shared__ bool last;
     const uint32_t nbp = min(s.ctr->last_n_blocks, s.cap);
-    const uint32_t lane = lane_id();
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr->n_blocks = nbp;  // a full build recounts
-    for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nbp; r += warps) {
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t per = (nbp + gridDim.x - 1) / gridDim.x;
+    const uint32_t lo = min(blockIdx.x * per, nbp), hi = min(lo + per, nbp);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        s.ctr->n_blocks = nbp;  // a full build recounts
+        s.ctr->reuse_per_cta = per;
+    }
+    for (uint32_t r = lo + warp; r < hi; r += nwarps) {
         const unsigned long long mask = s.touch[r];
         const size_t cb = (size_t)r * CELLS;
         const uint32_t q0 = s.prev_bcell[cb + 2 * lane], q1 = s.prev_bcell[cb + 2 * lane + 1];
@@ -115,20 +128,63 @@ template <int D> __global__ void k_grid_reuse(DevScene s) {
             if (lane == 0) s.touch[r] = 0ull;
         }
     }
-    // the decision, once every block is counted: each thread's rebuild flag
-    // store is made visible device-wide before its CTA counts itself done
+    __syncthreads();  // the range's block totals are written
+    if (warp == 0) {
+        // offsets of the range's blocks relative to the range, and its total
+        uint32_t carry = 0;
+        for (uint32_t b0 = lo; b0 < hi; b0 += 32) {
+            const uint32_t r = b0 + lane;
+            const uint32_t v = r < hi ? s.bnp[r] : 0u;
+            uint32_t incl = v;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
+                if (lane >= (uint32_t)off) incl += y;
+            }
+            if (r < hi) s.bfirst[r] = carry + incl - v;
+            carry += __shfl_sync(FULL_MASK, incl, 31);
+        }
+        if (lane == 0) {
+            s.reuse_cta[blockIdx.x] = carry;
+            cta_total = carry;
+        }
+    }
+    // the decision, once every block is counted: each thread's stores are
+    // made visible device-wide before its CTA counts itself done
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t t = atomicAdd(&s.ctr->reuse_done, 1u);
-        if (t == gridDim.x - 1u) {
-            __threadfence();
-            const uint32_t rb = *(volatile uint32_t *)&s.ctr->rebuild[s.par];
-            if (rb) s.ctr->n_rebuilds += 1u;
-            else s.ctr->n_reuses += 1u;
-            s.ctr->reuse_done = 0u;
-            if (s.use_cond) cudaGraphSetConditional(s.cond, rb ? 1u : 0u);
+    if (threadIdx.x == 0) last = atomicAdd(&s.ctr->reuse_done, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last CTA: exclusive scan of the CTAs' totals
+    {
+        __shared__ uint32_t wsum[32];
+        uint32_t carry = 0;
+        for (uint32_t c0 = 0; c0 < gridDim.x; c0 += blockDim.x) {
+            const uint32_t c = c0 + threadIdx.x;
+            const uint32_t v = c < gridDim.x ? *(volatile uint32_t *)&s.reuse_cta[c] : 0u;
+            uint32_t incl = v;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
+                if (lane >= (uint32_t)off) incl += y;
+            }
+            if (lane == 31) wsum[warp] = incl;
+            __syncthreads();
+            uint32_t before = carry;
+            for (uint32_t w = 0; w < warp; ++w) before += wsum[w];
+            if (c < gridDim.x) s.reuse_cta[REUSE_MAX_CTAS + c] = before + incl - v;
+            for (uint32_t w = 0; w < nwarps; ++w) carry += wsum[w];
+            __syncthreads();
         }
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t rb = *(volatile uint32_t *)&s.ctr->rebuild[s.par];
+        if (rb) s.ctr->n_rebuilds += 1u;
+        else s.ctr->n_reuses += 1u;
+        s.ctr->reuse_done = 0u;
+        if (s.use_cond) cudaGraphSetConditional(s.cond, rb ? 1u : 0u);
     }
 }
 
@@ -237,11 +293,15 @@ template <int D> __global__ void k_reuse_perm(DevScene s) {
         s.ctr->p2g_next = 0u;
         s.ctr->g2p_next = 0u;
     }
-    const uint32_t nb = s.ctr->n_blocks;
+    const uint32_t nb = s.ctr->n_blocks, per = max(s.ctr->reuse_per_cta, 1u);
     const uint32_t lane = lane_id();
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
-        const uint32_t first = s.bfirst[r], pf = s.prev_bfirst[r], np = s.bnp[r];
+        // the block's offset: k_grid_reuse's range-relative offset plus its range's base
+        const uint32_t first = s.bfirst[r] + s.reuse_cta[REUSE_MAX_CTAS + r / per];
+        const uint32_t pf = s.prev_bfirst[r], np = s.bnp[r];
+        __syncwarp();  // every lane has read the relative offset
+        if (lane == 0) s.bfirst[r] = first;
         if ((size_t)first + np > s.count) {
             if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;

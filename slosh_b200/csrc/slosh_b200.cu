@@ -58,6 +58,7 @@ struct slosh_ctx {
     uint32_t *bfirst2 = nullptr, *bnp2 = nullptr, *bcell2 = nullptr;
     int *cell_delta = nullptr;
     unsigned long long *touch = nullptr, *cur_touch = nullptr;
+    uint32_t *reuse_cta = nullptr;
     uint32_t reuse = 0;
     bool cond_graphs = false;  // the substep graphs pick the build through a conditional node
     // stage hooks (slosh's MpmPipelineHooks); while one is set, substeps are
@@ -224,6 +225,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
         s.cell_delta = c->cell_delta;
         s.touch = c->touch;
         s.cur_touch = c->cur_touch;
+        s.reuse_cta = c->reuse_cta;
         s.cond = 0;
         s.use_cond = 0u;
     }
@@ -275,8 +277,8 @@ const char *const KERNEL_NAMES[N_KERNELS] = {
     "k_rigid"};
 // Kernels a substep launches through the conditional graph: the decision,
 // the transfer kernels and the rigid update, plus the full build (9) or the
-// reuse (block scan and permutation).
-constexpr uint32_t KERNELS_FULL_BUILD = 14, KERNELS_REUSE = 7;
+// reuse's permutation (1).
+constexpr uint32_t KERNELS_FULL_BUILD = 14;
 
 // Optional per-kernel CUDA-event timing of the substep launches.
 struct Prof {
@@ -349,7 +351,8 @@ void enqueue_build_back(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
 // The decision between keeping the previous grid and a full build.
 template <int D> void enqueue_reuse_decision(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(0);
-    k_grid_reuse<D><<<grid_for((uint64_t)c->cap * 32, 256, (uint32_t)c->sm_count * 8), 256, 0, st>>>(s);
+    const uint32_t ctas = std::min<uint32_t>((uint32_t)c->sm_count * 8, REUSE_MAX_CTAS);
+    k_grid_reuse<D><<<grid_for((uint64_t)c->cap * 32, 256, ctas), 256, 0, st>>>(s);
     PROF_END(0);
 }
 
@@ -566,7 +569,6 @@ template <int D> cudaError_t capture_conditional(slosh_ctx *c, uint32_t par, cud
     enqueue_build_back(c, s, st, nullptr);
     if ((e = cudaStreamEndCapture(st, &full)) != cudaSuccess) return bail(e);
     if ((e = cudaStreamBeginCaptureToGraph(st, reuse, nullptr, nullptr, 0, mode)) != cudaSuccess) return bail(e);
-    enqueue_block_scan(c, s, st, nullptr);
     enqueue_reuse_perm<D>(c, s, st, nullptr);
     if ((e = cudaStreamEndCapture(st, &reuse)) != cudaSuccess) return bail(e);
     // the transfer kernels after either branch
@@ -779,7 +781,8 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->ctr, 1)) || (st = dalloc(c, &c->err, 1)) || (st = dalloc(c, &c->small, 4)) ||
         (st = dalloc(c, &c->staging, N)) || (st = dalloc(c, &c->bfirst2, cap)) || (st = dalloc(c, &c->bnp2, cap)) ||
         (st = dalloc(c, &c->bcell2, (size_t)cap * CELLS)) || (st = dalloc(c, &c->cell_delta, (size_t)cap * CELLS)) ||
-        (st = dalloc(c, &c->touch, cap)) || (st = dalloc(c, &c->cur_touch, cap)))
+        (st = dalloc(c, &c->touch, cap)) || (st = dalloc(c, &c->cur_touch, cap)) ||
+        (st = dalloc(c, &c->reuse_cta, 2 * (size_t)REUSE_MAX_CTAS)))
         return fail_create(st);
     cudaMemset(c->hkeys[0], 0xff, hcap * 4);
     cudaMemset(c->hkeys[1], 0xff, hcap * 4);

@@ -159,7 +159,9 @@ template <> struct SlabTile<2> {
 
 // FORCE: the substep adds the particles' pending force impulses (the first
 // substep after they were set); the other substeps compile without them.
-template <int D, bool B = false, bool FORCE = false>
+// NBUF: particles of a cell staged ahead through cp.async (batches tune it;
+// the results do not depend on it).
+template <int D, bool B = false, bool FORCE = false, int NBUF = 3>
 __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
@@ -169,7 +171,8 @@ __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
     // lanes a cell, the first and last cell possibly shared with the
     // neighbouring passes) in NBUF buffers; particle k + NBUF - 1 of every
     // cell is copied while particle k is summed.
-    constexpr int NBUF = 3, CS = 12;
+    constexpr int CS = 12;
+    static_assert(NBUF >= 2 && NBUF <= 4, "staging depth 2 to 4");
     __shared__ float4 stile[P2G_WARPS][3 * SSZ];
     __shared__ float4 sp_pm[P2G_WARPS][NBUF][CS];
     __shared__ float4 sp_vv[P2G_WARPS][NBUF][CS];

@@ -114,7 +114,7 @@ def test_mix_matches_oracle(cuda_lib):
 def test_launch_shapes_give_identical_bits(cuda_lib):
     scs = mix_scenes()
     results = []
-    for shape in [(8, 128, 8), (4, 64, 8), (16, 256, 4)]:
+    for shape in [(8, 128, 8, 3), (4, 64, 8, 2), (16, 256, 4, 4)]:
         b = new_batch()
         slots = [b.add(sc) for sc in scs]
         b.set_tuning(*shape)
