@@ -325,8 +325,9 @@ int slosh_sync(slosh_ctx *ctx, void *stream);
 
 /* Number of device kernels a substep launches that runs the full grid
  * build (for launch accounting).  With grid reuse and conditional graphs a
- * substep that keeps the previous grid launches 6: the reuse decision, the
- * permutation update, P2G, the grid update, G2P and the rigid update
+ * substep that keeps the previous grid launches 7: the reuse decision, the
+ * permutation update, the touched-cell gather, P2G, the grid update, G2P and
+ * the rigid update
  * (slosh_get_stats counts both kinds of substep). */
 uint32_t slosh_kernels_per_substep(const slosh_ctx *ctx);
 

@@ -312,7 +312,8 @@ struct Counters {
     uint32_t n_rebuilds;     // substeps that ran the full grid build (cumulative)
     uint32_t n_reuses;       // substeps that kept the previous grid (cumulative)
     uint32_t reuse_per_cta;  // blocks each CTA of k_grid_reuse counted (a contiguous range)
-    uint32_t pad[2];
+    uint32_t n_touched;      // touched cells listed by k_reuse_perm for k_reuse_cells
+    uint32_t pad;
 };
 
 }  // namespace slosh

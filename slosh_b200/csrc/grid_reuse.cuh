@@ -21,9 +21,9 @@
 //                  the block offsets are scanned by CTA ranges here and
 //                  completed in k_reuse_perm;
 //   k_reuse_perm:  the permutation.  A cell no particle entered or left is a
-//                  shifted range of storage; a touched cell is gathered from
-//                  its own old range and the touched cells around it, and
-//                  ordered by original index.
+//                  shifted range of storage; the touched cells are listed;
+//   k_reuse_cells: a warp per touched cell gathers it from its own old range
+//                  and the touched cells around it, ordered by original index.
 // The result is the layout the full build produces from the same positions,
 // bit for bit: blocks by key, cells slab-major, particles of a cell by
 // original index.
@@ -69,6 +69,7 @@ template <int D> __global__ void k_grid_reuse(DevScene s) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         s.ctr->n_blocks = nbp;  // a full build recounts
         s.ctr->reuse_per_cta = per;
+        s.ctr->n_touched = 0u;
     }
     for (uint32_t r = lo + warp; r < hi; r += nwarps) {
         const unsigned long long mask = s.touch[r];
@@ -157,26 +158,32 @@ template <int D> __global__ void k_grid_reuse(DevScene s) {
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // the last CTA: exclusive scan of the CTAs' totals
+    // the last CTA: exclusive scan of the CTAs' totals, each thread a run of
+    // consecutive CTAs (their loads independent, one round trip)
     {
         __shared__ uint32_t wsum[32];
-        uint32_t carry = 0;
-        for (uint32_t c0 = 0; c0 < gridDim.x; c0 += blockDim.x) {
-            const uint32_t c = c0 + threadIdx.x;
-            const uint32_t v = c < gridDim.x ? *(volatile uint32_t *)&s.reuse_cta[c] : 0u;
-            uint32_t incl = v;
+        constexpr uint32_t RUN = 16;  // REUSE_MAX_CTAS / 256
+        const uint32_t c0 = threadIdx.x * RUN;
+        uint32_t v[RUN], sum = 0;
 #pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
-                if (lane >= (uint32_t)off) incl += y;
-            }
-            if (lane == 31) wsum[warp] = incl;
-            __syncthreads();
-            uint32_t before = carry;
-            for (uint32_t w = 0; w < warp; ++w) before += wsum[w];
-            if (c < gridDim.x) s.reuse_cta[REUSE_MAX_CTAS + c] = before + incl - v;
-            for (uint32_t w = 0; w < nwarps; ++w) carry += wsum[w];
-            __syncthreads();
+        for (uint32_t k = 0; k < RUN; ++k) {
+            v[k] = c0 + k < gridDim.x ? *(volatile uint32_t *)&s.reuse_cta[c0 + k] : 0u;
+            sum += v[k];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL_MASK, incl, off);
+            if (lane >= (uint32_t)off) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t run = incl - sum;
+        for (uint32_t w = 0; w < warp; ++w) run += wsum[w];
+#pragma unroll
+        for (uint32_t k = 0; k < RUN; ++k) {
+            if (c0 + k < gridDim.x) s.reuse_cta[REUSE_MAX_CTAS + c0 + k] = run;
+            run += v[k];
         }
     }
     if (threadIdx.x == 0) {
@@ -321,16 +328,40 @@ template <int D> __global__ void k_reuse_perm(DevScene s) {
             const uint32_t plo = pf + s.prev_bcell[cb + c];
             for (uint32_t k = lo; k < hi; ++k) s.perm[first + k] = plo + (k - lo);
         }
+        // touched cells: listed for k_reuse_cells, which gathers them a warp each
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&s.ctr->n_touched, (uint32_t)__popcll(mask));
+        base = __shfl_sync(FULL_MASK, base, 0);
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+            const uint32_t c = 2u * lane + (uint32_t)hh;
+            if ((mask >> c) & 1ull)
+                s.touched_cells[base + (uint32_t)__popcll(mask & ((1ull << c) - 1ull))] = (r << 6) | c;
+        }
+    }
+}
+
+// The touched cells of a kept grid, one warp each (their gathers are chains
+// of dependent loads, so they run side by side rather than block by block).
+template <int D> __global__ void k_reuse_cells(DevScene s) {
+    if (s.ctr->rebuild[s.par]) return;
+    const uint32_t nt = s.ctr->n_touched;
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < nt; t += warps) {
+        const uint32_t e = s.touched_cells[t];
+        const uint32_t r = e >> 6, c = e & 63u;
+        const uint32_t first = s.bfirst[r], np = s.bnp[r];
+        const size_t cb = (size_t)r * CELLS;
+        const uint32_t lo = s.bcell[cb + c], hi = c < CELLS - 1 ? s.bcell[cb + c + 1] : np;
+        if ((size_t)first + np > s.count || hi < lo || hi > np) {
+            if (lane == 0) atomicOr(s.err, ERR_GRID_REUSE);
+            continue;
+        }
         int bv[D];
         unpack_key<D>(s.bkey[r], bv);
-        unsigned long long m = mask;
-        while (m != 0ull) {
-            const uint32_t c = (uint32_t)__ffsll((long long)m) - 1u;
-            m &= m - 1ull;
-            const uint32_t lo = s.bcell[cb + c], hi = c < CELLS - 1 ? s.bcell[cb + c + 1] : np;
-            const uint32_t got = gather_touched_cell<D>(s, r, c, bv, first + lo, hi - lo);
-            if (got != hi - lo && lane == 0) atomicOr(s.err, ERR_GRID_REUSE);
-        }
+        const uint32_t got = gather_touched_cell<D>(s, r, c, bv, first + lo, hi - lo);
+        if (got != hi - lo && lane == 0) atomicOr(s.err, ERR_GRID_REUSE);
     }
 }
 

@@ -58,7 +58,7 @@ struct slosh_ctx {
     uint32_t *bfirst2 = nullptr, *bnp2 = nullptr, *bcell2 = nullptr;
     int *cell_delta = nullptr;
     unsigned long long *touch = nullptr, *cur_touch = nullptr;
-    uint32_t *reuse_cta = nullptr;
+    uint32_t *reuse_cta = nullptr, *touched_cells = nullptr;
     uint32_t reuse = 0;
     bool cond_graphs = false;  // the substep graphs pick the build through a conditional node
     // stage hooks (slosh's MpmPipelineHooks); while one is set, substeps are
@@ -226,6 +226,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
         s.touch = c->touch;
         s.cur_touch = c->cur_touch;
         s.reuse_cta = c->reuse_cta;
+        s.touched_cells = c->touched_cells;
         s.cond = 0;
         s.use_cond = 0u;
     }
@@ -270,14 +271,14 @@ uint32_t grid_for(uint64_t work, uint32_t threads, uint32_t max_ctas) {
 }
 
 // Kernels of one substep, in launch order (profiling names).
-constexpr int N_KERNELS = 15;
+constexpr int N_KERNELS = 16;
 const char *const KERNEL_NAMES[N_KERNELS] = {
-    "k_grid_reuse", "k_touch",   "k_neighbors", "k_hist_scan", "k_bin_scatter", "k_rank",        "k_block_setup",
-    "k_block_scan", "k_reuse_perm", "k_scatter", "k_canon",     "k_p2g",         "k_grid_update", "k_g2p_update",
-    "k_rigid"};
+    "k_grid_reuse", "k_touch",      "k_neighbors",   "k_hist_scan", "k_bin_scatter", "k_rank",
+    "k_block_setup", "k_block_scan", "k_reuse_perm", "k_reuse_cells", "k_scatter",   "k_canon",
+    "k_p2g",        "k_grid_update", "k_g2p_update", "k_rigid"};
 // Kernels a substep launches through the conditional graph: the decision,
 // the transfer kernels and the rigid update, plus the full build (9) or the
-// reuse's permutation (1).
+// reuse's permutation and touched cells (2).
 constexpr uint32_t KERNELS_FULL_BUILD = 14;
 
 // Optional per-kernel CUDA-event timing of the substep launches.
@@ -330,22 +331,26 @@ void enqueue_block_scan(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
     PROF_END(7);
 }
 
-// The kept grid's permutation (returns at once when the full build runs).
+// The kept grid's permutation and its touched cells (both return at once
+// when the full build runs).
 template <int D> void enqueue_reuse_perm(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(8);
     k_reuse_perm<D><<<grid_for((uint64_t)c->cap * 32, 256, (uint32_t)c->sm_count * 8), 256, 0, st>>>(s);
     PROF_END(8);
+    PROF_BEGIN(9);
+    k_reuse_cells<D><<<(uint32_t)c->sm_count * 8, 256, 0, st>>>(s);
+    PROF_END(9);
 }
 
 // back: the permutation of the full build.
 void enqueue_build_back(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     const uint32_t sm = (uint32_t)c->sm_count;
-    PROF_BEGIN(9);
-    k_scatter<<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // longer chunks: fewer cells split for k_canon
-    PROF_END(9);
     PROF_BEGIN(10);
-    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    k_scatter<<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // longer chunks: fewer cells split for k_canon
     PROF_END(10);
+    PROF_BEGIN(11);
+    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    PROF_END(11);
 }
 
 // The decision between keeping the previous grid and a full build.
@@ -369,7 +374,7 @@ void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
 }
 
 template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
-    PROF_BEGIN(11);
+    PROF_BEGIN(12);
     if (c->p2g_variant == 3) {
         const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
         k_p2g_atomic<D><<<g, P2G_ATOMIC_THREADS, 0, st>>>(s);
@@ -378,13 +383,13 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
         if (s.force_pending) k_p2g<D, false, true><<<g, 32 * P2G_WARPS, 0, st>>>(s);
         else k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
     }
-    PROF_END(11);
+    PROF_END(12);
 }
 
 template <int D> void enqueue_grid_update(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
-    PROF_BEGIN(12);
+    PROF_BEGIN(13);
     k_grid_update<D><<<grid_for((uint64_t)c->cap * 64, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s);
-    PROF_END(12);
+    PROF_END(13);
 }
 
 // Restores the cleared state a debug build consumed, so that the next real
@@ -395,7 +400,7 @@ void enqueue_clear(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
 
 // P2G, grid update, fused G2P/update and the rigid update.
 template <int D> void enqueue_g2p(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
-    PROF_BEGIN(13);
+    PROF_BEGIN(14);
     // persistent: 8 CTAs of 64 fit an SM; each takes blocks from the queue.
     // Small CTAs wait less at the per-block barriers (tile load, the
     // slowest thread's last particle) than CTAs of 128 or 256.
@@ -410,16 +415,16 @@ template <int D> void enqueue_g2p(slosh_ctx *c, const DevScene &s, cudaStream_t 
     else if (c->model_mask == 1u << SLOSH_MODEL_FLUID_TAIT)
         k_g2p_update<D, 64, false, true, SLOSH_MODEL_FLUID_TAIT><<<g2p_grid, 64, 0, st>>>(s);
     else k_g2p_update<D, 64, false, true><<<g2p_grid, 64, 0, st>>>(s);
-    PROF_END(13);
+    PROF_END(14);
 }
 
 template <int D> void enqueue_transfer(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     enqueue_p2g<D>(c, s, st, p);
     enqueue_grid_update<D>(c, s, st, p);
     enqueue_g2p<D>(c, s, st, p);
-    PROF_BEGIN(14);
+    PROF_BEGIN(15);
     k_rigid<D><<<1, 32, 0, st>>>(s);
-    PROF_END(14);
+    PROF_END(15);
 }
 
 template <int D>
@@ -782,7 +787,8 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->staging, N)) || (st = dalloc(c, &c->bfirst2, cap)) || (st = dalloc(c, &c->bnp2, cap)) ||
         (st = dalloc(c, &c->bcell2, (size_t)cap * CELLS)) || (st = dalloc(c, &c->cell_delta, (size_t)cap * CELLS)) ||
         (st = dalloc(c, &c->touch, cap)) || (st = dalloc(c, &c->cur_touch, cap)) ||
-        (st = dalloc(c, &c->reuse_cta, 2 * (size_t)REUSE_MAX_CTAS)))
+        (st = dalloc(c, &c->reuse_cta, 2 * (size_t)REUSE_MAX_CTAS)) ||
+        (st = dalloc(c, &c->touched_cells, (size_t)cap * CELLS)))
         return fail_create(st);
     cudaMemset(c->hkeys[0], 0xff, hcap * 4);
     cudaMemset(c->hkeys[1], 0xff, hcap * 4);

@@ -9,7 +9,10 @@
 //   1. symmetric eigen-decomposition of A = F^T F by cyclic Jacobi rotations
 //      (exact rotation angles here, where the paper uses approximate ones),
 //   2. eigenvalues sorted in decreasing order, V kept a proper rotation,
-//   3. Givens QR of B = F V, so that F = U R V^T with U a proper rotation.
+//   3. Givens QR of B = F V, so that F = U R V^T with U a proper rotation
+//      (FP32 with a converged Jacobi, singular values within a factor 2 and
+//      F not inverted: the columns of B normalised instead, which the
+//      converged Jacobi leaves orthogonal to its residual).
 // The singular values are the diagonal of R: s0 >= s1 >= |s2|, the sign of
 // det F carried by s2.  The QR step keeps the factorisation backward stable
 // when singular values coincide or vanish.
@@ -132,13 +135,18 @@ template <typename T> __device__ void svd3_impl(const T (&F)[3][3], Svd3<T> &out
             a[j][i] = acc;
         }
     T V[3][3] = {{T(1), T(0), T(0)}, {T(0), T(1), T(0)}, {T(0), T(0), T(1)}};
+    bool converged = false;
+    T off = T(0);
     for (int sweep = 0; sweep < SvdT<T>::SWEEPS; ++sweep) {
         jacobi_rotate<T, 0, 1>(a, V);
         jacobi_rotate<T, 0, 2>(a, V);
         jacobi_rotate<T, 1, 2>(a, V);
-        const T off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
+        off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
         const T dia = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
-        if (!(off > dia * SvdT<T>::EPS)) break;
+        if (!(off > dia * SvdT<T>::EPS)) {
+            converged = true;
+            break;
+        }
     }
     T l0 = a[0][0], l1 = a[1][1], l2 = a[2][2];
     if (l0 < l1) swap_cols<T>(V, l0, l1, 0, 1);
@@ -150,6 +158,34 @@ template <typename T> __device__ void svd3_impl(const T (&F)[3][3], Svd3<T> &out
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) B[i][j] = F[i][0] * V[0][j] + F[i][1] * V[1][j] + F[i][2] * V[2][j];
+    if constexpr (sizeof(T) == 4) {
+        // FP32, the common case: a converged Jacobi leaves the columns of
+        // B = F V orthogonal up to its residual (B^T B = V^T F^T F V), so U is
+        // B with normalised columns.  That orthogonality error is at most
+        // the residual over s_i s_j, so this path is taken only when the
+        // singular values stay within a factor 2 of each other and F is not
+        // inverted (det B = det F); the Givens QR below keeps the other cases
+        // backward stable.
+        T n2[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) n2[j] = B[0][j] * B[0][j] + B[1][j] * B[1][j] + B[2][j] * B[2][j];
+        const T detb = B[0][0] * (B[1][1] * B[2][2] - B[1][2] * B[2][1]) - B[0][1] * (B[1][0] * B[2][2] - B[1][2] * B[2][0]) +
+                       B[0][2] * (B[1][0] * B[2][1] - B[1][1] * B[2][0]);
+        if (converged && n2[2] > T(0.25) * n2[0] && detb > T(0)) {
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const T inv = rsqrtf(n2[j]);
+                out.s[j] = n2[j] * inv;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    out.U[i][j] = B[i][j] * inv;
+                    out.V[i][j] = V[i][j];
+                }
+            }
+            out.offdiag = off * rsqrtf(n2[0]);  // the residual, in units of s0 like R's off-diagonal
+            return;
+        }
+    }
     // QR by Givens: rows (0,1) col 0, rows (0,2) col 0, rows (1,2) col 1.
     T U[3][3] = {{T(1), T(0), T(0)}, {T(0), T(1), T(0)}, {T(0), T(0), T(1)}};
     T c, s;
