@@ -244,8 +244,11 @@ int slosh_add_trimesh(slosh_ctx *ctx, const float *vertices, uint32_t n_vertices
  * blocks, ranks and hash map when no particle left the set of blocks that
  * hold particles, and only re-counts the cells particles entered or left;
  * the decision is taken on the device.  The layout is the one a full build
- * gives, bit for bit.  The environment variable SLOSH_GRID_REUSE=0 at
- * context creation makes every substep run the full build. */
+ * gives, bit for bit.  Scenes of at least 262,144 particles keep their grid
+ * this way; smaller ones are launch-bound, and the full build inside the
+ * substep graph is faster for them.  The environment variable
+ * SLOSH_GRID_REUSE at context creation overrides that: 0 makes every
+ * substep run the full build, 1 keeps grids at any size. */
 int slosh_step(slosh_ctx *ctx, uint32_t n_substeps, void *stream);
 
 /* ---- stage hooks ------------------------------------------------------------

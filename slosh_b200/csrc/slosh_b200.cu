@@ -60,6 +60,7 @@ struct slosh_ctx {
     unsigned long long *touch = nullptr, *cur_touch = nullptr;
     uint32_t *reuse_cta = nullptr, *touched_cells = nullptr;
     uint32_t reuse = 0;
+    uint32_t reuse_mode = 2;  // SLOSH_GRID_REUSE: 0 off, 1 on, 2 (unset) on from REUSE_MIN_PARTICLES
     bool cond_graphs = false;  // the substep graphs pick the build through a conditional node
     // stage hooks (slosh's MpmPipelineHooks); while one is set, substeps are
     // launched kernel by kernel with the hooks called between the stages
@@ -445,11 +446,30 @@ void enqueue_substep_any(slosh_ctx *c, cudaStream_t st, uint32_t parity, bool fo
 // previous substep's grid no longer describes storage.  G2P's pending
 // per-cell bookkeeping is dropped with it.
 int force_grid_rebuild(slosh_ctx *c, cudaStream_t st) {
-    if (!c->reuse) return SLOSH_OK;
+    if (!c->cell_delta) return SLOSH_OK;  // batches keep no bookkeeping
     CK(cudaMemsetAsync(c->cell_delta, 0, (size_t)c->cap * CELLS * sizeof(int), st));
     CK(cudaMemsetAsync(c->touch, 0, (size_t)c->cap * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(c->ctr->rebuild, 1, sizeof(c->ctr->rebuild), st));  // nonzero: rebuild
     return SLOSH_OK;
+}
+
+// Grid reuse pays once the grid build's kernels outweigh the reuse's own
+// launches: scenes below this many particles are launch-bound, and their
+// full build inside the substep graph is faster (measured: the 62,628-
+// particle dam break at 0.054 ms a substep with the full build, 0.061 with
+// reuse; the 524,288-particle elastic drop 0.152 and 0.147).
+constexpr uint32_t REUSE_MIN_PARTICLES = 262144;
+
+void destroy_graphs(slosh_ctx *c);
+
+// Sets whether substeps keep their grid, from the mode and the particle
+// count; the graphs are rebuilt when that changes.
+void update_reuse(slosh_ctx *c) {
+    const uint32_t want = c->reuse_mode == 1 || (c->reuse_mode == 2 && c->n >= REUSE_MIN_PARTICLES) ? 1u : 0u;
+    if (want != c->reuse) {
+        c->reuse = want;
+        destroy_graphs(c);
+    }
 }
 
 // One substep with the stage hooks called between its kernels, in the
@@ -801,8 +821,9 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     if (const char *variant = std::getenv("SLOSH_P2G")) {
         if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;
     }
-    c->reuse = 1u;
-    if (const char *r = std::getenv("SLOSH_GRID_REUSE")) c->reuse = std::strcmp(r, "0") == 0 ? 0u : 1u;
+    c->reuse_mode = 2u;
+    if (const char *r = std::getenv("SLOSH_GRID_REUSE")) c->reuse_mode = std::strcmp(r, "0") == 0 ? 0u : 1u;
+    update_reuse(c);
     cudaMemset(c->bcell, 0, (size_t)cap * CELLS * 4);
     cudaMemset(c->bcell2, 0, (size_t)cap * CELLS * 4);
     cudaMemset(c->bnp, 0, (size_t)cap * 4);
@@ -839,6 +860,7 @@ int slosh_upload_particles(slosh_ctx *c, const slosh_particle *particles, uint32
                    old_models = c->model_mask;
     if (n != c->n) destroy_graphs(c);
     c->n = n;
+    update_reuse(c);
     CK(cudaMemcpyAsync(c->staging, particles, (size_t)n * sizeof(slosh_particle), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(c->mat_hkeys, 0xff, MAT_HASH * 4, st));
     CK(cudaMemsetAsync(c->small, 0, 16, st));
@@ -920,6 +942,7 @@ int slosh_append_particles(slosh_ctx *c, const slosh_particle *particles, uint32
     CK(cudaMemcpyAsync(small, c->small, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     c->n = base + n;
+    update_reuse(c);
     c->n_materials = small[0];
     c->has_damping = (small[1] & SCENE_DAMPING) ? 1u : 0u;
     c->has_sand = (small[1] & SCENE_SAND) ? 1u : 0u;
@@ -953,6 +976,7 @@ int slosh_remove_particles(slosh_ctx *c, uint32_t start, uint32_t count, uint32_
     // B now holds the survivors in insertion order: make it the current storage
     std::swap(c->pb[c->parity & 1u], c->pb[(c->parity & 1u) ^ 1u]);
     c->n = left;
+    update_reuse(c);
     const DevScene s2 = make_scene(c, c->parity, false);
     if (left) {
         const uint32_t g2 = grid_for(left, 256, (uint32_t)c->sm_count * 16);

@@ -89,7 +89,8 @@ class Recorder(MpmPipelineHooks):
         self.calls.append("after_particles_update")
 
 
-def test_noop_hooks_called_in_order_and_bit_identical(cuda_lib):
+def test_noop_hooks_called_in_order_and_bit_identical(cuda_lib, monkeypatch):
+    monkeypatch.setenv("SLOSH_GRID_REUSE", "1")
     sc = scene()
     ref = plain(sc, 12)
     data = scenes.build_mpm_data(sc)
@@ -138,7 +139,8 @@ def test_after_p2g_sees_and_changes_the_nodes(cuda_lib):
     assert vy.max() <= 1e-9 and vy.min() >= -g_dt * (1 + 1e-5)
 
 
-def test_run_hooks_wrapping_the_builtin_are_bit_identical(cuda_lib):
+def test_run_hooks_wrapping_the_builtin_are_bit_identical(cuda_lib, monkeypatch):
+    monkeypatch.setenv("SLOSH_GRID_REUSE", "1")  # a replaced G2P must turn grid reuse off for a substep
     sc = scene()
     ref = plain(sc, 10)
 
@@ -161,7 +163,8 @@ def test_run_hooks_wrapping_the_builtin_are_bit_identical(cuda_lib):
     assert st["n_grid_reuses"] == 0
 
 
-def test_failing_hook_drops_its_substep(cuda_lib):
+def test_failing_hook_drops_its_substep(cuda_lib, monkeypatch):
+    monkeypatch.setenv("SLOSH_GRID_REUSE", "1")  # the dropped substep also resets the kept grid
     sc = scene()
     ref = plain(sc, 8)
 
