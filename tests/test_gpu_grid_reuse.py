@@ -106,3 +106,19 @@ def test_reuse_full_size_sand_column(cuda_lib, monkeypatch):
     print(f"4.74M: reuse {st['n_grid_reuses']} of 40, rebuilds {st['n_grid_rebuilds']}")
     assert st["n_grid_reuses"] > 0
     assert kept.tobytes() == full.tobytes()
+
+
+def test_reuse_with_forces_damping_fixed(cuda_lib, monkeypatch):
+    """Pending forces (a substep launched kernel by kernel), damping and
+    fixed particles under grid reuse: the same bits as full builds."""
+    sc = scenes.elastic_drop_3d(h=1 / 48)
+    parts = sc.particles.copy()
+    parts["force_dt"][::3] = (0.0, 2e-3, -1e-3)
+    parts["damping"][::5] = 3.0
+    parts["fixed"][::11] = 1
+    sc.particles = parts
+    full, _ = run(sc, [30], monkeypatch, reuse=False)
+    kept, st = run(sc, [30], monkeypatch, reuse=True)
+    print(f"forces/damping/fixed: reuse {st['n_grid_reuses']} of 30")
+    assert st["n_grid_reuses"] > 0
+    assert kept.tobytes() == full.tobytes()
