@@ -82,6 +82,21 @@ def main_ncu_case(args):
     from slosh_b200 import scenes
     from slosh_b200.pipeline import MpmPipeline
 
+    if args.workload == "batched":
+        from slosh_b200.batch import MpmBatch
+
+        scs = batched_scenes(args.scenes)
+        total = int(sum(sc.n for sc in scs))
+        b = MpmBatch(3, max_particles=total + 1024, grid_capacity=int(sum(max(64, 2.5 * sc.n / 512.0) for sc in scs)),
+                     max_scenes=max(args.scenes, 1), max_bodies=4 * args.scenes + 16)
+        for sc in scs:
+            b.add(sc)
+        b.set_tuning(5, 64, 8, 3)  # the shape the autotuner picks for this workload
+        b.step(args.steps)
+        b.sync()
+        print(json.dumps({"ncu_case": "batched", "scenes": len(scs), "particles": total, **b.stats()}))
+        b.close()
+        return 0
     if args.workload == "dam_break_2d":
         sc = scenes.dam_break_2d()
     elif args.workload == "elastic_drop_3d":

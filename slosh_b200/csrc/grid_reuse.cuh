@@ -286,9 +286,11 @@ __device__ uint32_t gather_touched_cell(const DevScene &s, uint32_t r, uint32_t 
     return found;
 }
 
-// The reused grid's primary permutation (warp per block), once
-// k_block_scan has placed the blocks; the previous map becomes this
-// substep's; the transfer kernels' block queues restart.
+// The reused grid's primary permutation (warp per block): each block's
+// offset completed from k_grid_reuse's two partial scans, its untouched
+// cells written as shifted ranges and its touched cells listed for
+// k_reuse_cells; the previous map becomes this substep's; the transfer
+// kernels' block queues restart.
 template <int D> __global__ void k_reuse_perm(DevScene s) {
     if (s.ctr->rebuild[s.par]) return;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;

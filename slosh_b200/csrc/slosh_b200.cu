@@ -650,6 +650,8 @@ int check_device_error(slosh_ctx *c) {
         return fail(c, SLOSH_E_OVERFLOW, "a block holds 2^26 particles or more (error bits 0x%x)", e);
     if (e & ERR_KEY_RANGE)
         return fail(c, SLOSH_E_OVERFLOW, "a particle left the packed block-key range (error bits 0x%x)", e);
+    if (e & ERR_GRID_REUSE)
+        return fail(c, SLOSH_E_STATE, "a kept grid's cell counts and gathered cells disagree (error bits 0x%x)", e);
     if (e & (ERR_MATERIALS | ERR_MATERIAL_HASH))
         return fail(c, SLOSH_E_MATERIAL, "material table error (bits 0x%x; max %u materials)", e, MAX_MATERIALS);
     return fail(c, SLOSH_E_CUDA, "device error bits 0x%x", e);
