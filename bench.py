@@ -511,6 +511,8 @@ def main_ours(args):
             for wl, k in (("dam_break_2d", 1000), ("elastic_drop_3d", 2000)):  # their whole runs
                 line[wl] = {key: v for key, v in plain_line(args, wl, k, args.warmup, 5.0).items() if key not in drop}
             line["batched"] = {k: v for k, v in batched_line(args, args.batched_substeps, args.warmup).items() if k not in drop}
+            # configuration 3's precision study: 500 substeps against the FP64 oracle
+            line["precision"] = precision_line(args, 500, 1.0 / 64.0)
             line["served"] = {k: v for k, v in served_line(args).items() if k not in drop}
         print(json.dumps(line))
     if pg is not None:
@@ -965,10 +967,10 @@ def main_plain(args):
     return 0
 
 
-def main_precision(args):
+def precision_line(args, steps: int, h: float) -> dict:
     """Precision study of the sand column: the FP32 GPU substep and the FP32
-    oracle against the FP64 oracle after K substeps, on the column at
-    dx = 1/64 (the FP64 oracle cannot run the 4.74 M-particle column for 500
+    oracle against the FP64 oracle after `steps` substeps, on the column at
+    dx = h (the FP64 oracle cannot run the 4.74 M-particle column for 500
     substeps in minutes; the material, geometry, bodies and dt are those of
     the full configuration)."""
     import numpy as np
@@ -980,9 +982,9 @@ def main_precision(args):
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    sc = scenes.sand_column_3d(h=args.h if args.h > 1.0 / 100 else 1.0 / 64, substeps=args.steps)
+    sc = scenes.sand_column_3d(h=h, substeps=steps)
     data = scenes.build_mpm_data(sc, device=local)
-    MpmPipeline().launch_step(data, args.steps)
+    MpmPipeline().launch_step(data, steps)
     g = data.download_particles()
     fp64_fallbacks = data.stats()["n_svd_fp64"]
     data.close()
@@ -990,8 +992,8 @@ def main_precision(args):
     o32 = O.from_scene(sc, threads=threads)
     o64 = O.from_scene(sc, double=True, threads=threads)
     t0 = time.perf_counter()
-    o32.step(args.steps)
-    o64.step(args.steps)
+    o32.step(steps)
+    o64.step(steps)
     cpu_s = time.perf_counter() - t0
     r32, r64 = o32.get_particles(), o64.get_particles()
     o32.close()
@@ -1015,9 +1017,9 @@ def main_precision(args):
         }
     line = {
         "metric": "error vs FP64 oracle (sand column)",
-        "workload": f"sand_column_3d at dx={sc.cell_width:.6g}: {sc.n} particles, {args.steps} substeps, dt=2e-5",
+        "workload": f"sand_column_3d at dx={sc.cell_width:.6g}: {sc.n} particles, {steps} substeps, dt=2e-5",
         "particles": sc.n,
-        "substeps": args.steps,
+        "substeps": steps,
         "cell_width": sc.cell_width,
         "errors": res,
         "position_max_err_in_cells": res["gpu_fp32"]["position"]["max"] / sc.cell_width,
@@ -1025,7 +1027,11 @@ def main_precision(args):
         "oracle_cpu_seconds": cpu_s,
         "oracle_threads": threads,
     }
-    print(json.dumps(line))
+    return line
+
+
+def main_precision(args):
+    print(json.dumps(precision_line(args, args.steps, args.h if args.h > 1.0 / 100 else 1.0 / 64)))
     return 0
 
 
