@@ -539,8 +539,9 @@ def batched_scenes(count: int, seed: int = 4):
 
 
 def batched_line(args, steps: int, warmup: int) -> dict:
-    """Config: 256 independent 3D scenes advanced by one batch (one graph
-    launch of 14 kernels per substep over all scenes) against the plain loop
+    """Config: 256 independent 3D scenes advanced by one batch (per substep
+    one graph launch of 14 kernels over all scenes, or one persistent
+    cooperative kernel, whichever the autotuner picks) against the plain loop
     of per-scene contexts (one graph launch of 13 kernels per scene and
     substep), same scenes, same substeps, same stream."""
     import numpy as np
@@ -585,6 +586,25 @@ def batched_line(args, steps: int, warmup: int) -> dict:
     ms = e0.elapsed_time(e1)
     value = total * steps / (ms / 1e3)
     st = b.stats()
+
+    # both substep forms on the same scenes: the 14-kernel graph (the shape
+    # the autotuner picks for it) and the one persistent cooperative kernel
+    forms = {}
+    n_form = min(steps, 200)
+    for name, shape in (("graph_14_kernels", (5, 64, 8, 3, 0)), ("fused_cooperative", (5, 64, 8, 3, 1))):
+        b.set_tuning(*shape)
+        b.step(3, sptr)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        b.step(n_form, sptr)
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        fms = f0.elapsed_time(f1) / n_form
+        forms[name] = {"ms_per_step": fms, "value": total / (fms / 1e3), "substeps": n_form}
+    b.set_tuning(tuning["p2g_ctas_per_sm"], tuning["g2p_threads"], tuning["g2p_ctas_per_sm"], tuning["p2g_stages"],
+                 tuning["fused"])
+    b.sync(sptr)
 
     # end to end through the public API: every scene uploaded from host
     # records in pinned memory, K substeps, every scene's positions read back
@@ -649,7 +669,8 @@ def batched_line(args, steps: int, warmup: int) -> dict:
         "data": "synthetic (seeded box blobs; no dataset)",
         "config": {
             "workload": f"batched: {len(scs)} independent 3D scenes, particles log-uniform [4k, 256k] "
-            f"(total {total}), materials {mats}, dx 1/64 or 1/128, Separate floor each; one batch graph per substep",
+            f"(total {total}), materials {mats}, dx 1/64 or 1/128, Separate floor each; one batch launch per substep "
+            f"({'fused cooperative kernel' if tuning['fused'] else 'graph of 14 kernels'}, autotuned)",
             "scenes": len(scs),
             "particles": total,
             "tuning": tuning,
@@ -662,6 +683,7 @@ def batched_line(args, steps: int, warmup: int) -> dict:
             "desc": "one single-scene context per scene, each substep a graph launch per scene",
         },
         "speedup_vs_plain": value / plain,
+        "substep_forms": forms,
         "e2e": {
             "value": total * steps / e2e_s,
             "unit": UNIT,
@@ -670,7 +692,7 @@ def batched_line(args, steps: int, warmup: int) -> dict:
             "api": "slosh_batch_add_scene x scenes + slosh_batch_step + slosh_batch_download_positions x scenes "
             "(host buffers, wall clock)",
         },
-        "gpu_launches": 14 * steps,
+        "gpu_launches": (1 if tuning["fused"] else 14) * steps,
         "clocks": ck,
     }
     return line

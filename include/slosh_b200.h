@@ -38,6 +38,7 @@ extern "C" {
 #define SLOSH_E_NOMEM (-5)     /* device allocation failed                */
 #define SLOSH_E_STATE (-6)     /* call out of order (e.g. no particles)   */
 #define SLOSH_E_MATERIAL (-7)  /* too many distinct materials             */
+#define SLOSH_E_TIMEOUT (-8)   /* a bounded device-side wait gave up      */
 
 /* ---- particle models: GpuParticleModel discriminants ------------------- */
 /* src/solver/particle_model.rs:89-98; shaders/slosh/models/default.slang:73-80 */
@@ -479,6 +480,11 @@ typedef struct slosh_tuning {
     uint32_t g2p_ctas_per_sm;  /* G2P grid = SMs x this                     */
     uint32_t p2g_stages;       /* particles of a cell P2G stages ahead
                                   through cp.async: 2, 3 or 4 (0: 3)        */
+    uint32_t fused;            /* 1: the whole substep as one persistent
+                                  cooperative kernel (CTAs of 128 threads,
+                                  all resident, grid barriers between the
+                                  phases; the fields above are then unused);
+                                  0: 14 kernels in one CUDA graph            */
 } slosh_tuning;
 
 typedef struct slosh_batch_stats {
@@ -505,7 +511,11 @@ int slosh_batch_add_scene(slosh_batch *b, const slosh_scene_desc *desc, const sl
 /* Drops a scene (its results should have been downloaded). */
 int slosh_batch_remove_scene(slosh_batch *b, uint32_t slot);
 
-/* Advances every live scene by n_substeps (graph launches on `stream`). */
+/* Advances every live scene by n_substeps (graph launches on `stream`; with
+ * the fused tuning one cooperative kernel a substep, captured in the graph
+ * where the runtime supports it).  SLOSH_E_TIMEOUT (at the next sync) when
+ * a grid barrier of the fused kernel gave up waiting; the batch's state is
+ * then undefined. */
 int slosh_batch_step(slosh_batch *b, uint32_t n_substeps, void *stream);
 
 /* Particles / positions (x, y, z, 0) of one scene, in its upload order. */
@@ -522,11 +532,12 @@ int slosh_batch_sync(slosh_batch *b, void *stream);
 int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out);
 
 /* Autotuner: times six launch shapes (P2G CTAs per SM; G2P CTA size and
- * CTAs per SM), then P2G's staging depth 2 and 4 with the best shape, each
- * on `substeps` real substeps of the current scenes (the simulation
- * advances; every candidate gives identical results), keeps the fastest,
- * and caches it per (dim, material mix, particle-count bucket) for later
- * batches in the process.  A cached entry is reused without timing. */
+ * CTAs per SM), then P2G's staging depth 2 and 4 with the best shape, then
+ * the fused persistent kernel, each on `substeps` real substeps of the
+ * current scenes (the simulation advances; every candidate gives identical
+ * results), keeps the fastest, and caches it per (dim, material mix,
+ * particle-count bucket) for later batches in the process.  A cached entry
+ * is reused without timing. */
 int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream);
 int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t);
 int slosh_batch_last_error(const slosh_batch *b, char *buf, size_t len);

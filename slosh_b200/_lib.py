@@ -23,6 +23,7 @@ SLOSH_E_CAPACITY = -4
 SLOSH_E_NOMEM = -5
 SLOSH_E_STATE = -6
 SLOSH_E_MATERIAL = -7
+SLOSH_E_TIMEOUT = -8
 
 STATUS_NAMES = {
     SLOSH_E_INVALID: "SLOSH_E_INVALID",
@@ -32,6 +33,7 @@ STATUS_NAMES = {
     SLOSH_E_NOMEM: "SLOSH_E_NOMEM",
     SLOSH_E_STATE: "SLOSH_E_STATE",
     SLOSH_E_MATERIAL: "SLOSH_E_MATERIAL",
+    SLOSH_E_TIMEOUT: "SLOSH_E_TIMEOUT",
 }
 
 # Particle model tags (GpuParticleModel discriminants + the Tait fluid).
@@ -155,6 +157,7 @@ class SloshTuning(ctypes.Structure):
         ("g2p_threads", ctypes.c_uint32),
         ("g2p_ctas_per_sm", ctypes.c_uint32),
         ("p2g_stages", ctypes.c_uint32),
+        ("fused", ctypes.c_uint32),
     ]
 
 

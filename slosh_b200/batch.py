@@ -143,6 +143,7 @@ class MpmBatch:
                 "g2p_threads": st.tuning.g2p_threads,
                 "g2p_ctas_per_sm": st.tuning.g2p_ctas_per_sm,
                 "p2g_stages": st.tuning.p2g_stages,
+                "fused": st.tuning.fused,
             },
         }
 
@@ -151,8 +152,12 @@ class MpmBatch:
         _check(self._lib, self._b, self._lib.slosh_batch_autotune(self._b, int(substeps), stream))
         return self.stats()["tuning"]
 
-    def set_tuning(self, p2g_ctas_per_sm: int, g2p_threads: int, g2p_ctas_per_sm: int, p2g_stages: int = 3):
-        t = SloshTuning(p2g_ctas_per_sm, g2p_threads, g2p_ctas_per_sm, p2g_stages)
+    def set_tuning(self, p2g_ctas_per_sm: int, g2p_threads: int, g2p_ctas_per_sm: int, p2g_stages: int = 3,
+                   fused: int = 0):
+        """Launch shape of the batched substep; ``fused=1`` runs each substep
+        as one persistent cooperative kernel (the shape fields are then
+        unused).  Results do not depend on the choice."""
+        t = SloshTuning(p2g_ctas_per_sm, g2p_threads, g2p_ctas_per_sm, p2g_stages, fused)
         _check(self._lib, self._b, self._lib.slosh_batch_set_tuning(self._b, ctypes.byref(t)))
 
     def close(self):

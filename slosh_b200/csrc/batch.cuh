@@ -52,7 +52,9 @@ struct slosh_batch {
     slosh_particle *up = nullptr;
     uint32_t up_cap = 0, up_used = 0, staged_n = 0;
     cudaStream_t up_stream = nullptr;
-    slosh_tuning tune{5, 64, 8, 3};
+    slosh_tuning tune{5, 64, 8, 3, 0};
+    uint32_t fused_ctas[2] = {0, 0};  // CTAs of the fused kernel (all resident), by POW2 variant
+    bool fused_direct = false;        // the fused kernel is launched directly (its graph capture failed)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
     uint32_t graph_flags = 0;       // has_damping | has_sand << 1 | all_pow2 << 2 the graphs were captured with
@@ -95,10 +97,53 @@ template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s
     else k_g2p_update<D, NT, true, false><<<g, NT, 0, st>>>(s);
 }
 
-// One batched substep: 14 kernels over all scenes.
+// CTAs of the fused substep: every CTA an SM holds (the cooperative launch
+// requires them all resident).  0 when the kernel fits no SM.
+template <int D, bool POW2> uint32_t fused_grid(slosh_batch *b) {
+    uint32_t &ctas = b->fused_ctas[POW2 ? 1 : 0];
+    if (ctas == 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_fused<D, POW2>, FUSED_THREADS,
+                                                          fused_smem_bytes<D>()) != cudaSuccess)
+            per_sm = 0;
+        ctas = (uint32_t)std::max(per_sm, 0) * (uint32_t)b->c.sm_count;
+    }
+    return ctas;
+}
+
+// The fused substep: one cooperative launch of k_batch_fused.
+template <int D, bool POW2> cudaError_t launch_batch_fused(slosh_batch *b, const DevScene &s, cudaStream_t st) {
+    const uint32_t ctas = fused_grid<D, POW2>(b);
+    if (ctas == 0) return cudaErrorCooperativeLaunchTooLarge;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(FUSED_THREADS);
+    cfg.dynamicSmemBytes = fused_smem_bytes<D>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_batch_fused<D, POW2>, s);
+}
+
+bool fused_fits(slosh_batch *b) {
+    int coop = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->c.device) != cudaSuccess || !coop) return false;
+    return b->c.dim == 3 ? fused_grid<3, true>(b) && fused_grid<3, false>(b)
+                         : fused_grid<2, true>(b) && fused_grid<2, false>(b);
+}
+
+// One batched substep: 14 kernels over all scenes, or the fused kernel.
 template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uint32_t parity) {
     slosh_ctx *c = &b->c;
     const DevScene s = make_batch_scene(b, parity);
+    if (b->tune.fused) {
+        if (b->all_pow2) launch_batch_fused<D, true>(b, s, st);
+        else launch_batch_fused<D, false>(b, s, st);
+        return;
+    }
     const uint32_t sm = (uint32_t)c->sm_count;
     k_touch<D, true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
     k_neighbors<D, true><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
@@ -145,10 +190,20 @@ int build_batch_graphs(slosh_batch *b) {
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         enqueue_batch_substep_any(b, c->stream, par);
         cudaGraph_t g = nullptr;
-        CK(cudaStreamEndCapture(c->stream, &g));
-        cudaError_t e = cudaGraphInstantiate(&b->graph[par], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (e == cudaSuccess) {
+            e = cudaGraphInstantiate(&b->graph[par], g, 0);
+            cudaGraphDestroy(g);
+        }
+        if (e != cudaSuccess && b->tune.fused) {
+            // the runtime does not capture the cooperative launch: launch
+            // the fused kernel directly, one launch a substep
+            cudaGetLastError();
+            destroy_batch_graphs(b);
+            b->fused_direct = true;
+            return SLOSH_OK;
+        }
+        if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
     }
     b->graphs_valid = true;
     b->graph_flags = c->has_damping | (c->has_sand << 1) | (b->all_pow2 << 2);
@@ -159,6 +214,12 @@ int batch_check_error(slosh_batch *b) {
     slosh_ctx *c = &b->c;
     uint32_t e = 0;
     CK(cudaMemcpy(&e, c->err, 4, cudaMemcpyDeviceToHost));
+    if (e & ERR_BARRIER) {
+        // the barrier words are left mid-count: restart them for the next launch
+        CK(cudaMemset(&c->ctr->bar_count, 0, 2 * sizeof(uint32_t)));
+        CK(cudaMemset(c->err, 0, 4));
+        return fail(c, SLOSH_E_TIMEOUT, "a grid barrier of the fused batch substep gave up waiting (error bits 0x%x)", e);
+    }
     if (e & ERR_SCENE_BLOCKS) {
         CK(cudaMemset(c->err, 0, 4));
         return fail(c, SLOSH_E_CAPACITY, "a scene exceeds %u active blocks (error bits 0x%x)", SCENE_SORT_MAX, e);
@@ -561,13 +622,26 @@ int slosh_batch_step(slosh_batch *b, uint32_t n_substeps, void *stream) {
     cudaStream_t st = pick(c, stream);
     for (uint32_t k = 0; k < n_substeps; ++k) {
         if (b->n_storage == 0) break;
-        if (!b->graphs_valid) {
+        if (!b->graphs_valid && !(b->tune.fused && b->fused_direct)) {
             CK(cudaStreamSynchronize(st));
             int r = build_batch_graphs(b);
             if (r) return r;
             CK(cudaStreamSynchronize(c->stream));
         }
-        CK(cudaGraphLaunch(b->graph[c->parity], st));
+        if (!(b->tune.fused && b->fused_direct)) {
+            const cudaError_t e = cudaGraphLaunch(b->graph[c->parity], st);
+            if (e != cudaSuccess && b->tune.fused) {
+                cudaGetLastError();  // the graph with the cooperative node does not launch: go direct
+                destroy_batch_graphs(b);
+                b->fused_direct = true;
+            } else {
+                CK(e);
+            }
+        }
+        if (b->tune.fused && b->fused_direct) {
+            enqueue_batch_substep_any(b, st, c->parity);
+            CK(cudaGetLastError());
+        }
         c->parity ^= 1u;
         if (!b->dropped.empty()) {  // their particles left storage in this substep
             for (uint32_t s : b->dropped) {
@@ -689,8 +763,10 @@ int slosh_batch_set_tuning(slosh_batch *b, const slosh_tuning *t) {
     if (!b || !t) return SLOSH_E_INVALID;
     if ((t->g2p_threads != 64 && t->g2p_threads != 128 && t->g2p_threads != 256) || t->p2g_ctas_per_sm == 0 ||
         t->p2g_ctas_per_sm > 64 || t->g2p_ctas_per_sm == 0 || t->g2p_ctas_per_sm > 64 || t->p2g_stages == 1 ||
-        t->p2g_stages > 4)
+        t->p2g_stages > 4 || t->fused > 1)
         return fail(&b->c, SLOSH_E_INVALID, "invalid tuning");
+    if (t->fused && !fused_fits(b))
+        return fail(&b->c, SLOSH_E_INVALID, "the fused substep needs cooperative launch on this device");
     b->tune = *t;
     if (b->tune.p2g_stages == 0) b->tune.p2g_stages = 3;
     destroy_batch_graphs(b);
@@ -717,20 +793,26 @@ int batch_autotune(slosh_batch *b, uint32_t substeps, void *stream, uint32_t *ra
     cudaStream_t st = pick(c, stream);
     // launch shapes first, then P2G's staging depth with the best shape
     constexpr int N_SHAPES = 6;
-    slosh_tuning cands[N_SHAPES + 2] = {{5, 64, 8, 3},  {5, 128, 8, 3}, {4, 128, 4, 3},
-                                        {10, 128, 16, 3}, {5, 64, 16, 3}, {4, 64, 8, 3}};
+    slosh_tuning cands[N_SHAPES + 3] = {{5, 64, 8, 3, 0},  {5, 128, 8, 3, 0}, {4, 128, 4, 3, 0},
+                                        {10, 128, 16, 3, 0}, {5, 64, 16, 3, 0}, {4, 64, 8, 3, 0}};
+    const bool fused_ok = fused_fits(b);
     const uint32_t reps = std::max<uint32_t>(substeps, 1u);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
     slosh_tuning pick_t = b->tune;
-    for (int ci = 0; ci < N_SHAPES + 2; ++ci) {
+    for (int ci = 0; ci < N_SHAPES + 3; ++ci) {
         if (ci == N_SHAPES) {
             cands[ci] = pick_t;
             cands[ci].p2g_stages = 2;
             cands[ci + 1] = pick_t;
             cands[ci + 1].p2g_stages = 4;
+        }
+        if (ci == N_SHAPES + 2) {
+            if (!fused_ok) break;
+            cands[ci] = pick_t;
+            cands[ci].fused = 1;
         }
         const slosh_tuning &t = cands[ci];
         b->tune = t;

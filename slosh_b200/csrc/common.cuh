@@ -29,6 +29,7 @@ constexpr uint32_t ERR_KEY_RANGE = 1u << 4;        // a block coordinate outside
 constexpr uint32_t ERR_BLOCK_PARTICLES = 1u << 6;  // a block holds 2^26 particles or more
 constexpr uint32_t ERR_SCENE_BLOCKS = 1u << 5;     // a batch scene has more blocks than the per-scene sort holds
 constexpr uint32_t ERR_GRID_REUSE = 1u << 7;       // a kept grid's cell counts and its gathered cells disagree
+constexpr uint32_t ERR_BARRIER = 1u << 8;          // a grid barrier of the fused batch substep gave up waiting
 
 // Sparse grid geometry per dimension (shaders/slosh/grid/grid.slang:224-257).
 template <int D> struct Geo;
@@ -313,7 +314,16 @@ struct Counters {
     uint32_t n_reuses;       // substeps that kept the previous grid (cumulative)
     uint32_t reuse_per_cta;  // blocks each CTA of k_grid_reuse counted (a contiguous range)
     uint32_t n_touched;      // touched cells listed by k_reuse_perm for k_reuse_cells
-    uint32_t pad;
+    uint32_t bar_count;      // fused batch substep: CTAs arrived at the current grid barrier
+    uint32_t bar_gen;        // fused batch substep: grid barriers completed (wraps)
+    uint32_t pad[2];
 };
+
+// The CTA index and CTA count a kernel body runs with: its own launch's
+// (blockIdx.x, gridDim.x), or the whole grid of the fused batch substep.
+struct Cta {
+    uint32_t id, n;
+};
+__device__ __forceinline__ Cta launch_cta() { return Cta{blockIdx.x, gridDim.x}; }
 
 }  // namespace slosh

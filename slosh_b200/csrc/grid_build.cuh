@@ -158,7 +158,7 @@ template <bool B = false> __global__ void k_clear(DevScene s) {
 // Multi-scene batches (B): the particle's scene comes from its flags, its
 // cell width from the scene table, and particles of a dropped scene get no
 // block (they leave storage at this substep).
-template <int D, bool B = false> __global__ void k_touch(DevScene s) {
+template <int D, bool B = false> __device__ __forceinline__ void touch_body(const DevScene &s, Cta g) {
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     // Each warp takes a contiguous chunk of storage.  Storage is in the
     // previous substep's canonical order (block by block), so successive
@@ -166,8 +166,8 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
     // remembers its last (key -> slot) and skips the hash CAS round trip.
     const uint32_t lane = lane_id();
     const uint32_t n = n_particles<B>(s);
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t warps = g.n * (blockDim.x >> 5);
+    const uint32_t wid = g.id * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const uint32_t chunk = (((n + warps - 1) / warps) + 31u) & ~31u;
     const uint32_t begin = wid * chunk;
     const uint32_t end = min(n, begin + chunk);
@@ -230,18 +230,19 @@ template <int D, bool B = false> __global__ void k_touch(DevScene s) {
         s.pslot[i] = bin;
     }
 }
+template <int D, bool B = false> __global__ void k_touch(DevScene s) { touch_body<D, B>(s, launch_cta()); }
 
 // Activates the +1 neighbours of every primary block, one thread per
 // (block, neighbour).  Replaces touch_neighbor_blocks (sort.slang:75-92).
 // Single scene: also counts the primary and the new blocks in the coarse
 // histogram (key >> 26), aggregated over the warp (a compact scene has one
 // or two coarse bins, so per-block atomics would all hit one address).
-template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
+template <int D, bool B = false> __device__ __forceinline__ void neighbors_body(const DevScene &s, Cta g) {
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t np = min(s.ctr->n_primary, s.cap);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < np * NN; t += stride) {
+    const uint32_t stride = g.n * blockDim.x;
+    for (uint32_t t = g.id * blockDim.x + threadIdx.x; t < np * NN; t += stride) {
         const uint32_t j = t / NN;
         const int sidx = (int)(t % NN) + 1;
         int b[D], o[D];
@@ -276,6 +277,7 @@ template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
         }
     }
 }
+template <int D, bool B = false> __global__ void k_neighbors(DevScene s) { neighbors_body<D, B>(s, launch_cta()); }
 
 // Block-wide exclusive scan of one value per thread (blockDim.x == NT,
 // NT <= 1024, a multiple of 32).  Writes the block total to *total.
@@ -478,7 +480,7 @@ __global__ void k_rank(DevScene s) {
 // so each scene gets the block order (and hence the particle storage order)
 // it would have alone.  Per-scene block counts were taken when the blocks
 // were inserted; one CTA scans them into per-scene rank bases.
-template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s) {
+template <int NT> __device__ __forceinline__ void scene_scan_body(const DevScene &s) {
     const uint32_t total = cta_scan_vec16<NT>(s.scene_nblk, s.scene_bbase, s.n_scenes);
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < s.n_scenes; q += NT) s.scene_fill[q] = s.scene_bbase[q];
@@ -487,12 +489,13 @@ template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s)
         s.ctr->n_blocks = min(total, s.cap);
     }
 }
+template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s) { scene_scan_body<NT>(s); }
 
 // Groups the appended blocks by scene (unordered within a scene).
-__global__ void k_scene_scatter(DevScene s) {
+__device__ __forceinline__ void scene_scatter_body(const DevScene &s, Cta g) {
     const uint32_t n1 = min(s.ctr->n_primary, s.cap), n2 = min(s.ctr->n_extra, s.cap);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n1 + n2; t += stride) {
+    const uint32_t stride = g.n * blockDim.x;
+    for (uint32_t t = g.id * blockDim.x + threadIdx.x; t < n1 + n2; t += stride) {
         const uint32_t key = t < n1 ? s.blist_key[t] : s.blist2_key[t - n1];
         const uint32_t slot = t < n1 ? s.blist_slot[t] : s.blist2_slot[t - n1];
         const uint32_t sc = (uint32_t)(s.hkeys64[slot] >> 32);
@@ -503,6 +506,7 @@ __global__ void k_scene_scatter(DevScene s) {
         }
     }
 }
+__global__ void k_scene_scatter(DevScene s) { scene_scatter_body(s, launch_cta()); }
 
 // Bitonic sort of P (a power of two) 64-bit values in shared memory.
 template <int NT> __device__ __forceinline__ void bitonic_sort_smem(unsigned long long *a, uint32_t P) {
@@ -559,23 +563,57 @@ template <int NT, uint32_t PMIN, uint32_t PMAX> __global__ void __launch_bounds_
     }
 }
 
+// Ranks of the fused batch substep: the blocks of each scene (grouped by
+// k_scene_scatter) ranked by counting the scene's smaller keys, RANK_LANES
+// lanes a block.  Keys are distinct inside a scene, so these are the ranks
+// k_scene_sort's bitonic sort gives, written to the same arrays; scenes
+// beyond SCENE_SORT_MAX blocks raise ERR_SCENE_BLOCKS as they do there.
+__device__ __forceinline__ void scene_rank_body(const DevScene &s, Cta g) {
+    const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
+    const uint32_t gl = threadIdx.x % RANK_LANES;
+    const unsigned gmask = ((1u << RANK_LANES) - 1u) << (lane_id() & ~(RANK_LANES - 1u));
+    const uint32_t stride = g.n * (blockDim.x / RANK_LANES);
+    for (uint32_t t = g.id * (blockDim.x / RANK_LANES) + threadIdx.x / RANK_LANES; t < total; t += stride) {
+        const uint32_t key = s.tmp_key[t], ts = s.tmp_slot[t], slot = ts & ~RANK_EXTRA;
+        const uint32_t sc = (uint32_t)(s.hkeys64[slot] >> 32);
+        const uint32_t m = s.scene_nblk[sc], base = s.scene_bbase[sc];
+        if (m > SCENE_SORT_MAX) {
+            if (gl == 0) atomicOr(s.err, ERR_SCENE_BLOCKS);
+            continue;
+        }
+        if (base + m > 2u * s.cap) continue;  // overflow, already flagged
+        uint32_t part = 0;
+#pragma unroll 4
+        for (uint32_t j = base + gl; j < base + m; j += RANK_LANES) part += (s.tmp_key[j] < key) ? 1u : 0u;
+#pragma unroll
+        for (uint32_t off = RANK_LANES / 2; off > 0; off >>= 1) part += __shfl_xor_sync(gmask, part, off);
+        const uint32_t r = base + part;
+        if (gl == 0 && r < s.cap) {
+            s.bkey[r] = key;
+            s.bslot[r] = slot;
+            s.bscene[r] = sc;
+            s.hvals[slot] = r | (ts & RANK_EXTRA);
+        }
+    }
+}
+
 // One warp per block: per-cell counts (cleared in the hash-slot array once
 // read) with their in-block exclusive scan, the block total, the cells in
 // decreasing count order for P2G's thread assignment, the +1 and -1
 // neighbour ranks (update_nbh_block_ids, sort.slang:100-117), the block's
 // rank in the previous substep's map (the grid update's collision cache) and, for the
 // atomic P2G variants, zeroed nodes (reset, grid.slang:455-485).
-template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
+template <int D, bool B = false> __device__ __forceinline__ void block_setup_body(const DevScene &s, Cta g) {
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     constexpr int NN = Geo<D>::NASSOC - 1;
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t lane = lane_id();
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {  // the transfer kernels' block queues, read after this kernel
+    const uint32_t warps = g.n * (blockDim.x >> 5);
+    if (g.id == 0 && threadIdx.x == 0) {  // the transfer kernels' block queues, read after this kernel
         s.ctr->p2g_next = 0u;
         s.ctr->g2p_next = 0u;
     }
-    for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
+    for (uint32_t r = g.id * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
         const uint32_t sl = s.bslot[r];
         uint32_t *cnt = s.slot_counts + ((size_t)sl << 6);
         const uint32_t c0 = cnt[2 * lane], c1 = cnt[2 * lane + 1];
@@ -636,11 +674,12 @@ template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
         }
     }
 }
+template <int D, bool B = false> __global__ void k_block_setup(DevScene s) { block_setup_body<D, B>(s, launch_cta()); }
 
 // Exclusive scan of the per-block primary totals into first_particle
 // (copy_particles_len_to_scan_value + prefix_sum +
 // copy_scan_values_to_first_particles, sort.slang:248-302).  One CTA.
-template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) {
+template <int NT> __device__ __forceinline__ void block_scan_body(const DevScene &s) {
     if (build_skipped(s)) return;  // a kept grid's offsets come from k_grid_reuse / k_reuse_perm
     const uint32_t nb = s.ctr->n_blocks;
     cta_scan_vec16<NT>(s.bnp, s.bfirst, nb);
@@ -666,6 +705,7 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < nb; r += NT) s.qorder[atomicAdd(&cnt[min(s.bnp[r] >> 3, 63u)], 1u)] = r;
 }
+template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) { block_scan_body<NT>(s); }
 
 // Per particle: claim its slot in the block's cell range (the primary part
 // of finalize_particles_sort, sort.slang:304-357), warp-aggregated.
@@ -677,12 +717,12 @@ template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s)
 // between two chunks (and cells entered from another cell) need k_canon's
 // fix-up.  Like k_touch, a warp remembers the block of its last lane (hash
 // slot -> rank, first entry), so most iterations go straight to the claim.
-template <bool B = false> __global__ void k_scatter(DevScene s) {
+template <bool B = false> __device__ __forceinline__ void scatter_body(const DevScene &s, Cta g) {
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t lane = lane_id();
     const uint32_t n = n_particles<B>(s);
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t warps = g.n * (blockDim.x >> 5);
+    const uint32_t wid = g.id * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const uint32_t chunk = (((n + warps - 1) / warps) + 31u) & ~31u;
     const uint32_t begin = wid * chunk;
     const uint32_t end = min(n, begin + chunk);
@@ -729,6 +769,7 @@ template <bool B = false> __global__ void k_scatter(DevScene s) {
         }
     }
 }
+template <bool B = false> __global__ void k_scatter(DevScene s) { scatter_body<B>(s, launch_cta()); }
 
 // Canonical order inside each (block, cell) range of the permutation:
 // ascending original id.  k_scatter stores beside every permutation entry
@@ -756,12 +797,12 @@ __device__ __forceinline__ void sort_cell_keys(unsigned long long *key, uint32_t
     }
 }
 
-__global__ void k_canon(DevScene s) {
+__device__ __forceinline__ void canon_body(const DevScene &s, Cta g) {
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t lane = lane_id();
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
+    const uint32_t warps = g.n * (blockDim.x >> 5);
+    for (uint32_t r = g.id * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
         const uint32_t first = s.bfirst[r], np = s.bnp[r];
         if (np < 2) continue;
         if ((size_t)first + np > s.n) {  // only after an earlier overflow left stale counts
@@ -806,5 +847,6 @@ __global__ void k_canon(DevScene s) {
         }
     }
 }
+__global__ void k_canon(DevScene s) { canon_body(s, launch_cta()); }
 
 }  // namespace slosh

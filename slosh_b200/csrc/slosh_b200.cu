@@ -19,6 +19,7 @@
 #include "io.cuh"
 #include "transfer.cuh"
 #include "timestep.cuh"
+#include "fused.cuh"
 
 using namespace slosh;
 

@@ -161,22 +161,31 @@ template <> struct SlabTile<2> {
 // substep after they were set); the other substeps compile without them.
 // NBUF: particles of a cell staged ahead through cp.async (batches tune it;
 // the results do not depend on it).
+// Shared memory of k_p2g's CTA (P2G_WARPS warps): each warp's three slab
+// tiles and its staged particles.  Staging: the particles of a pass's cells
+// (at most CS = 12: 32 lanes, 3 slab lanes a cell, the first and last cell
+// possibly shared with the neighbouring passes) in NBUF buffers; particle
+// k + NBUF - 1 of every cell is copied while particle k is summed.
+template <int D, int NBUF> struct P2gSmem {
+    static constexpr int CS = 12;
+    float4 stile[P2G_WARPS][3 * SlabTile<D>::SIZE];
+    float4 sp_pm[P2G_WARPS][NBUF][CS];
+    float4 sp_vv[P2G_WARPS][NBUF][CS];
+    float4 sp_cq[P2G_WARPS][NBUF][MQ<D>::Q][CS];
+};
+
 template <int D, bool B = false, bool FORCE = false, int NBUF = 3>
-__global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
+__device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
     constexpr int PY = SlabTile<D>::PY, PZ = SlabTile<D>::PZ, SSZ = SlabTile<D>::SIZE;
     constexpr int Q = MQ<D>::Q;
-    // Staging: the particles of a pass's cells (at most 12: 32 lanes, 3 slab
-    // lanes a cell, the first and last cell possibly shared with the
-    // neighbouring passes) in NBUF buffers; particle k + NBUF - 1 of every
-    // cell is copied while particle k is summed.
-    constexpr int CS = 12;
+    constexpr int CS = P2gSmem<D, NBUF>::CS;
     static_assert(NBUF >= 2 && NBUF <= 4, "staging depth 2 to 4");
-    __shared__ float4 stile[P2G_WARPS][3 * SSZ];
-    __shared__ float4 sp_pm[P2G_WARPS][NBUF][CS];
-    __shared__ float4 sp_vv[P2G_WARPS][NBUF][CS];
-    __shared__ float4 sp_cq[P2G_WARPS][NBUF][Q][CS];
+    auto &stile = sm.stile;
+    auto &sp_pm = sm.sp_pm;
+    auto &sp_vv = sm.sp_vv;
+    auto &sp_cq = sm.sp_cq;
     const uint32_t nb = s.ctr->n_blocks;
     const size_t n = s.n;
     const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
@@ -371,6 +380,11 @@ __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
         for (int t = (int)lane; t < TILE; t += 32) s.partial[(size_t)r * TILE + t] = tile_node(t, wl, wl + 1);
         __syncwarp();
     }
+}
+template <int D, bool B = false, bool FORCE = false, int NBUF = 3>
+__global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
+    __shared__ P2gSmem<D, NBUF> sm;
+    p2g_body<D, B, FORCE, NBUF>(s, sm);
 }
 
 // Particle-to-grid with float atomics, kept for comparison (SLOSH_P2G=direct):
@@ -804,14 +818,14 @@ __device__ __forceinline__ void project_velocity(uint32_t type, float friction, 
 // otherwise collide() runs; both are recorded for the next substep.
 // 4 CTAs of 256 per SM: the register cap (64) leaves the rare collision
 // queries (nodes without a cached collision) to spill, not the whole kernel.
-template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_grid_update(DevScene s) {
+template <int D, bool B = false> __device__ __forceinline__ void grid_update_body(const DevScene &s, Cta g) {
     constexpr int BW = Geo<D>::BW;
     const uint32_t nb = s.ctr->n_blocks;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t stride = g.n * blockDim.x;
     float h = s.h, dt = s.dt, grav[3] = {s.gravity[0], s.gravity[1], s.gravity[2]};
     const DevBody *bodies = s.bodies;
     uint32_t n_bodies = s.n_bodies, sc = 0;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * 64u; t += stride) {
+    for (uint32_t t = g.id * blockDim.x + threadIdx.x; t < nb * 64u; t += stride) {
         const uint32_t r = t >> 6, node = t & 63u;
         if constexpr (B) {
             sc = s.bscene[r];
@@ -952,6 +966,9 @@ template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_gri
         s.nodes[t] = make_float4(vel[0], vel[1], D == 3 ? vel[D - 1] : 0.f, mass);
     }
 }
+template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_grid_update(DevScene s) {
+    grid_update_body<D, B>(s, launch_cta());
+}
 
 // Clears the next substep's hash map and the key histogram / per-scene
 // block counts (their readers in this substep have all run), thread g0 of
@@ -1050,15 +1067,27 @@ __device__ __forceinline__ void note_cell_change(const DevScene &s, uint32_t r, 
 // exactly x * (1/h) and no division is compiled in.  MODEL >= 0: every
 // particle of the scene uses that model tag (known at upload), so only its
 // constitutive code is compiled in; MODEL < 0 reads each particle's tag.
+// Shared memory of k_g2p_update's CTA (NT threads): the block's node tile
+// (velocity, mass: one 16-byte load a node) and two buffers of staged
+// particles, one particle a thread.
+template <int D, int NT> struct G2pSmem {
+    float4 tv[Geo<D>::TILE];
+    float4 st_pm[2][NT];
+    float4 st_fq[2][MQ<D>::Q][NT];
+    uint4 st_fo[2][NT];
+    float4 st_ps[2][NT];
+    uint32_t next_r;
+};
+
 template <int D, int NT, bool B = false, bool POW2 = false, int MODEL = -1>
-__global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
+__device__ __forceinline__ void g2p_update_body(const DevScene &s, Cta g, G2pSmem<D, NT> &sm) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
-    __shared__ float4 tv[TILE];  // node (velocity, mass): one 16-byte load per node
     constexpr int Q = MQ<D>::Q;
-    __shared__ float4 st_pm[2][NT];
-    __shared__ float4 st_fq[2][Q][NT];
-    __shared__ uint4 st_fo[2][NT];
-    __shared__ float4 st_ps[2][NT];
+    auto &tv = sm.tv;
+    auto &st_pm = sm.st_pm;
+    auto &st_fq = sm.st_fq;
+    auto &st_fo = sm.st_fo;
+    auto &st_ps = sm.st_ps;
     const uint32_t nb = s.ctr->n_blocks;
     float h = s.h, dt = s.dt, inv_h = s.inv_h;
     uint32_t h_pow2 = s.h_pow2;
@@ -1066,7 +1095,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
     float vmax = h / dt;
     const size_t n = s.n;
     const uint32_t tid = threadIdx.x;
-    if (s.clear_tail) clear_next_map<B>(s, blockIdx.x * NT + tid, gridDim.x * NT);
+    if (s.clear_tail) clear_next_map<B>(s, g.id * NT + tid, g.n * NT);
     // Issues the copies of sorted entry e (storage index i) of the block into
     // buffer b (an empty group when e is past the block's particles).  The
     // storage index is loaded one iteration before the copies that need it.
@@ -1081,7 +1110,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
         cp_async_commit();
     };
     // blocks are taken from a queue, one atomic a block
-    __shared__ uint32_t next_r;
+    uint32_t &next_r = sm.next_r;
     for (;;) {
         __syncthreads();  // every thread has read next_r
         if (tid == 0) next_r = atomicAdd(&s.ctr->g2p_next, 1u);
@@ -1366,6 +1395,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
         __syncthreads();
     }
 }
+template <int D, int NT, bool B = false, bool POW2 = false, int MODEL = -1>
+__global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
+    __shared__ G2pSmem<D, NT> sm;
+    g2p_update_body<D, NT, B, POW2, MODEL>(s, launch_cta(), sm);
+}
 
 // Rigid-body update (shaders/slosh/solver/rigid_impulses.slang:72-121) with
 // integrate_velocity (shaders/slosh/rbd/dynamics/body.slang:117-130).  The
@@ -1376,8 +1410,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
 // Multi-scene batches (B): bodies of all scenes in one table, each with its
 // scene's dt and gravity (bodies of dropped scenes are left alone), and the
 // particle count in storage becomes this substep's sorted count.
-template <int D, bool B = false> __global__ void k_rigid(DevScene s) {
-    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+template <int D, bool B = false> __device__ __forceinline__ void rigid_body(const DevScene &s, uint32_t id) {
     if (id == 0 && s.clear_tail) {
         const uint32_t nb = s.ctr->n_blocks;
         s.ctr->last_n_blocks = nb;
@@ -1473,5 +1506,6 @@ template <int D, bool B = false> __global__ void k_rigid(DevScene s) {
     for (int k = 0; k < D; ++k) b.linvel[k] = b.linvel[k] + grav[k] * ((b.inv_mass[k] != 0.f) ? 1.f : 0.f) * dt;
     s.bodies[id] = b;
 }
+template <int D, bool B = false> __global__ void k_rigid(DevScene s) { rigid_body<D, B>(s, blockIdx.x * blockDim.x + threadIdx.x); }
 
 }  // namespace slosh

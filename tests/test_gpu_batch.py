@@ -5,7 +5,9 @@
   scenes join and leave (continuous batching);
 - every scene of a mix matches the oracle within the FP32 tolerance of the
   single-scene parity tests;
-- every launch shape the autotuner tries gives identical bits;
+- every launch shape the autotuner tries gives identical bits, the fused
+  persistent substep (one cooperative kernel) included, in 3D and 2D and
+  while scenes join and leave;
 - capacity, state and unsupported-input errors are reported, not faulted.
 """
 import numpy as np
@@ -114,14 +116,14 @@ def test_mix_matches_oracle(cuda_lib):
 def test_launch_shapes_give_identical_bits(cuda_lib):
     scs = mix_scenes()
     results = []
-    for shape in [(8, 128, 8, 3), (4, 64, 8, 2), (16, 256, 4, 4)]:
+    for shape in [(8, 128, 8, 3), (4, 64, 8, 2), (16, 256, 4, 4), (5, 64, 8, 3, 1)]:
         b = new_batch()
         slots = [b.add(sc) for sc in scs]
         b.set_tuning(*shape)
         b.step(8)
         results.append([b.download_particles(s).tobytes() for s in slots])
         b.close()
-    assert results[0] == results[1] == results[2]
+    assert results[0] == results[1] == results[2] == results[3]
     b = new_batch()
     for sc in scs:
         b.add(sc)
@@ -130,6 +132,37 @@ def test_launch_shapes_give_identical_bits(cuda_lib):
     b.step(2)
     b.sync()
     b.close()
+
+
+def run_mix(dim, scs, fused, steps=(6, 6, 6)):
+    """Scenes 0-1 from the start, scene 1 leaving and scene 2 joining after
+    steps[0] substeps, scene 3 joining after steps[1] more; all results."""
+    b = MpmBatch(dim, max_particles=1 << 17, grid_capacity=1 << 13, max_scenes=16, max_bodies=64)
+    b.set_tuning(5, 64, 8, 3, fused)
+    s0, s1 = b.add(scs[0]), b.add(scs[1])
+    b.step(steps[0])
+    gone = b.download_particles(s1).tobytes()
+    b.remove_scene(s1)
+    s2 = b.add(scs[2])
+    b.step(steps[1])
+    s3 = b.add(scs[3])
+    b.step(steps[2])
+    assert b.stats()["tuning"]["fused"] == fused
+    out = [gone] + [b.download_particles(s).tobytes() for s in (s0, s2, s3)]
+    b.sync()
+    b.close()
+    return out
+
+
+def test_fused_substep_bit_identical_to_graph(cuda_lib):
+    """The persistent cooperative substep gives the 14-kernel graph's bits,
+    3D (sand, elastic, fluid; two cell widths) and 2D, with scenes joining
+    and leaving between substeps."""
+    scs3 = mix_scenes()
+    assert run_mix(3, scs3, 1) == run_mix(3, scs3, 0)
+    scs2 = [scenes.dam_break_2d(h=1 / 64, substeps=10), scenes.dam_break_2d(h=1 / 128, substeps=10),
+            scenes.dam_break_2d(h=1 / 64, substeps=10), scenes.dam_break_2d(h=1 / 128, substeps=10)]
+    assert run_mix(2, scs2, 1) == run_mix(2, scs2, 0)
 
 
 def test_batch_errors_reported(cuda_lib):
