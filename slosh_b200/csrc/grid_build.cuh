@@ -634,6 +634,7 @@ template <int D, bool B = false> __device__ __forceinline__ void block_setup_bod
         if (lane == 31) {
             s.bnp[r] = incl;
             if (incl >= (1u << 26)) atomicOr(s.err, ERR_BLOCK_PARTICLES);  // beyond the 26-bit first in bord
+            if (s.bsrc) s.bsrc[r] = NONE;  // a full build's permutation is no shifted range
         }
         {
             // rank of each cell among the 64 by (count desc, cell asc): the

@@ -310,12 +310,17 @@ template <int D> __global__ void k_reuse_perm(DevScene s) {
         const uint32_t first = s.bfirst[r] + s.reuse_cta[REUSE_MAX_CTAS + r / per];
         const uint32_t pf = s.prev_bfirst[r], np = s.bnp[r];
         __syncwarp();  // every lane has read the relative offset
-        if (lane == 0) s.bfirst[r] = first;
+        const unsigned long long mask = s.cur_touch[r];
+        // the transfer kernels index an untouched block's particles from
+        // its storage start instead of loading the permutation
+        if (lane == 0) {
+            s.bfirst[r] = first;
+            s.bsrc[r] = (mask == 0ull && (size_t)pf + np <= s.count) ? pf : NONE;
+        }
         if ((size_t)first + np > s.count) {
             if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
         }
-        const unsigned long long mask = s.cur_touch[r];
         if (mask == 0ull) {  // the block's particles are a shifted range
             for (uint32_t e = lane; e < np; e += 32) s.perm[first + e] = pf + e;
             continue;

@@ -108,6 +108,8 @@ struct DevScene {
     unsigned long long *cur_touch;  // per block: the touched cells this substep's reuse applies
     uint32_t *reuse_cta;       // [2 * REUSE_MAX_CTAS]: k_grid_reuse's per-CTA particle totals, then their scan
     uint32_t *touched_cells;   // [cap * 64]: (block << 6 | cell) of the cells a kept grid re-gathers
+    uint32_t *bsrc;            // per block: storage index of its first particle when its particles are
+                               // one shifted range of storage (a kept grid's untouched block), else NONE
     cudaGraphConditionalHandle cond;  // inside the substep graph: full build (1) or reuse (0)
     uint32_t use_cond;
 

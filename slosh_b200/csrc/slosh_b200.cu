@@ -60,6 +60,7 @@ struct slosh_ctx {
     int *cell_delta = nullptr;
     unsigned long long *touch = nullptr, *cur_touch = nullptr;
     uint32_t *reuse_cta = nullptr, *touched_cells = nullptr;
+    uint32_t *bsrc = nullptr;  // per block: storage start of a shifted-range block, else NONE
     uint32_t reuse = 0;
     uint32_t reuse_mode = 2;  // SLOSH_GRID_REUSE: 0 off, 1 on, 2 (unset) on from REUSE_MIN_PARTICLES
     bool cond_graphs = false;  // the substep graphs pick the build through a conditional node
@@ -229,6 +230,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
         s.cur_touch = c->cur_touch;
         s.reuse_cta = c->reuse_cta;
         s.touched_cells = c->touched_cells;
+        s.bsrc = c->bsrc;
         s.cond = 0;
         s.use_cond = 0u;
     }
@@ -811,7 +813,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         (st = dalloc(c, &c->bcell2, (size_t)cap * CELLS)) || (st = dalloc(c, &c->cell_delta, (size_t)cap * CELLS)) ||
         (st = dalloc(c, &c->touch, cap)) || (st = dalloc(c, &c->cur_touch, cap)) ||
         (st = dalloc(c, &c->reuse_cta, 2 * (size_t)REUSE_MAX_CTAS)) ||
-        (st = dalloc(c, &c->touched_cells, (size_t)cap * CELLS)))
+        (st = dalloc(c, &c->touched_cells, (size_t)cap * CELLS)) || (st = dalloc(c, &c->bsrc, cap)))
         return fail_create(st);
     cudaMemset(c->hkeys[0], 0xff, hcap * 4);
     cudaMemset(c->hkeys[1], 0xff, hcap * 4);

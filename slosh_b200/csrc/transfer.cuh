@@ -186,6 +186,11 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
     auto &sp_pm = sm.sp_pm;
     auto &sp_vv = sm.sp_vv;
     auto &sp_cq = sm.sp_cq;
+    // storage index of the current block's first particle when its
+    // particles are one shifted range of storage, else NONE (the
+    // permutation is read)
+    uint32_t src = NONE;
+    const bool use_src = !B && s.reuse && s.bsrc != nullptr;
     const uint32_t nb = s.ctr->n_blocks;
     const size_t n = s.n;
     const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
@@ -236,7 +241,9 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
             }
             cp_async_commit();
         };
-        auto index = [&](uint32_t k) { return (loader && k < cnt) ? s.perm[first + lo + k] : 0u; };
+        auto index = [&](uint32_t k) {
+            return (loader && k < cnt) ? (src != NONE ? src + lo + k : s.perm[first + lo + k]) : 0u;
+        };
 #pragma unroll
         for (uint32_t k = 0; k + 1 < (uint32_t)NBUF; ++k) stage(k, index(k));
         uint32_t i_next = index(NBUF - 1u);  // loaded one iteration before its copies
@@ -249,7 +256,7 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
                 const int b = (int)(k % NBUF);
                 float fdt[3] = {0.f, 0.f, 0.f};
                 if constexpr (FORCE) {
-                    const uint32_t i = s.perm[first + lo + k];
+                    const uint32_t i = src != NONE ? src + lo + k : s.perm[first + lo + k];
 #pragma unroll
                     for (int d = 0; d < D; ++d) fdt[d] = s.fdt[d * n + i];
                 }
@@ -342,6 +349,7 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
             float h = s.h, inv_h = 1.0f / s.h;
             int bv[D];
             block_setup(r, h, inv_h, bv);
+            src = use_src ? s.bsrc[r] : NONE;
             for (uint32_t pass = wl; pass < 6u; pass += P2G_WARPS) {
                 uint2 ord = s.bord[(size_t)r * CELLS + (32u * pass + lane) / 3u];
                 if (!run_pass(r, first, bv, h, inv_h, pass, ord, false)) break;
@@ -353,16 +361,15 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
         return;
     }
     // One warp a block.  Blocks are taken from a queue (one atomic a
-    // block), so warps that get light blocks take more of them.
-    auto next_block = [&]() {
-        uint32_t r = 0;
-        if (lane == 0) {
-            const uint32_t q = atomicAdd(&s.ctr->p2g_next, 1u);
-            r = q < nb ? (s.p2g_heavy_first ? s.qorder[q] : q) : nb;
-        }
-        return __shfl_sync(FULL_MASK, r, 0);
-    };
-    for (uint32_t r = next_block(); r < nb; r = next_block()) {
+    // block), so warps that get light blocks take more of them.  The next
+    // entry is claimed when a block starts, so the atomic's round trip
+    // overlaps the block's work.
+    auto resolve = [&](uint32_t q) { return q < nb ? (s.p2g_heavy_first ? s.qorder[q] : q) : nb; };
+    uint32_t q = 0;
+    if (lane == 0) q = atomicAdd(&s.ctr->p2g_next, 1u);
+    for (uint32_t r = __shfl_sync(FULL_MASK, lane == 0 ? resolve(q) : 0u, 0); r < nb;
+         r = __shfl_sync(FULL_MASK, lane == 0 ? resolve(q) : 0u, 0)) {
+        if (lane == 0) q = atomicAdd(&s.ctr->p2g_next, 1u);
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
@@ -373,6 +380,7 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
         float h = s.h, inv_h = 1.0f / s.h;
         int bv[D];
         block_setup(r, h, inv_h, bv);
+        src = use_src ? s.bsrc[r] : NONE;
         uint2 ord = s.bord[(size_t)r * CELLS + lane / 3u];
         for (uint32_t pass = 0; pass < 6u; ++pass)
             if (!run_pass(r, first, bv, h, inv_h, pass, ord, pass < 5u)) break;  // later passes hold empty cells
@@ -1120,8 +1128,12 @@ __device__ __forceinline__ void g2p_update_body(const DevScene &s, Cta g, G2pSme
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];
-        stage(0, tid, np, tid < np ? s.perm[first + tid] : 0u);
-        uint32_t i_next = tid + NT < np ? s.perm[first + tid + NT] : 0u;
+        // storage index of entry e: from the block's storage start when its
+        // particles are one shifted range of storage, else the permutation
+        const uint32_t src = (!B && s.reuse && s.bsrc != nullptr) ? s.bsrc[r] : NONE;
+        auto pidx = [&](uint32_t e) { return src != NONE ? src + e : s.perm[first + e]; };
+        stage(0, tid, np, tid < np ? pidx(tid) : 0u);
+        uint32_t i_next = tid + NT < np ? pidx(tid + NT) : 0u;
         if constexpr (B) {
             const SceneRec &rec = s.scenes[s.bscene[r]];
             h = rec.h;
@@ -1143,7 +1155,7 @@ __device__ __forceinline__ void g2p_update_body(const DevScene &s, Cta g, G2pSme
         int buf = 0;
         for (uint32_t e = tid; e < np; e += NT, buf ^= 1) {
             stage(buf ^ 1, e + NT, np, i_next);
-            i_next = e + 2 * NT < np ? s.perm[first + e + 2 * NT] : 0u;
+            i_next = e + 2 * NT < np ? pidx(e + 2 * NT) : 0u;
             cp_async_wait<1>();
             const float4 p = st_pm[buf][tid];
             const float x[3] = {p.x, p.y, p.z};

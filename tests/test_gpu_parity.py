@@ -327,6 +327,46 @@ def test_force_damping_fixed(cuda_lib):
     data.close()
 
 
+@pytest.mark.parametrize("direction", ["axis", "diagonal"])
+@pytest.mark.parametrize("ulps", [-4, -1, 0, 1, 4])
+def test_speed_clamp_at_threshold(cuda_lib, direction, ulps):
+    """Particle speeds within a few FP32 ulps of h/dt on either side, where
+    particle_update.slang:75-77 rescales the velocity to h/dt.  The GPU
+    tests the squared norm first and takes the square root only near the
+    threshold; its result must match the oracle's plain test.  Along an
+    axis the grid's per-component clamp (grid_update.slang:159-161) acts
+    first; along the diagonal only the particle's norm clamp does."""
+    sc = scenes.elastic_drop_3d(h=1 / 32, substeps=1)
+    sc.params = SimulationParams(gravity=(0.0, 0.0, 0.0), dt=sc.params.dt)
+    vmax = np.float32(sc.cell_width) / np.float32(sc.params.dt)
+    speed = vmax
+    for _ in range(abs(ulps)):
+        speed = np.nextafter(speed, np.float32(np.inf if ulps > 0 else -np.inf))
+    d = np.array([1.0, 0.0, 0.0]) if direction == "axis" else np.ones(3) / np.sqrt(3.0)
+    parts = sc.particles.copy()
+    parts["velocity"][:] = (d * np.float64(speed)).astype(np.float32)
+    sc.particles = parts
+    data, orc = pair(sc)
+    MpmPipeline().launch_step(data, 1)
+    orc.step(1)
+    g, o = data.download_particles(), orc.get_particles()
+    # the affine velocity C is compared only through F: a uniform velocity
+    # of size h/dt leaves m grad v as rounding noise of the node velocities
+    # (a few ulps of h/dt times 4/h^2), whose order differs between the two
+    tag = f"clamp {direction} {ulps:+d} ulps"
+    assert np.array_equal(g["enabled"], o["enabled"])
+    close(f"{tag} position", g["position"], o["position"], 2e-6, 0)
+    close(f"{tag} velocity", g["velocity"], o["velocity"], 1e-6, 1e-6)
+    close(f"{tag} def_grad", g["def_grad"], o["def_grad"], 2e-6, 2e-6)
+    close(f"{tag} mass", g["mass"], o["mass"], 0, 0)
+    sg = np.linalg.norm(g["velocity"].astype(np.float64), axis=1)
+    so = np.linalg.norm(o["velocity"].astype(np.float64), axis=1)
+    print(f"speeds: gpu max {sg.max():.9e}, oracle max {so.max():.9e}, h/dt {float(vmax):.9e}")
+    assert sg.max() <= float(vmax) * (1 + 1e-6)
+    assert abs(sg.max() - so.max()) <= float(vmax) * 1e-6
+    data.close()
+
+
 def test_divergent_particle_disabled(cuda_lib):
     """A particle whose F is inverted is disabled (particle_update.slang:145-154)."""
     sc = scenes.elastic_drop_3d(h=1 / 32, substeps=1)
