@@ -53,16 +53,25 @@ __device__ __forceinline__ bool p2g_particle(const float4 p, const float4 vv, co
                                              float4 (&acc)[D == 3 ? 9 : 3]) {
     const float x[3] = {p.x, p.y, p.z};
     const float m = p.w;
-    float d0[D], w[D][3];
+    float d0[D], w[D][3], fs = 0.f;
     bool in_cell = true;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
         d0[k] = assoc[k] * h - x[k];
         const float f = -d0[k] * inv_h;
         in_cell = in_cell && f >= 0.49f && f <= 1.51f;
-        bspline_weights(f, w[k]);
+        if (k < D - 1) bspline_weights(f, w[k]);
+        else fs = f;
     }
     if (!in_cell) return false;
+    // Along the slab axis the lane needs its own slab's weight only, in
+    // bspline_weights' arithmetic: (0.5 t) t with t = f - 1.5 (= -(1.5 - f)
+    // exactly) or t = f - 0.5, and 0.75 - t t with t = f - 1.  The
+    // coefficients depend on the slab alone, so they stay out of the loop.
+    const float sb = slab == 0 ? 1.5f : (slab == 1 ? 1.0f : 0.5f);
+    const float sa = slab == 1 ? -1.0f : 0.5f, sc = slab == 1 ? 0.75f : 0.0f;
+    const float ts = fs - sb;
+    const float wsl = fmaf(sa * ts, ts, sc);
     float bm[D], hc[D][D], Cm[D][D];
     mat_from<D>(cq, vv.w, Cm);
     const float vel[3] = {vv.x, vv.y, vv.z};
@@ -83,7 +92,7 @@ __device__ __forceinline__ bool p2g_particle(const float4 p, const float4 vv, co
         // (b + s h C, m) is carried as the pairs (x, y) and (z, m); the m
         // lane's offsets are zero, so it stays m exactly.  Offset 0 adds
         // nothing to a finite value and is skipped.
-        const float wz = slab == 0 ? w[2][0] : (slab == 1 ? w[2][1] : w[2][2]);
+        const float wz = wsl;
         const float2 hx01 = make_float2(hc[0][0], hc[0][1]), hx2 = make_float2(hc[0][2], 0.f);
         const float2 hy01 = make_float2(hc[1][0], hc[1][1]), hy2 = make_float2(hc[1][2], 0.f);
         const float2 fs2 = make_float2(fsl, fsl);
@@ -115,7 +124,7 @@ __device__ __forceinline__ bool p2g_particle(const float4 p, const float4 vv, co
             }
         }
     } else {
-        const float wy = slab == 0 ? w[1][0] : (slab == 1 ? w[1][1] : w[1][2]);
+        const float wy = wsl;
         const float my0 = bm[0] + fsl * hc[1][0], my1 = bm[1] + fsl * hc[1][1];
 #pragma unroll
         for (int sx = 0; sx < 3; ++sx) {
