@@ -916,16 +916,18 @@ template <int D, bool B = false> __device__ __forceinline__ void grid_update_bod
             const float v = (pm[k] + mass * grav[k] * dt) * inv_mass;
             vel[k] = fminf(fmaxf(v, -vlim), vlim);
         }
-        float4 cn;
+        // The cached normal and distance are read, and recorded, only for a
+        // node that has a collision (cid != NONE), their only readers.
+        float4 cn = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t cid;
         const uint32_t prank = s.bprev[r];
         if (prank != NONE && !s.coll_dynamic) {
-            cn = s.prev_coll[(size_t)prank * 64u + node];
             cid = s.prev_coll_id[(size_t)prank * 64u + node];
+            if (cid != NONE) cn = s.prev_coll[(size_t)prank * 64u + node];
         } else {
             cid = collide<D>(bodies, n_bodies, h, cell_pos, cn, s.mesh_vtx, s.mesh_idx);
         }
-        s.coll[t] = cn;
+        if (cid != NONE) s.coll[t] = cn;
         s.coll_id[t] = cid;
         if (cid != NONE) {
             const DevBody &bd = bodies[cid];
