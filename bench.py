@@ -764,6 +764,7 @@ def run_trace(srv, reqs, arrivals, rate: float):
         "span_s": span,
         "gpu_busy_frac": st["busy_s"] / max(st["now_s"], 1e-9),
         "max_in_flight": st["max_in_flight_seen"],
+        "tuning": st["tuning"],
     }
 
 

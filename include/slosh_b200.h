@@ -535,7 +535,8 @@ int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out);
  * CTAs per SM), then P2G's staging depth 2 and 4 with the best shape, then
  * the fused persistent kernel, each on `substeps` real substeps of the
  * current scenes (the simulation advances; every candidate gives identical
- * results), keeps the fastest, and caches it per (dim, material mix,
+ * results), keeps the fastest (the fused kernel only when it is 5 % faster
+ * than the best graph shape), and caches it per (dim, material mix,
  * particle-count bucket) for later batches in the process.  A cached entry
  * is reused without timing. */
 int slosh_batch_autotune(slosh_batch *b, uint32_t substeps, void *stream);
@@ -594,6 +595,7 @@ typedef struct slosh_server_stats {
     double now_s;
     uint32_t in_flight, queued;
     uint32_t max_in_flight_seen, pad;
+    slosh_tuning tuning;         /* the batch's launch shape (after autotuning) */
 } slosh_server_stats;
 
 int slosh_server_create(const slosh_server_config *cfg, slosh_server **out);

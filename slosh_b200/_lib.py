@@ -228,6 +228,7 @@ class SloshServerStats(ctypes.Structure):
         ("queued", ctypes.c_uint32),
         ("max_in_flight_seen", ctypes.c_uint32),
         ("pad", ctypes.c_uint32),
+        ("tuning", SloshTuning),
     ]
 
 

@@ -829,7 +829,10 @@ int batch_autotune(slosh_batch *b, uint32_t substeps, void *stream, uint32_t *ra
         CK(cudaGetLastError());
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) {
+        // The fused kernel must win by 5 %: it loses ground as a batch grows
+        // (measured slower than the graph from 1 to 256 scenes), and a
+        // serving batch keeps the shape tuned on its first scenes.
+        if (t.fused ? ms < 0.95f * best : ms < best) {
             best = ms;
             pick_t = t;
         }

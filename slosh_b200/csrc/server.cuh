@@ -51,6 +51,7 @@ struct slosh_server {
     uint32_t blocks_in_flight = 0, max_seen = 0;
     double busy = 0.0;
     bool tuned = false;
+    slosh_tuning tuning{};  // the batch's launch shape, copied under the lock after tuning
     std::chrono::steady_clock::time_point t0;
     std::string last_error;
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
@@ -175,7 +176,10 @@ void server_loop(slosh_server *s) {
         if (st == SLOSH_OK) st = slosh_batch_sync(b, nullptr);
         const double tb = s->now();
         lk.lock();
-        if (tune) s->tuned = true;
+        if (tune) {
+            s->tuned = true;
+            s->tuning = b->tune;
+        }
         s->busy += tb - ta;
         if (st != SLOSH_OK) {
             s->last_error = b->c.last_error;
@@ -256,6 +260,7 @@ int slosh_server_create(const slosh_server_config *cfg, slosh_server **out) {
         delete s;
         return st;
     }
+    s->tuning = s->batch->tune;
     s->t0 = std::chrono::steady_clock::now();
     s->worker = std::thread(server_loop, s);
     *out = s;
@@ -333,6 +338,7 @@ int slosh_server_get_stats(slosh_server *s, slosh_server_stats *out) {
     out->in_flight = (uint32_t)(s->flight.size() + s->staging.size());
     out->queued = (uint32_t)s->queue.size();
     out->max_in_flight_seen = s->max_seen;
+    out->tuning = s->tuning;
     return SLOSH_OK;
 }
 

@@ -370,15 +370,16 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
         return;
     }
     // One warp a block.  Blocks are taken from a queue (one atomic a
-    // block), so warps that get light blocks take more of them.  The next
-    // entry is claimed when a block starts, so the atomic's round trip
-    // overlaps the block's work.
-    auto resolve = [&](uint32_t q) { return q < nb ? (s.p2g_heavy_first ? s.qorder[q] : q) : nb; };
-    uint32_t q = 0;
-    if (lane == 0) q = atomicAdd(&s.ctr->p2g_next, 1u);
-    for (uint32_t r = __shfl_sync(FULL_MASK, lane == 0 ? resolve(q) : 0u, 0); r < nb;
-         r = __shfl_sync(FULL_MASK, lane == 0 ? resolve(q) : 0u, 0)) {
-        if (lane == 0) q = atomicAdd(&s.ctr->p2g_next, 1u);
+    // block), so warps that get light blocks take more of them.
+    auto next_block = [&]() {
+        uint32_t r = 0;
+        if (lane == 0) {
+            const uint32_t q = atomicAdd(&s.ctr->p2g_next, 1u);
+            r = q < nb ? (s.p2g_heavy_first ? s.qorder[q] : q) : nb;
+        }
+        return __shfl_sync(FULL_MASK, r, 0);
+    };
+    for (uint32_t r = next_block(); r < nb; r = next_block()) {
         const uint32_t np = s.bnp[r];
         if (np == 0) continue;
         const uint32_t first = s.bfirst[r];

@@ -110,7 +110,9 @@ class MpmServer:
     def stats(self) -> dict:
         st = SloshServerStats()
         _check(self._lib, self._s, self._lib.slosh_server_get_stats(self._s, ctypes.byref(st)))
-        return {k: getattr(st, k) for k, _ in SloshServerStats._fields_ if k != "pad"}
+        out = {k: getattr(st, k) for k, _ in SloshServerStats._fields_ if k not in ("pad", "tuning")}
+        out["tuning"] = {k: getattr(st.tuning, k) for k, _ in st.tuning._fields_}
+        return out
 
     def close(self):
         if self._s:
