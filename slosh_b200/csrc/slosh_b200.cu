@@ -76,6 +76,7 @@ struct slosh_ctx {
     // bit-reproducible (default); 3 "direct": the same cell-owner kernel with
     // shared-memory and global float atomics, kept for A/B comparison.
     int p2g_variant = 0;
+    uint32_t g2p_threads = 0;  // G2P CTA size, 0: chosen by the scene size (SLOSH_G2P_THREADS)
     uint32_t *pslot = nullptr, *perm = nullptr;
     unsigned long long *skey = nullptr;
     float4 *nodes = nullptr, *partial = nullptr, *coll[2] = {nullptr, nullptr};
@@ -403,22 +404,33 @@ void enqueue_clear(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
 }
 
 // P2G, grid update, fused G2P/update and the rigid update.
+// Instantiated for a power-of-two cell width and, with it, for scenes of a
+// single model among the linear elastic, sand and fluid ones.
+template <int D, int NT> void launch_g2p(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
+    const uint32_t g2p_grid = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * (512u / NT));
+    if (!s.h_pow2) k_g2p_update<D, NT, false, false><<<g2p_grid, NT, 0, st>>>(s);
+    else if (c->model_mask == 1u << SLOSH_MODEL_SAND_LINEAR)
+        k_g2p_update<D, NT, false, true, SLOSH_MODEL_SAND_LINEAR><<<g2p_grid, NT, 0, st>>>(s);
+    else if (c->model_mask == 1u << SLOSH_MODEL_ELASTIC_LINEAR)
+        k_g2p_update<D, NT, false, true, SLOSH_MODEL_ELASTIC_LINEAR><<<g2p_grid, NT, 0, st>>>(s);
+    else if (c->model_mask == 1u << SLOSH_MODEL_FLUID_TAIT)
+        k_g2p_update<D, NT, false, true, SLOSH_MODEL_FLUID_TAIT><<<g2p_grid, NT, 0, st>>>(s);
+    else k_g2p_update<D, NT, false, true><<<g2p_grid, NT, 0, st>>>(s);
+}
+
+// Persistent CTAs taking blocks from the queue.  A large scene runs 8 CTAs
+// of 64 an SM: small CTAs wait less at the per-block barriers (tile load,
+// the slowest thread's last particle).  A small scene has too few blocks to
+// fill those CTAs, and a CTA of 64 takes several rounds for one block in
+// sequence; there CTAs of 256 (2 an SM) take a block in one round.
+// SLOSH_G2P_THREADS (64, 128 or 256) overrides the choice.
+constexpr uint32_t G2P_SMALL_PARTICLES = 262144;
 template <int D> void enqueue_g2p(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(14);
-    // persistent: 8 CTAs of 64 fit an SM; each takes blocks from the queue.
-    // Small CTAs wait less at the per-block barriers (tile load, the
-    // slowest thread's last particle) than CTAs of 128 or 256.
-    // Instantiated for a power-of-two cell width and, with it, for scenes
-    // of a single model among the linear elastic, sand and fluid ones.
-    const uint32_t g2p_grid = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
-    if (!s.h_pow2) k_g2p_update<D, 64, false, false><<<g2p_grid, 64, 0, st>>>(s);
-    else if (c->model_mask == 1u << SLOSH_MODEL_SAND_LINEAR)
-        k_g2p_update<D, 64, false, true, SLOSH_MODEL_SAND_LINEAR><<<g2p_grid, 64, 0, st>>>(s);
-    else if (c->model_mask == 1u << SLOSH_MODEL_ELASTIC_LINEAR)
-        k_g2p_update<D, 64, false, true, SLOSH_MODEL_ELASTIC_LINEAR><<<g2p_grid, 64, 0, st>>>(s);
-    else if (c->model_mask == 1u << SLOSH_MODEL_FLUID_TAIT)
-        k_g2p_update<D, 64, false, true, SLOSH_MODEL_FLUID_TAIT><<<g2p_grid, 64, 0, st>>>(s);
-    else k_g2p_update<D, 64, false, true><<<g2p_grid, 64, 0, st>>>(s);
+    const uint32_t nt = c->g2p_threads ? c->g2p_threads : (c->n < G2P_SMALL_PARTICLES ? 256u : 64u);
+    if (nt == 256u) launch_g2p<D, 256>(c, s, st);
+    else if (nt == 128u) launch_g2p<D, 128>(c, s, st);
+    else launch_g2p<D, 64>(c, s, st);
     PROF_END(14);
 }
 
@@ -825,6 +837,10 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
     cudaMemset(c->body_imp, 0, (size_t)MAX_BODIES * 6 * sizeof(unsigned long long));
     if (const char *variant = std::getenv("SLOSH_P2G")) {
         if (std::strcmp(variant, "direct") == 0) c->p2g_variant = 3;
+    }
+    if (const char *nt = std::getenv("SLOSH_G2P_THREADS")) {
+        const int v = std::atoi(nt);
+        if (v == 64 || v == 128 || v == 256) c->g2p_threads = (uint32_t)v;
     }
     c->reuse_mode = 2u;
     if (const char *r = std::getenv("SLOSH_GRID_REUSE")) c->reuse_mode = std::strcmp(r, "0") == 0 ? 0u : 1u;
