@@ -803,11 +803,18 @@ __device__ __forceinline__ void canon_body(const DevScene &s, Cta g) {
     const uint32_t nb = s.ctr->n_blocks;
     const uint32_t lane = lane_id();
     const uint32_t warps = g.n * (blockDim.x >> 5);
-    for (uint32_t r = g.id * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
+    // With few blocks (a small scene) G warps share a block, warp `part`
+    // sorting the cells c with c % G == part, so that a block's out-of-order
+    // cells are sorted side by side instead of one after another.  Cells
+    // are disjoint, so the result does not depend on G.
+    uint32_t G = 1u;
+    while (G < 8u && (size_t)nb * G * 2u <= warps) G <<= 1;
+    for (uint32_t t = g.id * (blockDim.x >> 5) + (threadIdx.x >> 5); t < nb * G; t += warps) {
+        const uint32_t r = t / G, part = t % G;
         const uint32_t first = s.bfirst[r], np = s.bnp[r];
         if (np < 2) continue;
         if ((size_t)first + np > s.n) {  // only after an earlier overflow left stale counts
-            if (lane == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
+            if (lane == 0 && part == 0) atomicOr(s.err, ERR_BLOCK_OVERFLOW);
             continue;
         }
         const unsigned long long *k = s.skey + first;
@@ -815,6 +822,11 @@ __device__ __forceinline__ void canon_body(const DevScene &s, Cta g) {
         for (uint32_t e = lane; e + 1 < np; e += 32) {
             const unsigned long long k0 = k[e], k1 = k[e + 1];
             if (k0 > k1 && (k0 >> 32) == (k1 >> 32)) bad |= 1ull << (uint32_t)(k0 >> 32);
+        }
+        if (G > 1u) {
+            unsigned long long mine = 0ull;
+            for (uint32_t c = part; c < CELLS; c += G) mine |= 1ull << c;
+            bad &= mine;
         }
         const uint32_t lo = __reduce_or_sync(FULL_MASK, (uint32_t)bad);
         const uint32_t hi = __reduce_or_sync(FULL_MASK, (uint32_t)(bad >> 32));
