@@ -161,6 +161,12 @@ uint32_t next_pow2(uint32_t v) {
 int nnb(int dim) { return dim == 3 ? Geo<3>::NASSOC - 1 : Geo<2>::NASSOC - 1; }
 int nbk(int dim) { return dim == 3 ? Geo<3>::NB : Geo<2>::NB; }
 
+// Scenes below this many particles have too few blocks to fill the transfer
+// kernels' persistent grids: G2P then runs CTAs of 256 (a block in one
+// round) and P2G takes blocks in rank order (with no more blocks than warps
+// the heaviest-first order balances nothing and its bucket sort is saved).
+constexpr uint32_t G2P_SMALL_PARTICLES = 262144;
+
 DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     DevScene s{};
     s.n = c->max_n;
@@ -251,7 +257,7 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     // P2G: one warp a block fills the GPU from about 10 blocks an SM; below
     // that a CTA's four warps share each block
     s.p2g_coop_below = (uint32_t)c->sm_count * 10u;
-    s.p2g_heavy_first = 1u;
+    s.p2g_heavy_first = c->n >= G2P_SMALL_PARTICLES ? 1u : 0u;
     s.coll = c->coll[cur];
     s.coll_id = c->coll_id[cur];
     s.prev_coll = c->coll[prv];
@@ -424,7 +430,6 @@ template <int D, int NT> void launch_g2p(slosh_ctx *c, const DevScene &s, cudaSt
 // fill those CTAs, and a CTA of 64 takes several rounds for one block in
 // sequence; there CTAs of 256 (2 an SM) take a block in one round.
 // SLOSH_G2P_THREADS (64, 128 or 256) overrides the choice.
-constexpr uint32_t G2P_SMALL_PARTICLES = 262144;
 template <int D> void enqueue_g2p(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(14);
     const uint32_t nt = c->g2p_threads ? c->g2p_threads : (c->n < G2P_SMALL_PARTICLES ? 256u : 64u);
