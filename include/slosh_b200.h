@@ -562,7 +562,8 @@ typedef struct slosh_server_config {
     uint32_t max_bodies;
     uint32_t tick_substeps;     /* substeps per batched step, at most          */
     uint32_t max_in_flight;     /* 0: no limit; 1: one request at a time       */
-    uint32_t autotune;          /* 1: tune the launch shape once under load    */
+    uint32_t autotune;          /* 1: tune the launch shape under load, again
+                                   whenever the in-flight mix changes bucket */
     uint32_t pad;
 } slosh_server_config;
 

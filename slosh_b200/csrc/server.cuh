@@ -50,7 +50,7 @@ struct slosh_server {
     uint64_t next_id = 1, submitted = 0, admitted = 0, completed = 0, work = 0, in_flight_bytes = 0;
     uint32_t blocks_in_flight = 0, max_seen = 0;
     double busy = 0.0;
-    bool tuned = false;
+    std::tuple<int, uint32_t, int> tuned_key{-1, 0u, -1};  // the mix the launch shape was tuned for
     slosh_tuning tuning{};  // the batch's launch shape, copied under the lock after tuning
     std::chrono::steady_clock::time_point t0;
     std::string last_error;
@@ -61,7 +61,7 @@ namespace {
 
 constexpr uint64_t POOL_BYTES_PER_PARTICLE = 280;
 constexpr uint64_t POOL_BYTES_PER_BLOCK = 8756;
-constexpr uint32_t AUTOTUNE_SUBSTEPS = 16;  // 8 candidates x (1 warm-up + 1 timed)
+constexpr uint32_t AUTOTUNE_SUBSTEPS = 18;  // 9 candidates x (1 warm-up + 1 timed)
 
 uint32_t request_blocks(uint32_t n) { return (uint32_t)(2.5 * (double)n / 512.0) + 64u; }
 
@@ -157,7 +157,11 @@ void server_loop(slosh_server *s) {
         }
         uint32_t tick = std::max<uint32_t>(s->cfg.tick_substeps, 1u);
         for (const auto &r : s->flight) tick = std::min(tick, r.remaining);
-        const bool tune = s->cfg.autotune && !s->tuned && tick >= AUTOTUNE_SUBSTEPS;
+        // the launch shape is tuned again whenever the in-flight mix moves to
+        // another (dim, material mix, particle-count bucket): a bucket seen
+        // before takes its cached shape at once
+        const auto mix = tune_key(b);
+        const bool tune = s->cfg.autotune && tick >= AUTOTUNE_SUBSTEPS && mix != s->tuned_key;
         lk.unlock();
         const double ta = s->now();
         int st = SLOSH_OK;
@@ -177,7 +181,7 @@ void server_loop(slosh_server *s) {
         const double tb = s->now();
         lk.lock();
         if (tune) {
-            s->tuned = true;
+            s->tuned_key = mix;
             s->tuning = b->tune;
         }
         s->busy += tb - ta;
