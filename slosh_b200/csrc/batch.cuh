@@ -54,6 +54,11 @@ struct slosh_batch {
     cudaStream_t up_stream = nullptr;
     slosh_tuning tune{5, 64, 8, 3, 0};
     uint32_t fused_ctas[2] = {0, 0};  // CTAs of the fused kernel (all resident), by POW2 variant
+    // SLOSH_FUSED_BARRIER_TEST="<extra arrivals>:<limit ns>": a test makes the
+    // fused kernel's first grid barrier wait for CTAs that never come, with
+    // a short limit, to see the timeout reported (0:0 otherwise)
+    uint32_t bar_extra = 0;
+    unsigned long long bar_ns = 0;
     bool fused_direct = false;        // the fused kernel is launched directly (its graph capture failed)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
@@ -86,6 +91,8 @@ DevScene make_batch_scene(slosh_batch *b, uint32_t parity) {
     // Batches of many small scenes have tens of thousands of blocks: one CTA
     // ordering them costs more than the balance gains, so P2G takes ranks in order.
     s.p2g_heavy_first = 0u;
+    s.bar_extra = b->bar_extra;
+    s.bar_ns = b->bar_ns;
     return s;
 }
 
@@ -289,6 +296,14 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     c->device = cfg->device;
     b->max_scenes = cfg->max_scenes;
     b->max_bodies = std::max<uint32_t>(cfg->max_bodies, 1u);
+    if (const char *bt = std::getenv("SLOSH_FUSED_BARRIER_TEST")) {
+        unsigned extra = 0;
+        unsigned long long ns = 0;
+        if (std::sscanf(bt, "%u:%llu", &extra, &ns) == 2) {
+            b->bar_extra = extra;
+            b->bar_ns = ns;
+        }
+    }
     auto fail_create = [&](int code) {
         slosh_batch_destroy(b);
         return code;

@@ -54,14 +54,14 @@ __device__ __forceinline__ bool grid_barrier(const DevScene &s) {
             const uint32_t g0 = *gen;
             __threadfence();
             ok = 1u;
-            if (atomicAdd(&s.ctr->bar_count, 1u) == gridDim.x - 1u) {
+            if (atomicAdd(&s.ctr->bar_count, 1u) == gridDim.x + s.bar_extra - 1u) {
                 atomicExch(&s.ctr->bar_count, 0u);
                 __threadfence();
                 atomicAdd(&s.ctr->bar_gen, 1u);
             } else {
-                const unsigned long long t0 = global_ns();
+                const unsigned long long t0 = global_ns(), limit = s.bar_ns ? s.bar_ns : BARRIER_NS;
                 for (uint32_t it = 0; *gen == g0; ++it) {
-                    if (it >= BARRIER_SPINS || global_ns() - t0 > BARRIER_NS) {
+                    if (it >= BARRIER_SPINS || global_ns() - t0 > limit) {
                         if (*gen == g0) {
                             atomicOr(s.err, ERR_BARRIER);
                             ok = 0u;

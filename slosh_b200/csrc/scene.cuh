@@ -127,6 +127,11 @@ struct DevScene {
     uint32_t *scene_nblk;            // blocks per scene this substep
     uint32_t *scene_bbase;           // first block rank of each scene
     uint32_t *scene_fill;            // scatter cursors
+    // fused substep's grid barrier: arrivals expected beyond the launch's
+    // CTAs (0; a test sets more to make the wait run out) and its time
+    // limit in ns (0: the default)
+    uint32_t bar_extra;
+    unsigned long long bar_ns;
 };
 
 // This substep keeps the previous grid: the full build's kernels return at

@@ -8,14 +8,15 @@
 - every launch shape the autotuner tries gives identical bits, the fused
   persistent substep (one cooperative kernel) included, in 3D and 2D and
   while scenes join and leave;
-- capacity, state and unsupported-input errors are reported, not faulted.
+- capacity, state and unsupported-input errors are reported, not faulted,
+  and so is a fused-kernel grid barrier that gives up waiting.
 """
 import numpy as np
 import pytest
 
 from oracle import oracle as O
 from slosh_b200 import scenes
-from slosh_b200._lib import SLOSH_E_CAPACITY, SLOSH_E_INVALID, SLOSH_E_STATE, SloshError
+from slosh_b200._lib import SLOSH_E_CAPACITY, SLOSH_E_INVALID, SLOSH_E_STATE, SLOSH_E_TIMEOUT, SloshError
 from slosh_b200.batch import MpmBatch
 from slosh_b200.pipeline import MpmPipeline
 
@@ -163,6 +164,27 @@ def test_fused_substep_bit_identical_to_graph(cuda_lib):
     scs2 = [scenes.dam_break_2d(h=1 / 64, substeps=10), scenes.dam_break_2d(h=1 / 128, substeps=10),
             scenes.dam_break_2d(h=1 / 64, substeps=10), scenes.dam_break_2d(h=1 / 128, substeps=10)]
     assert run_mix(2, scs2, 1) == run_mix(2, scs2, 0)
+
+
+def test_fused_barrier_timeout_reported(cuda_lib, monkeypatch):
+    """The fused kernel's grid barriers wait with a time limit.  Made to wait
+    for CTAs that never arrive (SLOSH_FUSED_BARRIER_TEST: 4 extra arrivals,
+    a 1 ms limit), the substep ends and the host reports SLOSH_E_TIMEOUT;
+    the device stays usable, and a new batch then runs normally."""
+    scs = mix_scenes()
+    monkeypatch.setenv("SLOSH_FUSED_BARRIER_TEST", "4:1000000")
+    b = new_batch()
+    for sc in scs[:2]:
+        b.add(sc)
+    b.set_tuning(5, 64, 8, 3, 1)
+    with pytest.raises(SloshError) as e:
+        b.step(1)
+        b.sync()
+    assert e.value.code == SLOSH_E_TIMEOUT
+    b.close()
+    monkeypatch.delenv("SLOSH_FUSED_BARRIER_TEST")
+    got = run_mix(3, scs, 1)
+    assert got == run_mix(3, scs, 0)
 
 
 def test_batch_errors_reported(cuda_lib):
