@@ -63,6 +63,7 @@ def parse():
         "Poisson request stream through the serving loop; precision: sand column vs the FP64 oracle",
     )
     ap.add_argument("--scenes", type=int, default=256, help="batched: number of scenes")
+    ap.add_argument("--scene-max", type=int, default=256000, help="batched: largest scene (particles)")
     ap.add_argument("--requests", type=int, default=200, help="served: requests in the trace")
     ap.add_argument("--rate", type=float, default=20.0, help="served: mean arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="served: HBM budget")
@@ -85,7 +86,7 @@ def main_ncu_case(args):
     if args.workload == "batched":
         from slosh_b200.batch import MpmBatch
 
-        scs = batched_scenes(args.scenes)
+        scs = batched_scenes(args.scenes, max_particles=args.scene_max)
         total = int(sum(sc.n for sc in scs))
         b = MpmBatch(3, max_particles=total + 1024, grid_capacity=int(sum(max(64, 2.5 * sc.n / 512.0) for sc in scs)),
                      max_scenes=max(args.scenes, 1), max_bodies=4 * args.scenes + 16)
@@ -520,16 +521,17 @@ def main_ours(args):
     return 0
 
 
-def batched_scenes(count: int, seed: int = 4):
+def batched_scenes(count: int, seed: int = 4, max_particles: int = 256000):
     """Scenes of the batched workload: particle counts log-uniform in
-    [4k, 256k], material uniform over {fluid, fixed-corotated, Drucker-Prager
-    sand}, cell width 1/64 or 1/128 (seeded)."""
+    [4k, max_particles] (256k for the configuration), material uniform over
+    {fluid, fixed-corotated, Drucker-Prager sand}, cell width 1/64 or 1/128
+    (seeded)."""
     import numpy as np
 
     from slosh_b200 import scenes
 
     rng = np.random.default_rng(seed)
-    ns = np.exp(rng.uniform(np.log(4000.0), np.log(256000.0), count))
+    ns = np.exp(rng.uniform(np.log(4000.0), np.log(float(max(max_particles, 4000))), count))
     mats = rng.choice(["fluid", "elastic", "sand"], count)
     hs = rng.choice([1.0 / 64.0, 1.0 / 128.0], count)
     return [
@@ -554,7 +556,7 @@ def batched_line(args, steps: int, warmup: int) -> dict:
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    scs = batched_scenes(args.scenes)
+    scs = batched_scenes(args.scenes, max_particles=args.scene_max)
     total = int(sum(sc.n for sc in scs))
     stream = torch.cuda.Stream(device=dev)
     sptr = ctypes.c_void_p(stream.cuda_stream)
@@ -668,7 +670,7 @@ def batched_line(args, steps: int, warmup: int) -> dict:
         "dtype": "f32",
         "data": "synthetic (seeded box blobs; no dataset)",
         "config": {
-            "workload": f"batched: {len(scs)} independent 3D scenes, particles log-uniform [4k, 256k] "
+            "workload": f"batched: {len(scs)} independent 3D scenes, particles log-uniform [4k, {args.scene_max // 1000}k] "
             f"(total {total}), materials {mats}, dx 1/64 or 1/128, Separate floor each; one batch launch per substep "
             f"({'fused cooperative kernel' if tuning['fused'] else 'graph of 14 kernels'}, autotuned)",
             "scenes": len(scs),
