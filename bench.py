@@ -604,6 +604,8 @@ def batched_line(args, steps: int, warmup: int) -> dict:
         torch.cuda.synchronize(dev)
         fms = f0.elapsed_time(f1) / n_form
         forms[name] = {"ms_per_step": fms, "value": total / (fms / 1e3), "substeps": n_form}
+        if shape[4]:
+            forms[name]["inside_graph"] = bool(b.stats()["fused_graph"])
     b.set_tuning(tuning["p2g_ctas_per_sm"], tuning["g2p_threads"], tuning["g2p_ctas_per_sm"], tuning["p2g_stages"],
                  tuning["fused"])
     b.sync(sptr)

@@ -494,7 +494,10 @@ typedef struct slosh_batch_stats {
     uint32_t n_materials;
     uint32_t n_svd_fp64;
     uint32_t n_bodies;         /* collider table entries in use             */
-    uint32_t pad[2];
+    uint32_t fused_graph;      /* 1: the fused kernel runs inside the substep
+                                  graph; 0: launched directly (the runtime
+                                  refused the capture) or not in use         */
+    uint32_t pad;
     slosh_tuning tuning;
 } slosh_batch_stats;
 

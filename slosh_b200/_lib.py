@@ -169,7 +169,8 @@ class SloshBatchStats(ctypes.Structure):
         ("n_materials", ctypes.c_uint32),
         ("n_svd_fp64", ctypes.c_uint32),
         ("n_bodies", ctypes.c_uint32),
-        ("pad", ctypes.c_uint32 * 2),
+        ("fused_graph", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
         ("tuning", SloshTuning),
     ]
 

@@ -138,6 +138,7 @@ class MpmBatch:
             "n_materials": st.n_materials,
             "n_svd_fp64": st.n_svd_fp64,
             "n_bodies": st.n_bodies,
+            "fused_graph": st.fused_graph,
             "tuning": {
                 "p2g_ctas_per_sm": st.tuning.p2g_ctas_per_sm,
                 "g2p_threads": st.tuning.g2p_threads,

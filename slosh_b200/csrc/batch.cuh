@@ -770,6 +770,7 @@ int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out) {
     out->n_materials = c->n_materials;
     out->n_svd_fp64 = ctr.n_svd_fp64;
     out->n_bodies = b->body_top;
+    out->fused_graph = (b->tune.fused && b->graphs_valid && !b->fused_direct) ? 1u : 0u;
     out->tuning = b->tune;
     return SLOSH_OK;
 }

@@ -148,7 +148,9 @@ def run_mix(dim, scs, fused, steps=(6, 6, 6)):
     b.step(steps[1])
     s3 = b.add(scs[3])
     b.step(steps[2])
-    assert b.stats()["tuning"]["fused"] == fused
+    st = b.stats()
+    assert st["tuning"]["fused"] == fused
+    print(f"fused={fused}: fused kernel inside the substep graph: {bool(st['fused_graph'])}")
     out = [gone] + [b.download_particles(s).tobytes() for s in (s0, s2, s3)]
     b.sync()
     b.close()
