@@ -542,7 +542,7 @@ def batched_scenes(count: int, seed: int = 4, max_particles: int = 256000):
 
 def batched_line(args, steps: int, warmup: int) -> dict:
     """Config: 256 independent 3D scenes advanced by one batch (per substep
-    one graph launch of 14 kernels over all scenes, or one persistent
+    one graph launch of 13 kernels over all scenes, or one persistent
     cooperative kernel, whichever the autotuner picks) against the plain loop
     of per-scene contexts (one graph launch of 13 kernels per scene and
     substep), same scenes, same substeps, same stream."""
@@ -589,11 +589,11 @@ def batched_line(args, steps: int, warmup: int) -> dict:
     value = total * steps / (ms / 1e3)
     st = b.stats()
 
-    # both substep forms on the same scenes: the 14-kernel graph (the shape
+    # both substep forms on the same scenes: the 13-kernel graph (the shape
     # the autotuner picks for it) and the one persistent cooperative kernel
     forms = {}
     n_form = min(steps, 200)
-    for name, shape in (("graph_14_kernels", (5, 64, 8, 3, 0)), ("fused_cooperative", (5, 64, 8, 3, 1))):
+    for name, shape in (("graph_13_kernels", (5, 64, 8, 3, 0)), ("fused_cooperative", (5, 64, 8, 3, 1))):
         b.set_tuning(*shape)
         b.step(3, sptr)
         f0 = torch.cuda.Event(enable_timing=True)
@@ -674,7 +674,7 @@ def batched_line(args, steps: int, warmup: int) -> dict:
         "config": {
             "workload": f"batched: {len(scs)} independent 3D scenes, particles log-uniform [4k, {args.scene_max // 1000}k] "
             f"(total {total}), materials {mats}, dx 1/64 or 1/128, Separate floor each; one batch launch per substep "
-            f"({'fused cooperative kernel' if tuning['fused'] else 'graph of 14 kernels'}, autotuned)",
+            f"({'fused cooperative kernel' if tuning['fused'] else 'graph of 13 kernels'}, autotuned)",
             "scenes": len(scs),
             "particles": total,
             "tuning": tuning,
@@ -696,7 +696,7 @@ def batched_line(args, steps: int, warmup: int) -> dict:
             "api": "slosh_batch_add_scene x scenes + slosh_batch_step + slosh_batch_download_positions x scenes "
             "(host buffers, wall clock)",
         },
-        "gpu_launches": (1 if tuning["fused"] else 14) * steps,
+        "gpu_launches": (1 if tuning["fused"] else 13) * steps,
         "clocks": ck,
     }
     return line

@@ -484,7 +484,7 @@ typedef struct slosh_tuning {
                                   cooperative kernel (CTAs of 128 threads,
                                   all resident, grid barriers between the
                                   phases; the fields above are then unused);
-                                  0: 14 kernels in one CUDA graph            */
+                                  0: 13 kernels in one CUDA graph            */
 } slosh_tuning;
 
 typedef struct slosh_batch_stats {

@@ -142,7 +142,7 @@ bool fused_fits(slosh_batch *b) {
                          : fused_grid<2, true>(b) && fused_grid<2, false>(b);
 }
 
-// One batched substep: 14 kernels over all scenes, or the fused kernel.
+// One batched substep: 13 kernels over all scenes, or the fused kernel.
 template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uint32_t parity) {
     slosh_ctx *c = &b->c;
     const DevScene s = make_batch_scene(b, parity);
@@ -156,11 +156,7 @@ template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uin
     k_neighbors<D, true><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
     k_scene_scan<1024><<<1, 1024, 0, st>>>(s);
     k_scene_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
-    const uint32_t ns = b->max_scenes;
-    k_scene_sort<256, 0, SCENE_SORT_SMALL>
-        <<<std::min<uint32_t>(ns, sm * 8), 256, SCENE_SORT_SMALL * sizeof(unsigned long long), st>>>(s);
-    k_scene_sort<1024, SCENE_SORT_SMALL, SCENE_SORT_MAX>
-        <<<std::min<uint32_t>(ns, sm), 1024, SCENE_SORT_MAX * sizeof(unsigned long long), st>>>(s);
+    k_scene_rank<<<grid_for(2ull * c->cap * RANK_LANES, 256, sm * 16), 256, 0, st>>>(s);
     k_block_setup<D, true><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
     k_block_scan<1024><<<1, 1024, 0, st>>>(s);
     k_scatter<true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
@@ -229,7 +225,7 @@ int batch_check_error(slosh_batch *b) {
     }
     if (e & ERR_SCENE_BLOCKS) {
         CK(cudaMemset(c->err, 0, 4));
-        return fail(c, SLOSH_E_CAPACITY, "a scene exceeds %u active blocks (error bits 0x%x)", SCENE_SORT_MAX, e);
+        return fail(c, SLOSH_E_CAPACITY, "a scene exceeds %u active blocks (error bits 0x%x)", SCENE_MAX_BLOCKS, e);
     }
     return check_device_error(c);
 }
@@ -361,8 +357,6 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     cudaMemset(b->scene_nblk, 0, b->max_scenes * 4);
     cudaMemset(b->scenes_dev, 0, b->max_scenes * sizeof(SceneRec));
     cudaMemset(b->n_dev, 0, 4);
-    cudaFuncSetAttribute(k_scene_sort<1024, SCENE_SORT_SMALL, SCENE_SORT_MAX>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, SCENE_SORT_MAX * sizeof(unsigned long long));
     if (cudaDeviceSynchronize() != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     b->scenes.assign(b->max_scenes, SceneRec{});
     b->slots.assign(b->max_scenes, slosh_batch::Slot{});

@@ -1,12 +1,9 @@
 // One persistent, cooperative launch per batched substep: the phases of the
-// 14-kernel batch substep (grid build, P2G, grid update, G2P with the
+// 13-kernel batch substep (grid build, P2G, grid update, G2P with the
 // particle update, bodies) run in order inside one kernel whose CTAs are all
 // resident (cudaLaunchAttributeCooperative), separated by grid barriers.
 // Every phase is the body of the corresponding stand-alone kernel, so the
-// results are those of the multi-kernel substep bit for bit; the one
-// difference is the block ranking, where the per-scene bitonic sort
-// (k_scene_sort) is replaced by counting ranks (scene_rank_body), which
-// yields the same ranks.
+// results are those of the multi-kernel substep bit for bit.
 //
 // The CTA is FUSED_THREADS = 128 threads (P2G's four warps, G2P's CTA of
 // 128 particles); P2G's and G2P's shared memory share one dynamic buffer.

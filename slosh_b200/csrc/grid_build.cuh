@@ -508,66 +508,15 @@ __device__ __forceinline__ void scene_scatter_body(const DevScene &s, Cta g) {
 }
 __global__ void k_scene_scatter(DevScene s) { scene_scatter_body(s, launch_cta()); }
 
-// Bitonic sort of P (a power of two) 64-bit values in shared memory.
-template <int NT> __device__ __forceinline__ void bitonic_sort_smem(unsigned long long *a, uint32_t P) {
-    for (uint32_t k = 2; k <= P; k <<= 1)
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < P / 2; i += NT) {
-                const uint32_t lo = 2u * j * (i / j) + (i % j), hi = lo + j;
-                const bool up = (lo & k) == 0u;
-                const unsigned long long x = a[lo], y = a[hi];
-                if ((x > y) == up) {
-                    a[lo] = y;
-                    a[hi] = x;
-                }
-            }
-            __syncthreads();
-        }
-}
+// Scenes beyond this many active blocks raise ERR_SCENE_BLOCKS (a scene of
+// about 7 M particles; larger ones belong in a context of their own).
+constexpr uint32_t SCENE_MAX_BLOCKS = 16384;
 
-// One CTA per scene whose block count m has PMIN < nextpow2(m) <= PMAX:
-// sorts (key << 32 | slot) in shared memory (PMAX * 8 bytes, dynamic) and
-// writes the ranked block arrays and the map's rank values.  Scenes beyond
-// SCENE_SORT_MAX blocks raise ERR_SCENE_BLOCKS.
-constexpr uint32_t SCENE_SORT_SMALL = 2048;
-constexpr uint32_t SCENE_SORT_MAX = 16384;
-template <int NT, uint32_t PMIN, uint32_t PMAX> __global__ void __launch_bounds__(NT) k_scene_sort(DevScene s) {
-    extern __shared__ unsigned long long sbuf[];
-    for (uint32_t sc = blockIdx.x; sc < s.n_scenes; sc += gridDim.x) {
-        const uint32_t m = s.scene_nblk[sc];
-        if (m == 0) continue;
-        uint32_t P = 1;
-        while (P < m) P <<= 1;
-        if (P <= PMIN) continue;
-        if (P > PMAX) {
-            if (PMAX == SCENE_SORT_MAX && threadIdx.x == 0) atomicOr(s.err, ERR_SCENE_BLOCKS);
-            continue;
-        }
-        const uint32_t base = s.scene_bbase[sc];
-        if (base + m > 2u * s.cap) continue;  // overflow, already flagged
-        for (uint32_t q = threadIdx.x; q < P; q += NT)
-            sbuf[q] = q < m ? (((unsigned long long)s.tmp_key[base + q] << 32) | s.tmp_slot[base + q]) : NONE64;
-        __syncthreads();
-        bitonic_sort_smem<NT>(sbuf, P);
-        for (uint32_t q = threadIdx.x; q < m; q += NT) {
-            const uint32_t r = base + q;
-            if (r >= s.cap) break;
-            const unsigned long long v = sbuf[q];
-            const uint32_t ts = (uint32_t)v, slot = ts & ~RANK_EXTRA;
-            s.bkey[r] = (uint32_t)(v >> 32);
-            s.bslot[r] = slot;
-            s.bscene[r] = sc;
-            s.hvals[slot] = r | (ts & RANK_EXTRA);
-        }
-        __syncthreads();
-    }
-}
-
-// Ranks of the fused batch substep: the blocks of each scene (grouped by
+// Block ranks of a batch: the blocks of each scene (grouped by
 // k_scene_scatter) ranked by counting the scene's smaller keys, RANK_LANES
-// lanes a block.  Keys are distinct inside a scene, so these are the ranks
-// k_scene_sort's bitonic sort gives, written to the same arrays; scenes
-// beyond SCENE_SORT_MAX blocks raise ERR_SCENE_BLOCKS as they do there.
+// lanes a block.  Keys are distinct inside a scene, so the rank is the
+// block's place in the scene's ascending key order.  Written: the block's
+// key, hash slot and scene at its rank, and the rank into the hash map.
 __device__ __forceinline__ void scene_rank_body(const DevScene &s, Cta g) {
     const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
     const uint32_t gl = threadIdx.x % RANK_LANES;
@@ -577,7 +526,7 @@ __device__ __forceinline__ void scene_rank_body(const DevScene &s, Cta g) {
         const uint32_t key = s.tmp_key[t], ts = s.tmp_slot[t], slot = ts & ~RANK_EXTRA;
         const uint32_t sc = (uint32_t)(s.hkeys64[slot] >> 32);
         const uint32_t m = s.scene_nblk[sc], base = s.scene_bbase[sc];
-        if (m > SCENE_SORT_MAX) {
+        if (m > SCENE_MAX_BLOCKS) {
             if (gl == 0) atomicOr(s.err, ERR_SCENE_BLOCKS);
             continue;
         }
@@ -596,6 +545,7 @@ __device__ __forceinline__ void scene_rank_body(const DevScene &s, Cta g) {
         }
     }
 }
+__global__ void k_scene_rank(DevScene s) { scene_rank_body(s, launch_cta()); }
 
 // One warp per block: per-cell counts (cleared in the hash-slot array once
 // read) with their in-block exclusive scan, the block total, the cells in

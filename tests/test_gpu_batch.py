@@ -158,7 +158,7 @@ def run_mix(dim, scs, fused, steps=(6, 6, 6)):
 
 
 def test_fused_substep_bit_identical_to_graph(cuda_lib):
-    """The persistent cooperative substep gives the 14-kernel graph's bits,
+    """The persistent cooperative substep gives the 13-kernel graph's bits,
     3D (sand, elastic, fluid; two cell widths) and 2D, with scenes joining
     and leaving between substeps."""
     scs3 = mix_scenes()
