@@ -534,7 +534,7 @@ int slosh_batch_timestep_bound(slosh_batch *b, uint32_t slot, float *dt_out, voi
 int slosh_batch_sync(slosh_batch *b, void *stream);
 int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out);
 
-/* Autotuner: times six launch shapes (P2G CTAs per SM; G2P CTA size and
+/* Autotuner: times seven launch shapes (P2G CTAs per SM; G2P CTA size and
  * CTAs per SM), then P2G's staging depth 2 and 4 with the best shape, then
  * the fused persistent kernel, each on `substeps` real substeps of the
  * current scenes (the simulation advances; every candidate gives identical

@@ -802,9 +802,10 @@ int batch_autotune(slosh_batch *b, uint32_t substeps, void *stream, uint32_t *ra
     CK(cudaSetDevice(c->device));
     cudaStream_t st = pick(c, stream);
     // launch shapes first, then P2G's staging depth with the best shape
-    constexpr int N_SHAPES = 6;
-    slosh_tuning cands[N_SHAPES + 3] = {{5, 64, 8, 3, 0},  {5, 128, 8, 3, 0}, {4, 128, 4, 3, 0},
-                                        {10, 128, 16, 3, 0}, {5, 64, 16, 3, 0}, {4, 64, 8, 3, 0}};
+    constexpr int N_SHAPES = 7;
+    slosh_tuning cands[N_SHAPES + 3] = {{5, 64, 8, 3, 0},   {5, 128, 8, 3, 0}, {4, 128, 4, 3, 0},
+                                        {10, 128, 16, 3, 0}, {5, 64, 16, 3, 0}, {4, 64, 8, 3, 0},
+                                        {5, 256, 2, 3, 0}};
     const bool fused_ok = fused_fits(b);
     const uint32_t reps = std::max<uint32_t>(substeps, 1u);
     cudaEvent_t e0, e1;

@@ -61,7 +61,7 @@ namespace {
 
 constexpr uint64_t POOL_BYTES_PER_PARTICLE = 280;
 constexpr uint64_t POOL_BYTES_PER_BLOCK = 8756;
-constexpr uint32_t AUTOTUNE_SUBSTEPS = 18;  // 9 candidates x (1 warm-up + 1 timed)
+constexpr uint32_t AUTOTUNE_SUBSTEPS = 20;  // 10 candidates x (1 warm-up + 1 timed)
 
 uint32_t request_blocks(uint32_t n) { return (uint32_t)(2.5 * (double)n / 512.0) + 64u; }
 
