@@ -62,7 +62,14 @@ struct slosh_batch {
     bool fused_direct = false;        // the fused kernel is launched directly (its graph capture failed)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_valid = false;
-    uint32_t graph_flags = 0;       // has_damping | has_sand << 1 | all_pow2 << 2 the graphs were captured with
+    uint32_t graph_flags = 0;       // has_damping | has_sand << 1 | all_pow2 << 2 | G2P classes << 3
+                                    // the graphs were captured with
+    uint32_t *g2p_lists = nullptr;  // G2P_CLASSES lists of `cap` block ranks
+    uint32_t *g2p_counts = nullptr; // 2 * G2P_CLASSES: list sizes, launch queues
+    // the class launches after the first run on side streams forked from
+    // and joined to the substep's stream (parallel branches of its graph)
+    cudaStream_t g2p_side[G2P_CLASSES - 1] = {};
+    cudaEvent_t g2p_fork = nullptr, g2p_join[G2P_CLASSES - 1] = {};
     uint32_t all_pow2 = 1;          // every scene admitted so far has a power-of-two cell width (sticky)
 };
 
@@ -93,15 +100,61 @@ DevScene make_batch_scene(slosh_batch *b, uint32_t parity) {
     s.p2g_heavy_first = 0u;
     s.bar_extra = b->bar_extra;
     s.bar_ns = b->bar_ns;
+    s.g2p_lists = b->g2p_lists;
+    s.g2p_counts = b->g2p_counts;
+    s.g2p_class = -1;
     return s;
+}
+
+// The G2P classes of the live and staged scenes (bit c: a launch for class c).
+uint32_t g2p_class_mask(const slosh_batch *b) {
+    uint32_t m = 0;
+    for (const auto &sl : b->slots)
+        if (sl.used) m |= 1u << g2p_class_of_tags(sl.tags);
+    return m;
+}
+
+// What the captured graphs depend on besides the buffers.
+uint32_t batch_graph_flags(const slosh_batch *b) {
+    const slosh_ctx *c = &b->c;
+    return c->has_damping | (c->has_sand << 1) | (b->all_pow2 << 2) | (g2p_class_mask(b) << 3);
 }
 
 // While every admitted scene has a power-of-two cell width, G2P compiles
 // x / h as the exact x * (1/h) of each scene.
-template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s, cudaStream_t st) {
+template <int D, int NT, int MODEL> void launch_batch_g2p_model(slosh_batch *b, const DevScene &s, cudaStream_t st) {
     const uint32_t g = std::min<uint32_t>(b->c.cap, (uint32_t)b->c.sm_count * b->tune.g2p_ctas_per_sm);
-    if (b->all_pow2) k_g2p_update<D, NT, true, true><<<g, NT, 0, st>>>(s);
-    else k_g2p_update<D, NT, true, false><<<g, NT, 0, st>>>(s);
+    if (b->all_pow2) k_g2p_update<D, NT, true, true, MODEL><<<g, NT, 0, st>>>(s);
+    else k_g2p_update<D, NT, true, false, MODEL><<<g, NT, 0, st>>>(s);
+}
+
+// One G2P launch per class of scene present, each compiled for its model
+// (the first one also clears the next substep's map).  The launches after
+// the first run side by side with it on side streams, so that one class's
+// last blocks overlap the others' instead of each launch draining alone.
+template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s, cudaStream_t st) {
+    const uint32_t mask = g2p_class_mask(b);
+    uint32_t n = 0, side = 0;
+    for (uint32_t cls = 0; cls < G2P_CLASSES; ++cls) {
+        if (!(mask >> cls & 1u)) continue;
+        DevScene sc = s;
+        sc.g2p_class = (int32_t)cls;
+        sc.clear_tail = n == 0 ? s.clear_tail : 0u;
+        cudaStream_t ls = st;
+        if (n > 0) {
+            if (side == 0) cudaEventRecord(b->g2p_fork, st);
+            ls = b->g2p_side[side];
+            cudaStreamWaitEvent(ls, b->g2p_fork, 0);
+        }
+        if (cls == 0) launch_batch_g2p_model<D, NT, SLOSH_MODEL_SAND_LINEAR>(b, sc, ls);
+        else if (cls == 1) launch_batch_g2p_model<D, NT, SLOSH_MODEL_ELASTIC_LINEAR>(b, sc, ls);
+        else if (cls == 2) launch_batch_g2p_model<D, NT, SLOSH_MODEL_FLUID_TAIT>(b, sc, ls);
+        else launch_batch_g2p_model<D, NT, -1>(b, sc, ls);
+        if (n > 0) cudaEventRecord(b->g2p_join[side++], ls);
+        ++n;
+    }
+    for (uint32_t k = 0; k < side; ++k) cudaStreamWaitEvent(st, b->g2p_join[k], 0);
+    if (n == 0) launch_batch_g2p_model<D, NT, -1>(b, s, st);  // no scene: the map is still cleared
 }
 
 // CTAs of the fused substep: every CTA an SM holds (the cooperative launch
@@ -146,9 +199,11 @@ bool fused_fits(slosh_batch *b) {
 template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uint32_t parity) {
     slosh_ctx *c = &b->c;
     const DevScene s = make_batch_scene(b, parity);
-    if (b->tune.fused) {
-        if (b->all_pow2) launch_batch_fused<D, true>(b, s, st);
-        else launch_batch_fused<D, false>(b, s, st);
+    if (b->tune.fused) {  // takes every block in rank order: no class lists
+        DevScene sf = s;
+        sf.g2p_lists = nullptr;
+        if (b->all_pow2) launch_batch_fused<D, true>(b, sf, st);
+        else launch_batch_fused<D, false>(b, sf, st);
         return;
     }
     const uint32_t sm = (uint32_t)c->sm_count;
@@ -209,7 +264,7 @@ int build_batch_graphs(slosh_batch *b) {
         if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
     }
     b->graphs_valid = true;
-    b->graph_flags = c->has_damping | (c->has_sand << 1) | (b->all_pow2 << 2);
+    b->graph_flags = batch_graph_flags(b);
     return SLOSH_OK;
 }
 
@@ -309,6 +364,11 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     if (cudaStreamCreateWithFlags(&b->up_stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail_create(SLOSH_E_CUDA);
+    for (uint32_t k = 0; k + 1 < G2P_CLASSES; ++k)
+        if (cudaStreamCreateWithFlags(&b->g2p_side[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->g2p_join[k], cudaEventDisableTiming) != cudaSuccess)
+            return fail_create(SLOSH_E_CUDA);
+    if (cudaEventCreateWithFlags(&b->g2p_fork, cudaEventDisableTiming) != cudaSuccess) return fail_create(SLOSH_E_CUDA);
     const size_t N = c->max_n;
     const int D = c->dim;
     const uint32_t cap = c->cap, hcap = c->hcap;
@@ -341,8 +401,10 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
         (st = dalloc(c, &c->ctr, 1)) || (st = dalloc(c, &c->err, 1)) || (st = dalloc(c, &c->small, 4)) ||
         (st = dalloc(c, &b->scene_nblk, b->max_scenes)) || (st = dalloc(c, &b->scene_bbase, b->max_scenes)) ||
         (st = dalloc(c, &b->scene_fill, b->max_scenes)) || (st = dalloc(c, &b->scenes_dev, b->max_scenes)) ||
-        (st = dalloc(c, &b->n_dev, 1)))
+        (st = dalloc(c, &b->n_dev, 1)) || (st = dalloc(c, &b->g2p_lists, (size_t)G2P_CLASSES * cap)) ||
+        (st = dalloc(c, &b->g2p_counts, 2 * G2P_CLASSES)))
         return fail_create(st);
+    cudaMemset(b->g2p_counts, 0, 2 * G2P_CLASSES * sizeof(uint32_t));
     cudaMemset(b->hkeys64[0], 0xff, (size_t)hcap * 8);
     cudaMemset(b->hkeys64[1], 0xff, (size_t)hcap * 8);
     cudaMemset(c->hvals[0], 0xff, (size_t)hcap * 4);
@@ -372,6 +434,14 @@ void slosh_batch_destroy(slosh_batch *b) {
         cudaStreamSynchronize(b->up_stream);
         cudaStreamDestroy(b->up_stream);
     }
+    for (uint32_t k = 0; k + 1 < G2P_CLASSES; ++k) {
+        if (b->g2p_side[k]) {
+            cudaStreamSynchronize(b->g2p_side[k]);
+            cudaStreamDestroy(b->g2p_side[k]);
+        }
+        if (b->g2p_join[k]) cudaEventDestroy(b->g2p_join[k]);
+    }
+    if (b->g2p_fork) cudaEventDestroy(b->g2p_fork);
     release_ctx(&b->c);
     delete b;
 }
@@ -537,6 +607,7 @@ int batch_activate(slosh_batch *b, cudaStream_t st) {
         rec.body_first = b->body_top;
         rec.n_bodies = (uint32_t)sg.bodies.size();
         rec.live = 1u;
+        rec.g2p_class = g2p_class_of_tags(sg.tags);
         CK(cudaMemcpyAsync(b->scenes_dev + sg.slot, &rec, sizeof(SceneRec), cudaMemcpyHostToDevice, st));
         slosh_batch::Slot &sl = b->slots[sg.slot];
         sl.live = true;
@@ -554,7 +625,7 @@ int batch_activate(slosh_batch *b, cudaStream_t st) {
     c->has_sand |= (small[1] & SCENE_SAND) ? 1u : 0u;
     b->n_storage = new_n;
     if (b->graphs_valid &&
-        (b->graph_flags != (c->has_damping | (c->has_sand << 1) | (b->all_pow2 << 2)) || new_bodies))
+        (b->graph_flags != batch_graph_flags(b) || new_bodies))
         destroy_batch_graphs(b);  // captured scene flags or body count changed
     b->staged.clear();
     b->up_used = 0;

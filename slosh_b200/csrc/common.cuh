@@ -240,7 +240,20 @@ struct SceneRec {
     uint32_t h_pow2;
     uint32_t body_first, n_bodies;  // the scene's colliders in the body table
     uint32_t live;                  // 0: the slot's particles are dropped at the next substep
+    uint32_t g2p_class;             // the G2P launch its blocks go to (G2P_CLASS_*)
 };
+
+// A batch's blocks are handed to one G2P launch per class of scene, each
+// compiled for one particle model (a scene of one linear-elastic, sand or
+// fluid model), or for every model (any other scene).
+constexpr uint32_t G2P_CLASSES = 4;
+constexpr uint32_t G2P_CLASS_GENERIC = 3;
+__host__ __device__ __forceinline__ uint32_t g2p_class_of_tags(uint32_t tags) {
+    if (tags == (1u << SLOSH_MODEL_SAND_LINEAR)) return 0u;
+    if (tags == (1u << SLOSH_MODEL_ELASTIC_LINEAR)) return 1u;
+    if (tags == (1u << SLOSH_MODEL_FLUID_TAIT)) return 2u;
+    return G2P_CLASS_GENERIC;
+}
 
 // Collider body on the device (slosh_body in device form).
 struct DevBody {

@@ -562,6 +562,9 @@ template <int D, bool B = false> __device__ __forceinline__ void block_setup_bod
     if (g.id == 0 && threadIdx.x == 0) {  // the transfer kernels' block queues, read after this kernel
         s.ctr->p2g_next = 0u;
         s.ctr->g2p_next = 0u;
+        if constexpr (B)
+            if (s.g2p_lists)
+                for (uint32_t c = 0; c < G2P_CLASSES; ++c) s.g2p_counts[G2P_CLASSES + c] = 0u;
     }
     for (uint32_t r = g.id * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nb; r += warps) {
         const uint32_t sl = s.bslot[r];
@@ -585,6 +588,11 @@ template <int D, bool B = false> __device__ __forceinline__ void block_setup_bod
             s.bnp[r] = incl;
             if (incl >= (1u << 26)) atomicOr(s.err, ERR_BLOCK_PARTICLES);  // beyond the 26-bit first in bord
             if (s.bsrc) s.bsrc[r] = NONE;  // a full build's permutation is no shifted range
+            if constexpr (B)
+                if (s.g2p_lists && incl != 0u) {  // the block goes to its scene's G2P launch
+                    const uint32_t cls = s.scenes[s.bscene[r]].g2p_class;
+                    s.g2p_lists[(size_t)cls * s.cap + atomicAdd(&s.g2p_counts[cls], 1u)] = r;
+                }
         }
         {
             // rank of each cell among the 64 by (count desc, cell asc): the

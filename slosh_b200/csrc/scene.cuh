@@ -132,6 +132,13 @@ struct DevScene {
     // limit in ns (0: the default)
     uint32_t bar_extra;
     unsigned long long bar_ns;
+    // G2P by scene class: the blocks of each class (G2P_CLASSES lists of
+    // `cap`, appended by k_block_setup), g2p_counts[c] their number and
+    // g2p_counts[G2P_CLASSES + c] the queue of class c's launch.  g2p_class:
+    // the class this G2P launch takes (-1: every block, in rank order).
+    uint32_t *g2p_lists;
+    uint32_t *g2p_counts;
+    int32_t g2p_class;
 };
 
 // This substep keeps the previous grid: the full build's kernels return at

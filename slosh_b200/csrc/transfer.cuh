@@ -1133,7 +1133,15 @@ __device__ __forceinline__ void g2p_update_body(const DevScene &s, Cta g, G2pSme
     uint32_t &next_r = sm.next_r;
     for (;;) {
         __syncthreads();  // every thread has read next_r
-        if (tid == 0) next_r = atomicAdd(&s.ctr->g2p_next, 1u);
+        if (tid == 0) {
+            if (B && s.g2p_class >= 0) {  // this launch's class of the batch's blocks
+                const uint32_t cls = (uint32_t)s.g2p_class;
+                const uint32_t q = atomicAdd(&s.g2p_counts[G2P_CLASSES + cls], 1u);
+                next_r = q < s.g2p_counts[cls] ? s.g2p_lists[(size_t)cls * s.cap + q] : nb;
+            } else {
+                next_r = atomicAdd(&s.ctr->g2p_next, 1u);
+            }
+        }
         __syncthreads();
         const uint32_t r = next_r;
         if (r >= nb) break;
@@ -1440,6 +1448,9 @@ template <int D, bool B = false> __device__ __forceinline__ void rigid_body(cons
         s.ctr->last_n_blocks = nb;
         if (!build_skipped(s)) s.ctr->last_n_primary = min(s.ctr->n_primary, s.cap);
         if (s.reuse) s.ctr->rebuild[s.par] = 0u;  // read by this substep only; G2P set the next one's
+        if constexpr (B)
+            if (s.g2p_lists)
+                for (uint32_t c = 0; c < G2P_CLASSES; ++c) s.g2p_counts[c] = 0u;  // the next block setup's lists
         s.ctr->n_primary = 0u;
         s.ctr->n_extra = 0u;
         s.ctr->n_blocks = 0u;
