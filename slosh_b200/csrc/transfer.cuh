@@ -834,8 +834,9 @@ __device__ __forceinline__ void project_velocity(uint32_t type, float friction, 
 // node.  The collision of a node is reused from the previous substep when
 // its block was active there (slosh's cache, which assumes static colliders),
 // otherwise collide() runs; both are recorded for the next substep.
-// 4 CTAs of 256 per SM: the register cap (64) leaves the rare collision
-// queries (nodes without a cached collision) to spill, not the whole kernel.
+// 8 CTAs of 256 per SM (64 warps): the node gather is a chain of dependent
+// loads, so occupancy pays; the register cap (32) leaves the rare collision
+// queries (nodes without a cached collision) to spill, not the common path.
 template <int D, bool B = false> __device__ __forceinline__ void grid_update_body(const DevScene &s, Cta g) {
     constexpr int BW = Geo<D>::BW;
     const uint32_t nb = s.ctr->n_blocks;
@@ -986,7 +987,7 @@ template <int D, bool B = false> __device__ __forceinline__ void grid_update_bod
         s.nodes[t] = make_float4(vel[0], vel[1], D == 3 ? vel[D - 1] : 0.f, mass);
     }
 }
-template <int D, bool B = false> __global__ void __launch_bounds__(256, 4) k_grid_update(DevScene s) {
+template <int D, bool B = false> __global__ void __launch_bounds__(256, 8) k_grid_update(DevScene s) {
     grid_update_body<D, B>(s, launch_cta());
 }
 
