@@ -390,9 +390,17 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
         const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
         k_p2g_atomic<D><<<g, P2G_ATOMIC_THREADS, 0, st>>>(s);
     } else {
-        const uint32_t g = std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, (uint32_t)c->sm_count * 5);
-        if (s.force_pending) k_p2g<D, false, true><<<g, 32 * P2G_WARPS, 0, st>>>(s);
-        else k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
+        if (c->n < G2P_SMALL_PARTICLES) {
+            // a small scene: CTAs of six warps, one pass of a shared block each
+            const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 3);
+            constexpr size_t smem = sizeof(P2gSmem<D, 3, P2G_WIDE_WARPS>);
+            if (s.force_pending) k_p2g_wide<D, true><<<g, 32 * P2G_WIDE_WARPS, smem, st>>>(s);
+            else k_p2g_wide<D, false><<<g, 32 * P2G_WIDE_WARPS, smem, st>>>(s);
+        } else {
+            const uint32_t g = std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, (uint32_t)c->sm_count * 5);
+            if (s.force_pending) k_p2g<D, false, true><<<g, 32 * P2G_WARPS, 0, st>>>(s);
+            else k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
+        }
     }
     PROF_END(12);
 }
@@ -847,6 +855,15 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
         const int v = std::atoi(nt);
         if (v == 64 || v == 128 || v == 256) c->g2p_threads = (uint32_t)v;
     }
+    // the small-scene P2G's shared memory is above the 48 KB a launch gets by default
+    cudaFuncSetAttribute(k_p2g_wide<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(P2gSmem<3, 3, P2G_WIDE_WARPS>));
+    cudaFuncSetAttribute(k_p2g_wide<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(P2gSmem<3, 3, P2G_WIDE_WARPS>));
+    cudaFuncSetAttribute(k_p2g_wide<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(P2gSmem<2, 3, P2G_WIDE_WARPS>));
+    cudaFuncSetAttribute(k_p2g_wide<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(P2gSmem<2, 3, P2G_WIDE_WARPS>));
     c->reuse_mode = 2u;
     if (const char *r = std::getenv("SLOSH_GRID_REUSE")) c->reuse_mode = std::strcmp(r, "0") == 0 ? 0u : 1u;
     update_reuse(c);

@@ -175,21 +175,21 @@ template <> struct SlabTile<2> {
 // (at most CS = 12: 32 lanes, 3 slab lanes a cell, the first and last cell
 // possibly shared with the neighbouring passes) in NBUF buffers; particle
 // k + NBUF - 1 of every cell is copied while particle k is summed.
-template <int D, int NBUF> struct P2gSmem {
+template <int D, int NBUF, int W = P2G_WARPS> struct P2gSmem {
     static constexpr int CS = 12;
-    float4 stile[P2G_WARPS][3 * SlabTile<D>::SIZE];
-    float4 sp_pm[P2G_WARPS][NBUF][CS];
-    float4 sp_vv[P2G_WARPS][NBUF][CS];
-    float4 sp_cq[P2G_WARPS][NBUF][MQ<D>::Q][CS];
+    float4 stile[W][3 * SlabTile<D>::SIZE];
+    float4 sp_pm[W][NBUF][CS];
+    float4 sp_vv[W][NBUF][CS];
+    float4 sp_cq[W][NBUF][MQ<D>::Q][CS];
 };
 
-template <int D, bool B = false, bool FORCE = false, int NBUF = 3>
-__device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm) {
+template <int D, bool B = false, bool FORCE = false, int NBUF = 3, int W = P2G_WARPS>
+__device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF, W> &sm) {
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
     constexpr int PY = SlabTile<D>::PY, PZ = SlabTile<D>::PZ, SSZ = SlabTile<D>::SIZE;
     constexpr int Q = MQ<D>::Q;
-    constexpr int CS = P2gSmem<D, NBUF>::CS;
+    constexpr int CS = P2gSmem<D, NBUF, W>::CS;
     static_assert(NBUF >= 2 && NBUF <= 4, "staging depth 2 to 4");
     auto &stile = sm.stile;
     auto &sp_pm = sm.sp_pm;
@@ -335,8 +335,8 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
         for (uint32_t q = lane; q < 3u * SSZ; q += 32u) tiles[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     };
     if (!B && nb < s.p2g_coop_below) {
-        // Few blocks (a small scene): the CTA's warps share a block, warp w
-        // taking passes w and w + 4, and the block's tile sums the warps'
+        // Few blocks (a small scene): the CTA's W warps share a block, warp w
+        // taking passes w, w + W, ..., and the block's tile sums the warps'
         // slab tiles in warp order.
         __shared__ uint32_t coop_r;
         for (;;) {
@@ -359,13 +359,13 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF> &sm
             int bv[D];
             block_setup(r, h, inv_h, bv);
             src = use_src ? s.bsrc[r] : NONE;
-            for (uint32_t pass = wl; pass < 6u; pass += P2G_WARPS) {
+            for (uint32_t pass = wl; pass < 6u; pass += W) {
                 uint2 ord = s.bord[(size_t)r * CELLS + (32u * pass + lane) / 3u];
                 if (!run_pass(r, first, bv, h, inv_h, pass, ord, false)) break;
             }
             __syncthreads();
-            for (int t = (int)threadIdx.x; t < TILE; t += 32 * P2G_WARPS)
-                s.partial[(size_t)r * TILE + t] = tile_node(t, 0, P2G_WARPS);
+            for (int t = (int)threadIdx.x; t < TILE; t += 32 * W)
+                s.partial[(size_t)r * TILE + t] = tile_node(t, 0, W);
         }
         return;
     }
@@ -403,6 +403,16 @@ template <int D, bool B = false, bool FORCE = false, int NBUF = 3>
 __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
     __shared__ P2gSmem<D, NBUF> sm;
     p2g_body<D, B, FORCE, NBUF>(s, sm);
+}
+
+// Small scenes: CTAs of P2G_WIDE_WARPS warps, which take one pass each of a
+// shared block (3 CTAs an SM by registers); their shared memory (54 KB in
+// 3D) is dynamic.
+constexpr int P2G_WIDE_WARPS = 6;
+template <int D, bool FORCE>
+__global__ void __launch_bounds__(32 * P2G_WIDE_WARPS, 3) k_p2g_wide(DevScene s) {
+    extern __shared__ __align__(16) unsigned char psm[];
+    p2g_body<D, false, FORCE, 3, P2G_WIDE_WARPS>(s, *reinterpret_cast<P2gSmem<D, 3, P2G_WIDE_WARPS> *>(psm));
 }
 
 // Particle-to-grid with float atomics, kept for comparison (SLOSH_P2G=direct):
