@@ -166,6 +166,7 @@ int nbk(int dim) { return dim == 3 ? Geo<3>::NB : Geo<2>::NB; }
 // round) and P2G takes blocks in rank order (with no more blocks than warps
 // the heaviest-first order balances nothing and its bucket sort is saved).
 constexpr uint32_t G2P_SMALL_PARTICLES = 262144;
+constexpr uint32_t P2G_WIDE_PARTICLES = 1048576;  // P2G in CTAs of six warps below this
 
 DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     DevScene s{};
@@ -255,8 +256,10 @@ DevScene make_scene(slosh_ctx *c, uint32_t parity, bool force) {
     s.use_partial = (c->p2g_variant == 0) ? 1u : 0u;
     s.gather_only = 0u;
     // P2G: one warp a block fills the GPU from about 10 blocks an SM; below
-    // that a CTA's four warps share each block
-    s.p2g_coop_below = (uint32_t)c->sm_count * 10u;
+    // that a CTA's warps share each block.  Scenes below P2G_WIDE_PARTICLES
+    // run CTAs of six warps (3 an SM), which share blocks up to about 5
+    // blocks a CTA (16 an SM): one pass a warp beats six passes a warp there
+    s.p2g_coop_below = c->n < P2G_WIDE_PARTICLES ? (uint32_t)c->sm_count * 16u : (uint32_t)c->sm_count * 10u;
     s.p2g_heavy_first = c->n >= G2P_SMALL_PARTICLES ? 1u : 0u;
     s.coll = c->coll[cur];
     s.coll_id = c->coll_id[cur];
@@ -390,7 +393,7 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
         const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
         k_p2g_atomic<D><<<g, P2G_ATOMIC_THREADS, 0, st>>>(s);
     } else {
-        if (c->n < G2P_SMALL_PARTICLES) {
+        if (c->n < P2G_WIDE_PARTICLES) {
             // a small scene: CTAs of six warps, one pass of a shared block each
             const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 3);
             constexpr size_t smem = sizeof(P2gSmem<D, 3, P2G_WIDE_WARPS>);
