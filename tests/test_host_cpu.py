@@ -184,3 +184,17 @@ def test_integration_rust_records_match_header():
     for rname, cname in pairs.items():
         want = [(f, c_to_rust[t], k) for f, t, k in c[cname]]
         assert rust[rname] == want, (rname, rust[rname], want)
+
+
+def test_environment_settings_documented():
+    """Every SLOSH_* setting the library reads from the environment is listed
+    in INTEGRATION.md's table of settings."""
+    src = os.path.join(ROOT, "slosh_b200", "csrc")
+    names = set()
+    for f in os.listdir(src):
+        if f.endswith((".cu", ".cuh")):
+            names |= set(re.findall(r'getenv\("(SLOSH_[A-Z0-9_]+)"\)', open(os.path.join(src, f)).read()))
+    assert names, "no settings found"
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = sorted(n for n in names if f"`{n}" not in doc)
+    assert not missing, missing
