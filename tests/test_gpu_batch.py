@@ -189,6 +189,63 @@ def test_fused_barrier_timeout_reported(cuda_lib, monkeypatch):
     assert got == run_mix(3, scs, 0)
 
 
+def mixed_model_scene():
+    """A scene mixing every model (it goes to the G2P launch compiled for all
+    models; one-model scenes go to launches compiled for their model)."""
+    from slosh_b200.pipeline import ParticleModel, RigidBody, SimulationParams, make_particles
+
+    h = 1 / 64
+    rng = np.random.default_rng(23)
+    models = [
+        ParticleModel.sand(3.5e5, 0.3, friction_angle_deg=30.0),
+        ParticleModel.elastic(1e5, 0.3),
+        ParticleModel.elastic_neo_hookean(1e5, 0.3),
+        ParticleModel.sand_neo_hookean(3.5e5, 0.3, friction_angle_deg=30.0),
+        ParticleModel.fluid_tait(1000.0, 1e4, 7.0),
+    ]
+    parts = []
+    for k, model in enumerate(models):
+        lo = np.array([0.2 + 0.12 * k, 0.12, 0.45])
+        parts.append(make_particles(lo + rng.uniform(0.0, 0.08, size=(600, 3)), h / 4, 1000.0, model, dim=3))
+    parts = np.concatenate(parts)
+    parts["velocity"][:, :3] = rng.normal(scale=0.3, size=(len(parts), 3)).astype(np.float32)
+    floor = RigidBody(("cuboid", (4.0, 4 * h, 4.0)), translation=(0.5, 0.05 - 4 * h, 0.5))
+    return scenes.Scene("mixed_models", 3, h, SimulationParams((0.0, -9.81, 0.0), 1e-4), parts, [floor], 10, 4096)
+
+
+def test_mixed_model_scene_in_batch(cuda_lib):
+    """A mixed-model scene beside one-model scenes (four G2P launches side
+    by side): its bits equal the same scene alone in a batch, and it agrees
+    with its own single-scene context to FP32 summation order."""
+    mixed = mixed_model_scene()
+    alone = new_batch()
+    s0 = alone.add(mixed)
+    alone.step(8)
+    ref = alone.download_particles(s0)
+    alone.close()
+    mix = new_batch()
+    others = mix_scenes()
+    mix.add(others[0])
+    sm = mix.add(mixed)
+    mix.add(others[1])
+    mix.add(others[2])
+    mix.step(8)
+    got = mix.download_particles(sm)
+    mix.close()
+    assert got.tobytes() == ref.tobytes()
+    data = scenes.build_mpm_data(mixed)
+    MpmPipeline().launch_step(data, 8)
+    single = data.download_particles()
+    data.close()
+    # the context sums each P2G block in a different (fixed) grouping; over
+    # 8 substeps of five models the velocities drift to the single-substep
+    # parity bound (1e-4 of the scale, plus 2e-6), the other fields stay within
+    # the batch-of-one bound
+    for k, v in fields(single).items():
+        loose = k in ("velocity", "affine")
+        close(f"mixed-model batch vs context {k}", got[k], v, 2e-6 if loose else 1e-6, 1e-4 if loose else 1e-5)
+
+
 def test_batch_errors_reported(cuda_lib):
     b = new_batch(max_particles=5000, max_scenes=2)
     sc = scenes.random_scene_3d(4000, "fluid", 1 / 64, seed=31)
