@@ -124,16 +124,20 @@ uint32_t batch_graph_flags(const slosh_batch *b) {
 // x / h as the exact x * (1/h) of each scene.
 template <int D, int NT, int MODEL> void launch_batch_g2p_model(slosh_batch *b, const DevScene &s, cudaStream_t st) {
     const uint32_t g = std::min<uint32_t>(b->c.cap, (uint32_t)b->c.sm_count * b->tune.g2p_ctas_per_sm);
-    if (b->all_pow2) k_g2p_update<D, NT, true, true, MODEL><<<g, NT, 0, st>>>(s);
-    else k_g2p_update<D, NT, true, false, MODEL><<<g, NT, 0, st>>>(s);
+    if (b->all_pow2) launch_k(&b->c, g, NT, 0, st, k_g2p_update<D, NT, true, true, MODEL>, s);
+    else launch_k(&b->c, g, NT, 0, st, k_g2p_update<D, NT, true, false, MODEL>, s);
 }
 
 // One G2P launch per class of scene present, each compiled for its model
 // (the first one also clears the next substep's map).  The launches after
-// the first run side by side with it on side streams, so that one class's
-// last blocks overlap the others' instead of each launch draining alone.
+// the first run side by side with it on side streams, forked before the
+// first, so that one class's last blocks overlap the others' instead of
+// each launch draining alone.  The classes' blocks, and so their particles,
+// are disjoint, and the map the first launch clears is the next substep's.
 template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s, cudaStream_t st) {
+    slosh_ctx *c = &b->c;
     const uint32_t mask = g2p_class_mask(b);
+    if (mask & (mask - 1u)) cudaEventRecord(b->g2p_fork, st);  // two classes or more
     uint32_t n = 0, side = 0;
     for (uint32_t cls = 0; cls < G2P_CLASSES; ++cls) {
         if (!(mask >> cls & 1u)) continue;
@@ -142,9 +146,9 @@ template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s
         sc.clear_tail = n == 0 ? s.clear_tail : 0u;
         cudaStream_t ls = st;
         if (n > 0) {
-            if (side == 0) cudaEventRecord(b->g2p_fork, st);
             ls = b->g2p_side[side];
             cudaStreamWaitEvent(ls, b->g2p_fork, 0);
+            c->pdl_link = false;  // a side stream's first kernel: a plain edge
         }
         if (cls == 0) launch_batch_g2p_model<D, NT, SLOSH_MODEL_SAND_LINEAR>(b, sc, ls);
         else if (cls == 1) launch_batch_g2p_model<D, NT, SLOSH_MODEL_ELASTIC_LINEAR>(b, sc, ls);
@@ -154,6 +158,7 @@ template <int D, int NT> void launch_batch_g2p(slosh_batch *b, const DevScene &s
         ++n;
     }
     for (uint32_t k = 0; k < side; ++k) cudaStreamWaitEvent(st, b->g2p_join[k], 0);
+    if (side) c->pdl_link = false;  // the kernel after the join waits on several
     if (n == 0) launch_batch_g2p_model<D, NT, -1>(b, s, st);  // no scene: the map is still cleared
 }
 
@@ -207,24 +212,24 @@ template <int D> void enqueue_batch_substep(slosh_batch *b, cudaStream_t st, uin
         return;
     }
     const uint32_t sm = (uint32_t)c->sm_count;
-    k_touch<D, true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
-    k_neighbors<D, true><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
-    k_scene_scan<1024><<<1, 1024, 0, st>>>(s);
-    k_scene_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
-    k_scene_rank<<<grid_for(2ull * c->cap * RANK_LANES, 256, sm * 16), 256, 0, st>>>(s);
-    k_block_setup<D, true><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
-    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
-    k_scatter<true><<<grid_for(c->max_n, 256, sm * 16), 256, 0, st>>>(s);
-    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    launch_k(c, grid_for(c->max_n, 256, sm * 16), 256, 0, st, k_touch<D, true>, s);
+    launch_k(c, grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st, k_neighbors<D, true>, s);
+    launch_k(c, 1, 1024, 0, st, k_scene_scan<1024>, s);
+    launch_k(c, grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st, k_scene_scatter, s);
+    launch_k(c, grid_for(2ull * c->cap * RANK_LANES, 256, sm * 16), 256, 0, st, k_scene_rank, s);
+    launch_k(c, grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st, k_block_setup<D, true>, s);
+    launch_k(c, 1, 1024, 0, st, k_block_scan<1024>, s);
+    launch_k(c, grid_for(c->max_n, 256, sm * 16), 256, 0, st, k_scatter<true>, s);
+    launch_k(c, grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st, k_canon, s);
     const uint32_t p2g_grid = std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, sm * b->tune.p2g_ctas_per_sm);
-    if (b->tune.p2g_stages == 2) k_p2g<D, true, false, 2><<<p2g_grid, 32 * P2G_WARPS, 0, st>>>(s);
-    else if (b->tune.p2g_stages == 4) k_p2g<D, true, false, 4><<<p2g_grid, 32 * P2G_WARPS, 0, st>>>(s);
-    else k_p2g<D, true><<<p2g_grid, 32 * P2G_WARPS, 0, st>>>(s);
-    k_grid_update<D, true><<<grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st>>>(s);
+    if (b->tune.p2g_stages == 2) launch_k(c, p2g_grid, 32 * P2G_WARPS, 0, st, k_p2g<D, true, false, 2>, s);
+    else if (b->tune.p2g_stages == 4) launch_k(c, p2g_grid, 32 * P2G_WARPS, 0, st, k_p2g<D, true, false, 4>, s);
+    else launch_k(c, p2g_grid, 32 * P2G_WARPS, 0, st, k_p2g<D, true>, s);
+    launch_k(c, grid_for((uint64_t)c->cap * 64, 256, sm * 16), 256, 0, st, k_grid_update<D, true>, s);
     if (b->tune.g2p_threads == 64) launch_batch_g2p<D, 64>(b, s, st);
     else if (b->tune.g2p_threads == 256) launch_batch_g2p<D, 256>(b, s, st);
     else launch_batch_g2p<D, 128>(b, s, st);
-    k_rigid<D, true><<<std::max<uint32_t>(1, (b->max_bodies + 127) / 128), 128, 0, st>>>(s);
+    launch_k(c, std::max<uint32_t>(1, (b->max_bodies + 127) / 128), 128, 0, st, k_rigid<D, true>, s);
 }
 
 void enqueue_batch_substep_any(slosh_batch *b, cudaStream_t st, uint32_t parity) {
@@ -246,7 +251,10 @@ int build_batch_graphs(slosh_batch *b) {
     destroy_batch_graphs(b);
     for (uint32_t par = 0; par < 2; ++par) {
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->pdl_capture = c->pdl;
+        c->pdl_link = false;
         enqueue_batch_substep_any(b, c->stream, par);
+        c->pdl_capture = false;
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         if (e == cudaSuccess) {
@@ -260,6 +268,12 @@ int build_batch_graphs(slosh_batch *b) {
             destroy_batch_graphs(b);
             b->fused_direct = true;
             return SLOSH_OK;
+        }
+        if (e != cudaSuccess && c->pdl) {
+            // a runtime that refuses the programmatic edges: plain ones
+            cudaGetLastError();
+            c->pdl = false;
+            return build_batch_graphs(b);
         }
         if (e != cudaSuccess) return fail(c, SLOSH_E_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
     }
@@ -347,6 +361,7 @@ int slosh_batch_create(const slosh_batch_config *cfg, slosh_batch **out) {
     c->device = cfg->device;
     b->max_scenes = cfg->max_scenes;
     b->max_bodies = std::max<uint32_t>(cfg->max_bodies, 1u);
+    if (const char *pdl = std::getenv("SLOSH_PDL")) b->c.pdl = std::strcmp(pdl, "0") != 0;
     if (const char *bt = std::getenv("SLOSH_FUSED_BARRIER_TEST")) {
         unsigned extra = 0;
         unsigned long long ns = 0;

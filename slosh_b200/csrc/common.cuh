@@ -339,4 +339,18 @@ struct Cta {
 };
 __device__ __forceinline__ Cta launch_cta() { return Cta{blockIdx.x, gridDim.x}; }
 
+// Programmatic dependent launch.  A kernel of the substep graph that was
+// launched with cudaLaunchAttributeProgrammaticStreamSerialization may be
+// scheduled while the kernel before it in the stream still runs; it waits
+// here, before its first memory access, until that kernel has completed and
+// its writes are visible, then lets its own successor be scheduled.  Every
+// stand-alone kernel of the substep enters this way, also those that read
+// nothing of their predecessor's output, so that a kernel's completion
+// implies the completion of all kernels before it.  Launched without the
+// attribute, both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace slosh

@@ -132,6 +132,7 @@ template <int D> __device__ __forceinline__ uint32_t cell_index(const int *a) {
 // k_block_setup after they are read; after a substep that raised an error
 // (blocks left without a rank keep their counts) they are all cleared here.
 template <bool B = false> __global__ void k_clear(DevScene s) {
+    pdl_enter();
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = tid; i < s.hcap; i += stride) {
@@ -230,7 +231,7 @@ template <int D, bool B = false> __device__ __forceinline__ void touch_body(cons
         s.pslot[i] = bin;
     }
 }
-template <int D, bool B = false> __global__ void k_touch(DevScene s) { touch_body<D, B>(s, launch_cta()); }
+template <int D, bool B = false> __global__ void k_touch(DevScene s) { pdl_enter(); touch_body<D, B>(s, launch_cta()); }
 
 // Activates the +1 neighbours of every primary block, one thread per
 // (block, neighbour).  Replaces touch_neighbor_blocks (sort.slang:75-92).
@@ -277,7 +278,7 @@ template <int D, bool B = false> __device__ __forceinline__ void neighbors_body(
         }
     }
 }
-template <int D, bool B = false> __global__ void k_neighbors(DevScene s) { neighbors_body<D, B>(s, launch_cta()); }
+template <int D, bool B = false> __global__ void k_neighbors(DevScene s) { pdl_enter(); neighbors_body<D, B>(s, launch_cta()); }
 
 // Block-wide exclusive scan of one value per thread (blockDim.x == NT,
 // NT <= 1024, a multiple of 32).  Writes the block total to *total.
@@ -394,6 +395,7 @@ template <int NT> __device__ __forceinline__ uint32_t cta_scan_vec16(const uint3
 // scans bins [1024 c, 1024 c + 1024), one uint4 a thread, on top of the
 // coarse counts of the bins before them.
 template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) {
+    pdl_enter();
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     constexpr uint32_t PER = HIST_BINS / HIST_COARSE, NW = NT / 32;
     static_assert(PER == 4 * NT && HIST_COARSE <= 64, "one uint4 of bins a thread");
@@ -432,6 +434,7 @@ template <int NT> __global__ void __launch_bounds__(NT) k_hist_scan(DevScene s) 
 
 // Groups the appended block keys by their top 16 bits.
 __global__ void k_bin_scatter(DevScene s) {
+    pdl_enter();
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t n1 = min(s.ctr->n_primary, s.cap), n2 = min(s.ctr->n_extra, s.cap);
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -451,6 +454,7 @@ __global__ void k_bin_scatter(DevScene s) {
 // whole z slab of a compact scene, hundreds of keys).
 constexpr uint32_t RANK_LANES = 8;
 __global__ void k_rank(DevScene s) {
+    pdl_enter();
     if (build_skipped(s)) return;  // this substep keeps the previous grid
     const uint32_t total = min(s.ctr->n_primary, s.cap) + min(s.ctr->n_extra, s.cap);
     const uint32_t g = threadIdx.x % RANK_LANES;
@@ -489,7 +493,7 @@ template <int NT> __device__ __forceinline__ void scene_scan_body(const DevScene
         s.ctr->n_blocks = min(total, s.cap);
     }
 }
-template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s) { scene_scan_body<NT>(s); }
+template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s) { pdl_enter(); scene_scan_body<NT>(s); }
 
 // Groups the appended blocks by scene (unordered within a scene).
 __device__ __forceinline__ void scene_scatter_body(const DevScene &s, Cta g) {
@@ -506,7 +510,7 @@ __device__ __forceinline__ void scene_scatter_body(const DevScene &s, Cta g) {
         }
     }
 }
-__global__ void k_scene_scatter(DevScene s) { scene_scatter_body(s, launch_cta()); }
+__global__ void k_scene_scatter(DevScene s) { pdl_enter(); scene_scatter_body(s, launch_cta()); }
 
 // Scenes beyond this many active blocks raise ERR_SCENE_BLOCKS (a scene of
 // about 7 M particles; larger ones belong in a context of their own).
@@ -545,7 +549,7 @@ __device__ __forceinline__ void scene_rank_body(const DevScene &s, Cta g) {
         }
     }
 }
-__global__ void k_scene_rank(DevScene s) { scene_rank_body(s, launch_cta()); }
+__global__ void k_scene_rank(DevScene s) { pdl_enter(); scene_rank_body(s, launch_cta()); }
 
 // One warp per block: per-cell counts (cleared in the hash-slot array once
 // read) with their in-block exclusive scan, the block total, the cells in
@@ -633,7 +637,7 @@ template <int D, bool B = false> __device__ __forceinline__ void block_setup_bod
         }
     }
 }
-template <int D, bool B = false> __global__ void k_block_setup(DevScene s) { block_setup_body<D, B>(s, launch_cta()); }
+template <int D, bool B = false> __global__ void k_block_setup(DevScene s) { pdl_enter(); block_setup_body<D, B>(s, launch_cta()); }
 
 // Exclusive scan of the per-block primary totals into first_particle
 // (copy_particles_len_to_scan_value + prefix_sum +
@@ -664,7 +668,7 @@ template <int NT> __device__ __forceinline__ void block_scan_body(const DevScene
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < nb; r += NT) s.qorder[atomicAdd(&cnt[min(s.bnp[r] >> 3, 63u)], 1u)] = r;
 }
-template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) { block_scan_body<NT>(s); }
+template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) { pdl_enter(); block_scan_body<NT>(s); }
 
 // Per particle: claim its slot in the block's cell range (the primary part
 // of finalize_particles_sort, sort.slang:304-357), warp-aggregated.
@@ -728,7 +732,7 @@ template <bool B = false> __device__ __forceinline__ void scatter_body(const Dev
         }
     }
 }
-template <bool B = false> __global__ void k_scatter(DevScene s) { scatter_body<B>(s, launch_cta()); }
+template <bool B = false> __global__ void k_scatter(DevScene s) { pdl_enter(); scatter_body<B>(s, launch_cta()); }
 
 // Canonical order inside each (block, cell) range of the permutation:
 // ascending original id.  k_scatter stores beside every permutation entry
@@ -818,6 +822,6 @@ __device__ __forceinline__ void canon_body(const DevScene &s, Cta g) {
         }
     }
 }
-__global__ void k_canon(DevScene s) { canon_body(s, launch_cta()); }
+__global__ void k_canon(DevScene s) { pdl_enter(); canon_body(s, launch_cta()); }
 
 }  // namespace slosh

@@ -60,6 +60,7 @@ constexpr uint32_t REUSE_MAX_CTAS = 4096;
 // last CTA also reads the decision and, inside the substep graph, sets the
 // conditional node that picks the full build or the reuse.
 template <int D> __global__ void k_grid_reuse(DevScene s) {
+    pdl_enter();
     __shared__ uint32_t cta_total;
     __shared__ bool last;
     const uint32_t nbp = min(s.ctr->last_n_blocks, s.cap);
@@ -292,6 +293,7 @@ __device__ uint32_t gather_touched_cell(const DevScene &s, uint32_t r, uint32_t 
 // k_reuse_cells; the previous map becomes this substep's; the transfer
 // kernels' block queues restart.
 template <int D> __global__ void k_reuse_perm(DevScene s) {
+    pdl_enter();
     if (s.ctr->rebuild[s.par]) return;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     for (uint32_t q = tid; q < s.hcap; q += stride) {
@@ -351,6 +353,7 @@ template <int D> __global__ void k_reuse_perm(DevScene s) {
 // The touched cells of a kept grid, one warp each (their gathers are chains
 // of dependent loads, so they run side by side rather than block by block).
 template <int D> __global__ void k_reuse_cells(DevScene s) {
+    pdl_enter();
     if (s.ctr->rebuild[s.par]) return;
     const uint32_t nt = s.ctr->n_touched;
     const uint32_t lane = lane_id();

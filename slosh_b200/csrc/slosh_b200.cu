@@ -77,6 +77,10 @@ struct slosh_ctx {
     // shared-memory and global float atomics, kept for A/B comparison.
     int p2g_variant = 0;
     uint32_t g2p_threads = 0;  // G2P CTA size, 0: chosen by the scene size (SLOSH_G2P_THREADS)
+    // Programmatic dependent launch inside the substep graphs (SLOSH_PDL=0
+    // turns it off).  pdl_capture: a substep graph is being captured;
+    // pdl_link: the previous operation captured on the stream is a kernel.
+    bool pdl = true, pdl_capture = false, pdl_link = false;
     uint32_t *pslot = nullptr, *perm = nullptr;
     unsigned long long *skey = nullptr;
     float4 *nodes = nullptr, *partial = nullptr, *coll[2] = {nullptr, nullptr};
@@ -126,6 +130,30 @@ int fail(slosh_ctx *c, int code, const char *fmt, ...) {
         cudaError_t e_ = (call);                                                                  \
         if (e_ != cudaSuccess) return fail(c, SLOSH_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
+
+// Launches one kernel of the substep.  While a substep graph is captured and
+// the previous operation captured on the stream is a kernel, the launch
+// carries cudaLaunchAttributeProgrammaticStreamSerialization: the graph edge
+// between the two becomes programmatic, and the kernel's CTAs are scheduled
+// once all of its predecessor's CTAs have started, instead of after the
+// predecessor has drained and the graph has processed its completion.  The
+// kernel itself waits in pdl_enter() for that completion, so the results are
+// the same bits.
+template <typename... P, typename... A>
+void launch_k(slosh_ctx *c, uint32_t grid, uint32_t block, size_t smem, cudaStream_t st, void (*k)(P...), A... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = c->pdl_capture && c->pdl_link ? 1u : 0u;
+    cudaLaunchKernelEx(&cfg, k, args...);
+    c->pdl_link = c->pdl_capture;
+}
 
 template <typename T> int dalloc(slosh_ctx *c, T **p, size_t count) {
     void *q = nullptr;
@@ -320,28 +348,28 @@ struct Prof {
 template <int D> void enqueue_build_front(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     const uint32_t sm = (uint32_t)c->sm_count;
     PROF_BEGIN(1);
-    k_touch<D><<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // one wave of warps, a chunk each
+    launch_k(c, grid_for(c->n, 256, sm * 8), 256, 0, st, k_touch<D>, s);  // one wave of warps, a chunk each
     PROF_END(1);
     PROF_BEGIN(2);
-    k_neighbors<D><<<grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st>>>(s);
+    launch_k(c, grid_for((uint64_t)c->cap * (Geo<D>::NASSOC - 1), 256, sm * 8), 256, 0, st, k_neighbors<D>, s);
     PROF_END(2);
     PROF_BEGIN(3);
-    k_hist_scan<256><<<HIST_COARSE, 256, 0, st>>>(s);
+    launch_k(c, HIST_COARSE, 256, 0, st, k_hist_scan<256>, s);
     PROF_END(3);
     PROF_BEGIN(4);
-    k_bin_scatter<<<grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st>>>(s);
+    launch_k(c, grid_for(2ull * c->cap, 256, sm * 8), 256, 0, st, k_bin_scatter, s);
     PROF_END(4);
     PROF_BEGIN(5);
-    k_rank<<<grid_for(2ull * c->cap * RANK_LANES, 256, sm * 8), 256, 0, st>>>(s);
+    launch_k(c, grid_for(2ull * c->cap * RANK_LANES, 256, sm * 8), 256, 0, st, k_rank, s);
     PROF_END(5);
     PROF_BEGIN(6);
-    k_block_setup<D><<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    launch_k(c, grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st, k_block_setup<D>, s);
     PROF_END(6);
 }
 
 void enqueue_block_scan(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(7);
-    k_block_scan<1024><<<1, 1024, 0, st>>>(s);
+    launch_k(c, 1, 1024, 0, st, k_block_scan<1024>, s);
     PROF_END(7);
 }
 
@@ -349,10 +377,10 @@ void enqueue_block_scan(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
 // when the full build runs).
 template <int D> void enqueue_reuse_perm(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(8);
-    k_reuse_perm<D><<<grid_for((uint64_t)c->cap * 32, 256, (uint32_t)c->sm_count * 8), 256, 0, st>>>(s);
+    launch_k(c, grid_for((uint64_t)c->cap * 32, 256, (uint32_t)c->sm_count * 8), 256, 0, st, k_reuse_perm<D>, s);
     PROF_END(8);
     PROF_BEGIN(9);
-    k_reuse_cells<D><<<(uint32_t)c->sm_count * 8, 256, 0, st>>>(s);
+    launch_k(c, (uint32_t)c->sm_count * 8, 256, 0, st, k_reuse_cells<D>, s);
     PROF_END(9);
 }
 
@@ -360,10 +388,10 @@ template <int D> void enqueue_reuse_perm(slosh_ctx *c, const DevScene &s, cudaSt
 void enqueue_build_back(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     const uint32_t sm = (uint32_t)c->sm_count;
     PROF_BEGIN(10);
-    k_scatter<<<grid_for(c->n, 256, sm * 8), 256, 0, st>>>(s);  // longer chunks: fewer cells split for k_canon
+    launch_k(c, grid_for(c->n, 256, sm * 8), 256, 0, st, k_scatter<false>, s);  // longer chunks: fewer cells split for k_canon
     PROF_END(10);
     PROF_BEGIN(11);
-    k_canon<<<grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st>>>(s);
+    launch_k(c, grid_for((uint64_t)c->cap * 32, 256, sm * 16), 256, 0, st, k_canon, s);
     PROF_END(11);
 }
 
@@ -371,7 +399,7 @@ void enqueue_build_back(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *
 template <int D> void enqueue_reuse_decision(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p) {
     PROF_BEGIN(0);
     const uint32_t ctas = std::min<uint32_t>((uint32_t)c->sm_count * 8, REUSE_MAX_CTAS);
-    k_grid_reuse<D><<<grid_for((uint64_t)c->cap * 32, 256, ctas), 256, 0, st>>>(s);
+    launch_k(c, grid_for((uint64_t)c->cap * 32, 256, ctas), 256, 0, st, k_grid_reuse<D>, s);
     PROF_END(0);
 }
 
@@ -380,7 +408,7 @@ template <int D> void enqueue_reuse_decision(slosh_ctx *c, const DevScene &s, cu
 // substep's decision selects them; standalone builds run with reuse off.
 template <int D>
 void enqueue_grid_build(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr, bool standalone = false) {
-    if (standalone) k_clear<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
+    if (standalone) launch_k(c, (uint32_t)c->sm_count * 4, 256, 0, st, k_clear<false>, s);
     enqueue_build_front<D>(c, s, st, p);
     enqueue_block_scan(c, s, st, p);
     if (s.reuse) enqueue_reuse_perm<D>(c, s, st, p);
@@ -391,18 +419,18 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
     PROF_BEGIN(12);
     if (c->p2g_variant == 3) {
         const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 8);
-        k_p2g_atomic<D><<<g, P2G_ATOMIC_THREADS, 0, st>>>(s);
+        launch_k(c, g, P2G_ATOMIC_THREADS, 0, st, k_p2g_atomic<D>, s);
     } else {
         if (c->n < P2G_WIDE_PARTICLES) {
             // a small scene: CTAs of six warps, one pass of a shared block each
             const uint32_t g = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * 3);
             constexpr size_t smem = sizeof(P2gSmem<D, 3, P2G_WIDE_WARPS>);
-            if (s.force_pending) k_p2g_wide<D, true><<<g, 32 * P2G_WIDE_WARPS, smem, st>>>(s);
-            else k_p2g_wide<D, false><<<g, 32 * P2G_WIDE_WARPS, smem, st>>>(s);
+            if (s.force_pending) launch_k(c, g, 32 * P2G_WIDE_WARPS, smem, st, k_p2g_wide<D, true>, s);
+            else launch_k(c, g, 32 * P2G_WIDE_WARPS, smem, st, k_p2g_wide<D, false>, s);
         } else {
             const uint32_t g = std::min<uint32_t>((c->cap + P2G_WARPS - 1) / P2G_WARPS, (uint32_t)c->sm_count * 5);
-            if (s.force_pending) k_p2g<D, false, true><<<g, 32 * P2G_WARPS, 0, st>>>(s);
-            else k_p2g<D><<<g, 32 * P2G_WARPS, 0, st>>>(s);
+            if (s.force_pending) launch_k(c, g, 32 * P2G_WARPS, 0, st, k_p2g<D, false, true>, s);
+            else launch_k(c, g, 32 * P2G_WARPS, 0, st, k_p2g<D>, s);
         }
     }
     PROF_END(12);
@@ -410,14 +438,14 @@ template <int D> void enqueue_p2g(slosh_ctx *c, const DevScene &s, cudaStream_t 
 
 template <int D> void enqueue_grid_update(slosh_ctx *c, const DevScene &s, cudaStream_t st, Prof *p = nullptr) {
     PROF_BEGIN(13);
-    k_grid_update<D><<<grid_for((uint64_t)c->cap * 64, 256, (uint32_t)c->sm_count * 16), 256, 0, st>>>(s);
+    launch_k(c, grid_for((uint64_t)c->cap * 64, 256, (uint32_t)c->sm_count * 16), 256, 0, st, k_grid_update<D>, s);
     PROF_END(13);
 }
 
 // Restores the cleared state a debug build consumed, so that the next real
 // substep starts from a cleared hash map and counters.
 void enqueue_clear(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
-    k_clear<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
+    launch_k(c, (uint32_t)c->sm_count * 4, 256, 0, st, k_clear<false>, s);
 }
 
 // P2G, grid update, fused G2P/update and the rigid update.
@@ -425,14 +453,14 @@ void enqueue_clear(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
 // single model among the linear elastic, sand and fluid ones.
 template <int D, int NT> void launch_g2p(slosh_ctx *c, const DevScene &s, cudaStream_t st) {
     const uint32_t g2p_grid = std::min<uint32_t>(c->cap, (uint32_t)c->sm_count * (512u / NT));
-    if (!s.h_pow2) k_g2p_update<D, NT, false, false><<<g2p_grid, NT, 0, st>>>(s);
+    if (!s.h_pow2) launch_k(c, g2p_grid, NT, 0, st, k_g2p_update<D, NT, false, false>, s);
     else if (c->model_mask == 1u << SLOSH_MODEL_SAND_LINEAR)
-        k_g2p_update<D, NT, false, true, SLOSH_MODEL_SAND_LINEAR><<<g2p_grid, NT, 0, st>>>(s);
+        launch_k(c, g2p_grid, NT, 0, st, k_g2p_update<D, NT, false, true, SLOSH_MODEL_SAND_LINEAR>, s);
     else if (c->model_mask == 1u << SLOSH_MODEL_ELASTIC_LINEAR)
-        k_g2p_update<D, NT, false, true, SLOSH_MODEL_ELASTIC_LINEAR><<<g2p_grid, NT, 0, st>>>(s);
+        launch_k(c, g2p_grid, NT, 0, st, k_g2p_update<D, NT, false, true, SLOSH_MODEL_ELASTIC_LINEAR>, s);
     else if (c->model_mask == 1u << SLOSH_MODEL_FLUID_TAIT)
-        k_g2p_update<D, NT, false, true, SLOSH_MODEL_FLUID_TAIT><<<g2p_grid, NT, 0, st>>>(s);
-    else k_g2p_update<D, NT, false, true><<<g2p_grid, NT, 0, st>>>(s);
+        launch_k(c, g2p_grid, NT, 0, st, k_g2p_update<D, NT, false, true, SLOSH_MODEL_FLUID_TAIT>, s);
+    else launch_k(c, g2p_grid, NT, 0, st, k_g2p_update<D, NT, false, true>, s);
 }
 
 // Persistent CTAs taking blocks from the queue.  A large scene runs 8 CTAs
@@ -455,7 +483,7 @@ template <int D> void enqueue_transfer(slosh_ctx *c, const DevScene &s, cudaStre
     enqueue_grid_update<D>(c, s, st, p);
     enqueue_g2p<D>(c, s, st, p);
     PROF_BEGIN(15);
-    k_rigid<D><<<1, 32, 0, st>>>(s);
+    launch_k(c, 1, 32, 0, st, k_rigid<D>, s);
     PROF_END(15);
 }
 
@@ -521,7 +549,7 @@ template <int D> int enqueue_substep_hooked(slosh_ctx *c, cudaStream_t st, uint3
     // untouched, and the grid state is reset so that the substep can run
     // again from a full build.
     auto drop = [&](int code) {
-        k_clear<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
+        launch_k(c, (uint32_t)c->sm_count * 4, 256, 0, st, k_clear<false>, s);
         force_grid_rebuild(c, st);
         return code;
     };
@@ -553,14 +581,14 @@ template <int D> int enqueue_substep_hooked(slosh_ctx *c, cudaStream_t st, uint3
     if (r < 0) return drop(r);
     if (r == 1) {
         // a replaced update records no cell changes: the next substep rebuilds
-        k_after_replaced_g2p<<<(uint32_t)c->sm_count * 4, 256, 0, st>>>(s);
+        launch_k(c, (uint32_t)c->sm_count * 4, 256, 0, st, k_after_replaced_g2p, s);
         if (c->reuse && cudaMemsetAsync(&c->ctr->rebuild[s.par ^ 1u], 1, 4, st) != cudaSuccess) return SLOSH_E_CUDA;
     } else {
         enqueue_g2p<D>(c, s, st, nullptr);
     }
     if ((r = call_hook(c, s, SLOSH_HOOK_AFTER_G2P, st)) < 0) return drop(r);
     if ((r = call_hook(c, s, SLOSH_HOOK_AFTER_PARTICLES_UPDATE, st)) < 0) return drop(r);
-    k_rigid<D><<<1, 32, 0, st>>>(s);
+    launch_k(c, 1, 32, 0, st, k_rigid<D>, s);
     return cudaGetLastError() == cudaSuccess ? SLOSH_OK : SLOSH_E_CUDA;
 }
 
@@ -599,6 +627,7 @@ template <int D> cudaError_t capture_conditional(slosh_ctx *c, uint32_t par, cud
     s.use_cond = 1u;
     // the decision
     if ((e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode)) != cudaSuccess) return bail(e);
+    c->pdl_link = false;
     enqueue_reuse_decision<D>(c, s, st, nullptr);
     cudaStreamCaptureStatus cs;
     const cudaGraphNode_t *deps = nullptr;
@@ -620,22 +649,25 @@ template <int D> cudaError_t capture_conditional(slosh_ctx *c, uint32_t par, cud
     if ((e = cudaGraphAddNode(&cnode, g, &decision, 1, &cp)) != cudaSuccess) return bail(e);
     cudaGraph_t full = cp.conditional.phGraph_out[0], reuse = cp.conditional.phGraph_out[1];
     if ((e = cudaStreamBeginCaptureToGraph(st, full, nullptr, nullptr, 0, mode)) != cudaSuccess) return bail(e);
+    c->pdl_link = false;
     enqueue_build_front<D>(c, s, st, nullptr);
     enqueue_block_scan(c, s, st, nullptr);
     enqueue_build_back(c, s, st, nullptr);
     if ((e = cudaStreamEndCapture(st, &full)) != cudaSuccess) return bail(e);
     if ((e = cudaStreamBeginCaptureToGraph(st, reuse, nullptr, nullptr, 0, mode)) != cudaSuccess) return bail(e);
+    c->pdl_link = false;
     enqueue_reuse_perm<D>(c, s, st, nullptr);
     if ((e = cudaStreamEndCapture(st, &reuse)) != cudaSuccess) return bail(e);
     // the transfer kernels after either branch
     if ((e = cudaStreamBeginCaptureToGraph(st, g, &cnode, nullptr, 1, mode)) != cudaSuccess) return bail(e);
+    c->pdl_link = false;  // after the conditional node
     enqueue_transfer<D>(c, s, st, nullptr);
     if ((e = cudaStreamEndCapture(st, &captured)) != cudaSuccess) return bail(e);
     *out = g;
     return cudaSuccess;
 }
 
-int build_graphs(slosh_ctx *c) {
+int build_graphs_once(slosh_ctx *c) {
     destroy_graphs(c);
     c->cond_graphs = false;
     if (c->reuse) {
@@ -659,6 +691,7 @@ int build_graphs(slosh_ctx *c) {
     }
     for (uint32_t par = 0; par < 2; ++par) {
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->pdl_link = false;
         enqueue_substep_any(c, c->stream, par, false);
         cudaGraph_t g = nullptr;
         CK(cudaStreamEndCapture(c->stream, &g));
@@ -668,6 +701,25 @@ int build_graphs(slosh_ctx *c) {
     }
     c->graphs_valid = true;
     return SLOSH_OK;
+}
+
+// The substep graphs, with programmatic edges between consecutive kernels
+// unless SLOSH_PDL=0; a runtime that refuses those captures gets the graphs
+// with plain edges.
+int build_graphs(slosh_ctx *c) {
+    c->pdl_capture = c->pdl;
+    int r = build_graphs_once(c);
+    // a grid-reusing scene prefers the conditional graph with plain edges to
+    // the unconditional one with programmatic edges
+    if (c->pdl && (r != SLOSH_OK || (c->reuse && !c->cond_graphs))) {
+        cudaGetLastError();
+        c->pdl = false;
+        c->pdl_capture = false;
+        r = build_graphs_once(c);
+    }
+    c->pdl_capture = false;
+    c->pdl_link = false;
+    return r;
 }
 
 int check_device_error(slosh_ctx *c) {
@@ -867,6 +919,7 @@ int slosh_ctx_create(const slosh_config *cfg, slosh_ctx **out) {
                          (int)sizeof(P2gSmem<2, 3, P2G_WIDE_WARPS>));
     cudaFuncSetAttribute(k_p2g_wide<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(P2gSmem<2, 3, P2G_WIDE_WARPS>));
+    if (const char *pdl = std::getenv("SLOSH_PDL")) c->pdl = std::strcmp(pdl, "0") != 0;
     c->reuse_mode = 2u;
     if (const char *r = std::getenv("SLOSH_GRID_REUSE")) c->reuse_mode = std::strcmp(r, "0") == 0 ? 0u : 1u;
     update_reuse(c);

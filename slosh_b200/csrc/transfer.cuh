@@ -401,6 +401,7 @@ __device__ __forceinline__ void p2g_body(const DevScene &s, P2gSmem<D, NBUF, W> 
 }
 template <int D, bool B = false, bool FORCE = false, int NBUF = 3>
 __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
+    pdl_enter();
     __shared__ P2gSmem<D, NBUF> sm;
     p2g_body<D, B, FORCE, NBUF>(s, sm);
 }
@@ -411,6 +412,7 @@ __global__ void __launch_bounds__(32 * P2G_WARPS, 5) k_p2g(DevScene s) {
 constexpr int P2G_WIDE_WARPS = 6;
 template <int D, bool FORCE>
 __global__ void __launch_bounds__(32 * P2G_WIDE_WARPS, 3) k_p2g_wide(DevScene s) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char psm[];
     p2g_body<D, false, FORCE, 3, P2G_WIDE_WARPS>(s, *reinterpret_cast<P2gSmem<D, 3, P2G_WIDE_WARPS> *>(psm));
 }
@@ -421,6 +423,7 @@ __global__ void __launch_bounds__(32 * P2G_WIDE_WARPS, 3) k_p2g_wide(DevScene s)
 // then 16-byte global atomics into the nodes.  Not bit-reproducible.
 constexpr int P2G_ATOMIC_THREADS = 192;
 template <int D> __global__ void __launch_bounds__(P2G_ATOMIC_THREADS, 4) k_p2g_atomic(DevScene s) {
+    pdl_enter();
     constexpr int TW = Geo<D>::TW, TILE = Geo<D>::TILE, BW = Geo<D>::BW;
     constexpr int NACC = (D == 3) ? 9 : 3;
     constexpr int NT = P2G_ATOMIC_THREADS;
@@ -998,6 +1001,7 @@ template <int D, bool B = false> __device__ __forceinline__ void grid_update_bod
     }
 }
 template <int D, bool B = false> __global__ void __launch_bounds__(256, 8) k_grid_update(DevScene s) {
+    pdl_enter();
     grid_update_body<D, B>(s, launch_cta());
 }
 
@@ -1025,6 +1029,7 @@ template <bool B> __device__ __forceinline__ void clear_next_map(const DevScene 
 // map cleared as G2P would, and the original-index plane of the next
 // storage taken from its flags plane.
 __global__ void k_after_replaced_g2p(DevScene s) {
+    pdl_enter();
     const uint32_t g0 = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
     clear_next_map<false>(s, g0, gs);
     for (uint32_t i = g0; i < s.count; i += gs) s.out_oid[i] = s.out_fo[i].y;
@@ -1440,6 +1445,7 @@ __device__ __forceinline__ void g2p_update_body(const DevScene &s, Cta g, G2pSme
 }
 template <int D, int NT, bool B = false, bool POW2 = false, int MODEL = -1>
 __global__ void __launch_bounds__(NT, 512 / NT) k_g2p_update(DevScene s) {
+    pdl_enter();
     __shared__ G2pSmem<D, NT> sm;
     g2p_update_body<D, NT, B, POW2, MODEL>(s, launch_cta(), sm);
 }
@@ -1552,6 +1558,6 @@ template <int D, bool B = false> __device__ __forceinline__ void rigid_body(cons
     for (int k = 0; k < D; ++k) b.linvel[k] = b.linvel[k] + grav[k] * ((b.inv_mass[k] != 0.f) ? 1.f : 0.f) * dt;
     s.bodies[id] = b;
 }
-template <int D, bool B = false> __global__ void k_rigid(DevScene s) { rigid_body<D, B>(s, blockIdx.x * blockDim.x + threadIdx.x); }
+template <int D, bool B = false> __global__ void k_rigid(DevScene s) { pdl_enter(); rigid_body<D, B>(s, blockIdx.x * blockDim.x + threadIdx.x); }
 
 }  // namespace slosh
