@@ -230,11 +230,12 @@ class ClockSampler:
 def timed_launches(data, st0: dict, st1: dict, steps: int):
     """Kernels launched by `steps` substeps between two stats snapshots, and
     how many of them kept their grid: with conditional graphs a substep that
-    keeps its grid launches 7 kernels, one that rebuilds it 14."""
+    keeps its grid launches 7 kernels fewer than one that rebuilds it."""
     reused = st1["n_grid_reuses"] - st0["n_grid_reuses"]
     rebuilt = st1["n_grid_rebuilds"] - st0["n_grid_rebuilds"]
+    full = data.kernels_per_substep
     if st1["conditional_graphs"]:
-        launches = 14 * rebuilt + 7 * reused
+        launches = full * rebuilt + (full - 7) * reused
     else:
         launches = data.kernels_per_substep * steps
     return launches, {"reused_substeps": reused, "rebuilt_substeps": rebuilt,
@@ -696,7 +697,7 @@ def batched_line(args, steps: int, warmup: int) -> dict:
             "api": "slosh_batch_add_scene x scenes + slosh_batch_step + slosh_batch_download_positions x scenes "
             "(host buffers, wall clock)",
         },
-        "gpu_launches": (1 if tuning["fused"] else 13) * steps,
+        "gpu_launches": (1 if tuning["fused"] else 12 + st["g2p_launches"]) * steps,
         "clocks": ck,
     }
     return line

@@ -329,10 +329,9 @@ int slosh_sync(slosh_ctx *ctx, void *stream);
 
 /* Number of device kernels a substep launches that runs the full grid
  * build (for launch accounting).  With grid reuse and conditional graphs a
- * substep that keeps the previous grid launches 7: the reuse decision, the
- * permutation update, the touched-cell gather, P2G, the grid update, G2P and
- * the rigid update
- * (slosh_get_stats counts both kinds of substep). */
+ * substep that keeps the previous grid launches 7 fewer: the reuse's
+ * permutation update and touched-cell gather instead of the 9 build
+ * kernels (slosh_get_stats counts both kinds of substep). */
 uint32_t slosh_kernels_per_substep(const slosh_ctx *ctx);
 
 /* Runs `n_substeps` substeps with direct launches (not the CUDA graph) and a
@@ -497,7 +496,9 @@ typedef struct slosh_batch_stats {
     uint32_t fused_graph;      /* 1: the fused kernel runs inside the substep
                                   graph; 0: launched directly (the runtime
                                   refused the capture) or not in use         */
-    uint32_t pad;
+    uint32_t g2p_launches;     /* G2P launches of a graph-form substep: one
+                                  per class of scene present (sand, linear
+                                  elastic, fluid, other), at least one       */
     slosh_tuning tuning;
 } slosh_batch_stats;
 

@@ -170,7 +170,7 @@ class SloshBatchStats(ctypes.Structure):
         ("n_svd_fp64", ctypes.c_uint32),
         ("n_bodies", ctypes.c_uint32),
         ("fused_graph", ctypes.c_uint32),
-        ("pad", ctypes.c_uint32),
+        ("g2p_launches", ctypes.c_uint32),
         ("tuning", SloshTuning),
     ]
 

@@ -139,6 +139,7 @@ class MpmBatch:
             "n_svd_fp64": st.n_svd_fp64,
             "n_bodies": st.n_bodies,
             "fused_graph": st.fused_graph,
+            "g2p_launches": st.g2p_launches,
             "tuning": {
                 "p2g_ctas_per_sm": st.tuning.p2g_ctas_per_sm,
                 "g2p_threads": st.tuning.g2p_threads,

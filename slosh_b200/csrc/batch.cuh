@@ -851,6 +851,7 @@ int slosh_batch_get_stats(slosh_batch *b, slosh_batch_stats *out) {
     out->n_svd_fp64 = ctr.n_svd_fp64;
     out->n_bodies = b->body_top;
     out->fused_graph = (b->tune.fused && b->graphs_valid && !b->fused_direct) ? 1u : 0u;
+    out->g2p_launches = std::max(__builtin_popcount(g2p_class_mask(b)), 1);
     out->tuning = b->tune;
     return SLOSH_OK;
 }

@@ -318,10 +318,6 @@ const char *const KERNEL_NAMES[N_KERNELS] = {
     "k_grid_reuse", "k_touch",      "k_neighbors",   "k_hist_scan", "k_bin_scatter", "k_rank",
     "k_block_setup", "k_block_scan", "k_reuse_perm", "k_reuse_cells", "k_scatter",   "k_canon",
     "k_p2g",        "k_grid_update", "k_g2p_update", "k_rigid"};
-// Kernels a substep launches through the conditional graph: the decision,
-// the transfer kernels and the rigid update, plus the full build (9) or the
-// reuse's permutation and touched cells (2).
-constexpr uint32_t KERNELS_FULL_BUILD = 14;
 
 // Optional per-kernel CUDA-event timing of the substep launches.
 struct Prof {
@@ -1303,8 +1299,12 @@ int slosh_sync(slosh_ctx *c, void *stream) {
 
 uint32_t slosh_kernels_per_substep(const slosh_ctx *c) {
     if (!c) return 0;
-    if (!c->reuse) return (uint32_t)N_KERNELS - 2u;
-    return c->cond_graphs ? KERNELS_FULL_BUILD : (uint32_t)N_KERNELS;
+    // the full build's 9 kernels, P2G, the grid update, G2P and the rigid
+    // update; with grid reuse the decision, and without conditional graphs
+    // also the two reuse kernels, which return at once in a full build
+    uint32_t k = 9u + 4u;
+    if (c->reuse) k += c->cond_graphs ? 1u : 3u;
+    return k;
 }
 
 int slosh_profile_substeps(slosh_ctx *c, uint32_t n_substeps, void *stream, float *kernel_ms, uint32_t cap,
