@@ -198,3 +198,16 @@ def test_environment_settings_documented():
     doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     missing = sorted(n for n in names if f"`{n}" not in doc)
     assert not missing, missing
+
+
+def test_bench_l2_note():
+    """bench.py states, per line, whether the particle storage its timed
+    substeps touch outgrows the L2 (no flush runs between substeps)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert bench.l2_note(62628 * bench.STORAGE_BYTES).startswith("inputs smaller than L2")  # dam break
+    assert bench.l2_note(4741888 * bench.STORAGE_BYTES).startswith("inputs larger than L2")  # sand column
+    assert "4.9 GB" in bench.l2_note(17607256 * bench.STORAGE_BYTES)  # 256-scene batch
