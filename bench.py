@@ -272,7 +272,7 @@ def workload_config(scene, extra=None):
         "particles": scene.n,
         "dim": 3,
         "material": "sand_linear (Drucker-Prager 30 deg, E=3.5e5, nu=0.3, rho=2200)",
-        "l2": "inputs larger than L2 (about 0.7 GB of particle state resident per GPU)",
+        "l2": l2_note(scene.n * STORAGE_BYTES),
         "parallelism": "independent replica per GPU",
     }
     if extra:

@@ -211,3 +211,5 @@ def test_bench_l2_note():
     assert bench.l2_note(62628 * bench.STORAGE_BYTES).startswith("inputs smaller than L2")  # dam break
     assert bench.l2_note(4741888 * bench.STORAGE_BYTES).startswith("inputs larger than L2")  # sand column
     assert "4.9 GB" in bench.l2_note(17607256 * bench.STORAGE_BYTES)  # 256-scene batch
+    cfg = bench.workload_config(scenes.sand_column_3d(h=1.0 / 64.0))
+    assert cfg["l2"].startswith("inputs smaller than L2")  # a reduced column: about 20 MB
