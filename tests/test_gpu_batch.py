@@ -221,6 +221,7 @@ def test_mixed_model_scene_in_batch(cuda_lib):
     alone = new_batch()
     s0 = alone.add(mixed)
     alone.step(8)
+    assert alone.stats()["g2p_launches"] == 1  # the launch compiled for every model
     ref = alone.download_particles(s0)
     alone.close()
     mix = new_batch()
@@ -230,6 +231,7 @@ def test_mixed_model_scene_in_batch(cuda_lib):
     mix.add(others[1])
     mix.add(others[2])
     mix.step(8)
+    assert mix.stats()["g2p_launches"] == 4  # sand, linear elastic, fluid, every model
     got = mix.download_particles(sm)
     mix.close()
     assert got.tobytes() == ref.tobytes()
