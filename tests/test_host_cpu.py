@@ -157,11 +157,12 @@ def _c_structs(src):
 
 
 def _rust_structs(md):
-    """#[repr(C)] structs of INTEGRATION.md's Rust binding block."""
-    block = md.split("## Rust binding", 1)[1].split("```rust", 1)[1].split("```", 1)[0]
+    """#[repr(C)] structs of INTEGRATION.md's Rust blocks."""
+    block = "\n".join(b.split("```", 1)[0] for b in md.split("```rust")[1:])
     block = re.sub(r"//[^\n]*", "", block)
     out = {}
     for name, body in re.findall(r"#\[repr\(C\)\][^{]*?pub struct (\w+)\s*\{(.*?)\}", block, re.S):
+        assert name not in out, name
         fields = []
         for m in re.finditer(r"(?:pub\s+)?(\w+)\s*:\s*(\[\s*\w+\s*;\s*\d+\s*\]|\w+)", body):
             ty = m.group(2).replace(" ", "")
@@ -177,9 +178,11 @@ def test_integration_rust_records_match_header():
     the library's exact layouts."""
     c = _c_structs(open(HEADER).read())
     rust = _rust_structs(open(os.path.join(ROOT, "INTEGRATION.md")).read())
-    c_to_rust = {"float": "f32", "uint32_t": "u32", "int32_t": "i32", "slosh_model": "SloshModel"}
+    c_to_rust = {"float": "f32", "uint32_t": "u32", "int32_t": "i32", "slosh_model": "SloshModel",
+                 "slosh_params": "SloshParams", "slosh_tuning": "SloshTuning"}
     pairs = {"SloshModel": "slosh_model", "SloshParticle": "slosh_particle", "SloshBody": "slosh_body",
-             "SloshConfig": "slosh_config", "SloshParams": "slosh_params"}
+             "SloshConfig": "slosh_config", "SloshParams": "slosh_params", "SloshBatchConfig": "slosh_batch_config",
+             "SloshSceneDesc": "slosh_scene_desc", "SloshTuning": "slosh_tuning", "SloshBatchStats": "slosh_batch_stats"}
     assert set(pairs) <= set(rust), sorted(rust)
     for rname, cname in pairs.items():
         want = [(f, c_to_rust[t], k) for f, t, k in c[cname]]
