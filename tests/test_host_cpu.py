@@ -178,11 +178,13 @@ def test_integration_rust_records_match_header():
     the library's exact layouts."""
     c = _c_structs(open(HEADER).read())
     rust = _rust_structs(open(os.path.join(ROOT, "INTEGRATION.md")).read())
-    c_to_rust = {"float": "f32", "uint32_t": "u32", "int32_t": "i32", "slosh_model": "SloshModel",
-                 "slosh_params": "SloshParams", "slosh_tuning": "SloshTuning"}
+    c_to_rust = {"float": "f32", "double": "f64", "uint32_t": "u32", "int32_t": "i32", "uint64_t": "u64",
+                 "slosh_model": "SloshModel", "slosh_params": "SloshParams", "slosh_tuning": "SloshTuning"}
     pairs = {"SloshModel": "slosh_model", "SloshParticle": "slosh_particle", "SloshBody": "slosh_body",
              "SloshConfig": "slosh_config", "SloshParams": "slosh_params", "SloshBatchConfig": "slosh_batch_config",
-             "SloshSceneDesc": "slosh_scene_desc", "SloshTuning": "slosh_tuning", "SloshBatchStats": "slosh_batch_stats"}
+             "SloshSceneDesc": "slosh_scene_desc", "SloshTuning": "slosh_tuning", "SloshBatchStats": "slosh_batch_stats",
+             "SloshServerConfig": "slosh_server_config", "SloshCompletion": "slosh_completion",
+             "SloshServerStats": "slosh_server_stats"}
     assert set(pairs) <= set(rust), sorted(rust)
     for rname, cname in pairs.items():
         want = [(f, c_to_rust[t], k) for f, t, k in c[cname]]
