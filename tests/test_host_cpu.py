@@ -184,7 +184,7 @@ def test_integration_rust_records_match_header():
              "SloshConfig": "slosh_config", "SloshParams": "slosh_params", "SloshBatchConfig": "slosh_batch_config",
              "SloshSceneDesc": "slosh_scene_desc", "SloshTuning": "slosh_tuning", "SloshBatchStats": "slosh_batch_stats",
              "SloshServerConfig": "slosh_server_config", "SloshCompletion": "slosh_completion",
-             "SloshServerStats": "slosh_server_stats"}
+             "SloshServerStats": "slosh_server_stats", "SloshStats": "slosh_stats"}
     assert set(pairs) <= set(rust), sorted(rust)
     for rname, cname in pairs.items():
         want = [(f, c_to_rust[t], k) for f, t, k in c[cname]]
@@ -218,3 +218,25 @@ def test_bench_l2_note():
     assert "4.9 GB" in bench.l2_note(17607256 * bench.STORAGE_BYTES)  # 256-scene batch
     cfg = bench.workload_config(scenes.sand_column_3d(h=1.0 / 64.0))
     assert cfg["l2"].startswith("inputs smaller than L2")  # a reduced column: about 20 MB
+
+
+def test_integration_rust_declares_every_export():
+    """INTEGRATION.md's Rust blocks declare every function the header
+    declares, each with the header's number of parameters."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    c_args = {}
+    for name, params in re.findall(r"^\s*(?:int|void|uint32_t)\s+\*?\s*(slosh_\w+)\s*\(([^)]*)\)\s*;", src, re.M):
+        params = params.strip()
+        c_args[name] = 0 if params in ("", "void") else params.count(",") + 1
+    assert set(c_args) == set(declared_functions())
+    md = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    rust = "\n".join(b.split("```", 1)[0] for b in md.split("```rust")[1:])
+    rust = re.sub(r"//[^\n]*", "", rust)
+    r_args = {}
+    for name, params in re.findall(r"pub fn (slosh_\w+)\s*\(([^)]*)\)", rust, re.S):
+        params = params.strip()
+        r_args[name] = 0 if not params else params.count(",") + 1
+    missing = sorted(set(c_args) - set(r_args))
+    assert not missing, missing
+    wrong = sorted(n for n in c_args if r_args[n] != c_args[n])
+    assert not wrong, [(n, c_args[n], r_args[n]) for n in wrong]
