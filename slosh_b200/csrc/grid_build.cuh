@@ -231,7 +231,10 @@ template <int D, bool B = false> __device__ __forceinline__ void touch_body(cons
         s.pslot[i] = bin;
     }
 }
-template <int D, bool B = false> __global__ void k_touch(DevScene s) { pdl_enter(); touch_body<D, B>(s, launch_cta()); }
+template <int D, bool B = false> __global__ void k_touch(DevScene s) {
+    pdl_enter();
+    touch_body<D, B>(s, launch_cta());
+}
 
 // Activates the +1 neighbours of every primary block, one thread per
 // (block, neighbour).  Replaces touch_neighbor_blocks (sort.slang:75-92).
@@ -278,7 +281,10 @@ template <int D, bool B = false> __device__ __forceinline__ void neighbors_body(
         }
     }
 }
-template <int D, bool B = false> __global__ void k_neighbors(DevScene s) { pdl_enter(); neighbors_body<D, B>(s, launch_cta()); }
+template <int D, bool B = false> __global__ void k_neighbors(DevScene s) {
+    pdl_enter();
+    neighbors_body<D, B>(s, launch_cta());
+}
 
 // Block-wide exclusive scan of one value per thread (blockDim.x == NT,
 // NT <= 1024, a multiple of 32).  Writes the block total to *total.
@@ -493,7 +499,10 @@ template <int NT> __device__ __forceinline__ void scene_scan_body(const DevScene
         s.ctr->n_blocks = min(total, s.cap);
     }
 }
-template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s) { pdl_enter(); scene_scan_body<NT>(s); }
+template <int NT> __global__ void __launch_bounds__(NT) k_scene_scan(DevScene s) {
+    pdl_enter();
+    scene_scan_body<NT>(s);
+}
 
 // Groups the appended blocks by scene (unordered within a scene).
 __device__ __forceinline__ void scene_scatter_body(const DevScene &s, Cta g) {
@@ -637,7 +646,10 @@ template <int D, bool B = false> __device__ __forceinline__ void block_setup_bod
         }
     }
 }
-template <int D, bool B = false> __global__ void k_block_setup(DevScene s) { pdl_enter(); block_setup_body<D, B>(s, launch_cta()); }
+template <int D, bool B = false> __global__ void k_block_setup(DevScene s) {
+    pdl_enter();
+    block_setup_body<D, B>(s, launch_cta());
+}
 
 // Exclusive scan of the per-block primary totals into first_particle
 // (copy_particles_len_to_scan_value + prefix_sum +
@@ -668,7 +680,10 @@ template <int NT> __device__ __forceinline__ void block_scan_body(const DevScene
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < nb; r += NT) s.qorder[atomicAdd(&cnt[min(s.bnp[r] >> 3, 63u)], 1u)] = r;
 }
-template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) { pdl_enter(); block_scan_body<NT>(s); }
+template <int NT> __global__ void __launch_bounds__(NT) k_block_scan(DevScene s) {
+    pdl_enter();
+    block_scan_body<NT>(s);
+}
 
 // Per particle: claim its slot in the block's cell range (the primary part
 // of finalize_particles_sort, sort.slang:304-357), warp-aggregated.
@@ -732,7 +747,10 @@ template <bool B = false> __device__ __forceinline__ void scatter_body(const Dev
         }
     }
 }
-template <bool B = false> __global__ void k_scatter(DevScene s) { pdl_enter(); scatter_body<B>(s, launch_cta()); }
+template <bool B = false> __global__ void k_scatter(DevScene s) {
+    pdl_enter();
+    scatter_body<B>(s, launch_cta());
+}
 
 // Canonical order inside each (block, cell) range of the permutation:
 // ascending original id.  k_scatter stores beside every permutation entry

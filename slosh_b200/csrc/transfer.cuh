@@ -1558,6 +1558,9 @@ template <int D, bool B = false> __device__ __forceinline__ void rigid_body(cons
     for (int k = 0; k < D; ++k) b.linvel[k] = b.linvel[k] + grav[k] * ((b.inv_mass[k] != 0.f) ? 1.f : 0.f) * dt;
     s.bodies[id] = b;
 }
-template <int D, bool B = false> __global__ void k_rigid(DevScene s) { pdl_enter(); rigid_body<D, B>(s, blockIdx.x * blockDim.x + threadIdx.x); }
+template <int D, bool B = false> __global__ void k_rigid(DevScene s) {
+    pdl_enter();
+    rigid_body<D, B>(s, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 }  // namespace slosh
