@@ -10,6 +10,8 @@ from slosh_b200 import scenes
 from slosh_b200.pipeline import ParticleModel, RigidBody, GpuBoundaryCondition, make_particles
 from slosh_b200._lib import BODY_DTYPE
 
+from physics_checks import dam_front_checks
+
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
@@ -408,3 +410,13 @@ def test_heightfield_mesh_sides(oracle_lib):
         r = oracle_lib.project_on_trimesh(v, t, rec, (0.43, y, 0.61), 0.05)
         assert r is not None and r[1] == inside
         assert np.allclose(r[0], (0.43, 0.2, 0.61), atol=1e-6)
+
+
+def test_dam_break_front_against_validation_criterion(oracle_lib):
+    """The oracle's 2D dam break at h = 1/64 (3,876 particles, 3,000
+    substeps) keeps its front within 10 % of the validation criterion up to
+    tau = 2; soon after, the front meets the box's far wall (x / a = 2.24)."""
+    h = 1.0 / 64.0
+    o = oracle_lib.from_scene(scenes.dam_break_2d(h=h))
+    dam_front_checks(o.step, lambda: float(o.get_particles()["position"][:, 0].max()), 0.4 + 3.0 * h,
+                     (0.5, 1.0, 1.5, 2.0), 0.10)
