@@ -19,3 +19,49 @@ def dam_front_checks(advance, front_x, a, taus, tol):
         print(f"tau {k * t:.2f}: front {front:.3f} a, criterion {model:.3f} a")
         assert abs(front / model - 1.0) <= tol, (k * t, front, model)
 
+
+
+def cantilever_scene(h=1.0 / 64.0, young=9.2e6):
+    """A 2D cantilever after slosh's elastic-beam validation scenario
+    (validation_tests/src/scenarios/elastic_beam.rs:58-63): a fixed-corotated
+    beam (Poisson ratio 0, so plane strain and plane stress agree) of length
+    L = 0.5 and height H = 0.1, clamped by embedding its first 4 cells in a
+    sticky wall, loaded by gravity from rest.  Returns the scene, the mask of
+    the particles within a cell of the tip, the analytic static tip
+    deflection q L^4 / (8 E I) and the first bending period in substeps."""
+    import numpy as np
+
+    from slosh_b200 import scenes
+    from slosh_b200.pipeline import GpuBoundaryCondition, ParticleModel, RigidBody, SimulationParams, make_particles
+
+    rho, g, length, height, x0, dt = 1000.0, 9.81, 0.5, 0.1, 0.2, 5e-5
+    xs = np.arange(x0 - 4 * h + h / 4, x0 + length, h / 2)
+    ys = np.arange(0.5 - height / 2 + h / 4, 0.5 + height / 2, h / 2)
+    pts = np.stack(np.meshgrid(xs, ys, indexing="ij"), -1).reshape(-1, 2)
+    parts = make_particles(pts, h / 4, rho, ParticleModel.elastic(young, 0.0), dim=2)
+    wall = RigidBody(("cuboid", (0.1, 0.2)), translation=(x0 - 0.1, 0.5), rotation=0.0,
+                     boundary_condition=GpuBoundaryCondition.stick())
+    sc = scenes.Scene("cantilever_2d", 2, h, SimulationParams((0.0, -g), dt), parts, [wall], 10, 4096)
+    inertia = height**3 / 12.0
+    delta = rho * g * height * length**4 / (8.0 * young * inertia)
+    omega = 1.875**2 * math.sqrt(young * inertia / (rho * height * length**4))
+    return sc, pts[:, 0] > x0 + length - h, delta, int(2.0 * math.pi / omega / dt)
+
+
+def cantilever_checks(advance, tip_y, tip, delta, period, tol):
+    """Samples the tip's mean deflection 40 times over two bending periods.
+    Released from rest under a suddenly applied load, the undamped beam
+    swings between 0 and twice the static deflection, so the samples'
+    mean is the static deflection (within `tol` of the analytic one) and
+    their largest is about twice it."""
+    import numpy as np
+
+    y0 = float(tip_y()[tip].mean())
+    d = []
+    for _ in range(40):
+        advance(period // 20)
+        d.append(y0 - float(tip_y()[tip].mean()))
+    d = np.asarray(d)
+    print(f"tip deflection: mean {d.mean():.5f}, peak {d.max():.5f}; analytic static {delta:.5f}")
+    assert abs(d.mean() / delta - 1.0) <= tol, (d.mean(), delta)
+    assert 1.8 <= d.max() / delta <= 2.2, (d.max(), delta)

@@ -7,12 +7,17 @@ of the criterion of slosh's validation scenario
 front runs ahead of that rough curve (the oracle gives +9 % at tau = 1 and
 +15 % at tau = 1.5, against +6 % at most at h = 1/64, where the CPU test
 holds 10 %).
+
+A 2D cantilever after slosh's elastic-beam scenario
+(validation_tests/src/scenarios/elastic_beam.rs:58-63), loaded by gravity
+from rest: its mean tip deflection over two bending periods is within 5 %
+of Euler-Bernoulli's q L^4 / (8 E I) and its peak about twice that.
 """
 import pytest
 
 from slosh_b200 import scenes
 from slosh_b200.pipeline import MpmPipeline
-from physics_checks import dam_front_checks
+from physics_checks import cantilever_checks, cantilever_scene, dam_front_checks
 
 pytestmark = pytest.mark.gpu
 
@@ -24,4 +29,15 @@ def test_dam_break_front_against_validation_criterion(cuda_lib):
     dam_front_checks(lambda n: pipe.launch_step(data, n),
                      lambda: float(data.download_particles()["position"][:, 0].max()), 0.4 + 3.0 * h,
                      (0.5, 1.0, 1.5), 0.20)
+    data.close()
+
+
+def test_cantilever_tip_deflection(cuda_lib):
+    """The same 2D cantilever through the C ABI: mean tip deflection within
+    5 % of Euler-Bernoulli's q L^4 / (8 E I), peak about twice it."""
+    sc, tip, delta, period = cantilever_scene()
+    data = scenes.build_mpm_data(sc)
+    pipe = MpmPipeline()
+    cantilever_checks(lambda n: pipe.launch_step(data, n), lambda: data.download_particles()["position"][:, 1],
+                      tip, delta, period, 0.05)
     data.close()
