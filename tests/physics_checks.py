@@ -65,3 +65,44 @@ def cantilever_checks(advance, tip_y, tip, delta, period, tol):
     print(f"tip deflection: mean {d.mean():.5f}, peak {d.max():.5f}; analytic static {delta:.5f}")
     assert abs(d.mean() / delta - 1.0) <= tol, (d.mean(), delta)
     assert 1.8 <= d.max() / delta <= 2.2, (d.max(), delta)
+
+
+def tank_scene(h=1.0 / 64.0, depth=0.2):
+    """A 2D layer of the Tait fluid (rest density 1000, K = 1e4, gamma = 7)
+    filling the unit box's width to `depth`, released at rest with J = 1
+    (no initial pressure), sticky walls."""
+    import numpy as np
+
+    from slosh_b200 import scenes
+    from slosh_b200.pipeline import GpuBoundaryCondition, ParticleModel, SimulationParams, make_particles
+
+    xs = np.arange(h / 4, 1.0, h / 2)
+    ys = np.arange(h / 4, depth, h / 2)
+    pts = np.stack(np.meshgrid(xs, ys, indexing="ij"), -1).reshape(-1, 2)
+    parts = make_particles(pts, h / 4, 1000.0, ParticleModel.fluid_tait(1000.0, 1.0e4, 7.0), dim=2)
+    return scenes.Scene("tank_2d", 2, h, SimulationParams((0.0, -9.81), 1e-4), parts,
+                        scenes._walls_2d(h, GpuBoundaryCondition.stick()), 10, 8192)
+
+
+def hydrostatic_check(advance, particles, depth, tol):
+    """Lets the layer settle for 0.5 s, then averages the particles' Tait
+    pressure p = (K / gamma) (J^-gamma - 1) (J = F00, the fluid's volume
+    ratio) in ten depth bins over the next second.  Between the bottom's
+    boundary layer (the first two bins) and the free surface (the last) the
+    profile is hydrostatic: its slope is rho0 g within `tol`."""
+    import numpy as np
+
+    advance(5000)
+    bins = np.linspace(0.0, depth, 11)
+    prof = np.zeros(10)
+    for _ in range(20):
+        advance(500)
+        p = particles()
+        J = p["def_grad"][:, 0]
+        pr = (1.0e4 / 7.0) * (J**-7.0 - 1.0)
+        idx = np.digitize(p["position"][:, 1], bins) - 1
+        prof += np.array([pr[idx == i].mean() for i in range(10)]) / 20.0
+    mid = 0.5 * (bins[1:] + bins[:-1])
+    slope = -np.polyfit(mid[2:9], prof[2:9], 1)[0]
+    print("pressure by depth bin:", np.round(prof, 1), f"slope {slope:.0f} (rho0 g = 9810)")
+    assert abs(slope / 9810.0 - 1.0) <= tol, slope
