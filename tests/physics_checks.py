@@ -21,14 +21,16 @@ def dam_front_checks(advance, front_x, a, taus, tol):
 
 
 
-def cantilever_scene(h=1.0 / 64.0, young=9.2e6):
+def cantilever_scene(h=1.0 / 64.0, young=9.2e6, dim=2):
     """A 2D cantilever after slosh's elastic-beam validation scenario
     (validation_tests/src/scenarios/elastic_beam.rs:58-63): a fixed-corotated
     beam (Poisson ratio 0, so plane strain and plane stress agree) of length
     L = 0.5 and height H = 0.1, clamped by embedding its first 4 cells in a
     sticky wall, loaded by gravity from rest.  Returns the scene, the mask of
     the particles within a cell of the tip, the analytic static tip
-    deflection q L^4 / (8 E I) and the first bending period in substeps."""
+    deflection q L^4 / (8 E I) and the first bending period in substeps.
+    In 3D the beam's cross-section is H x H (I = H^4 / 12, q = rho g H^2:
+    the same deflection and period)."""
     import numpy as np
 
     from slosh_b200 import scenes
@@ -37,11 +39,19 @@ def cantilever_scene(h=1.0 / 64.0, young=9.2e6):
     rho, g, length, height, x0, dt = 1000.0, 9.81, 0.5, 0.1, 0.2, 5e-5
     xs = np.arange(x0 - 4 * h + h / 4, x0 + length, h / 2)
     ys = np.arange(0.5 - height / 2 + h / 4, 0.5 + height / 2, h / 2)
-    pts = np.stack(np.meshgrid(xs, ys, indexing="ij"), -1).reshape(-1, 2)
-    parts = make_particles(pts, h / 4, rho, ParticleModel.elastic(young, 0.0), dim=2)
-    wall = RigidBody(("cuboid", (0.1, 0.2)), translation=(x0 - 0.1, 0.5), rotation=0.0,
-                     boundary_condition=GpuBoundaryCondition.stick())
-    sc = scenes.Scene("cantilever_2d", 2, h, SimulationParams((0.0, -g), dt), parts, [wall], 10, 4096)
+    axes = (xs, ys) if dim == 2 else (xs, ys, ys)
+    pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, dim)
+    parts = make_particles(pts, h / 4, rho, ParticleModel.elastic(young, 0.0), dim=dim)
+    if dim == 2:
+        wall = RigidBody(("cuboid", (0.1, 0.2)), translation=(x0 - 0.1, 0.5), rotation=0.0,
+                         boundary_condition=GpuBoundaryCondition.stick())
+        gravity = (0.0, -g)
+    else:
+        wall = RigidBody(("cuboid", (0.1, 0.2, 0.2)), translation=(x0 - 0.1, 0.5, 0.5),
+                         boundary_condition=GpuBoundaryCondition.stick())
+        gravity = (0.0, -g, 0.0)
+    sc = scenes.Scene(f"cantilever_{dim}d", dim, h, SimulationParams(gravity, dt), parts, [wall], 10,
+                      4096 if dim == 2 else 8192)
     inertia = height**3 / 12.0
     delta = rho * g * height * length**4 / (8.0 * young * inertia)
     omega = 1.875**2 * math.sqrt(young * inertia / (rho * height * length**4))

@@ -439,3 +439,14 @@ def test_tait_fluid_settles_hydrostatic(oracle_lib):
     to 6 % above rho0 there)."""
     o = oracle_lib.from_scene(tank_scene())
     hydrostatic_check(o.step, o.get_particles, 0.2, 0.10)
+
+
+def test_cantilever_tip_deflection_3d(oracle_lib):
+    """The same cantilever in 3D (square cross-section; the 3x3 SVD and
+    model path) at h = 1/32 (1,440 particles): the beam is only 3.2 cells
+    thick and clamped by a sticky wall, so the coarse check holds 15 %
+    (measured +7.9 %; 0.87-1.07 of the analytic value at other cells and
+    thicknesses, with no clean convergence), and the peak about twice it."""
+    sc, tip, delta, period = cantilever_scene(h=1.0 / 32.0, dim=3)
+    o = oracle_lib.from_scene(sc)
+    cantilever_checks(o.step, lambda: o.get_particles()["position"][:, 1], tip, delta, period, 0.15)
