@@ -21,12 +21,13 @@ def dam_front_checks(advance, front_x, a, taus, tol):
 
 
 
-def cantilever_scene(h=1.0 / 64.0, young=9.2e6, dim=2):
+def cantilever_scene(h=1.0 / 64.0, young=9.2e6, dim=2, neo_hookean=False):
     """A 2D cantilever after slosh's elastic-beam validation scenario
     (validation_tests/src/scenarios/elastic_beam.rs:58-63): a fixed-corotated
     beam (Poisson ratio 0, so plane strain and plane stress agree) of length
     L = 0.5 and height H = 0.1, clamped by embedding its first 4 cells in a
-    sticky wall, loaded by gravity from rest.  Returns the scene, the mask of
+    sticky wall, loaded by gravity from rest (`neo_hookean`: the Neo-Hookean
+    model, which agrees with it at these small strains).  Returns the scene, the mask of
     the particles within a cell of the tip, the analytic static tip
     deflection q L^4 / (8 E I) and the first bending period in substeps.
     In 3D the beam's cross-section is H x H (I = H^4 / 12, q = rho g H^2:
@@ -41,7 +42,8 @@ def cantilever_scene(h=1.0 / 64.0, young=9.2e6, dim=2):
     ys = np.arange(0.5 - height / 2 + h / 4, 0.5 + height / 2, h / 2)
     axes = (xs, ys) if dim == 2 else (xs, ys, ys)
     pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, dim)
-    parts = make_particles(pts, h / 4, rho, ParticleModel.elastic(young, 0.0), dim=dim)
+    model = ParticleModel.elastic_neo_hookean(young, 0.0) if neo_hookean else ParticleModel.elastic(young, 0.0)
+    parts = make_particles(pts, h / 4, rho, model, dim=dim)
     if dim == 2:
         wall = RigidBody(("cuboid", (0.1, 0.2)), translation=(x0 - 0.1, 0.5), rotation=0.0,
                          boundary_condition=GpuBoundaryCondition.stick())

@@ -422,11 +422,14 @@ def test_dam_break_front_against_validation_criterion(oracle_lib):
                      (0.5, 1.0, 1.5, 2.0), 0.10)
 
 
-def test_cantilever_tip_deflection(oracle_lib):
+@pytest.mark.parametrize("neo_hookean", [False, True])
+def test_cantilever_tip_deflection(oracle_lib, neo_hookean):
     """The oracle's 2D cantilever (936 particles, 6,454 substeps) against
     Euler-Bernoulli: mean tip deflection within 5 % of q L^4 / (8 E I)
-    (0.3 % measured at h = 1/64; 8 % at h = 1/32, 1.5 % at h = 1/128)."""
-    sc, tip, delta, period = cantilever_scene()
+    (0.3 % measured at h = 1/64; 8 % at h = 1/32, 1.5 % at h = 1/128), with
+    the fixed-corotated model and with the Neo-Hookean one (the same to
+    1e-6 at these strains)."""
+    sc, tip, delta, period = cantilever_scene(neo_hookean=neo_hookean)
     o = oracle_lib.from_scene(sc)
     cantilever_checks(o.step, lambda: o.get_particles()["position"][:, 1], tip, delta, period, 0.05)
 
