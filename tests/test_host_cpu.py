@@ -240,3 +240,22 @@ def test_integration_rust_declares_every_export():
     assert not missing, missing
     wrong = sorted(n for n in c_args if r_args[n] != c_args[n])
     assert not wrong, [(n, c_args[n], r_args[n]) for n in wrong]
+
+
+def test_bench_launch_accounting():
+    """bench.py counts a kept-grid substep 7 kernels below a full-build one
+    (the 9 build kernels replaced by the 2 reuse kernels) when the graphs
+    are conditional, and every substep at the library's count otherwise."""
+    import importlib.util
+    from types import SimpleNamespace
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    st0 = {"n_grid_reuses": 10, "n_grid_rebuilds": 3, "conditional_graphs": 1}
+    st1 = {"n_grid_reuses": 27, "n_grid_rebuilds": 6, "conditional_graphs": 1}
+    launches, reuse = bench.timed_launches(SimpleNamespace(kernels_per_substep=14), st0, st1, 20)
+    assert launches == 14 * 3 + 7 * 17 and reuse["reused_substeps"] == 17 and reuse["rebuilt_substeps"] == 3
+    st1 = {"n_grid_reuses": 0, "n_grid_rebuilds": 0, "conditional_graphs": 0}
+    launches, _ = bench.timed_launches(SimpleNamespace(kernels_per_substep=13), st1, st1, 1000)
+    assert launches == 13000
