@@ -453,3 +453,17 @@ def test_cantilever_tip_deflection_3d(oracle_lib):
     sc, tip, delta, period = cantilever_scene(h=1.0 / 32.0, dim=3)
     o = oracle_lib.from_scene(sc)
     cantilever_checks(o.step, lambda: o.get_particles()["position"][:, 1], tip, delta, period, 0.15)
+
+
+def test_oracle_bits_independent_of_threads(oracle_lib):
+    """The oracle's state after 10 substeps of the sand column (h = 1/32)
+    is the same bits with 1, 3 and 8 host threads, so its answers do not
+    depend on the machine that checks against it."""
+    sc = scenes.sand_column_3d(h=1.0 / 32.0, substeps=10)
+    runs = []
+    for threads in (1, 3, 8):
+        o = oracle_lib.from_scene(sc, threads=threads)
+        o.step(10)
+        runs.append(o.get_particles())
+    for other in runs[1:]:
+        assert other.tobytes() == runs[0].tobytes()
