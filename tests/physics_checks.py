@@ -118,3 +118,45 @@ def hydrostatic_check(advance, particles, depth, tol):
     slope = -np.polyfit(mid[2:9], prof[2:9], 1)[0]
     print("pressure by depth bin:", np.round(prof, 1), f"slope {slope:.0f} (rho0 g = 9810)")
     assert abs(slope / 9810.0 - 1.0) <= tol, slope
+
+
+def sand_layer_check(h=1.0 / 64.0, depth=0.2, tol=0.10, oracle=None):
+    """A 2D layer of Drucker-Prager sand (the benchmark's material: friction
+    angle 30 deg, E = 3.5e5, nu = 0.3, density 2200) filling the unit box's
+    width to `depth` between frictionless (slip) walls settles for 0.5 s;
+    averaged over the next second, the Cauchy stress sigma_yy of its
+    fixed-corotated elasticity, tau = 2 mu (F - R) F^T + lambda (J - 1) J I
+    over J, grows with depth at rho g within `tol` between the bottom's
+    boundary layer and the surface: the layer carries its own weight."""
+    import numpy as np
+
+    from slosh_b200 import scenes
+    from slosh_b200.pipeline import GpuBoundaryCondition, ParticleModel, SimulationParams, make_particles
+
+    rho, g = 2200.0, 9.81
+    xs = np.arange(h / 4, 1.0, h / 2)
+    ys = np.arange(h / 4, depth, h / 2)
+    pts = np.stack(np.meshgrid(xs, ys, indexing="ij"), -1).reshape(-1, 2)
+    parts = make_particles(pts, h / 4, rho, ParticleModel.sand(3.5e5, 0.3, friction_angle_deg=30.0), dim=2)
+    lam, mu = float(parts["model"][0][9]), float(parts["model"][0][10])
+    sc = scenes.Scene("sand_layer_2d", 2, h, SimulationParams((0.0, -g), 1e-4), parts,
+                      scenes._walls_2d(h, GpuBoundaryCondition.slip()), 10, 8192)
+    o = oracle.from_scene(sc)
+    o.step(5000)
+    bins = np.linspace(0.0, depth, 11)
+    prof = np.zeros(10)
+    for _ in range(20):
+        o.step(500)
+        p = o.get_particles()
+        f = p["def_grad"].astype(np.float64)
+        F = np.stack([np.stack([f[:, 0], f[:, 3]], -1), np.stack([f[:, 1], f[:, 4]], -1)], 1)  # column-major
+        u, _, vt = np.linalg.svd(F)
+        J = np.linalg.det(F)
+        tau = 2.0 * mu * (F - u @ vt) @ np.transpose(F, (0, 2, 1)) + (lam * (J - 1.0) * J)[:, None, None] * np.eye(2)
+        syy = tau[:, 1, 1] / J
+        idx = np.digitize(p["position"][:, 1], bins) - 1
+        prof += np.array([syy[idx == i].mean() for i in range(10)]) / 20.0
+    mid = 0.5 * (bins[1:] + bins[:-1])
+    slope = np.polyfit(mid[2:9], prof[2:9], 1)[0]
+    print("sigma_yy by depth bin:", np.round(prof, 0), f"slope {slope:.0f} (rho g = {rho * g:.0f})")
+    assert abs(slope / (rho * g) - 1.0) <= tol, slope
